@@ -1,0 +1,202 @@
+/*
+ * scrna_cle.h — C ABI of the B200 batched Chemical Langevin Equation library
+ * (libscrna_cle.so, sm_100a).
+ *
+ * The library replaces the GPU CLE of Msturroc/SyntheticscRNAseq.jl
+ * (ext/SyntheticscRNAseqCUDAExt.jl) behind the package's own Julia interface.
+ * Every entry point below names the reference function it stands in for.
+ * Conventions:
+ *   - All functions return an int status (SCRNA_OK == 0, negative on error);
+ *     scrna_last_error() returns a thread-local message for the last failure.
+ *   - Host arrays follow Julia: matrices are column-major.  The interaction
+ *     matrix A is G x G with A[i + j*G] = effect of protein j on gene i
+ *     (src/network.jl:44-45).  Edge gene indices are `index_base`-based
+ *     (1 for Julia callers, 0 for C callers).
+ *   - Output matrices are cells x G (or cells x 2G for SCRNA_READOUT_BOTH),
+ *     column-major, exactly the Matrix{Float64} the reference returns
+ *     (src/algorithms/cle.jl:123-129).  Count matrices are cells x G int32.
+ *   - The caller owns host buffers; the library owns device memory and frees
+ *     it in the matching *_destroy call.
+ *   - A context is bound to one device and one CUDA stream; calls on one
+ *     context must not run concurrently from several threads.
+ */
+#ifndef SCRNA_CLE_H
+#define SCRNA_CLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCRNA_ABI_VERSION 1
+
+enum scrna_status {
+    SCRNA_OK = 0,
+    SCRNA_EINVAL = -1,    /* bad argument (reference: @assert / error(), src/network.jl:66-68) */
+    SCRNA_ENOMEM = -2,    /* device or host allocation failed, or admission refused */
+    SCRNA_ECUDA = -3,     /* CUDA runtime error */
+    SCRNA_ETIMEOUT = -4,  /* wait ran out of time */
+    SCRNA_EBUSY = -5,     /* queue full / request still running */
+    SCRNA_ENOTSUP = -6,   /* configuration not supported by this build */
+    SCRNA_ECANCELED = -7  /* request was cancelled */
+};
+
+enum scrna_readout { SCRNA_READOUT_MRNA = 0, SCRNA_READOUT_PROTEIN = 1, SCRNA_READOUT_BOTH = 2 };
+
+/* Division partition: binomial split of rounded counts (ext/SyntheticscRNAseqCUDAExt.jl:641-651)
+ * or deterministic halving (src/algorithms/cle.jl:249-261). */
+enum scrna_partition { SCRNA_PARTITION_BINOMIAL = 0, SCRNA_PARTITION_HALVE = 1 };
+
+/* Arithmetic of a run: the fused FP32 path (tensor-core contraction at large dense G), or the
+ * plain FP64 one-kernel-per-step path kept as the comparison baseline. */
+enum scrna_precision { SCRNA_PRECISION_FP32 = 0, SCRNA_PRECISION_FP64_PLAIN = 1 };
+
+/* Contraction path for the FP32 precision. AUTO picks the register path for sparse
+ * networks and the tensor-core path for large dense ones. */
+enum scrna_path { SCRNA_PATH_AUTO = 0, SCRNA_PATH_REGISTER = 1, SCRNA_PATH_TENSOR = 2 };
+
+typedef struct scrna_ctx scrna_ctx;
+typedef struct scrna_net scrna_net;
+typedef struct scrna_state scrna_state;
+
+/* KineticParams (src/kinetics.jl:25-32). */
+typedef struct {
+    double k_t, K_d, n, mu_m, mu_p, dilution;
+} scrna_kinetics;
+
+/* PopulationConfig (src/population.jl:27-34) plus the partition and Moran modes.
+ * exclude_mother = 1 picks the replaced slot among the other N-1 cells
+ * (src/algorithms/cle.jl:265-268); 0 picks any cell (ext/SyntheticscRNAseqCUDAExt.jl:509). */
+typedef struct {
+    int64_t cell_num;
+    double growth_rate;
+    double V_div;
+    double V_init_lo, V_init_hi;
+    int32_t div_check_interval;
+    int32_t partition;        /* enum scrna_partition */
+    int32_t exclude_mother;
+    int32_t reserved;
+    double growth_noise;      /* accepted for interface parity; the CLE ignores it (cle.jl:237) */
+} scrna_population;
+
+/* CaptureModel (src/population.jl:57-61).  mean_correction = 1 uses the reference's
+ * mu_log = log(efficiency) - sigma^2/2 (src/capture.jl:30); 0 uses mu_log = log(efficiency). */
+typedef struct {
+    double efficiency, efficiency_std;
+    int32_t readout;          /* SCRNA_READOUT_MRNA or SCRNA_READOUT_PROTEIN */
+    int32_t mean_correction;
+} scrna_capture;
+
+/* CLE(dt) (src/algorithms/cle.jl:21-23) plus the simulate keywords (cle.jl:34-39). */
+typedef struct {
+    double dt;
+    double T;
+    int64_t cell_num;         /* ignored when a population config is given (pop.cell_num wins) */
+    int32_t readout;          /* enum scrna_readout */
+    int32_t precision;        /* enum scrna_precision */
+    uint64_t seed;            /* Philox key */
+    uint32_t stream;          /* Philox stream id (24 bits); distinct per network in a batch */
+    int32_t path;             /* enum scrna_path */
+    int64_t n_steps;          /* <= 0: ceil(T/dt) (cle.jl:56); > 0: exactly this many steps */
+    int64_t cell_offset;      /* global index of cell 0 (cell sharding across GPUs) */
+} scrna_cle_opts;
+
+/* ---- library / context ---------------------------------------------------- */
+const char* scrna_last_error(void);
+int scrna_version(void);
+int scrna_ctx_create(int device, scrna_ctx** out);
+int scrna_ctx_destroy(scrna_ctx* ctx);
+/* Use the caller's cudaStream_t (passed as void*) for all work of this context. */
+int scrna_ctx_set_stream(scrna_ctx* ctx, void* cuda_stream);
+int scrna_ctx_synchronize(scrna_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+int64_t scrna_ctx_launch_count(const scrna_ctx* ctx);
+
+/* ---- networks ---------------------------------------------------------------
+ * Uploads a GeneNetwork (src/network.jl:55-63): basals, A, cooperative and
+ * redundant edges (network.jl:16-34), telegraph rates k_on/k_off (+Inf =
+ * constitutive).  Edge e has target coop_target[e] and sources
+ * coop_src[coop_ptr[e] .. coop_ptr[e+1]-1]; strengths are the raw edge
+ * strengths (the library multiplies by basals[target] as cle.jl:96,103 do). */
+int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals, const double* A_colmajor,
+                     int32_t n_coop, const int32_t* coop_target, const int32_t* coop_ptr,
+                     const int32_t* coop_src, const double* coop_strength,
+                     int32_t n_redun, const int32_t* redun_target, const int32_t* redun_ptr,
+                     const int32_t* redun_src, const double* redun_strength,
+                     const double* k_on, const double* k_off, int32_t index_base,
+                     scrna_net** out);
+int scrna_net_destroy(scrna_net* net);
+int32_t scrna_net_genes(const scrna_net* net);
+
+/* ---- simulate -----------------------------------------------------------------
+ * Replaces simulate(net, CLE(dt), kin, Val(:gpu); cell_num, T, readout)
+ * (ext/SyntheticscRNAseqCUDAExt.jl:48-117) and, with pop != NULL,
+ * simulate(net, CLE(dt), kin, Val(:gpu), pop; T, readout) (ext:409-529).
+ * `out` (host, cells x G or cells x 2G, column-major) receives the readout.
+ * With cap != NULL, `counts` (host, cells x G int32) receives the captured
+ * counts (src/capture.jl:25-47) and `efficiencies` (host, cells, nullable) the
+ * per-cell capture efficiencies.  Blocks until the results are on the host. */
+int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                       const scrna_population* pop, const scrna_capture* cap,
+                       const scrna_cle_opts* opts, double* out, int32_t* counts,
+                       double* efficiencies);
+
+/* Replaces simulate_gpu_batch(networks, CLE(dt), kin; cell_num, T, readout)
+ * (ext/SyntheticscRNAseqCUDAExt.jl:132-213; stub src/SyntheticscRNAseq.jl:75-76).
+ * Unlike the reference, networks may differ in G and in cell count, and each may
+ * carry its own population config (pops[b] nullable; pops itself nullable).
+ * All B networks run in one persistent launch fed by a device work queue.
+ * kins: B entries, or 1 entry shared by all.  cell_nums: per network cell
+ * counts (ignored for networks with a population config).  Network b uses
+ * Philox stream opts->stream + b.  outs[b] / counts[b] as in scrna_cle_simulate. */
+int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets,
+                             const scrna_kinetics* kins, int32_t n_kins,
+                             const int64_t* cell_nums, const scrna_population* const* pops,
+                             const scrna_capture* cap, const scrna_cle_opts* opts,
+                             double* const* outs, int32_t* const* counts);
+
+/* Replaces apply_capture(X, capture; rng) (src/capture.jl:25-47): X is a host
+ * cells x G column-major Float64 matrix of molecule values.  Y (host, cells x G
+ * int32) gets the captured counts, eff (host, cells, nullable) the efficiencies. */
+int scrna_apply_capture(scrna_ctx* ctx, int64_t N, int32_t G, const double* X,
+                        const scrna_capture* cap, uint64_t seed, uint32_t stream, int32_t* Y,
+                        double* eff);
+
+/* ---- device-resident runs ------------------------------------------------------
+ * A state object keeps one network's simulation state and outputs in device
+ * memory so repeated runs touch no host memory.  scrna_cle_run_device enqueues
+ * a whole run on the context stream and returns without waiting;
+ * scrna_state_read copies the readout / counts / efficiencies to the host. */
+int scrna_state_create(scrna_ctx* ctx, const scrna_net* net, int64_t cell_num, int32_t readout,
+                       int32_t with_capture, scrna_state** out);
+int scrna_state_destroy(scrna_state* st);
+int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                         const scrna_population* pop, const scrna_capture* cap,
+                         const scrna_cle_opts* opts, scrna_state* st);
+int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, int32_t* counts,
+                     double* efficiencies);
+/* Device pointers of the state's FP32 [G][N] mRNA / protein arrays (for tests). */
+int scrna_state_device_ptrs(scrna_state* st, void** d_mrna, void** d_protein);
+/* Copies the raw simulation state of the last run to the host: mRNA and protein as
+ * [G][N] float32 (FP32 path) or float64 (FP64 baseline path, then pass doubles),
+ * promoter states [G][N] uint8 and volumes [N] float64 (population runs).
+ * Any pointer may be NULL. */
+int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* protein,
+                         uint8_t* promoter, double* volume);
+
+/* ---- diagnostics ----------------------------------------------------------------
+ * Runs Philox4x32-10 on the device for n counters (host arrays ctr[4n], key[2]) and
+ * returns the words in out[4n]; used to check the device generator against the
+ * published known-answer vectors. */
+int scrna_debug_philox(scrna_ctx* ctx, int32_t n, const uint32_t* ctr, const uint32_t* key,
+                       uint32_t* out);
+/* Measures the sustained issue rate of the FP32 FMA pipe and of the special-function
+ * unit (MUFU) pipe with two microkernels; results in operations per second. */
+int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma_ops_per_s, double* sfu_ops_per_s,
+                             double* int_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCRNA_CLE_H */

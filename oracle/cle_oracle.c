@@ -1,0 +1,500 @@
+/*
+ * CPU oracle for the batched CLE path — TEST INFRASTRUCTURE ONLY (see cle_oracle.h).
+ *
+ * Built with -ffp-contract=off so that every FP64 expression rounds exactly as
+ * written, like Julia's broadcasts (which do not contract to FMA).
+ */
+#include "cle_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+ * as 1, 2, 3", SC'11).  Round: two 32x32->64 multiplies, the high halves
+ * xor'ed with the other counter words and the key; key bumped by the Weyl
+ * constants between rounds.
+ * ------------------------------------------------------------------------- */
+#define PHILOX_M0 0xD2511F53u
+#define PHILOX_M1 0xCD9E8D57u
+#define PHILOX_W0 0x9E3779B9u
+#define PHILOX_W1 0xBB67AE85u
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += PHILOX_W0; k1 += PHILOX_W1; }
+        uint64_t p0 = (uint64_t)PHILOX_M0 * c0;
+        uint64_t p1 = (uint64_t)PHILOX_M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static inline void draw(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t tag,
+                        uint32_t stream, uint32_t out[4]) {
+    uint32_t ctr[4] = {c0, c1, c2, (tag << 24) | (stream & 0xFFFFFFu)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    orc_philox4x32_10(ctr, key, out);
+}
+
+/* Box-Muller on two 32-bit words (same uniforms as the device code):
+ *   u1 = 1 - (w0>>9)*2^-23 in (0,1],  u2 = (w1>>9)*2^-23 in [0,1)
+ *   theta = 2*pi*(u2 - 1/2),  r = sqrt(-2 ln u1),  z0 = r cos theta, z1 = r sin theta. */
+static inline void box_muller(uint32_t w0, uint32_t w1, double* z0, double* z1) {
+    double u1 = (double)(8388608u - (w0 >> 9)) / 8388608.0;
+    double u2 = (double)(w1 >> 9) / 8388608.0;
+    double th = 6.283185307179586 * (u2 - 0.5);
+    double r = sqrt(-2.0 * log(u1));
+    *z0 = r * cos(th);
+    *z1 = r * sin(th);
+}
+
+/* 53-bit uniform in [0,1) from two words. */
+static inline double u53(uint32_t a, uint32_t b) {
+    return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+void orc_step_normals(uint64_t seed, uint32_t stream, uint32_t cell, uint32_t step,
+                      uint32_t gene, double* zm, double* zp) {
+    uint32_t w[4];
+    draw(seed, cell, step, gene >> 1, ORC_TAG_NORMAL, stream, w);
+    if (gene & 1u) box_muller(w[2], w[3], zm, zp);
+    else box_muller(w[0], w[1], zm, zp);
+}
+
+/* Probability -> 32-bit threshold: an event fires when the word is < thr. */
+static inline uint32_t prob_threshold(double p) {
+    if (!(p > 0.0)) return 0u;
+    double t = floor(p * 4294967296.0);
+    if (t >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)t;
+}
+
+/* ---------------------------------------------------------------------------
+ * Binomial samplers (bit-exact with the device code).
+ * ------------------------------------------------------------------------- */
+#define CAPTURE_CHUNK 512
+
+/* (1-p)^n by binary exponentiation, then the pmf recurrence
+ *   pmf(k+1) = ((pmf(k) * (n-k)) / (k+1)) * (p/(1-p)),
+ * returning the smallest k with u < cdf(k). Requires p <= 1/2 and n <= 512 so
+ * the starting pmf stays a normal double. */
+static int64_t invcdf_chunk(int64_t n, double p, double u) {
+    double q = 1.0 - p;
+    double ratio = p / q;
+    double base = q, pmf = 1.0;
+    int64_t e = n;
+    while (e) { if (e & 1) pmf = pmf * base; base = base * base; e >>= 1; }
+    double cdf = pmf;
+    int64_t k = 0;
+    while (u >= cdf && k < n) {
+        pmf = ((pmf * (double)(n - k)) / (double)(k + 1)) * ratio;
+        k += 1;
+        cdf = cdf + pmf;
+    }
+    return k;
+}
+
+int64_t orc_binomial_invcdf(int64_t n, double p, uint64_t seed, uint32_t stream,
+                            uint32_t cell, uint32_t gene) {
+    if (n <= 0 || !(p > 0.0)) return 0;
+    int flip = p > 0.5;
+    double pp = flip ? 1.0 - p : p;
+    int64_t total = 0;
+    int64_t nchunks = (n + CAPTURE_CHUNK - 1) / CAPTURE_CHUNK;
+    for (int64_t i = 0; i < nchunks; ++i) {
+        int64_t ni = n - i * CAPTURE_CHUNK;
+        if (ni > CAPTURE_CHUNK) ni = CAPTURE_CHUNK;
+        uint32_t w[4];
+        draw(seed, cell, (uint32_t)i, gene, ORC_TAG_CAPTURE, stream, w);
+        total += invcdf_chunk(ni, pp, u53(w[0], w[1]));
+    }
+    return flip ? n - total : total;
+}
+
+#define PARTITION_POPCOUNT_MAX 131072
+
+int64_t orc_binomial_half(int64_t n, uint64_t seed, uint32_t stream, uint32_t cell,
+                          uint32_t step, uint32_t gene, uint32_t species) {
+    if (n <= 0) return 0;
+    if (n > PARTITION_POPCOUNT_MAX) {
+        /* Rounded normal approximation (documented: not bit-exact territory). */
+        uint32_t w[4];
+        draw(seed, cell, step, (gene << 1) | species, ORC_TAG_PARTITION, stream, w);
+        double z0, z1;
+        box_muller(w[0], w[1], &z0, &z1);
+        double x = rint(0.5 * (double)n + 0.5 * sqrt((double)n) * z0);
+        if (x < 0) x = 0;
+        if (x > (double)n) x = (double)n;
+        return (int64_t)x;
+    }
+    int64_t total = 0, left = n;
+    for (uint32_t b = 0; left > 0; ++b) {
+        uint32_t w[4];
+        draw(seed, cell, step, (b << 22) | (gene << 1) | species, ORC_TAG_PARTITION, stream, w);
+        for (int j = 0; j < 4 && left > 0; ++j) {
+            uint32_t x = w[j];
+            if (left < 32) x &= (1u << left) - 1u;
+            total += __builtin_popcount(x);
+            left -= 32;
+        }
+    }
+    return total;
+}
+
+/* ---------------------------------------------------------------------------
+ * CLE
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int G;
+    double* Apos;  /* [G*G] row-major, precompute_hill_matrices (network.jl:206-219) */
+    double* Aneg;
+    uint32_t* thr_on;
+    uint32_t* thr_off;
+    uint32_t* thr_init;
+    uint8_t* tel;       /* switching active: isfinite(k_on) (tauleap_binomial.jl:86) */
+    uint8_t* init_rand; /* both rates finite: random initial state (tauleap_binomial.jl:69) */
+    int bursty;
+} prep_t;
+
+static void prep_build(const orc_net* net, double dt, prep_t* pp) {
+    int G = net->G;
+    pp->G = G;
+    pp->Apos = (double*)calloc((size_t)G * G, sizeof(double));
+    pp->Aneg = (double*)calloc((size_t)G * G, sizeof(double));
+    for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j) {
+            if (i == j) continue;
+            double a = net->A[(size_t)i * G + j] * net->basals[i];
+            pp->Apos[(size_t)i * G + j] = a > 0.0 ? a : 0.0;
+            pp->Aneg[(size_t)i * G + j] = -a > 0.0 ? -a : 0.0;
+        }
+    pp->thr_on = (uint32_t*)calloc(G, 4);
+    pp->thr_off = (uint32_t*)calloc(G, 4);
+    pp->thr_init = (uint32_t*)calloc(G, 4);
+    pp->tel = (uint8_t*)calloc(G, 1);
+    pp->init_rand = (uint8_t*)calloc(G, 1);
+    pp->bursty = 0;
+    for (int g = 0; g < G; ++g) {
+        double kon = net->k_on[g], koff = net->k_off[g];
+        if (isfinite(kon) || isfinite(koff)) pp->bursty = 1;
+        pp->tel[g] = isfinite(kon) ? 1 : 0;
+        pp->init_rand[g] = (isfinite(kon) && isfinite(koff)) ? 1 : 0;
+        pp->thr_on[g] = prob_threshold(1.0 - exp(-kon * dt));
+        pp->thr_off[g] = isfinite(koff) ? prob_threshold(1.0 - exp(-koff * dt)) : 0xFFFFFFFFu;
+        if (pp->init_rand[g]) pp->thr_init[g] = prob_threshold(kon / (kon + koff));
+    }
+}
+
+static void prep_free(prep_t* pp) {
+    free(pp->Apos); free(pp->Aneg); free(pp->thr_on); free(pp->thr_off);
+    free(pp->thr_init); free(pp->tel); free(pp->init_rand);
+}
+
+typedef struct {
+    double k_t, Kn, hill_n, mu_m, mu_p, dt, sqrt_dt;
+} coef_t;
+
+/* One Euler-Maruyama step for one cell (cle.jl:78-121; population form cle.jl:185-234
+ * when vol > 0).  m, p, on are this cell's G-vectors; act/rep/reg are scratch. */
+static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, uint64_t seed,
+                      uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
+                      double* p, uint8_t* on, double* act, double* rep, double* reg) {
+    int G = net->G;
+    /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121) */
+    if (pp->bursty) {
+        for (int g0 = 0; g0 < G; g0 += 4) {
+            int any = 0;
+            for (int g = g0; g < G && g < g0 + 4; ++g) any |= pp->tel[g];
+            if (!any) continue;
+            uint32_t w[4];
+            draw(seed, cell, step, (uint32_t)(g0 >> 2), ORC_TAG_SWITCH, stream, w);
+            for (int g = g0; g < G && g < g0 + 4; ++g) {
+                if (!pp->tel[g]) continue;
+                uint32_t x = w[g - g0];
+                if (on[g]) { if (x < pp->thr_off[g]) on[g] = 0; }
+                else { if (x < pp->thr_on[g]) on[g] = 1; }
+            }
+        }
+    }
+    /* Hill fractions (cle.jl:79-82) */
+    for (int g = 0; g < G; ++g) {
+        double pn = pow(p[g], cf->hill_n);
+        double den = pn + cf->Kn;
+        act[g] = pn / den;
+        rep[g] = cf->Kn / den;
+    }
+    /* reg = A_pos*act + A_neg*rep (cle.jl:84-86) */
+    for (int i = 0; i < G; ++i) {
+        double s1 = 0.0, s2 = 0.0;
+        const double* ap = pp->Apos + (size_t)i * G;
+        const double* an = pp->Aneg + (size_t)i * G;
+        for (int j = 0; j < G; ++j) s1 = s1 + ap[j] * act[j];
+        for (int j = 0; j < G; ++j) s2 = s2 + an[j] * rep[j];
+        reg[i] = s1 + s2;
+    }
+    /* cooperative / redundant corrections (cle.jl:89-106) */
+    for (int e = 0; e < net->n_coop; ++e) {
+        double prod = 1.0;
+        for (int k = net->coop_ptr[e]; k < net->coop_ptr[e + 1]; ++k) prod = prod * act[net->coop_src[k]];
+        int t = net->coop_target[e];
+        reg[t] = reg[t] + net->coop_strength[e] * net->basals[t] * prod;
+    }
+    for (int e = 0; e < net->n_redun; ++e) {
+        double prod = 1.0;
+        for (int k = net->redun_ptr[e]; k < net->redun_ptr[e + 1]; ++k)
+            prod = prod * (1.0 - act[net->redun_src[k]]);
+        int t = net->redun_target[e];
+        reg[t] = reg[t] + net->redun_strength[e] * net->basals[t] * (1.0 - prod);
+    }
+    /* M then P update with the new M (cle.jl:109-120) */
+    for (int g = 0; g < G; ++g) {
+        uint32_t w[4];
+        double zm, zp;
+        /* one Philox block serves genes 2k (words 0,1) and 2k+1 (words 2,3) */
+        draw(seed, cell, step, (uint32_t)(g >> 1), ORC_TAG_NORMAL, stream, w);
+        if (g & 1) box_muller(w[2], w[3], &zm, &zp);
+        else box_muller(w[0], w[1], &zm, &zp);
+
+        double tx = reg[g] + net->basals[g];
+        if (vol > 0.0) tx = tx * vol;
+        if (pp->bursty && !on[g]) tx = 0.0;
+        double mg = m[g], pg = p[g];
+        double var_m = tx + cf->mu_m * (mg > 0.0 ? mg : 0.0);
+        if (!(var_m > 0.0)) var_m = 0.0;
+        double nm = zm * cf->sqrt_dt * sqrt(var_m);
+        mg = mg + (tx - cf->mu_m * mg) * cf->dt + nm;
+        if (!(mg > 0.0)) mg = 0.0;
+        double var_p = cf->k_t * (mg > 0.0 ? mg : 0.0) + cf->mu_p * (pg > 0.0 ? pg : 0.0);
+        if (!(var_p > 0.0)) var_p = 0.0;
+        double np_ = zp * cf->sqrt_dt * sqrt(var_p);
+        pg = pg + (cf->k_t * mg - cf->mu_p * pg) * cf->dt + np_;
+        if (!(pg > 0.0)) pg = 0.0;
+        m[g] = mg;
+        p[g] = pg;
+    }
+}
+
+static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uint32_t cell,
+                           uint8_t* on) {
+    int G = pp->G;
+    for (int g0 = 0; g0 < G; g0 += 4) {
+        uint32_t w[4];
+        int any = 0;
+        for (int g = g0; g < G && g < g0 + 4; ++g) any |= pp->init_rand[g];
+        if (any) draw(seed, cell, 0, (uint32_t)(g0 >> 2), ORC_TAG_PROMOTER, stream, w);
+        for (int g = g0; g < G && g < g0 + 4; ++g)
+            on[g] = pp->init_rand[g] ? (w[g - g0] < pp->thr_init[g]) : 1;
+    }
+}
+
+int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
+                     const orc_opts* opt, double* M, double* P, double* V, uint8_t* prom,
+                     int nthreads) {
+    int G = net->G;
+    int64_t N = opt->cell_num;
+    if (G <= 0 || N <= 0 || !(opt->dt > 0.0)) return 1;
+    if (pop && N < 2 && pop->exclude_mother) return 1;
+    if (pop && pop->div_check_interval <= 0) return 1;
+    int64_t n_steps = opt->n_steps > 0 ? opt->n_steps : (int64_t)ceil(opt->T / opt->dt);
+
+    prep_t pp;
+    prep_build(net, opt->dt, &pp);
+    coef_t cf;
+    cf.k_t = kin->k_t;
+    cf.Kn = pow(kin->K_d, kin->n);
+    cf.hill_n = kin->n;
+    /* plain CLE: decay includes dilution (cle.jl:60-61); population: intrinsic only (cle.jl:166-167) */
+    cf.mu_m = pop ? kin->mu_m : kin->mu_m + kin->dilution;
+    cf.mu_p = pop ? kin->mu_p : kin->mu_p + kin->dilution;
+    cf.dt = opt->dt;
+    cf.sqrt_dt = sqrt(opt->dt);
+
+    /* initial condition: ceil of the steady state (cle.jl:49-53, kinetics.jl:65-70) */
+    double* m0 = (double*)malloc(sizeof(double) * G);
+    double* p0 = (double*)malloc(sizeof(double) * G);
+    for (int g = 0; g < G; ++g) {
+        double mss = net->basals[g] / (kin->mu_m + kin->dilution);
+        double pss = kin->k_t * mss / (kin->mu_p + kin->dilution);
+        m0[g] = ceil(mss);
+        p0[g] = ceil(pss);
+    }
+    uint64_t seed = opt->seed;
+    uint32_t stream = opt->stream;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+
+    if (!pop) {
+        /* cells are independent: cell-major loop, parallel over cells */
+#pragma omp parallel
+        {
+            double* m = (double*)malloc(sizeof(double) * G);
+            double* p = (double*)malloc(sizeof(double) * G);
+            double* act = (double*)malloc(sizeof(double) * G);
+            double* rep = (double*)malloc(sizeof(double) * G);
+            double* reg = (double*)malloc(sizeof(double) * G);
+            uint8_t* on = (uint8_t*)malloc(G);
+#pragma omp for schedule(static)
+            for (int64_t c = 0; c < N; ++c) {
+                memcpy(m, m0, sizeof(double) * G);
+                memcpy(p, p0, sizeof(double) * G);
+                init_promoters(&pp, seed, stream, (uint32_t)c, on);
+                for (int64_t s = 1; s <= n_steps; ++s)
+                    cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, 0.0, m, p,
+                              on, act, rep, reg);
+                for (int g = 0; g < G; ++g) {
+                    M[(size_t)g * N + c] = m[g];
+                    P[(size_t)g * N + c] = p[g];
+                    if (prom) prom[(size_t)g * N + c] = on[g];
+                }
+            }
+            free(m); free(p); free(act); free(rep); free(reg); free(on);
+        }
+    } else {
+        /* population: cells in lockstep, state cell-major [c][g] for the step loop */
+        double* Ms = (double*)malloc(sizeof(double) * G * N);
+        double* Ps = (double*)malloc(sizeof(double) * G * N);
+        uint8_t* On = (uint8_t*)malloc((size_t)G * N);
+        double* Vs = (double*)malloc(sizeof(double) * N);
+        double growth_factor = exp(pop->growth_rate * opt->dt);
+        for (int64_t c = 0; c < N; ++c) {
+            memcpy(Ms + c * G, m0, sizeof(double) * G);
+            memcpy(Ps + c * G, p0, sizeof(double) * G);
+            init_promoters(&pp, seed, stream, (uint32_t)c, On + c * G);
+            uint32_t w[4];
+            draw(seed, (uint32_t)c, 0, 0, ORC_TAG_VOLUME, stream, w);
+            Vs[c] = pop->V_lo + (pop->V_hi - pop->V_lo) * u53(w[0], w[1]); /* cle.jl:158-159 */
+        }
+        int64_t* dividers = (int64_t*)malloc(sizeof(int64_t) * N);
+        double* dM = (double*)malloc(sizeof(double) * G * N);
+        double* dP = (double*)malloc(sizeof(double) * G * N);
+        uint8_t* dOn = (uint8_t*)malloc((size_t)G * N);
+        double* dV = (double*)malloc(sizeof(double) * N);
+        for (int64_t s = 1; s <= n_steps; ++s) {
+#pragma omp parallel
+            {
+                double* act = (double*)malloc(sizeof(double) * G);
+                double* rep = (double*)malloc(sizeof(double) * G);
+                double* reg = (double*)malloc(sizeof(double) * G);
+#pragma omp for schedule(static)
+                for (int64_t c = 0; c < N; ++c) {
+                    cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, Vs[c],
+                              Ms + c * G, Ps + c * G, On + c * G, act, rep, reg);
+                    Vs[c] = Vs[c] * growth_factor; /* cle.jl:237 */
+                }
+                free(act); free(rep); free(reg);
+            }
+            if (s % pop->div_check_interval != 0) continue;
+            /* division (cle.jl:240-273) */
+            int64_t nd = 0;
+            for (int64_t c = 0; c < N; ++c)
+                if (Vs[c] > pop->V_div) dividers[nd++] = c;
+            for (int64_t k = 0; k < nd; ++k) {
+                int64_t c = dividers[k];
+                for (int g = 0; g < G; ++g) {
+                    double* mm = Ms + c * G + g;
+                    double* pq = Ps + c * G + g;
+                    if (pop->partition == 1) {
+                        double hm = *mm / 2.0, hp = *pq / 2.0;
+                        *mm = hm; dM[k * G + g] = hm;
+                        *pq = hp; dP[k * G + g] = hp;
+                    } else {
+                        int64_t mi = (int64_t)rint(*mm);
+                        int64_t mmth = mi > 0 ? orc_binomial_half(mi, seed, stream, (uint32_t)c,
+                                                                  (uint32_t)s, (uint32_t)g, 0) : 0;
+                        *mm = (double)mmth; dM[k * G + g] = (double)(mi - mmth);
+                        int64_t pi = (int64_t)rint(*pq);
+                        int64_t pmth = pi > 0 ? orc_binomial_half(pi, seed, stream, (uint32_t)c,
+                                                                  (uint32_t)s, (uint32_t)g, 1) : 0;
+                        *pq = (double)pmth; dP[k * G + g] = (double)(pi - pmth);
+                    }
+                    dOn[k * G + g] = On[c * G + g];
+                }
+                Vs[c] = Vs[c] / 2.0;
+                dV[k] = Vs[c];
+            }
+            for (int64_t k = 0; k < nd; ++k) {
+                int64_t c = dividers[k];
+                uint32_t w[4];
+                draw(seed, (uint32_t)c, (uint32_t)s, 0, ORC_TAG_MORAN, stream, w);
+                int64_t r;
+                if (pop->exclude_mother) {
+                    r = (int64_t)(((uint64_t)w[0] * (uint64_t)(N - 1)) >> 32);
+                    if (r >= c) r += 1;
+                } else {
+                    r = (int64_t)(((uint64_t)w[0] * (uint64_t)N) >> 32);
+                }
+                memcpy(Ms + r * G, dM + k * G, sizeof(double) * G);
+                memcpy(Ps + r * G, dP + k * G, sizeof(double) * G);
+                memcpy(On + r * G, dOn + k * G, (size_t)G);
+                Vs[r] = dV[k];
+            }
+        }
+        for (int64_t c = 0; c < N; ++c) {
+            for (int g = 0; g < G; ++g) {
+                M[(size_t)g * N + c] = Ms[c * G + g];
+                P[(size_t)g * N + c] = Ps[c * G + g];
+                if (prom) prom[(size_t)g * N + c] = On[c * G + g];
+            }
+            if (V) V[c] = Vs[c];
+        }
+        free(Ms); free(Ps); free(On); free(Vs); free(dividers); free(dM); free(dP);
+        free(dOn); free(dV);
+    }
+    free(m0); free(p0);
+    prep_free(&pp);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Capture (capture.jl:25-47)
+ * ------------------------------------------------------------------------- */
+void orc_capture_efficiency(int64_t N, double efficiency, double efficiency_std,
+                            int32_t mean_correction, uint64_t seed, uint32_t stream,
+                            double* eff) {
+    double mu_log = log(efficiency);
+    if (mean_correction) mu_log = mu_log - efficiency_std * efficiency_std / 2.0;
+    for (int64_t c = 0; c < N; ++c) {
+        uint32_t w[4];
+        draw(seed, (uint32_t)c, 0, 0, ORC_TAG_EFFICIENCY, stream, w);
+        double z0, z1;
+        box_muller(w[0], w[1], &z0, &z1);
+        double p = exp(mu_log + efficiency_std * z0);
+        if (p < 0.0) p = 0.0;
+        if (p > 1.0) p = 1.0;
+        eff[c] = p;
+    }
+}
+
+void orc_capture_counts(int64_t N, int32_t G, const double* X, const double* eff,
+                        uint64_t seed, uint32_t stream, int32_t* Y, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < N; ++c) {
+        for (int g = 0; g < G; ++g) {
+            double x = rint(X[(size_t)g * N + c]);
+            int64_t n = x > 0.0 ? (int64_t)x : 0;
+            double p = eff[c];
+            int64_t y = 0;
+            if (n > 0 && p != 0.0) y = orc_binomial_invcdf(n, p, seed, stream, (uint32_t)c, (uint32_t)g);
+            Y[(size_t)g * N + c] = (int32_t)y;
+        }
+    }
+}

@@ -1,0 +1,25 @@
+"""B200-native batched CLE for synthetic scRNA-seq (drop-in for the GPU CLE of
+Msturroc/SyntheticscRNAseq.jl).
+
+Compute runs in libscrna_cle.so (hand-written sm_100a CUDA behind the C ABI in
+include/scrna_cle.h); this package is the host-side mirror of the reference's
+Julia interface.  The directory name is not a Python identifier, so the package
+is imported under the name ``scrna_b200`` (see __graft_entry__.load_package).
+"""
+from .model import (CLE, INF, CaptureModel, CoopEdge, GeneNetwork, KineticParams, PopulationConfig,
+                    RedunEdge, default_algorithm, hill_activation, hill_repression, is_bursty, n_steps,
+                    precompute_hill_matrices, steady_state)
+from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
+                      dense_network, sample_network)
+from .api import (Context, DeviceRun, NetHandle, apply_capture, debug_philox, default_context,
+                  measure_pipe_peaks, simulate, simulate_gpu_batch)
+from ._lib import ScrnaError
+
+__all__ = [
+    "CLE", "CaptureModel", "CoopEdge", "GeneNetwork", "KineticParams", "PopulationConfig", "RedunEdge",
+    "default_algorithm", "hill_activation", "hill_repression", "is_bursty", "n_steps",
+    "precompute_hill_matrices", "steady_state", "sample_network", "dense_network", "config0", "config1",
+    "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
+    "NetHandle", "apply_capture", "debug_philox", "default_context", "measure_pipe_peaks", "simulate",
+    "simulate_gpu_batch", "ScrnaError", "INF",
+]

@@ -1,0 +1,318 @@
+"""Reference-facing entry points of the GPU CLE, over the C ABI.
+
+simulate(net, CLE(dt), kin, gpu=True; cell_num, T, readout)      ext/SyntheticscRNAseqCUDAExt.jl:48-117
+simulate(net, CLE(dt), kin, gpu=True, population=pop; T, readout) ext:409-529
+simulate_gpu_batch(networks, CLE(dt), kin; cell_num, T, readout)  ext:132-213
+apply_capture(X, capture)                                          src/capture.jl:25-47
+
+Outputs are cells x G (cells x 2G for readout "both") float64 arrays in
+column-major (Fortran) order, the layout of the reference's Matrix{Float64}.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import List, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import Capture, Kinetics, Opts, Population, check
+from .model import CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig
+
+READOUT = {"mrna": 0, "protein": 1, "both": 2}
+PRECISION = {"fp32": 0, "fp64_plain": 1}
+PATH = {"auto": 0, "register": 1, "tensor": 2}
+
+
+class Context:
+    """One device + one CUDA stream (scrna_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.scrna_ctx_create(int(device), C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def set_stream(self, cuda_stream_handle: int):
+        check(self.lib.scrna_ctx_set_stream(self.h, C.c_void_p(int(cuda_stream_handle))))
+
+    def synchronize(self):
+        check(self.lib.scrna_ctx_synchronize(self.h))
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.scrna_ctx_launch_count(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.scrna_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class _Keep(list):
+    def arr(self, x, dtype):
+        a = np.ascontiguousarray(np.asarray(x, dtype=dtype))
+        self.append(a)
+        return a.ctypes.data if a.size else None
+
+
+def _edge_arrays(keep: _Keep, edges):
+    tgt = [e.target for e in edges]
+    ptr = [0]
+    src: List[int] = []
+    for e in edges:
+        src.extend(e.sources)
+        ptr.append(len(src))
+    st = [e.strength for e in edges]
+    if not edges:
+        return 0, None, None, None, None
+    return (len(edges), keep.arr(tgt, np.int32), keep.arr(ptr, np.int32), keep.arr(src, np.int32),
+            keep.arr(st, np.float64))
+
+
+class NetHandle:
+    """A network uploaded to the device (scrna_net)."""
+
+    def __init__(self, net: GeneNetwork, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.net = net
+        keep = _Keep()
+        A_col = np.asfortranarray(net.interactions, dtype=np.float64)
+        keep.append(A_col)
+        c = _edge_arrays(keep, net.cooperative)
+        r = _edge_arrays(keep, net.redundant)
+        h = C.c_void_p()
+        check(self.ctx.lib.scrna_net_create(
+            self.ctx.h, int(net.G), keep.arr(net.basals, np.float64), A_col.ctypes.data,
+            c[0], c[1], c[2], c[3], c[4], r[0], r[1], r[2], r[3], r[4],
+            keep.arr(net.k_on, np.float64), keep.arr(net.k_off, np.float64), 0, C.byref(h)))
+        self.h = h
+        self.G = int(net.G)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.scrna_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _kin(kin: KineticParams) -> Kinetics:
+    return Kinetics(kin.k_t, kin.K_d, kin.n, kin.mu_m, kin.mu_p, kin.dilution)
+
+
+def _pop(pop: Optional[PopulationConfig]):
+    if pop is None:
+        return None
+    lo, hi = pop.V_init
+    return Population(int(pop.cell_num), float(pop.growth_rate), float(pop.V_div), float(lo), float(hi),
+                      int(pop.div_check_interval), int(pop.partition_code), int(bool(pop.exclude_mother)),
+                      0, float(pop.growth_noise))
+
+
+def _cap(cap: Optional[CaptureModel]):
+    if cap is None:
+        return None
+    return Capture(float(cap.efficiency), float(cap.efficiency_std), READOUT[cap.readout],
+                   int(bool(cap.mean_correction)))
+
+
+def _opts(alg: CLE, *, T, cell_num, readout, seed, stream, precision, path, n_steps, cell_offset):
+    if readout not in READOUT:
+        raise ValueError("readout must be 'mrna', 'protein' or 'both'")
+    return Opts(float(alg.dt), float(T), int(cell_num), READOUT[readout], PRECISION[precision], int(seed),
+                int(stream), PATH[path], int(n_steps), int(cell_offset))
+
+
+def _ptr(x):
+    return None if x is None else C.byref(x)
+
+
+def simulate(net: GeneNetwork, alg: CLE, kin: KineticParams, gpu: bool = True, population=None, *,
+             cell_num: int = 1000, T: float = 50.0, readout: str = "protein", seed: int = 0,
+             stream: int = 0, capture: Optional[CaptureModel] = None, precision: str = "fp32",
+             path: str = "auto", n_steps: int = 0, cell_offset: int = 0,
+             ctx: Optional[Context] = None, handle: Optional[NetHandle] = None):
+    """GPU CLE run.  Returns the readout matrix, or (matrix, counts, efficiencies)
+    when `capture` is given.  With `population`, pop.cell_num cells are simulated."""
+    if not gpu:
+        raise NotImplementedError("only the GPU path is provided by this library")
+    ctx = ctx or default_context()
+    h = handle or NetHandle(net, ctx)
+    N = population.cell_num if population is not None else cell_num
+    cols = net.G * (2 if readout == "both" else 1)
+    out = np.empty((N, cols), dtype=np.float64, order="F")
+    counts = np.empty((N, net.G), dtype=np.int32, order="F") if capture is not None else None
+    eff = np.empty(N, dtype=np.float64) if capture is not None else None
+    k, p, c = _kin(kin), _pop(population), _cap(capture)
+    o = _opts(alg, T=T, cell_num=N, readout=readout, seed=seed, stream=stream, precision=precision,
+              path=path, n_steps=n_steps, cell_offset=cell_offset)
+    check(ctx.lib.scrna_cle_simulate(ctx.h, h.h, C.byref(k), _ptr(p), _ptr(c), C.byref(o),
+                                     out.ctypes.data, None if counts is None else counts.ctypes.data,
+                                     None if eff is None else eff.ctypes.data))
+    if capture is not None:
+        return out, counts, eff
+    return out
+
+
+def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg: CLE, kin, *,
+                       cell_num: Union[int, Sequence[int]] = 1000, T: float = 50.0,
+                       readout: str = "protein", seed: int = 0, stream: int = 0,
+                       populations: Optional[Sequence[Optional[PopulationConfig]]] = None,
+                       capture: Optional[CaptureModel] = None, ctx: Optional[Context] = None):
+    """Batched GPU CLE over networks of any sizes.  `kin` is one KineticParams or one
+    per network; `cell_num` one count or one per network.  Network b uses Philox
+    stream `stream + b`.  Returns a list of readout matrices (and count matrices
+    when `capture` is given)."""
+    ctx = ctx or default_context()
+    B = len(networks)
+    kins = list(kin) if isinstance(kin, (list, tuple)) else [kin]
+    cns = list(cell_num) if isinstance(cell_num, (list, tuple, np.ndarray)) else [int(cell_num)] * B
+    handles = [NetHandle(n, ctx) for n in networks]
+    pops = list(populations) if populations is not None else [None] * B
+    outs, cnts = [], []
+    for b, n in enumerate(networks):
+        N = pops[b].cell_num if pops[b] is not None else cns[b]
+        cols = n.G * (2 if readout == "both" else 1)
+        outs.append(np.empty((N, cols), dtype=np.float64, order="F"))
+        if capture is not None:
+            cnts.append(np.empty((N, n.G), dtype=np.int32, order="F"))
+    karr = (Kinetics * len(kins))(*[_kin(k) for k in kins])
+    harr = (C.c_void_p * B)(*[h.h.value for h in handles])
+    cn_arr = (C.c_int64 * B)(*[int(x) for x in cns])
+    pop_structs = [_pop(p) for p in pops]
+    parr = (C.c_void_p * B)(*[None if p is None else C.addressof(p) for p in pop_structs])
+    oarr = (C.c_void_p * B)(*[o.ctypes.data for o in outs])
+    carr = (C.c_void_p * B)(*[c.ctypes.data for c in cnts]) if capture is not None else None
+    c = _cap(capture)
+    o = _opts(alg, T=T, cell_num=0, readout=readout, seed=seed, stream=stream, precision="fp32",
+              path="auto", n_steps=0, cell_offset=0)
+    check(ctx.lib.scrna_cle_simulate_batch(ctx.h, B, harr, karr, len(kins), cn_arr, parr, _ptr(c),
+                                           C.byref(o), oarr, carr))
+    if capture is not None:
+        return outs, cnts
+    return outs
+
+
+def apply_capture(X: np.ndarray, capture: CaptureModel, *, seed: int = 0, stream: int = 0,
+                  ctx: Optional[Context] = None, return_efficiencies: bool = False):
+    """GPU LogNormal-Binomial capture of a cells x G molecule matrix (capture.jl:25-47)."""
+    ctx = ctx or default_context()
+    Xf = np.asfortranarray(X, dtype=np.float64)
+    N, G = Xf.shape
+    Y = np.empty((N, G), dtype=np.int32, order="F")
+    eff = np.empty(N, dtype=np.float64)
+    c = _cap(capture)
+    check(ctx.lib.scrna_apply_capture(ctx.h, N, G, Xf.ctypes.data, C.byref(c), int(seed), int(stream),
+                                      Y.ctypes.data, eff.ctypes.data))
+    return (Y, eff) if return_efficiencies else Y
+
+
+class DeviceRun:
+    """Device-resident run of one network (scrna_state): `launch()` enqueues a whole
+    simulation on the context stream without host traffic; `read()` fetches results."""
+
+    def __init__(self, net: GeneNetwork, alg: CLE, kin: KineticParams, *, cell_num: int, T: float,
+                 readout: str = "protein", seed: int = 0, stream: int = 0,
+                 capture: Optional[CaptureModel] = None, population: Optional[PopulationConfig] = None,
+                 precision: str = "fp32", n_steps: int = 0, cell_offset: int = 0,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.handle = NetHandle(net, self.ctx)
+        self.N = population.cell_num if population is not None else cell_num
+        self.G = net.G
+        self.readout = readout
+        self.capture = capture
+        self.k, self.p, self.c = _kin(kin), _pop(population), _cap(capture)
+        self.o = _opts(alg, T=T, cell_num=self.N, readout=readout, seed=seed, stream=stream,
+                       precision=precision, path="auto", n_steps=n_steps, cell_offset=cell_offset)
+        h = C.c_void_p()
+        check(self.ctx.lib.scrna_state_create(self.ctx.h, self.handle.h, self.N, READOUT[readout],
+                                              int(capture is not None), C.byref(h)))
+        self.st = h
+
+    def launch(self):
+        check(self.ctx.lib.scrna_cle_run_device(self.ctx.h, self.handle.h, C.byref(self.k), _ptr(self.p),
+                                                _ptr(self.c), C.byref(self.o), self.st))
+
+    def read(self):
+        cols = self.G * (2 if self.readout == "both" else 1)
+        out = np.empty((self.N, cols), dtype=np.float64, order="F")
+        counts = eff = None
+        if self.capture is not None:
+            counts = np.empty((self.N, self.G), dtype=np.int32, order="F")
+            eff = np.empty(self.N, dtype=np.float64)
+        check(self.ctx.lib.scrna_state_read(self.ctx.h, self.st, out.ctypes.data,
+                                            None if counts is None else counts.ctypes.data,
+                                            None if eff is None else eff.ctypes.data))
+        return (out, counts, eff) if self.capture is not None else out
+
+    def read_raw(self):
+        """Raw state of the last run: dict with M, P ([G, N]; float32, or float64 for the
+        FP64 baseline), prom ([G, N] uint8) and V ([N], population runs)."""
+        dt = np.float64 if self.o.precision == PRECISION["fp64_plain"] else np.float32
+        M = np.empty((self.G, self.N), dtype=dt)
+        Pm = np.empty((self.G, self.N), dtype=dt)
+        prom = np.empty((self.G, self.N), dtype=np.uint8)
+        V = np.empty(self.N, dtype=np.float64) if self.p is not None else None
+        check(self.ctx.lib.scrna_state_read_raw(self.ctx.h, self.st, M.ctypes.data, Pm.ctypes.data,
+                                                prom.ctypes.data, None if V is None else V.ctypes.data))
+        out = {"M": M, "P": Pm, "prom": prom}
+        if V is not None:
+            out["V"] = V
+        return out
+
+    def device_state(self):
+        m, p = C.c_void_p(), C.c_void_p()
+        check(self.ctx.lib.scrna_state_device_ptrs(self.st, C.byref(m), C.byref(p)))
+        return m.value, p.value
+
+    def close(self):
+        if getattr(self, "st", None):
+            self.ctx.lib.scrna_state_destroy(self.st)
+            self.st = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def debug_philox(ctr: np.ndarray, key, ctx: Optional[Context] = None) -> np.ndarray:
+    ctx = ctx or default_context()
+    c = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros_like(c)
+    check(ctx.lib.scrna_debug_philox(ctx.h, c.shape[0], c.ctypes.data, k.ctypes.data, out.ctypes.data))
+    return out
+
+
+def measure_pipe_peaks(ctx: Optional[Context] = None):
+    """(fma_ops/s, sfu_ops/s, int_ops/s) measured by the library's microkernels."""
+    ctx = ctx or default_context()
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    check(ctx.lib.scrna_measure_pipe_peaks(ctx.h, C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value

@@ -1,0 +1,792 @@
+// C ABI of libscrna_cle.so: contexts, network upload, run planning and the
+// reference-facing simulate / simulate_gpu_batch / apply_capture entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/scrna_cle.h"
+#include "cle_internal.h"
+
+namespace scrna {
+FusedLaunch fused_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int n_quads);
+int fused_max_quads();
+cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st);
+cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
+cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
+                              uint32_t key0, uint32_t key1, uint32_t stream, double* M, double* P,
+                              uint8_t* prom, cudaStream_t st);
+cudaError_t plain_readout_launch(int G, int64_t N, const double* M, const double* P, int readout,
+                                 double* out, cudaStream_t st);
+cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* X, double mu_log,
+                           double sigma, uint32_t key0, uint32_t key1, uint32_t stream, double* eff,
+                           int32_t* Y, cudaStream_t st);
+cudaError_t philox_check_launch(int n, const uint32_t* d_ctr, uint32_t k0, uint32_t k1,
+                                uint32_t* d_out, cudaStream_t st);
+cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStream_t st);
+}  // namespace scrna
+
+using namespace scrna;
+
+// ---- errors ------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(SCRNA_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+// ---- device buffers -----------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; n = 0; }
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct scrna_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::atomic<int64_t> launches{0};
+    int sm_count = 0;
+};
+
+struct scrna_net {
+    scrna_ctx* ctx = nullptr;
+    int32_t G = 0;
+    std::vector<double> basals;
+    std::vector<double> A;  // row-major A[i*G+j]
+    std::vector<double> k_on, k_off;
+    // host tables
+    std::vector<int32_t> reg_slot;   // gene -> slot or -1
+    std::vector<int32_t> reg_gene;   // slot -> gene
+    std::vector<int32_t> in_begin, in_end;
+    std::vector<float2> in_edge;
+    std::vector<double> in_w64;
+    std::vector<double> cneg64;
+    std::vector<int32_t> na_begin, na_count;
+    std::vector<NonAdd> na;
+    std::vector<double> na_coef64;
+    std::vector<int32_t> na_src;
+    NetDev dev;
+    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64;
+    // per-run tables cached for the last (kinetics, dt, population mode)
+    DevBuf b_genes, b_ginit, b_quad_tel;
+    bool cache_valid = false;
+    double c_dt = 0, c_kin[6] = {0};
+    bool c_pop = false;
+};
+
+struct scrna_state {
+    scrna_ctx* ctx = nullptr;
+    int32_t G = 0;
+    int64_t N = 0;
+    int32_t readout = 1;
+    bool capture = false;
+    DevBuf M, P, prom, V, out, counts, eff;
+    DevBuf dM[2], dP[2], dprom[2], dV[2], owner[2];
+    DevBuf M64, P64a, P64b;  // FP64 baseline state
+    bool have_counts = false;
+    bool last_plain = false;
+    bool last_pop = false;
+    const double* p64_final = nullptr;
+};
+
+// ---- helpers ----------------------------------------------------------------------------------
+static uint32_t prob_threshold(double p) {
+    if (!(p > 0.0)) return 0u;
+    double t = std::floor(p * 4294967296.0);
+    if (t >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)t;
+}
+
+static int check_ctx(scrna_ctx* ctx) {
+    if (!ctx) return fail(SCRNA_EINVAL, "context is NULL");
+    return SCRNA_OK;
+}
+
+static int set_device(scrna_ctx* ctx) {
+    CU(cudaSetDevice(ctx->device));
+    return SCRNA_OK;
+}
+
+extern "C" const char* scrna_last_error(void) { return g_err.c_str(); }
+extern "C" int scrna_version(void) { return SCRNA_ABI_VERSION; }
+
+extern "C" int scrna_ctx_create(int device, scrna_ctx** out) {
+    if (!out) return fail(SCRNA_EINVAL, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    CU(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(SCRNA_EINVAL, "device %d out of range (%d devices)", device, n);
+    CU(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(SCRNA_ENOTSUP, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+    auto* c = new scrna_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return fail(SCRNA_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
+    c->own_stream = true;
+    *out = c;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_ctx_destroy(scrna_ctx* ctx) {
+    if (!ctx) return SCRNA_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_ctx_set_stream(scrna_ctx* ctx, void* s) {
+    if (int r = check_ctx(ctx)) return r;
+    if (ctx->own_stream && ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    ctx->stream = static_cast<cudaStream_t>(s);
+    ctx->own_stream = false;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_ctx_synchronize(scrna_ctx* ctx) {
+    if (int r = check_ctx(ctx)) return r;
+    if (int r = set_device(ctx)) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SCRNA_OK;
+}
+
+extern "C" int64_t scrna_ctx_launch_count(const scrna_ctx* ctx) { return ctx ? ctx->launches.load() : -1; }
+
+// ---- networks ---------------------------------------------------------------------------------
+static int build_edges(scrna_net* n, int32_t n_e, const int32_t* tgt, const int32_t* ptr,
+                       const int32_t* src, const double* str, int base, int kind,
+                       std::vector<std::vector<std::pair<NonAdd, std::vector<int32_t>>>>& per_target,
+                       std::vector<std::vector<double>>& coef64) {
+    const int G = n->G;
+    if (n_e < 0) return fail(SCRNA_EINVAL, "negative edge count");
+    if (n_e == 0) return SCRNA_OK;
+    if (!tgt || !ptr || !src || !str) return fail(SCRNA_EINVAL, "edge arrays are NULL");
+    if (ptr[0] != 0) return fail(SCRNA_EINVAL, "edge pointer array must start at 0");
+    for (int e = 0; e < n_e; ++e) {
+        const int t = tgt[e] - base;
+        if (t < 0 || t >= G) return fail(SCRNA_EINVAL, "edge %d target %d out of range", e, tgt[e]);
+        if (ptr[e + 1] < ptr[e]) return fail(SCRNA_EINVAL, "edge pointers not monotone");
+        if (ptr[e + 1] == ptr[e]) return fail(SCRNA_EINVAL, "edge %d has no sources", e);
+        std::vector<int32_t> s;
+        for (int k = ptr[e]; k < ptr[e + 1]; ++k) {
+            const int j = src[k] - base;
+            if (j < 0 || j >= G) return fail(SCRNA_EINVAL, "edge %d source %d out of range", e, src[k]);
+            s.push_back(j);
+        }
+        NonAdd na{};
+        na.kind = kind;
+        na.coef = (float)(str[e] * n->basals[t]);
+        per_target[t].push_back({na, s});
+        coef64[t].push_back(str[e] * n->basals[t]);
+    }
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals, const double* A_colmajor,
+                                int32_t n_coop, const int32_t* coop_target, const int32_t* coop_ptr,
+                                const int32_t* coop_src, const double* coop_strength,
+                                int32_t n_redun, const int32_t* redun_target, const int32_t* redun_ptr,
+                                const int32_t* redun_src, const double* redun_strength,
+                                const double* k_on, const double* k_off, int32_t index_base,
+                                scrna_net** out) {
+    if (int r = check_ctx(ctx)) return r;
+    if (!out) return fail(SCRNA_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (G <= 0) return fail(SCRNA_EINVAL, "G must be positive (got %d)", G);
+    if (!basals) return fail(SCRNA_EINVAL, "basals is NULL");
+    if (index_base != 0 && index_base != 1) return fail(SCRNA_EINVAL, "index_base must be 0 or 1");
+    auto n = std::make_unique<scrna_net>();
+    n->ctx = ctx;
+    n->G = G;
+    n->basals.assign(basals, basals + G);
+    n->A.assign((size_t)G * G, 0.0);
+    if (A_colmajor)
+        for (int i = 0; i < G; ++i)
+            for (int j = 0; j < G; ++j) n->A[(size_t)i * G + j] = A_colmajor[i + (size_t)j * G];
+    for (int i = 0; i < G; ++i)
+        if (n->A[(size_t)i * G + i] != 0.0) return fail(SCRNA_EINVAL, "interaction diagonal must be zero (gene %d)", i + index_base);
+    for (int i = 0; i < G; ++i)
+        if (!std::isfinite(n->basals[i])) return fail(SCRNA_EINVAL, "basal %d is not finite", i + index_base);
+    n->k_on.assign(G, INFINITY);
+    n->k_off.assign(G, INFINITY);
+    if (k_on) n->k_on.assign(k_on, k_on + G);
+    if (k_off) n->k_off.assign(k_off, k_off + G);
+    for (int i = 0; i < G; ++i)
+        if (n->k_on[i] < 0 || n->k_off[i] < 0 || std::isnan(n->k_on[i]) || std::isnan(n->k_off[i]))
+            return fail(SCRNA_EINVAL, "switching rates of gene %d must be >= 0", i + index_base);
+
+    std::vector<std::vector<std::pair<NonAdd, std::vector<int32_t>>>> per_t(G);
+    std::vector<std::vector<double>> coef64(G);
+    if (int r = build_edges(n.get(), n_coop, coop_target, coop_ptr, coop_src, coop_strength, index_base, 0, per_t, coef64)) return r;
+    if (int r = build_edges(n.get(), n_redun, redun_target, redun_ptr, redun_src, redun_strength, index_base, 1, per_t, coef64)) return r;
+
+    // regulator slots: genes whose protein enters any additive, cooperative or redundant term
+    std::vector<char> is_reg(G, 0);
+    for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j)
+            if (i != j && n->A[(size_t)i * G + j] * n->basals[i] != 0.0) is_reg[j] = 1;
+    for (int t = 0; t < G; ++t)
+        for (auto& pr : per_t[t])
+            for (int j : pr.second) is_reg[j] = 1;
+    n->reg_slot.assign(G, -1);
+    for (int j = 0; j < G; ++j)
+        if (is_reg[j]) { n->reg_slot[j] = (int)n->reg_gene.size(); n->reg_gene.push_back(j); }
+
+    // additive in-edges per target (A_eff = A[i,j] beta_i, network.jl:206-219), sorted by source gene
+    n->in_begin.resize(G); n->in_end.resize(G); n->cneg64.assign(G, 0.0);
+    for (int i = 0; i < G; ++i) {
+        n->in_begin[i] = (int)n->in_edge.size();
+        for (int j = 0; j < G; ++j) {
+            if (i == j) continue;
+            const double w = n->A[(size_t)i * G + j] * n->basals[i];
+            if (w == 0.0) continue;
+            float2 e;
+            e.x = (float)w;
+            int32_t slot = n->reg_slot[j];
+            std::memcpy(&e.y, &slot, 4);
+            n->in_edge.push_back(e);
+            n->in_w64.push_back(w);
+            if (w < 0.0) n->cneg64[i] += -w;
+        }
+        n->in_end[i] = (int)n->in_edge.size();
+    }
+    n->na_begin.resize(G); n->na_count.resize(G);
+    for (int t = 0; t < G; ++t) {
+        n->na_begin[t] = (int)n->na.size();
+        n->na_count[t] = (int)per_t[t].size();
+        for (size_t k = 0; k < per_t[t].size(); ++k) {
+            NonAdd na = per_t[t][k].first;
+            na.src_begin = (int)n->na_src.size();
+            for (int j : per_t[t][k].second) n->na_src.push_back(n->reg_slot[j]);
+            na.src_end = (int)n->na_src.size();
+            n->na.push_back(na);
+            n->na_coef64.push_back(coef64[t][k]);
+        }
+    }
+    if (n->na.size() >= 65536) return fail(SCRNA_ENOTSUP, "more than 65535 cooperative/redundant edges");
+
+    if (int r = set_device(ctx)) return r;
+    NetDev& d = n->dev;
+    d.G = G;
+    d.n_reg = (int)n->reg_gene.size();
+    d.n_in = (int)n->in_edge.size();
+    d.n_na = (int)n->na.size();
+    d.n_na_src = (int)n->na_src.size();
+    d.n_quads = (G + 3) / 4;
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = b.ensure(bytes);
+        if (e != cudaSuccess) return e;
+        if (bytes) return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+        return cudaSuccess;
+    };
+    CU(up(n->b_in_edge, n->in_edge.data(), n->in_edge.size() * sizeof(float2)));
+    CU(up(n->b_na, n->na.data(), n->na.size() * sizeof(NonAdd)));
+    CU(up(n->b_na_src, n->na_src.data(), n->na_src.size() * sizeof(int32_t)));
+    CU(up(n->b_reg_gene, n->reg_gene.data(), n->reg_gene.size() * sizeof(int32_t)));
+    CU(up(n->b_in_w64, n->in_w64.data(), n->in_w64.size() * sizeof(double)));
+    CU(up(n->b_na_coef64, n->na_coef64.data(), n->na_coef64.size() * sizeof(double)));
+    CU(up(n->b_beta64, n->basals.data(), n->basals.size() * sizeof(double)));
+    d.in_edge = n->b_in_edge.as<float2>();
+    d.na = n->b_na.as<NonAdd>();
+    d.na_src = n->b_na_src.as<int32_t>();
+    d.reg_gene = n->b_reg_gene.as<int32_t>();
+    d.in_w64 = n->b_in_w64.as<double>();
+    d.na_coef64 = n->b_na_coef64.as<double>();
+    d.beta64 = n->b_beta64.as<double>();
+    *out = n.release();
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_net_destroy(scrna_net* net) {
+    if (!net) return SCRNA_OK;
+    cudaSetDevice(net->ctx->device);
+    cudaStreamSynchronize(net->ctx->stream);
+    delete net;
+    return SCRNA_OK;
+}
+
+extern "C" int32_t scrna_net_genes(const scrna_net* net) { return net ? net->G : -1; }
+
+// Per-run gene tables (thresholds depend on dt, initial values on the kinetics).
+static int ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt, bool pop) {
+    const double kv[6] = {kin->k_t, kin->K_d, kin->n, kin->mu_m, kin->mu_p, kin->dilution};
+    if (n->cache_valid && n->c_dt == dt && n->c_pop == pop && std::memcmp(kv, n->c_kin, sizeof kv) == 0)
+        return SCRNA_OK;
+    const int G = n->G;
+    std::vector<GeneRec> gr(G);
+    std::vector<GeneInit> gi(G);
+    const int nq = (G + 3) / 4;
+    std::vector<uint8_t> qt(nq, 0);
+    for (int g = 0; g < G; ++g) {
+        GeneRec& r = gr[g];
+        r.beta = (float)n->basals[g];
+        r.cneg = (float)n->cneg64[g];
+        const double kon = n->k_on[g], koff = n->k_off[g];
+        const bool tel = std::isfinite(kon);
+        if (tel) {
+            r.thr_on = prob_threshold(1.0 - std::exp(-kon * dt));
+            r.thr_off = std::isfinite(koff) ? prob_threshold(1.0 - std::exp(-koff * dt)) : 0xFFFFFFFFu;
+            qt[g >> 2] = 1;
+        } else {
+            r.thr_on = 0u;
+            r.thr_off = 0u;
+        }
+        r.slot = n->reg_slot[g];
+        r.in_begin = n->in_begin[g];
+        r.in_end = n->in_end[g];
+        r.na_range = (n->na_begin[g] << 16) | n->na_count[g];
+        // initial condition: ceil of the deterministic steady state (kinetics.jl:65-70)
+        const double mss = n->basals[g] / (kin->mu_m + kin->dilution);
+        const double pss = kin->k_t * mss / (kin->mu_p + kin->dilution);
+        gi[g].m0 = (float)std::ceil(mss);
+        gi[g].p0 = (float)std::ceil(pss);
+        gi[g].init_rand = (std::isfinite(kon) && std::isfinite(koff)) ? 1 : 0;
+        gi[g].thr_init = gi[g].init_rand ? prob_threshold(kon / (kon + koff)) : 0u;
+    }
+    if (int r = set_device(n->ctx)) return r;
+    CU(cudaStreamSynchronize(n->ctx->stream));
+    CU(n->b_genes.ensure(G * sizeof(GeneRec)));
+    CU(n->b_ginit.ensure(G * sizeof(GeneInit)));
+    CU(n->b_quad_tel.ensure(nq));
+    CU(cudaMemcpy(n->b_genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(n->b_ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(n->b_quad_tel.p, qt.data(), nq, cudaMemcpyHostToDevice));
+    n->cache_valid = true;
+    n->c_dt = dt;
+    n->c_pop = pop;
+    std::memcpy(n->c_kin, kv, sizeof kv);
+    return SCRNA_OK;
+}
+
+// ---- states ------------------------------------------------------------------------------------
+static int state_alloc(scrna_state* st, bool pop, bool plain) {
+    const size_t gn = (size_t)st->G * st->N;
+    const int outcols = st->readout == SCRNA_READOUT_BOTH ? 2 : 1;
+    CU(st->M.ensure(gn * 4));
+    CU(st->P.ensure(gn * 4));
+    CU(st->prom.ensure(gn));
+    CU(st->out.ensure(gn * outcols * 8));
+    if (st->capture) {
+        CU(st->counts.ensure(gn * 4));
+        CU(st->eff.ensure((size_t)st->N * 8));
+    }
+    if (pop) {
+        CU(st->V.ensure((size_t)st->N * 8));
+        for (int k = 0; k < 2; ++k) {
+            CU(st->dM[k].ensure(gn * 4));
+            CU(st->dP[k].ensure(gn * 4));
+            CU(st->dprom[k].ensure(gn));
+            CU(st->dV[k].ensure((size_t)st->N * 8));
+            CU(st->owner[k].ensure((size_t)st->N * 8));
+        }
+    }
+    if (plain) {
+        CU(st->M64.ensure(gn * 8));
+        CU(st->P64a.ensure(gn * 8));
+        CU(st->P64b.ensure(gn * 8));
+    }
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_state_create(scrna_ctx* ctx, const scrna_net* net, int64_t cell_num, int32_t readout,
+                                  int32_t with_capture, scrna_state** out) {
+    if (int r = check_ctx(ctx)) return r;
+    if (!net || !out) return fail(SCRNA_EINVAL, "net/out is NULL");
+    if (cell_num <= 0) return fail(SCRNA_EINVAL, "cell_num must be positive");
+    if (readout < 0 || readout > 2) return fail(SCRNA_EINVAL, "readout must be 0 (mrna), 1 (protein) or 2 (both)");
+    auto* st = new scrna_state();
+    st->ctx = ctx;
+    st->G = net->G;
+    st->N = cell_num;
+    st->readout = readout;
+    st->capture = with_capture != 0;
+    *out = st;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_state_destroy(scrna_state* st) {
+    if (!st) return SCRNA_OK;
+    cudaSetDevice(st->ctx->device);
+    cudaStreamSynchronize(st->ctx->stream);
+    delete st;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_state_device_ptrs(scrna_state* st, void** m, void** p) {
+    if (!st) return fail(SCRNA_EINVAL, "state is NULL");
+    if (m) *m = st->M.p;
+    if (p) *p = st->P.p;
+    return SCRNA_OK;
+}
+
+// ---- run planning ---------------------------------------------------------------------------
+static int validate_run(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                        const scrna_capture* cap, const scrna_cle_opts* o) {
+    if (!net || !kin || !o) return fail(SCRNA_EINVAL, "net, kinetics and opts are required");
+    if (!(o->dt > 0.0) || !std::isfinite(o->dt)) return fail(SCRNA_EINVAL, "dt must be positive and finite");
+    if (o->n_steps <= 0 && !(o->T >= 0.0)) return fail(SCRNA_EINVAL, "T must be >= 0");
+    if (o->readout < 0 || o->readout > 2) return fail(SCRNA_EINVAL, "readout must be 0, 1 or 2");
+    if (!(kin->K_d > 0.0) || !(kin->n > 0.0)) return fail(SCRNA_EINVAL, "K_d and n must be positive");
+    if (!(kin->mu_m + kin->dilution > 0.0) || !(kin->mu_p + kin->dilution > 0.0))
+        return fail(SCRNA_EINVAL, "decay rates must be positive");
+    if (pop) {
+        if (pop->cell_num < 2) return fail(SCRNA_EINVAL, "population needs at least 2 cells");
+        if (pop->div_check_interval <= 0) return fail(SCRNA_EINVAL, "div_check_interval must be positive");
+        if (!(pop->V_div > 0.0) || !(pop->V_init_hi >= pop->V_init_lo)) return fail(SCRNA_EINVAL, "bad volume config");
+        if (pop->partition != SCRNA_PARTITION_BINOMIAL && pop->partition != SCRNA_PARTITION_HALVE)
+            return fail(SCRNA_EINVAL, "partition must be 0 (binomial) or 1 (halve)");
+    }
+    if (cap) {
+        if (!(cap->efficiency > 0.0) || !(cap->efficiency_std >= 0.0)) return fail(SCRNA_EINVAL, "capture efficiency must be > 0 and std >= 0");
+        if (cap->readout != SCRNA_READOUT_MRNA && cap->readout != SCRNA_READOUT_PROTEIN)
+            return fail(SCRNA_EINVAL, "readout must be :mrna or :protein");  // population.jl:63
+    }
+    return SCRNA_OK;
+}
+
+static int64_t n_steps_of(const scrna_cle_opts* o) {
+    if (o->n_steps > 0) return o->n_steps;
+    return (int64_t)std::ceil(o->T / o->dt);  // cle.jl:56
+}
+
+static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st) {
+    const NetDev& d = net->dev;
+    if (d.n_quads > fused_max_quads())
+        return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
+    const int64_t n_steps = n_steps_of(o);
+    if (n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
+    FusedArgs a{};
+    a.G = d.G; a.n_quads = d.n_quads; a.n_reg = d.n_reg; a.n_in = d.n_in; a.n_na = d.n_na; a.n_na_src = d.n_na_src;
+    a.N = st->N;
+    a.cell_offset = o->cell_offset;
+    a.k_t = (float)kin->k_t;
+    a.Kn = (float)std::pow(kin->K_d, kin->n);
+    a.hill_n = (float)kin->n;
+    a.hill_int = (kin->n == std::floor(kin->n) && kin->n >= 1.0 && kin->n <= 16.0) ? (int)kin->n : 0;
+    a.mu_m = (float)(pop ? kin->mu_m : kin->mu_m + kin->dilution);
+    a.mu_p = (float)(pop ? kin->mu_p : kin->mu_p + kin->dilution);
+    a.dt = (float)o->dt;
+    a.key0 = (uint32_t)o->seed; a.key1 = (uint32_t)(o->seed >> 32); a.stream = o->stream & 0xFFFFFFu;
+    if (pop) {
+        a.growth_factor = std::exp(pop->growth_rate * o->dt);
+        a.V_div = pop->V_div; a.V_lo = pop->V_init_lo; a.V_hi = pop->V_init_hi;
+        a.partition = pop->partition; a.exclude_mother = pop->exclude_mother ? 1 : 0;
+    }
+    a.genes = net->b_genes.as<GeneRec>();
+    a.ginit = net->b_ginit.as<GeneInit>();
+    a.in_edge = d.in_edge; a.na = d.na; a.na_src = d.na_src;
+    a.quad_tel = net->b_quad_tel.as<uint8_t>();
+    a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>();
+    if (pop) {
+        a.V = st->V.as<double>();
+        for (int k = 0; k < 2; ++k) {
+            a.dM[k] = st->dM[k].as<float>(); a.dP[k] = st->dP[k].as<float>();
+            a.dprom[k] = st->dprom[k].as<uint8_t>(); a.dV[k] = st->dV[k].as<double>();
+            a.owner[k] = st->owner[k].as<unsigned long long>();
+        }
+    }
+    a.out = st->out.as<double>();
+    a.readout = st->readout;
+    if (cap) {
+        a.counts = st->counts.as<int32_t>();
+        a.eff = st->eff.as<double>();
+        a.capture_species = cap->readout == SCRNA_READOUT_MRNA ? 0 : 1;
+        a.cap_mu_log = std::log(cap->efficiency) - (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
+        a.cap_sigma = cap->efficiency_std;
+    }
+    const FusedLaunch L = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
+    if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
+    cudaStream_t s = ctx->stream;
+    if (!pop) {
+        a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;
+        CU(fused_launch(a, L, false, s));
+        ctx->launches++;
+        return SCRNA_OK;
+    }
+    for (int k = 0; k < 2; ++k) CU(cudaMemsetAsync(st->owner[k].p, 0, (size_t)st->N * 8, s));
+    const int64_t I = pop->div_check_interval;
+    int64_t s0 = 1;
+    int epoch = 0;
+    bool first = true;
+    while (true) {
+        int64_t s1 = std::min(n_steps, ((s0 - 1) / I + 1) * I);
+        if (n_steps == 0) s1 = 0;
+        const bool check = s1 >= s0 && (s1 % I == 0);
+        const bool final_chunk = s1 >= n_steps;
+        a.step_begin = (int)s0; a.step_end = (int)s1;
+        a.first = first ? 1 : 0;
+        a.epoch = epoch;
+        a.check = check ? 1 : 0;
+        a.last = (final_chunk && !check) ? 1 : 0;
+        CU(fused_launch(a, L, true, s));
+        ctx->launches++;
+        first = false;
+        if (check) epoch += 1;
+        if (final_chunk) {
+            if (check) {  // apply the last division's placements, then read out
+                a.step_begin = (int)s1 + 1; a.step_end = (int)s1;
+                a.first = 0; a.epoch = epoch; a.check = 0; a.last = 1;
+                CU(fused_launch(a, L, true, s));
+                ctx->launches++;
+            }
+            break;
+        }
+        s0 = s1 + 1;
+    }
+    return SCRNA_OK;
+}
+
+static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_capture* cap,
+                     const scrna_cle_opts* o, scrna_state* st) {
+    const NetDev& d = net->dev;
+    const int64_t n_steps = n_steps_of(o);
+    const uint32_t k0 = (uint32_t)o->seed, k1 = (uint32_t)(o->seed >> 32), sid = o->stream & 0xFFFFFFu;
+    cudaStream_t s = ctx->stream;
+    double* M = st->M64.as<double>();
+    double* Pa = st->P64a.as<double>();
+    double* Pb = st->P64b.as<double>();
+    CU(plain_init_launch(d.G, st->N, o->cell_offset, net->b_ginit.as<GeneInit>(), k0, k1, sid, M, Pa,
+                         st->prom.as<uint8_t>(), s));
+    ctx->launches++;
+    PlainArgs a{};
+    a.G = d.G; a.n_quads = d.n_quads; a.N = st->N; a.cell_offset = o->cell_offset;
+    a.k_t = kin->k_t; a.Kn = std::pow(kin->K_d, kin->n); a.hill_n = kin->n;
+    a.mu_m = kin->mu_m + kin->dilution; a.mu_p = kin->mu_p + kin->dilution;
+    a.dt = o->dt; a.sqrt_dt = std::sqrt(o->dt);
+    a.key0 = k0; a.key1 = k1; a.stream = sid;
+    a.genes = net->b_genes.as<GeneRec>();
+    a.in_edge = d.in_edge; a.in_w64 = d.in_w64; a.na = d.na; a.na_coef64 = d.na_coef64;
+    a.na_src = d.na_src; a.reg_gene = d.reg_gene; a.quad_tel = net->b_quad_tel.as<uint8_t>();
+    a.beta64 = d.beta64;
+    a.M = M; a.prom = st->prom.as<uint8_t>();
+    for (int64_t step = 1; step <= n_steps; ++step) {
+        a.step = (int)step;
+        a.Pold = (step & 1) ? Pa : Pb;
+        a.Pnew = (step & 1) ? Pb : Pa;
+        CU(plain_step_launch(a, s));
+        ctx->launches++;
+    }
+    const double* Pfinal = (n_steps & 1) ? Pb : Pa;
+    st->p64_final = Pfinal;
+    CU(plain_readout_launch(d.G, st->N, M, Pfinal, st->readout, st->out.as<double>(), s));
+    ctx->launches++;
+    if (cap) {
+        const double mu_log = std::log(cap->efficiency) -
+                              (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
+        const double* X = cap->readout == SCRNA_READOUT_MRNA ? M : Pfinal;
+        CU(capture_launch(d.G, st->N, o->cell_offset, X, mu_log, cap->efficiency_std, k0, k1, sid,
+                          st->eff.as<double>(), st->counts.as<int32_t>(), s));
+        ctx->launches += 2;
+    }
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetics* kin,
+                                    const scrna_population* pop, const scrna_capture* cap,
+                                    const scrna_cle_opts* o, scrna_state* st) {
+    if (int r = check_ctx(ctx)) return r;
+    if (int r = validate_run(cnet, kin, pop, cap, o)) return r;
+    if (!st) return fail(SCRNA_EINVAL, "state is NULL");
+    scrna_net* net = const_cast<scrna_net*>(cnet);
+    if (st->G != net->G) return fail(SCRNA_EINVAL, "state was created for G=%d, network has G=%d", st->G, net->G);
+    const int64_t N = pop ? pop->cell_num : o->cell_num;
+    if (N != st->N) return fail(SCRNA_EINVAL, "state holds %lld cells, run asks for %lld", (long long)st->N, (long long)N);
+    if (cap && !st->capture) return fail(SCRNA_EINVAL, "state was created without capture buffers");
+    if (o->readout != st->readout) return fail(SCRNA_EINVAL, "readout differs from the state's readout");
+    if (o->cell_offset < 0 || o->cell_offset + N > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
+    const bool plain = o->precision == SCRNA_PRECISION_FP64_PLAIN;
+    if (plain && pop) return fail(SCRNA_ENOTSUP, "the FP64 baseline path has no population dynamics");
+    if (o->precision != SCRNA_PRECISION_FP32 && !plain) return fail(SCRNA_EINVAL, "unknown precision");
+    if (int r = set_device(ctx)) return r;
+    if (int r = ensure_gene_tables(net, kin, o->dt, pop != nullptr)) return r;
+    if (int r = state_alloc(st, pop != nullptr, plain)) return r;
+    st->have_counts = cap != nullptr;
+    st->last_plain = plain;
+    st->last_pop = pop != nullptr;
+    if (plain) return run_plain(ctx, net, kin, cap, o, st);
+    return run_fused(ctx, net, kin, pop, cap, o, st);
+}
+
+extern "C" int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, int32_t* counts, double* eff) {
+    if (int r = check_ctx(ctx)) return r;
+    if (!st) return fail(SCRNA_EINVAL, "state is NULL");
+    if (int r = set_device(ctx)) return r;
+    const size_t gn = (size_t)st->G * st->N;
+    const int outcols = st->readout == SCRNA_READOUT_BOTH ? 2 : 1;
+    if (out) CU(cudaMemcpyAsync(out, st->out.p, gn * outcols * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if ((counts || eff) && !st->have_counts) return fail(SCRNA_EINVAL, "the last run had no capture");
+    if (counts) CU(cudaMemcpyAsync(counts, st->counts.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (eff) CU(cudaMemcpyAsync(eff, st->eff.p, (size_t)st->N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* protein,
+                                    uint8_t* promoter, double* volume) {
+    if (int r = check_ctx(ctx)) return r;
+    if (!st) return fail(SCRNA_EINVAL, "state is NULL");
+    if (int r = set_device(ctx)) return r;
+    const size_t gn = (size_t)st->G * st->N;
+    const size_t esz = st->last_plain ? 8 : 4;
+    const void* dm = st->last_plain ? st->M64.p : st->M.p;
+    const void* dp = st->last_plain ? (const void*)st->p64_final : st->P.p;
+    if (!dm || !dp) return fail(SCRNA_EINVAL, "the state has not been run");
+    if (mrna) CU(cudaMemcpyAsync(mrna, dm, gn * esz, cudaMemcpyDeviceToHost, ctx->stream));
+    if (protein) CU(cudaMemcpyAsync(protein, dp, gn * esz, cudaMemcpyDeviceToHost, ctx->stream));
+    if (promoter) CU(cudaMemcpyAsync(promoter, st->prom.p, gn, cudaMemcpyDeviceToHost, ctx->stream));
+    if (volume) {
+        if (!st->last_pop) return fail(SCRNA_EINVAL, "the last run had no population");
+        CU(cudaMemcpyAsync(volume, st->V.p, (size_t)st->N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                                  const scrna_population* pop, const scrna_capture* cap,
+                                  const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+    if (int r = check_ctx(ctx)) return r;
+    if (int r = validate_run(net, kin, pop, cap, o)) return r;
+    if (!out) return fail(SCRNA_EINVAL, "out is NULL");
+    if (cap && !counts) return fail(SCRNA_EINVAL, "counts is NULL but capture was requested");
+    const int64_t N = pop ? pop->cell_num : o->cell_num;
+    if (N <= 0) return fail(SCRNA_EINVAL, "cell_num must be positive");
+    scrna_state* st = nullptr;
+    if (int r = scrna_state_create(ctx, net, N, o->readout, cap != nullptr, &st)) return r;
+    std::unique_ptr<scrna_state, int (*)(scrna_state*)> guard(st, scrna_state_destroy);
+    if (int r = scrna_cle_run_device(ctx, net, kin, pop, cap, o, st)) return r;
+    return scrna_state_read(ctx, st, out, cap ? counts : nullptr, cap ? eff : nullptr);
+}
+
+extern "C" int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets,
+                                        const scrna_kinetics* kins, int32_t n_kins, const int64_t* cell_nums,
+                                        const scrna_population* const* pops, const scrna_capture* cap,
+                                        const scrna_cle_opts* opts, double* const* outs, int32_t* const* counts) {
+    if (int r = check_ctx(ctx)) return r;
+    if (B <= 0 || !nets || !kins || !opts || !outs) return fail(SCRNA_EINVAL, "bad batch arguments");
+    if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
+    std::vector<scrna_state*> states(B, nullptr);
+    int rc = SCRNA_OK;
+    for (int b = 0; b < B && rc == SCRNA_OK; ++b) {
+        const scrna_population* pop = pops ? pops[b] : nullptr;
+        scrna_cle_opts o = *opts;
+        o.stream = (opts->stream + (uint32_t)b) & 0xFFFFFFu;
+        if (!pop) {
+            if (!cell_nums) { rc = fail(SCRNA_EINVAL, "cell_nums is NULL"); break; }
+            o.cell_num = cell_nums[b];
+        }
+        const int64_t N = pop ? pop->cell_num : o.cell_num;
+        rc = scrna_state_create(ctx, nets[b], N, o.readout, cap != nullptr, &states[b]);
+        if (rc == SCRNA_OK) rc = scrna_cle_run_device(ctx, nets[b], &kins[n_kins == 1 ? 0 : b], pop, cap, &o, states[b]);
+    }
+    for (int b = 0; b < B && rc == SCRNA_OK; ++b)
+        rc = scrna_state_read(ctx, states[b], outs[b], (cap && counts) ? counts[b] : nullptr, nullptr);
+    for (auto* st : states) scrna_state_destroy(st);
+    return rc;
+}
+
+extern "C" int scrna_apply_capture(scrna_ctx* ctx, int64_t N, int32_t G, const double* X, const scrna_capture* cap,
+                                   uint64_t seed, uint32_t stream, int32_t* Y, double* eff) {
+    if (int r = check_ctx(ctx)) return r;
+    if (N <= 0 || G <= 0 || !X || !cap || !Y) return fail(SCRNA_EINVAL, "bad capture arguments");
+    if (!(cap->efficiency > 0.0) || !(cap->efficiency_std >= 0.0)) return fail(SCRNA_EINVAL, "capture efficiency must be > 0 and std >= 0");
+    if (int r = set_device(ctx)) return r;
+    const size_t gn = (size_t)G * N;
+    DevBuf dX, dY, dE;
+    CU(dX.ensure(gn * 8));
+    CU(dY.ensure(gn * 4));
+    CU(dE.ensure((size_t)N * 8));
+    CU(cudaMemcpyAsync(dX.p, X, gn * 8, cudaMemcpyHostToDevice, ctx->stream));
+    const double mu_log = std::log(cap->efficiency) -
+                          (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
+    CU(capture_launch(G, N, 0, dX.as<double>(), mu_log, cap->efficiency_std, (uint32_t)seed,
+                      (uint32_t)(seed >> 32), stream & 0xFFFFFFu, dE.as<double>(), dY.as<int32_t>(), ctx->stream));
+    ctx->launches += 2;
+    CU(cudaMemcpyAsync(Y, dY.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (eff) CU(cudaMemcpyAsync(eff, dE.p, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_debug_philox(scrna_ctx* ctx, int32_t n, const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    if (int r = check_ctx(ctx)) return r;
+    if (n <= 0 || !ctr || !key || !out) return fail(SCRNA_EINVAL, "bad arguments");
+    if (int r = set_device(ctx)) return r;
+    DevBuf dc, dout;
+    CU(dc.ensure((size_t)n * 16));
+    CU(dout.ensure((size_t)n * 16));
+    CU(cudaMemcpyAsync(dc.p, ctr, (size_t)n * 16, cudaMemcpyHostToDevice, ctx->stream));
+    CU(philox_check_launch(n, dc.as<uint32_t>(), key[0], key[1], dout.as<uint32_t>(), ctx->stream));
+    ctx->launches++;
+    CU(cudaMemcpyAsync(out, dout.p, (size_t)n * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma, double* sfu, double* iops) {
+    if (int r = check_ctx(ctx)) return r;
+    if (int r = set_device(ctx)) return r;
+    DevBuf sink;
+    CU(sink.ensure(256 * 4));
+    const int blocks = ctx->sm_count * 8;
+    const int iters[3] = {4096, 1024, 2048};
+    double res[3];
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    for (int w = 0; w < 3; ++w) {
+        CU(peak_launch(w, blocks, iters[w] / 8, sink.as<float>(), ctx->stream));  // warm-up
+        CU(cudaEventRecord(e0, ctx->stream));
+        CU(peak_launch(w, blocks, iters[w], sink.as<float>(), ctx->stream));
+        CU(cudaEventRecord(e1, ctx->stream));
+        CU(cudaEventSynchronize(e1));
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        ctx->launches += 2;
+        res[w] = (double)blocks * 256.0 * iters[w] * 16.0 * 8.0 / (ms * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (fma) *fma = res[0];
+    if (sfu) *sfu = res[1];
+    if (iops) *iops = res[2];
+    return SCRNA_OK;
+}

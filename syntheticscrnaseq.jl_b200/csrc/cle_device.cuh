@@ -1,0 +1,162 @@
+// Device-side building blocks shared by the CLE kernels: Philox4x32-10, the
+// Box-Muller transform on Philox words, probability thresholds and the
+// bit-reproducible binomial samplers used for capture and division.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace scrna {
+
+// Random-stream tags (bits 31..24 of counter word 3).  The counter layout is part of
+// the library's reproducibility contract: a run is a pure function of (seed, stream).
+enum : uint32_t {
+    TAG_NORMAL = 1,      // (cell, step, gene_pair)    -> Box-Muller pairs for genes 2k, 2k+1
+    TAG_SWITCH = 2,      // (cell, step, gene_quad)    -> one telegraph word per gene
+    TAG_PROMOTER = 3,    // (cell, 0, gene_quad)       -> initial promoter state
+    TAG_VOLUME = 4,      // (cell, 0, 0)               -> initial volume
+    TAG_MORAN = 5,       // (mother, step, 0)          -> replaced slot
+    TAG_PARTITION = 6,   // (cell, step, b<<22|g<<1|s) -> partition bits
+    TAG_EFFICIENCY = 7,  // (cell, 0, 0)               -> capture efficiency normal
+    TAG_CAPTURE = 8      // (cell, chunk, gene)        -> capture inverse-CDF uniform
+};
+
+constexpr int kCaptureChunk = 512;
+constexpr int64_t kPartitionPopcountMax = 131072;
+
+struct Key { uint32_t k0, k1; };
+
+// Philox4x32-10 (Salmon et al., SC'11): 10 rounds of two 32x32->64 products whose
+// high halves are xor'ed with the other counter words and the round key.
+__device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                        Key key) {
+    uint32_t k0 = key.k0, k1 = key.k1;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0;
+        const uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+__device__ __forceinline__ uint32_t tagword(uint32_t tag, uint32_t stream) {
+    return (tag << 24) | (stream & 0xFFFFFFu);
+}
+
+// FP32 Box-Muller pieces for one pair of words:
+//   u1 = 1 - (w0>>9) 2^-23 in (0,1],  h = (w1>>9) 2^-23 - 1/2 in [-1/2,1/2)
+//   L = -2 ln u1,  (z0, z1) = sqrt(L) (cos 2 pi h, sin 2 pi h).
+// Returned as (L, cos, sin) so callers can fold sqrt(L) into another square root.
+struct BM { float L, c, s; };
+__device__ __forceinline__ BM box_muller_parts(uint32_t w0, uint32_t w1) {
+    const float u1 = 2.0f - __int_as_float(int((w0 >> 9) | 0x3F800000u));
+    const float h = __int_as_float(int((w1 >> 9) | 0x3F800000u)) - 1.5f;
+    const float th = 6.28318530717958648f * h;
+    BM r;
+    r.L = -1.38629436111989061f * __log2f(u1);  // -2 ln 2 * log2(u1)
+    __sincosf(th, &r.s, &r.c);
+    return r;
+}
+
+// FP64 Box-Muller (first normal of the pair), same uniforms as above.
+__device__ __forceinline__ double box_muller_z0_f64(uint32_t w0, uint32_t w1) {
+    const double u1 = (double)(8388608u - (w0 >> 9)) / 8388608.0;
+    const double u2 = (double)(w1 >> 9) / 8388608.0;
+    const double th = 6.283185307179586 * (u2 - 0.5);
+    return sqrt(-2.0 * log(u1)) * cos(th);
+}
+__device__ __forceinline__ void box_muller_f64(uint32_t w0, uint32_t w1, double* z0, double* z1) {
+    const double u1 = (double)(8388608u - (w0 >> 9)) / 8388608.0;
+    const double u2 = (double)(w1 >> 9) / 8388608.0;
+    const double th = 6.283185307179586 * (u2 - 0.5);
+    const double r = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincos(th, &s, &c);
+    *z0 = r * c;
+    *z1 = r * s;
+}
+
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    return __dmul_rn(__dadd_rn(__dmul_rn((double)(a >> 5), 67108864.0), (double)(b >> 6)),
+                     1.0 / 9007199254740992.0);
+}
+
+// Inverse-CDF Binomial(n, p) for n <= kCaptureChunk and p <= 1/2, every operation an
+// explicitly rounded IEEE op so that a CPU restatement compiled without FMA contraction
+// returns the identical integer:  pmf(0) = (1-p)^n by binary powering, then
+// pmf(k+1) = ((pmf(k) (n-k)) / (k+1)) (p/(1-p)); result = smallest k with u < cdf(k).
+__device__ __forceinline__ int invcdf_chunk(int n, double p, double u) {
+    const double q = __dadd_rn(1.0, -p);
+    const double ratio = __ddiv_rn(p, q);
+    double base = q, pmf = 1.0;
+    for (int e = n; e; e >>= 1) {
+        if (e & 1) pmf = __dmul_rn(pmf, base);
+        base = __dmul_rn(base, base);
+    }
+    double cdf = pmf;
+    int k = 0;
+    while (u >= cdf && k < n) {
+        pmf = __dmul_rn(__ddiv_rn(__dmul_rn(pmf, (double)(n - k)), (double)(k + 1)), ratio);
+        k += 1;
+        cdf = __dadd_rn(cdf, pmf);
+    }
+    return k;
+}
+
+// Binomial(n, p) as a sum of chunks of at most kCaptureChunk trials, each with its own
+// uniform (counter (cell, chunk, gene)); p > 1/2 is sampled as n - Binomial(n, 1-p).
+__device__ __forceinline__ int64_t binomial_capture(int64_t n, double p, Key key, uint32_t stream,
+                                                    uint32_t cell, uint32_t gene) {
+    if (n <= 0 || !(p > 0.0)) return 0;
+    const bool flip = p > 0.5;
+    const double pp = flip ? __dadd_rn(1.0, -p) : p;
+    int64_t total = 0;
+    const int64_t nch = (n + kCaptureChunk - 1) / kCaptureChunk;
+    for (int64_t i = 0; i < nch; ++i) {
+        int64_t ni = n - i * kCaptureChunk;
+        if (ni > kCaptureChunk) ni = kCaptureChunk;
+        const uint4 w = philox(cell, (uint32_t)i, gene, tagword(TAG_CAPTURE, stream), key);
+        total += invcdf_chunk((int)ni, pp, u53(w.x, w.y));
+    }
+    return flip ? n - total : total;
+}
+
+// Binomial(n, 1/2) for the division partition: the popcount of n Philox bits.
+__device__ __forceinline__ int64_t binomial_half(int64_t n, Key key, uint32_t stream, uint32_t cell,
+                                                 uint32_t step, uint32_t gene, uint32_t species) {
+    if (n <= 0) return 0;
+    if (n > kPartitionPopcountMax) {
+        const uint4 w = philox(cell, step, (gene << 1) | species, tagword(TAG_PARTITION, stream), key);
+        double z0, z1;
+        box_muller_f64(w.x, w.y, &z0, &z1);
+        double x = rint(0.5 * (double)n + 0.5 * sqrt((double)n) * z0);
+        x = fmin(fmax(x, 0.0), (double)n);
+        return (int64_t)x;
+    }
+    int64_t total = 0, left = n;
+    for (uint32_t b = 0; left > 0; ++b) {
+        const uint4 w = philox(cell, step, (b << 22) | (gene << 1) | species,
+                               tagword(TAG_PARTITION, stream), key);
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (left <= 0) break;
+            uint32_t x = ws[j];
+            if (left < 32) x &= (1u << left) - 1u;
+            total += __popc(x);
+            left -= 32;
+        }
+    }
+    return total;
+}
+
+__device__ __forceinline__ float fsqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+}  // namespace scrna

@@ -1,0 +1,374 @@
+// Fused FP32 register-path CLE kernel (sm_100a).
+//
+// One launch advances a tile of cells through a chunk of Euler-Maruyama steps
+// (src/algorithms/cle.jl:78-121, population form cle.jl:185-237) with the state
+// held in registers for the whole chunk:
+//   * lanes are cells (32 per warp), warps are gene quads: thread (lane, warp w)
+//     owns genes 4q..4q+3 of one cell for q = w, w+NW, ... (UPT quads);
+//   * per step, genes whose protein regulates others publish their Hill
+//     activation to a shared-memory slot table (double-buffered, one barrier
+//     per step); targets read their sparse in-edges from it;
+//   * the additive term uses reg = cneg + sum_j A_eff[g,j] act_j, which equals
+//     A_pos act + A_neg rep because rep = 1 - act (network.jl:206-219);
+//   * increments come from counter-based Philox keyed by (seed, stream, cell,
+//     step, gene), so results do not depend on the tiling;
+//   * HBM is touched only at chunk boundaries (state, division buffers) and for
+//     the final readout / capture.
+#pragma once
+#include "cle_device.cuh"
+#include "cle_internal.h"
+
+namespace scrna {
+
+__device__ __forceinline__ float frcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float hill_act(float p, float Kn, float hill_n, int hill_int) {
+    float pn;
+    if (hill_int == 2) {
+        pn = p * p;
+    } else if (hill_int > 0) {
+        pn = 1.0f;
+        for (int i = 0; i < hill_int; ++i) pn *= p;
+    } else {
+        pn = exp2f(hill_n * __log2f(p));
+    }
+    // pn / (pn + Kn); an infinite pn gives NaN in the product and fminf returns 1.
+    return fminf(pn * frcp_approx(pn + Kn), 1.0f);
+}
+
+// Shared-memory layout of one block: regulator activations (2 x n_reg x 32 floats),
+// then the gene table, the edge tables and the per-quad switching flags.
+struct Smem {
+    float* act;
+    GeneRec* genes;
+    float2* in_edge;
+    NonAdd* na;
+    int32_t* na_src;
+    uint8_t* quad_tel;
+};
+
+__host__ __device__ inline size_t fused_smem_bytes(int G, int n_reg, int n_in, int n_na,
+                                                   int n_na_src, int n_quads) {
+    size_t b = (size_t)2 * n_reg * 32 * sizeof(float);
+    b += (size_t)G * sizeof(GeneRec);
+    b += (size_t)n_in * sizeof(float2);
+    b += (size_t)n_na * sizeof(NonAdd);
+    b += (size_t)n_na_src * sizeof(int32_t);
+    b += (size_t)n_quads;
+    return (b + 15) & ~(size_t)15;
+}
+
+template <int UPT, bool POP>
+__global__ void __launch_bounds__(UPT <= 2 ? 256 : 512)
+cle_fused_kernel(const FusedArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem sm;
+    {
+        unsigned char* p = smem_raw;
+        sm.act = reinterpret_cast<float*>(p);       p += (size_t)2 * a.n_reg * 32 * sizeof(float);
+        sm.genes = reinterpret_cast<GeneRec*>(p);   p += (size_t)a.G * sizeof(GeneRec);
+        sm.in_edge = reinterpret_cast<float2*>(p);  p += (size_t)a.n_in * sizeof(float2);
+        sm.na = reinterpret_cast<NonAdd*>(p);       p += (size_t)a.n_na * sizeof(NonAdd);
+        sm.na_src = reinterpret_cast<int32_t*>(p);  p += (size_t)a.n_na_src * sizeof(int32_t);
+        sm.quad_tel = p;
+    }
+    const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
+    for (int i = tid; i < a.G; i += nthr) sm.genes[i] = a.genes[i];
+    for (int i = tid; i < a.n_in; i += nthr) sm.in_edge[i] = a.in_edge[i];
+    for (int i = tid; i < a.n_na; i += nthr) sm.na[i] = a.na[i];
+    for (int i = tid; i < a.n_na_src; i += nthr) sm.na_src[i] = a.na_src[i];
+    for (int i = tid; i < a.n_quads; i += nthr) sm.quad_tel[i] = a.quad_tel[i];
+    __syncthreads();
+
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int NW = nthr >> 5;
+    const int64_t N = a.N;
+    const int64_t cell = (int64_t)blockIdx.x * 32 + lane;
+    const bool live = cell < N;
+    const int64_t cidx = live ? cell : N - 1;  // dead lanes shadow the last cell, never store
+    const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
+    const Key key{a.key0, a.key1};
+    const int G = a.G;
+    const bool has_reg = a.n_reg > 0;
+
+    float m[UPT][4], p[UPT][4];
+    uint32_t on = 0xFFFFFFFFu;  // bit 4j+i: promoter of gene 4q_j+i is ON
+    double V = 0.0;
+
+    // ---- prologue: initial condition or state of the previous chunk -------------
+    if (a.first) {
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            const int q = warp + j * NW;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int g = 4 * q + i;
+                m[j][i] = (q < a.n_quads && g < G) ? a.ginit[g].m0 : 0.0f;
+                p[j][i] = (q < a.n_quads && g < G) ? a.ginit[g].p0 : 0.0f;
+            }
+            if (q < a.n_quads) {
+                bool any = false;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int g = 4 * q + i;
+                    any |= (g < G) && a.ginit[g].init_rand;
+                }
+                if (any) {
+                    const uint4 w = philox(gcell, 0u, (uint32_t)q, tagword(TAG_PROMOTER, a.stream), key);
+                    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int g = 4 * q + i;
+                        if (g < G && a.ginit[g].init_rand && !(ws[i] < a.ginit[g].thr_init))
+                            on &= ~(1u << (4 * j + i));
+                    }
+                }
+            }
+        }
+        if (POP) {
+            const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
+            V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
+        }
+    } else {
+        // A cell replaced at the previous division takes the daughter of its new owner.
+        int64_t src = cidx;
+        bool from_daughter = false;
+        const int par = a.epoch & 1;
+        if (POP && a.epoch > 0) {
+            const unsigned long long o = a.owner[par][cidx];
+            if ((uint32_t)(o >> 32) == (uint32_t)a.epoch) {
+                src = (int64_t)(o & 0xFFFFFFFFull);
+                from_daughter = true;
+            }
+        }
+        const float* Ms = from_daughter ? a.dM[par] : a.M;
+        const float* Ps = from_daughter ? a.dP[par] : a.P;
+        const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            const int q = warp + j * NW;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int g = 4 * q + i;
+                const bool ok = q < a.n_quads && g < G;
+                m[j][i] = ok ? Ms[(size_t)g * N + src] : 0.0f;
+                p[j][i] = ok ? Ps[(size_t)g * N + src] : 0.0f;
+                if (ok && !Os[(size_t)g * N + src]) on &= ~(1u << (4 * j + i));
+            }
+        }
+        if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
+    }
+
+    // ---- fused step loop ---------------------------------------------------------
+    const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
+    int buf = 0;
+    for (int s = a.step_begin; s <= a.step_end; ++s) {
+        // telegraph switching before the transcription update (tauleap_binomial.jl:111-121)
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            const int q = warp + j * NW;
+            if (q < a.n_quads && sm.quad_tel[q]) {
+                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)q, tagword(TAG_SWITCH, a.stream), key);
+                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int g = 4 * q + i;
+                    if (g < G) {
+                        const uint32_t bit = 1u << (4 * j + i);
+                        const bool is_on = on & bit;
+                        const uint32_t thr = is_on ? sm.genes[g].thr_off : sm.genes[g].thr_on;
+                        if (ws[i] < thr) on ^= bit;
+                    }
+                }
+            }
+        }
+        // Hill activations of regulator genes -> slot table
+        float* act = sm.act + (size_t)buf * a.n_reg * 32;
+        if (has_reg) {
+#pragma unroll
+            for (int j = 0; j < UPT; ++j) {
+                const int q = warp + j * NW;
+                if (q < a.n_quads) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int g = 4 * q + i;
+                        if (g < G) {
+                            const int slot = sm.genes[g].slot;
+                            if (slot >= 0) act[slot * 32 + lane] = hill_act(p[j][i], a.Kn, a.hill_n, a.hill_int);
+                        }
+                    }
+                }
+            }
+            if (NW > 1) __syncthreads(); else __syncwarp();
+        }
+        const float Vf = POP ? (float)V : 1.0f;
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            const int q = warp + j * NW;
+            if (q >= a.n_quads) continue;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {  // gene pairs 2q, 2q+1 of this quad
+                const int g0 = 4 * q + 2 * h;
+                if (g0 >= G) continue;
+                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h),
+                                       tagword(TAG_NORMAL, a.stream), key);
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int i = 2 * h + k;
+                    const int g = g0 + k;
+                    if (g >= G) continue;
+                    const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+                    const GeneRec gr = sm.genes[g];
+                    float reg = gr.cneg;
+                    for (int e = gr.in_begin; e < gr.in_end; ++e) {
+                        const float2 ed = sm.in_edge[e];
+                        reg = fmaf(ed.x, act[__float_as_int(ed.y) * 32 + lane], reg);
+                    }
+                    const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
+                    for (int e = nab; e < nab + nac; ++e) {
+                        const NonAdd na = sm.na[e];
+                        float prod = 1.0f;
+                        if (na.kind == 0) {
+                            for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[sm.na_src[t] * 32 + lane];
+                            reg = fmaf(na.coef, prod, reg);
+                        } else {
+                            for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[sm.na_src[t] * 32 + lane];
+                            reg = fmaf(na.coef, 1.0f - prod, reg);
+                        }
+                    }
+                    float tx = reg + gr.beta;
+                    if (POP) tx *= Vf;
+                    if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
+                    // Euler-Maruyama with collapsed noise; z*sqrt(dt*var) = cos(th)*sqrt(L*dt*var).
+                    const float Ldt = bm.L * dt;
+                    const float mo = m[j][i], po = p[j][i];
+                    const float var_m = fmaxf(fmaf(mu_m, mo, tx), 0.0f);
+                    float mn = fmaf(fmaf(-mu_m, mo, tx), dt, mo) + bm.c * fsqrt_approx(Ldt * var_m);
+                    mn = fmaxf(mn, 0.0f);
+                    const float var_p = fmaf(k_t, mn, mu_p * po);
+                    float pn = fmaf(fmaf(k_t, mn, -mu_p * po), dt, po) + bm.s * fsqrt_approx(Ldt * var_p);
+                    pn = fmaxf(pn, 0.0f);
+                    m[j][i] = mn;
+                    p[j][i] = pn;
+                }
+            }
+        }
+        if (POP) V = __dmul_rn(V, a.growth_factor);
+        buf ^= 1;
+    }
+
+    // ---- epilogue --------------------------------------------------------------------
+    if (POP && a.check) {
+        // division (cle.jl:240-273): partition in registers, daughters to the
+        // next-epoch buffers, replaced slot claimed with a last-writer-wins max.
+        const bool divides = V > a.V_div;
+        const int ne = a.epoch + 1;
+        const int par = ne & 1;
+        if (divides) {
+            V = V * 0.5;
+            if (live && warp == 0) {
+                const uint4 w = philox((uint32_t)(a.cell_offset + cidx), (uint32_t)a.step_end, 0u,
+                                       tagword(TAG_MORAN, a.stream), key);
+                int64_t r;
+                if (a.exclude_mother) {
+                    r = (int64_t)(((uint64_t)w.x * (uint64_t)(N - 1)) >> 32);
+                    if (r >= cidx) r += 1;
+                } else {
+                    r = (int64_t)(((uint64_t)w.x * (uint64_t)N) >> 32);
+                }
+                a.dV[par][cidx] = V;
+                atomicMax(&a.owner[par][r], ((unsigned long long)(uint32_t)ne << 32) | (unsigned long long)cidx);
+            }
+#pragma unroll
+            for (int j = 0; j < UPT; ++j) {
+                const int q = warp + j * NW;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int g = 4 * q + i;
+                    if (!(live && q < a.n_quads && g < G)) continue;
+                    float mm, dm, pm, dp;
+                    if (a.partition == 1) {  // halve
+                        mm = dm = m[j][i] * 0.5f;
+                        pm = dp = p[j][i] * 0.5f;
+                    } else {  // binomial split of rounded counts
+                        const int64_t mi = (int64_t)rintf(m[j][i]);
+                        const int64_t pi = (int64_t)rintf(p[j][i]);
+                        const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 0u);
+                        const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 1u);
+                        mm = (float)mk; dm = (float)(mi - mk);
+                        pm = (float)pk; dp = (float)(pi - pk);
+                    }
+                    m[j][i] = mm;
+                    p[j][i] = pm;
+                    const size_t idx = (size_t)g * N + cidx;
+                    a.dM[par][idx] = dm;
+                    a.dP[par][idx] = dp;
+                    a.dprom[par][idx] = (on >> (4 * j + i)) & 1u;
+                }
+            }
+        }
+    }
+    if (!live) return;
+    const bool write_state = !a.last || POP;
+#pragma unroll
+    for (int j = 0; j < UPT; ++j) {
+        const int q = warp + j * NW;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int g = 4 * q + i;
+            if (!(q < a.n_quads && g < G)) continue;
+            const size_t idx = (size_t)g * N + cell;
+            if (write_state || a.last) {
+                a.M[idx] = m[j][i];
+                a.P[idx] = p[j][i];
+                a.prom[idx] = (on >> (4 * j + i)) & 1u;
+            }
+            if (a.last && a.out) {
+                if (a.readout == 0) a.out[idx] = (double)m[j][i];
+                else if (a.readout == 1) a.out[idx] = (double)p[j][i];
+                else { a.out[idx] = (double)m[j][i]; a.out[(size_t)(G + g) * N + cell] = (double)p[j][i]; }
+            }
+        }
+    }
+    if (POP && warp == 0) a.V[cell] = V;
+    if (a.last && a.counts) {
+        // capture (capture.jl:30-44): per-cell LogNormal efficiency, then inverse-CDF binomials
+        const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, a.stream), key);
+        const double z = box_muller_z0_f64(w.x, w.y);
+        double pe = exp(a.cap_mu_log + a.cap_sigma * z);
+        pe = fmin(fmax(pe, 0.0), 1.0);
+        if (warp == 0 && a.eff) a.eff[cell] = pe;
+#pragma unroll
+        for (int j = 0; j < UPT; ++j) {
+            const int q = warp + j * NW;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int g = 4 * q + i;
+                if (!(q < a.n_quads && g < G)) continue;
+                const double x = rint((double)(a.capture_species == 0 ? m[j][i] : p[j][i]));
+                const int64_t n = x > 0.0 ? (int64_t)x : 0;
+                int64_t y = 0;
+                if (n > 0 && pe != 0.0) y = binomial_capture(n, pe, key, a.stream, gcell, (uint32_t)g);
+                a.counts[(size_t)g * N + cell] = (int32_t)y;
+            }
+        }
+    }
+}
+
+template <int UPT, bool POP>
+cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st) {
+    auto k = cle_fused_kernel<UPT, POP>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = (unsigned)((a.N + 31) / 32);
+    k<<<blocks, nw * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace scrna

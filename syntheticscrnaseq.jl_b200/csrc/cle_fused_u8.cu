@@ -1,0 +1,7 @@
+// Instantiations of the fused register-path kernel with 8 gene quad(s) per thread.
+#include "cle_fused.cuh"
+
+namespace scrna {
+template cudaError_t fused_launch_t<8, false>(const FusedArgs&, int, size_t, cudaStream_t);
+template cudaError_t fused_launch_t<8, true>(const FusedArgs&, int, size_t, cudaStream_t);
+}  // namespace scrna

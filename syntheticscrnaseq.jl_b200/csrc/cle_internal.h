@@ -1,0 +1,126 @@
+// Internal structures shared by the host side of the library (capi.cu) and the
+// kernels.  Not part of the public ABI.
+#pragma once
+#include <cstdint>
+
+namespace scrna {
+
+// Per-gene record, rebuilt for every run (thresholds depend on dt, initial values on
+// the kinetics).  32 bytes, read by the kernels with two 16-byte loads.
+struct GeneRec {
+    float beta;        // basal rate beta_g
+    float cneg;        // sum_j max(-A_eff[g,j], 0): the repression constant of the one-GEMM form
+    uint32_t thr_on;   // OFF->ON fires when the switch word < thr_on  (1-exp(-k_on dt))
+    uint32_t thr_off;  // ON->OFF fires when the switch word < thr_off (1-exp(-k_off dt)); 0 if no switching
+    int32_t slot;      // regulator slot of this gene (-1 when no edge reads its protein)
+    int32_t in_begin;  // additive in-edges [in_begin, in_end) in the edge table
+    int32_t in_end;
+    int32_t na_range;  // cooperative/redundant edges targeting g: begin << 16 | count
+};
+struct GeneInit {
+    float m0, p0;       // ceil of the steady state (cle.jl:49-53)
+    uint32_t thr_init;  // initial ON when word < thr_init (k_on/(k_on+k_off))
+    int32_t init_rand;  // 1: initial promoter state drawn (both rates finite)
+};
+
+// Cooperative (kind 0) / redundant (kind 1) edge with coefficient s*beta_target and
+// sources na_src[src_begin, src_end) (as regulator slots).
+struct NonAdd {
+    int32_t kind;
+    float coef;
+    int32_t src_begin;
+    int32_t src_end;
+};
+
+// Device-resident network tables (owned by scrna_net).
+struct NetDev {
+    int32_t G = 0;
+    int32_t n_reg = 0;      // regulator slots
+    int32_t n_in = 0;       // additive edges
+    int32_t n_na = 0;       // cooperative + redundant edges
+    int32_t n_na_src = 0;
+    int32_t n_quads = 0;
+    float2* in_edge = nullptr;   // {w, slot bits}, grouped by target gene
+    NonAdd* na = nullptr;
+    int32_t* na_src = nullptr;
+    int32_t* reg_gene = nullptr; // gene of each regulator slot
+    double* in_w64 = nullptr;    // FP64 additive weights (baseline path)
+    double* na_coef64 = nullptr; // FP64 s*beta_target (baseline path)
+    double* beta64 = nullptr;    // FP64 basals (baseline path)
+};
+
+// Arguments of the fused FP32 register-path kernel.
+struct FusedArgs {
+    int32_t G, n_quads, n_reg, n_in, n_na, n_na_src;
+    int64_t N;              // cells of this network
+    int64_t cell_offset;    // global index of cell 0 (Philox counter)
+    int32_t step_begin;     // first step of this launch (1-based)
+    int32_t step_end;       // last step of this launch (inclusive)
+    int32_t first;          // 1: initialise state from GeneInit instead of reading it
+    int32_t last;           // 1: write readout / capture after the last step
+    int32_t check;          // 1: step_end is a division check step
+    int32_t epoch;          // division epoch of this launch's prologue
+    float k_t, Kn, hill_n, mu_m, mu_p, dt;
+    int32_t hill_int;       // >0: integer Hill exponent (repeated products)
+    uint32_t key0, key1, stream;
+    // population
+    double growth_factor, V_div, V_lo, V_hi;
+    int32_t partition, exclude_mother;
+    // tables
+    const GeneRec* genes;
+    const GeneInit* ginit;
+    const float2* in_edge;
+    const NonAdd* na;
+    const int32_t* na_src;
+    const uint8_t* quad_tel;     // per quad: any gene switches
+    // state [G][N]
+    float* M;
+    float* P;
+    uint8_t* prom;
+    double* V;
+    // division scratch (two parities)
+    float* dM[2];
+    float* dP[2];
+    uint8_t* dprom[2];
+    double* dV[2];
+    unsigned long long* owner[2];
+    // outputs
+    double* out;            // readout, cells x G (x2) column-major, nullable
+    int32_t readout;
+    int32_t* counts;        // cells x G, nullable
+    double* eff;            // cells, nullable
+    int32_t capture_species;
+    double cap_mu_log, cap_sigma;
+};
+
+// Launch shape of the fused kernel chosen for a network: quads per thread (UPT),
+// warps per block (NW, so 32 cells x NW warps) and dynamic shared memory.
+struct FusedLaunch {
+    int upt;
+    int nw;
+    size_t smem;
+};
+
+// Arguments of the plain FP64 one-kernel-per-step baseline.
+struct PlainArgs {
+    int32_t G, n_quads;
+    int64_t N, cell_offset;
+    int32_t step;
+    double k_t, Kn, hill_n, mu_m, mu_p, dt, sqrt_dt;
+    uint32_t key0, key1, stream;
+    const GeneRec* genes;
+    const float2* in_edge;   // weights used in double
+    const double* in_w64;    // FP64 weights (A_pos/A_neg split) of the additive edges
+    const NonAdd* na;
+    const double* na_coef64;
+    const int32_t* na_src;
+    const int32_t* reg_gene;
+    const uint8_t* quad_tel;
+    const double* beta64;
+    double* M;
+    const double* Pold;
+    double* Pnew;
+    uint8_t* prom;
+};
+
+}  // namespace scrna
