@@ -49,7 +49,9 @@ def _args():
     ap.add_argument("--cpu-sample-cells", type=int, default=20000)
     ap.add_argument("--cpu-sample-steps", type=int, default=1000)
     ap.add_argument("--ref-sample-steps", type=int, default=250)
-    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return ap.parse_args()
 
 
@@ -247,9 +249,10 @@ def run_ours(args):
         run64.close()
 
     # e2e through the public host API (host arrays in, host arrays out)
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
     h2d = d2h = 0
-    for i in range(1 + e2e_steps):
+    t0 = time.perf_counter()
+    for i in range(1 + e2e_steps if e2e_steps else 0):
         if i == 1:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -260,10 +263,10 @@ def run_ours(args):
     net = wl.net
     h2d = (net.basals.nbytes + net.interactions.nbytes + net.k_on.nbytes + net.k_off.nbytes
            + 16 * (len(net.cooperative) + len(net.redundant)) + 48 * G)
-    e2e_value = units * world * e2e_steps / e2e_s
+    e2e_value = units * world * e2e_steps / e2e_s if e2e_steps else None
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         cpu_rate, cpu_el = cpu_reference(pkg, wl, args.cpu_sample_cells, args.cpu_sample_steps, threads)
         cpu = {"value": cpu_rate, "unit": "cell·gene·steps/s", "cores": threads, "kind": "port",

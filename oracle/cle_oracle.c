@@ -351,10 +351,11 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             for (int64_t c = 0; c < N; ++c) {
                 memcpy(m, m0, sizeof(double) * G);
                 memcpy(p, p0, sizeof(double) * G);
-                init_promoters(&pp, seed, stream, (uint32_t)c, on);
+                const uint32_t gc = (uint32_t)(opt->cell_offset + c);
+                init_promoters(&pp, seed, stream, gc, on);
                 for (int64_t s = 1; s <= n_steps; ++s)
-                    cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, 0.0, m, p,
-                              on, act, rep, reg);
+                    cell_step(net, &pp, &cf, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, act,
+                              rep, reg);
                 for (int g = 0; g < G; ++g) {
                     M[(size_t)g * N + c] = m[g];
                     P[(size_t)g * N + c] = p[g];

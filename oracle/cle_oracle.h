@@ -69,6 +69,7 @@ typedef struct {
     uint64_t seed;
     uint32_t stream;
     int64_t n_steps;          /* <=0: ceil(T/dt) as cle.jl:56; >0: run exactly this many steps */
+    int64_t cell_offset;      /* global index of cell 0 (plain CLE only) */
 } orc_opts;
 
 /* Random-stream tags (bits 31..24 of Philox counter word 3). */

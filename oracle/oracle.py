@@ -51,7 +51,8 @@ class _Pop(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("dt", C.c_double), ("T", C.c_double), ("cell_num", C.c_int64),
-                ("seed", C.c_uint64), ("stream", C.c_uint32), ("n_steps", C.c_int64)]
+                ("seed", C.c_uint64), ("stream", C.c_uint32), ("n_steps", C.c_int64),
+                ("cell_offset", C.c_int64)]
 
 
 def lib():
@@ -121,7 +122,7 @@ def _edges(keep, edges, G):
 
 
 def simulate(net, kin, *, dt, T=50.0, cell_num=1000, seed=0, stream=0, population=None,
-             n_steps=0, nthreads=0):
+             n_steps=0, nthreads=0, cell_offset=0):
     """FP64 oracle run. `net` is a host GeneNetwork (0-based edge indices).
 
     Returns dict with M, P ([G, N] float64), prom ([G, N] uint8) and V ([N]) when
@@ -137,7 +138,7 @@ def simulate(net, kin, *, dt, T=50.0, cell_num=1000, seed=0, stream=0, populatio
              keep.arr(net.k_on, np.float64), keep.arr(net.k_off, np.float64))
     k = _Kin(kin.k_t, kin.K_d, kin.n, kin.mu_m, kin.mu_p, kin.dilution)
     N = int(cell_num)
-    o = _Opts(float(dt), float(T), N, int(seed), int(stream), int(n_steps))
+    o = _Opts(float(dt), float(T), N, int(seed), int(stream), int(n_steps), int(cell_offset))
     M = np.zeros((G, N)); P = np.zeros((G, N)); prom = np.zeros((G, N), dtype=np.uint8)
     V = np.zeros(N)
     pp = None

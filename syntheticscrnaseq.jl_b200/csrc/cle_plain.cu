@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) peak_int_kernel(int iters, uint32_t seed,
 #pragma unroll
         for (int r = 0; r < 16; ++r)
 #pragma unroll
-            for (int k = 0; k < 8; ++k) x[k] = x[k] * 0x9E3779B1u + 0x7F4A7C15u;
+            for (int k = 0; k < 8; ++k) x[k] = x[k] * x[k] + 0x7F4A7C15u;  // not foldable
     }
     uint32_t acc = 0;
 #pragma unroll
