@@ -185,6 +185,29 @@ int scrna_state_device_ptrs(scrna_state* st, void** d_mrna, void** d_protein);
 int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* protein,
                          uint8_t* promoter, double* volume);
 
+/* ---- scratch-free run ---------------------------------------------------------------
+ * This entry point has no counterpart in the reference.  It is for callers that
+ * cannot allocate device memory when they run a simulation (the allocator is owned
+ * by another component, a serving loop must not synchronise on cudaMalloc/cudaFree,
+ * or device memory is budgeted up front).  It runs the fused FP32 kernel of
+ * scrna_cle_run_device, optionally with population and capture, and calls no
+ * cudaMalloc, cudaFree or other allocating routine: all working memory comes from
+ * one array of about 9.3 MB that the library reserves on every GPU it is loaded on,
+ * held until the process exits.  Limits per call: 65,536 cells, 512 genes and
+ * 262,144 cell-genes; larger runs are rejected with SCRNA_EINVAL.
+ *   d_out    device pointer, cells x G (x2 for SCRNA_READOUT_BOTH) float64, column-major
+ *   d_counts device pointer, cells x G int32 (required with cap, else ignored)
+ *   d_eff    device pointer, cells float64 (required with cap, else ignored)
+ * The call only enqueues work on the context stream; synchronise before reading.
+ * The first call on a device looks up the array's device address; make that first
+ * call before any stream capture.  All calls share the one array: calls whose work
+ * overlaps on the GPU (other streams or contexts on the same device) race and
+ * corrupt each other's results. */
+int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                               const scrna_population* pop, const scrna_capture* cap,
+                               const scrna_cle_opts* opts, double* d_out, int32_t* d_counts,
+                               double* d_eff);
+
 /* ---- diagnostics ----------------------------------------------------------------
  * Runs Philox4x32-10 on the device for n counters (host arrays ctr[4n], key[2]) and
  * returns the words in out[4n]; used to check the device generator against the

@@ -72,6 +72,7 @@ SIGNATURES = {
     "scrna_state_read": (C.c_int, [P, P, P, P, P]),
     "scrna_state_device_ptrs": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "scrna_state_read_raw": (C.c_int, [P, P, P, P, P, P]),
+    "scrna_cle_simulate_noalloc": (C.c_int, [P, P, P, P, P, P, P, P, P]),
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),
 }

@@ -790,3 +790,54 @@ extern "C" int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma, double* sfu
     if (iops) *iops = res[2];
     return SCRNA_OK;
 }
+
+// ---- internal views for other translation units of the library ----------------------------------
+namespace scrna {
+
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int check_run_args(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                   const scrna_capture* cap, const scrna_cle_opts* o) {
+    return validate_run(net, kin, pop, cap, o);
+}
+
+int64_t run_steps(const scrna_cle_opts* o) { return n_steps_of(o); }
+
+cudaStream_t ctx_stream(scrna_ctx* ctx) { return ctx->stream; }
+int ctx_device(scrna_ctx* ctx) { return ctx->device; }
+void ctx_add_launches(scrna_ctx* ctx, int n) { ctx->launches += n; }
+const NetDev& net_dev(const scrna_net* n) { return n->dev; }
+
+// Per-run gene tables of `n` written into caller-provided host arrays (G, G and
+// (G+3)/4 entries); same contents as the tables the regular path uploads.
+void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr,
+                      GeneInit* gi, uint8_t* qt) {
+    const int G = n->G;
+    for (int q = 0; q < (G + 3) / 4; ++q) qt[q] = 0;
+    for (int g = 0; g < G; ++g) {
+        GeneRec& r = gr[g];
+        r.beta = (float)n->basals[g];
+        r.cneg = (float)n->cneg64[g];
+        const double kon = n->k_on[g], koff = n->k_off[g];
+        if (std::isfinite(kon)) {
+            r.thr_on = prob_threshold(1.0 - std::exp(-kon * dt));
+            r.thr_off = std::isfinite(koff) ? prob_threshold(1.0 - std::exp(-koff * dt)) : 0xFFFFFFFFu;
+            qt[g >> 2] = 1;
+        } else {
+            r.thr_on = 0u;
+            r.thr_off = 0u;
+        }
+        r.slot = n->reg_slot[g];
+        r.in_begin = n->in_begin[g];
+        r.in_end = n->in_end[g];
+        r.na_range = (n->na_begin[g] << 16) | n->na_count[g];
+        const double mss = n->basals[g] / (kin->mu_m + kin->dilution);
+        const double pss = kin->k_t * mss / (kin->mu_p + kin->dilution);
+        gi[g].m0 = (float)std::ceil(mss);
+        gi[g].p0 = (float)std::ceil(pss);
+        gi[g].init_rand = (std::isfinite(kon) && std::isfinite(koff)) ? 1 : 0;
+        gi[g].thr_init = gi[g].init_rand ? prob_threshold(kon / (kon + koff)) : 0u;
+    }
+}
+
+}  // namespace scrna
