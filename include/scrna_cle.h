@@ -52,9 +52,14 @@ enum scrna_partition { SCRNA_PARTITION_BINOMIAL = 0, SCRNA_PARTITION_HALVE = 1 }
  * plain FP64 one-kernel-per-step path kept as the comparison baseline. */
 enum scrna_precision { SCRNA_PRECISION_FP32 = 0, SCRNA_PRECISION_FP64_PLAIN = 1 };
 
-/* Contraction path for the FP32 precision. AUTO picks the register path for sparse
- * networks and the tensor-core path for large dense ones. */
-enum scrna_path { SCRNA_PATH_AUTO = 0, SCRNA_PATH_REGISTER = 1, SCRNA_PATH_TENSOR = 2 };
+/* Kernel family for the FP32 precision.  AUTO picks the register path for sparse
+ * networks (the warp-per-cell-group kernel when G <= 32 with <= 16 regulator genes,
+ * block tiles otherwise) and the tensor-core path for large dense ones.  BLOCK and
+ * WARP force one register-path kernel (both give identical results). */
+enum scrna_path {
+    SCRNA_PATH_AUTO = 0, SCRNA_PATH_REGISTER = 1, SCRNA_PATH_TENSOR = 2,
+    SCRNA_PATH_BLOCK = 3, SCRNA_PATH_WARP = 4
+};
 
 typedef struct scrna_ctx scrna_ctx;
 typedef struct scrna_net scrna_net;

@@ -22,7 +22,7 @@ from .model import CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConf
 
 READOUT = {"mrna": 0, "protein": 1, "both": 2}
 PRECISION = {"fp32": 0, "fp64_plain": 1}
-PATH = {"auto": 0, "register": 1, "tensor": 2}
+PATH = {"auto": 0, "register": 1, "tensor": 2, "block": 3, "warp": 4}
 
 
 class Context:
@@ -238,7 +238,7 @@ class DeviceRun:
                  readout: str = "protein", seed: int = 0, stream: int = 0,
                  capture: Optional[CaptureModel] = None, population: Optional[PopulationConfig] = None,
                  precision: str = "fp32", n_steps: int = 0, cell_offset: int = 0,
-                 ctx: Optional[Context] = None):
+                 path: str = "auto", ctx: Optional[Context] = None):
         self.ctx = ctx or default_context()
         self.handle = NetHandle(net, self.ctx)
         self.N = population.cell_num if population is not None else cell_num
@@ -247,7 +247,7 @@ class DeviceRun:
         self.capture = capture
         self.k, self.p, self.c = _kin(kin), _pop(population), _cap(capture)
         self.o = _opts(alg, T=T, cell_num=self.N, readout=readout, seed=seed, stream=stream,
-                       precision=precision, path="auto", n_steps=n_steps, cell_offset=cell_offset)
+                       precision=precision, path=path, n_steps=n_steps, cell_offset=cell_offset)
         h = C.c_void_p()
         check(self.ctx.lib.scrna_state_create(self.ctx.h, self.handle.h, self.N, READOUT[readout],
                                               int(capture is not None), C.byref(h)))

@@ -19,6 +19,10 @@ namespace scrna {
 FusedLaunch fused_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int n_quads);
 int fused_max_quads();
 cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st);
+int warpcell_max_genes();
+int warpcell_max_regs();
+int warpcell_pick_gpl(int G, bool bursty);
+cudaError_t warpcell_launch(const FusedArgs& a, const float* wdense, int gpl, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               uint32_t key0, uint32_t key1, uint32_t stream, double* M, double* P,
@@ -96,7 +100,7 @@ struct scrna_net {
     std::vector<double> na_coef64;
     std::vector<int32_t> na_src;
     NetDev dev;
-    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64;
+    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_wdense;
     // per-run tables cached for the last (kinetics, dt, population mode)
     DevBuf b_genes, b_ginit, b_quad_tel;
     bool cache_valid = false;
@@ -330,6 +334,19 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     d.in_w64 = n->b_in_w64.as<double>();
     d.na_coef64 = n->b_na_coef64.as<double>();
     d.beta64 = n->b_beta64.as<double>();
+    for (int g = 0; g < G; ++g) d.bursty = d.bursty || std::isfinite(n->k_on[g]);
+    if (G <= warpcell_max_genes() && d.n_reg <= warpcell_max_regs()) {
+        // dense rows W[g][slot] = A_eff[g, reg_gene[slot]] for the warp-per-cell-group kernel
+        std::vector<float> wd((size_t)G * std::max(d.n_reg, 1), 0.0f);
+        for (int g = 0; g < G; ++g)
+            for (int e = n->in_begin[g]; e < n->in_end[g]; ++e) {
+                int32_t slot;
+                std::memcpy(&slot, &n->in_edge[e].y, 4);
+                wd[(size_t)g * d.n_reg + slot] = n->in_edge[e].x;
+            }
+        CU(up(n->b_wdense, wd.data(), wd.size() * sizeof(float)));
+        d.wdense = n->b_wdense.as<float>();
+    }
     *out = n.release();
     return SCRNA_OK;
 }
@@ -535,9 +552,17 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     const FusedLaunch L = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
     if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
     cudaStream_t s = ctx->stream;
+    // kernel choice: warp-per-cell-group for small networks, block tiles otherwise
+    const bool warp_ok = d.wdense != nullptr;
+    const bool use_warp = o->path == SCRNA_PATH_WARP ? true : o->path == SCRNA_PATH_BLOCK ? false : warp_ok;
+    if (use_warp && !warp_ok) return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d and <= %d regulators", warpcell_max_genes(), warpcell_max_regs());
+    const int gpl = warpcell_pick_gpl(d.G, d.bursty);
+    auto launch = [&](bool is_pop) -> cudaError_t {
+        return use_warp ? warpcell_launch(a, d.wdense, gpl, is_pop, s) : fused_launch(a, L, is_pop, s);
+    };
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;
-        CU(fused_launch(a, L, false, s));
+        CU(launch(false));
         ctx->launches++;
         return SCRNA_OK;
     }
@@ -556,7 +581,7 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         a.epoch = epoch;
         a.check = check ? 1 : 0;
         a.last = (final_chunk && !check) ? 1 : 0;
-        CU(fused_launch(a, L, true, s));
+        CU(launch(true));
         ctx->launches++;
         first = false;
         if (check) epoch += 1;
@@ -564,7 +589,7 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
             if (check) {  // apply the last division's placements, then read out
                 a.step_begin = (int)s1 + 1; a.step_end = (int)s1;
                 a.first = 0; a.epoch = epoch; a.check = 0; a.last = 1;
-                CU(fused_launch(a, L, true, s));
+                CU(launch(true));
                 ctx->launches++;
             }
             break;

@@ -159,4 +159,41 @@ __device__ __forceinline__ float fsqrt_approx(float x) {
     return r;
 }
 
+__device__ __forceinline__ float frcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float hill_act(float p, float Kn, float hill_n, int hill_int) {
+    float pn;
+    if (hill_int == 2) {
+        pn = p * p;
+    } else if (hill_int > 0) {
+        pn = 1.0f;
+        for (int i = 0; i < hill_int; ++i) pn *= p;
+    } else {
+        pn = exp2f(hill_n * __log2f(p));
+    }
+    // pn / (pn + Kn); an infinite pn gives NaN in the product and fminf returns 1.
+    return fminf(pn * frcp_approx(pn + Kn), 1.0f);
+}
+
+// One Euler-Maruyama step of (m, p) with collapsed noise (cle.jl:109-120): M first, then P
+// with the new M.  z sqrt(dt var) is evaluated as cos(theta) sqrt(L dt var), folding the
+// Box-Muller radius sqrt(L) into the variance square root.  m, p >= 0 on entry.
+__device__ __forceinline__ void em_update(float& m, float& p, float tx, const BM& bm, float mu_m,
+                                          float mu_p, float k_t, float dt) {
+    const float Ldt = bm.L * dt;
+    const float mo = m, po = p;
+    const float var_m = fmaxf(fmaf(mu_m, mo, tx), 0.0f);
+    float mn = fmaf(bm.c, fsqrt_approx(Ldt * var_m), fmaf(fmaf(-mu_m, mo, tx), dt, mo));
+    mn = fmaxf(mn, 0.0f);
+    const float var_p = fmaf(k_t, mn, mu_p * po);
+    float pn = fmaf(bm.s, fsqrt_approx(Ldt * var_p), fmaf(fmaf(k_t, mn, -mu_p * po), dt, po));
+    pn = fmaxf(pn, 0.0f);
+    m = mn;
+    p = pn;
+}
+
 }  // namespace scrna

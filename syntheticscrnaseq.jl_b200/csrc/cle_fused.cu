@@ -45,4 +45,47 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
     }
 }
 
+// ---- warp-per-cell-group variant for small networks ---------------------------------------
+template <int GPL, int NREG, bool POP>
+cudaError_t warpcell_launch_t(const FusedArgs& a, const float* wdense, cudaStream_t st);
+
+int warpcell_max_genes() { return 32; }
+int warpcell_max_regs() { return 16; }
+
+// Genes per lane for a network: a cost model of issue slots per cell-gene-step
+// (Philox calls per gene, plus lanes left idle by the cell packing).
+int warpcell_pick_gpl(int G, bool bursty) {
+    double best = 1e30;
+    int pick = 2;
+    for (int gpl : {2, 4}) {
+        const int lpc = (G + gpl - 1) / gpl;
+        const int cpw = 32 / lpc;
+        const double philox = 0.5 + (bursty ? (gpl == 2 ? 0.5 : 0.25) : 0.0);
+        const double waste = 32.0 * gpl / ((double)G * cpw);
+        const double cost = (48.0 + 42.0 * philox) * waste;
+        if (cost < best) { best = cost; pick = gpl; }
+    }
+    return pick;
+}
+
+cudaError_t warpcell_launch(const FusedArgs& a, const float* wdense, int gpl, bool pop, cudaStream_t st) {
+    const int nreg = a.n_reg <= 4 ? 4 : a.n_reg <= 8 ? 8 : 16;
+    const int key = (gpl == 4 ? 100 : 0) + nreg * 2 + (pop ? 1 : 0);
+    switch (key) {
+        case 8: return warpcell_launch_t<2, 4, false>(a, wdense, st);
+        case 9: return warpcell_launch_t<2, 4, true>(a, wdense, st);
+        case 16: return warpcell_launch_t<2, 8, false>(a, wdense, st);
+        case 17: return warpcell_launch_t<2, 8, true>(a, wdense, st);
+        case 32: return warpcell_launch_t<2, 16, false>(a, wdense, st);
+        case 33: return warpcell_launch_t<2, 16, true>(a, wdense, st);
+        case 108: return warpcell_launch_t<4, 4, false>(a, wdense, st);
+        case 109: return warpcell_launch_t<4, 4, true>(a, wdense, st);
+        case 116: return warpcell_launch_t<4, 8, false>(a, wdense, st);
+        case 117: return warpcell_launch_t<4, 8, true>(a, wdense, st);
+        case 132: return warpcell_launch_t<4, 16, false>(a, wdense, st);
+        case 133: return warpcell_launch_t<4, 16, true>(a, wdense, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace scrna

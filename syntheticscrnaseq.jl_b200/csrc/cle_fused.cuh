@@ -20,26 +20,6 @@
 
 namespace scrna {
 
-__device__ __forceinline__ float frcp_approx(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-__device__ __forceinline__ float hill_act(float p, float Kn, float hill_n, int hill_int) {
-    float pn;
-    if (hill_int == 2) {
-        pn = p * p;
-    } else if (hill_int > 0) {
-        pn = 1.0f;
-        for (int i = 0; i < hill_int; ++i) pn *= p;
-    } else {
-        pn = exp2f(hill_n * __log2f(p));
-    }
-    // pn / (pn + Kn); an infinite pn gives NaN in the product and fminf returns 1.
-    return fminf(pn * frcp_approx(pn + Kn), 1.0f);
-}
-
 // Shared-memory layout of one block: regulator activations (2 x n_reg x 32 floats),
 // then the gene table, the edge tables and the per-quad switching flags.
 struct Smem {
@@ -245,17 +225,7 @@ cle_fused_kernel(const FusedArgs a) {
                     float tx = reg + gr.beta;
                     if (POP) tx *= Vf;
                     if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
-                    // Euler-Maruyama with collapsed noise; z*sqrt(dt*var) = cos(th)*sqrt(L*dt*var).
-                    const float Ldt = bm.L * dt;
-                    const float mo = m[j][i], po = p[j][i];
-                    const float var_m = fmaxf(fmaf(mu_m, mo, tx), 0.0f);
-                    float mn = fmaf(fmaf(-mu_m, mo, tx), dt, mo) + bm.c * fsqrt_approx(Ldt * var_m);
-                    mn = fmaxf(mn, 0.0f);
-                    const float var_p = fmaf(k_t, mn, mu_p * po);
-                    float pn = fmaf(fmaf(k_t, mn, -mu_p * po), dt, po) + bm.s * fsqrt_approx(Ldt * var_p);
-                    pn = fmaxf(pn, 0.0f);
-                    m[j][i] = mn;
-                    p[j][i] = pn;
+                    em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
                 }
             }
         }

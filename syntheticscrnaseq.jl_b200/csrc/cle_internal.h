@@ -47,6 +47,8 @@ struct NetDev {
     double* in_w64 = nullptr;    // FP64 additive weights (baseline path)
     double* na_coef64 = nullptr; // FP64 s*beta_target (baseline path)
     double* beta64 = nullptr;    // FP64 basals (baseline path)
+    float* wdense = nullptr;     // [G][n_reg] dense regulation rows (small networks), or null
+    bool bursty = false;         // any gene switches (finite k_on)
 };
 
 // Arguments of the fused FP32 register-path kernel.

@@ -1,0 +1,298 @@
+// Warp-per-cell-group register-path CLE kernel for small networks (sm_100a).
+//
+// For G <= 32 genes with at most 16 regulator genes, a whole cell lives inside one
+// warp: lane = (cell, unit) where a unit is GPL consecutive genes (a gene pair or a
+// gene quad).  All lanes of a warp run the same instruction stream; what differs per
+// lane (basal rate, telegraph thresholds, the dense row of regulation weights over the
+// regulator slots) sits in registers, loaded once.  Per Euler step:
+//   telegraph switch -> Hill of the lane's regulator genes into a per-warp shared slot
+//   table -> Philox + Box-Muller for the lane's genes -> __syncwarp -> read the cell's
+//   regulator activations -> reg = cneg + W_row . act (+ cooperative / redundant terms)
+//   -> M, P update.
+// There is no block-wide barrier: warps are independent.  The arithmetic and the
+// Philox streams are those of cle_fused_kernel (same sums in the same order: the
+// dense row adds exact zeros for absent edges), so both kernels give identical results.
+#pragma once
+#include "cle_device.cuh"
+#include "cle_internal.h"
+
+namespace scrna {
+
+constexpr int kWarpcellWarps = 4;  // warps per block
+
+__host__ __device__ inline int warpcell_lanes_per_cell(int G, int gpl) { return (G + gpl - 1) / gpl; }
+__host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 32 / warpcell_lanes_per_cell(G, gpl); }
+
+template <int NREG>
+__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_na, int n_na_src) {
+    const int cpw = warpcell_cells_per_warp(G, gpl);
+    size_t b = (size_t)kWarpcellWarps * 2 * (cpw + 1) * (NREG + 1) * sizeof(float);
+    b += (size_t)n_na * sizeof(NonAdd) + (size_t)n_na_src * sizeof(int32_t);
+    return (b + 15) & ~(size_t)15;
+}
+
+// Word of gene u*GPL+i in the quad's Philox block (word index (u*GPL+i) mod 4), selected
+// without indexing a register array by a runtime value.
+template <int GPL>
+__device__ __forceinline__ uint32_t quad_word(const uint4& w, int u, int i) {
+    if (GPL == 4) return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
+    const bool hi = u & 1;
+    return i == 0 ? (hi ? w.z : w.x) : (hi ? w.w : w.y);
+}
+
+template <int GPL, int NREG, bool POP>
+__global__ void __launch_bounds__(32 * kWarpcellWarps)
+cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int G = a.G;
+    const int lpc = warpcell_lanes_per_cell(G, GPL);
+    const int cpw = 32 / lpc;
+    const int ld = NREG + 1;
+    float* act_all = reinterpret_cast<float*>(smem_raw);
+    NonAdd* sna = reinterpret_cast<NonAdd*>(act_all + (size_t)kWarpcellWarps * 2 * (cpw + 1) * ld);
+    int32_t* sna_src = reinterpret_cast<int32_t*>(sna + a.n_na);
+    for (int i = threadIdx.x; i < a.n_na; i += blockDim.x) sna[i] = a.na[i];
+    for (int i = threadIdx.x; i < a.n_na_src; i += blockDim.x) sna_src[i] = a.na_src[i];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    int cl = lane / lpc;
+    const int u = lane - cl * lpc;
+    const bool lane_ok = cl < cpw;
+    if (!lane_ok) cl = cpw;  // spare lanes work on a private dummy row
+    const int64_t N = a.N;
+    const int64_t cell = ((int64_t)blockIdx.x * kWarpcellWarps + warp) * cpw + (lane_ok ? cl : 0);
+    const bool live = lane_ok && cell < N;
+    const int64_t cidx = cell < N ? cell : N - 1;
+    const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
+    const Key key{a.key0, a.key1};
+    const int n_reg = a.n_reg;
+    float* act_w = act_all + (size_t)warp * 2 * (cpw + 1) * ld;
+
+    // per-lane gene constants
+    float beta[GPL], cneg[GPL], W[GPL][NREG];
+    uint32_t thr_on[GPL], thr_off[GPL];
+    int slot[GPL], na_range[GPL];
+    bool valid[GPL];
+#pragma unroll
+    for (int i = 0; i < GPL; ++i) {
+        const int g = u * GPL + i;
+        valid[i] = g < G;
+        const int gg = valid[i] ? g : 0;
+        const GeneRec gr = a.genes[gg];
+        beta[i] = gr.beta;
+        cneg[i] = gr.cneg;
+        thr_on[i] = gr.thr_on;
+        thr_off[i] = valid[i] ? gr.thr_off : 0u;
+        slot[i] = valid[i] ? gr.slot : -1;
+        na_range[i] = valid[i] ? gr.na_range : 0;
+#pragma unroll
+        for (int r = 0; r < NREG; ++r) W[i][r] = (valid[i] && r < n_reg) ? wdense[(size_t)gg * n_reg + r] : 0.0f;
+    }
+    const int quad = GPL == 4 ? u : (u >> 1);
+    const bool tel = quad * 4 < G && a.quad_tel[quad];
+
+    float m[GPL], p[GPL];
+    uint32_t on = 0xFFFFFFFFu;  // bit i: promoter of gene u*GPL+i is ON
+    double V = 0.0;
+
+    // ---- prologue (as cle_fused_kernel) ----------------------------------------------
+    if (a.first) {
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) {
+            const int g = u * GPL + i;
+            m[i] = valid[i] ? a.ginit[g].m0 : 0.0f;
+            p[i] = valid[i] ? a.ginit[g].p0 : 0.0f;
+        }
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) any |= valid[i] && a.ginit[u * GPL + i].init_rand;
+        if (any) {
+            const uint4 w = philox(gcell, 0u, (uint32_t)quad, tagword(TAG_PROMOTER, a.stream), key);
+#pragma unroll
+            for (int i = 0; i < GPL; ++i) {
+                const int g = u * GPL + i;
+                if (valid[i] && a.ginit[g].init_rand && !(quad_word<GPL>(w, u, i) < a.ginit[g].thr_init))
+                    on &= ~(1u << i);
+            }
+        }
+        if (POP) {
+            const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
+            V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
+        }
+    } else {
+        int64_t src = cidx;
+        bool from_daughter = false;
+        const int par = a.epoch & 1;
+        if (POP && a.epoch > 0) {
+            const unsigned long long o = a.owner[par][cidx];
+            if ((uint32_t)(o >> 32) == (uint32_t)a.epoch) {
+                src = (int64_t)(o & 0xFFFFFFFFull);
+                from_daughter = true;
+            }
+        }
+        const float* Ms = from_daughter ? a.dM[par] : a.M;
+        const float* Ps = from_daughter ? a.dP[par] : a.P;
+        const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) {
+            const int g = u * GPL + i;
+            m[i] = valid[i] ? Ms[(size_t)g * N + src] : 0.0f;
+            p[i] = valid[i] ? Ps[(size_t)g * N + src] : 0.0f;
+            if (valid[i] && !Os[(size_t)g * N + src]) on &= ~(1u << i);
+        }
+        if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
+    }
+
+    // ---- fused step loop --------------------------------------------------------------
+    const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
+    int buf = 0;
+    for (int s = a.step_begin; s <= a.step_end; ++s) {
+        if (tel) {
+            const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)quad, tagword(TAG_SWITCH, a.stream), key);
+#pragma unroll
+            for (int i = 0; i < GPL; ++i) {
+                const uint32_t x = quad_word<GPL>(w, u, i);
+                const uint32_t bit = 1u << i;
+                const uint32_t thr = (on & bit) ? thr_off[i] : thr_on[i];
+                if (x < thr) on ^= bit;
+            }
+        }
+        float* act = act_w + (size_t)buf * (cpw + 1) * ld + (size_t)cl * ld;
+        if (n_reg > 0) {
+#pragma unroll
+            for (int i = 0; i < GPL; ++i)
+                if (slot[i] >= 0) act[slot[i]] = hill_act(p[i], a.Kn, a.hill_n, a.hill_int);
+        }
+        BM bm[GPL];
+#pragma unroll
+        for (int h = 0; h < GPL / 2; ++h) {
+            const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(u * (GPL / 2) + h),
+                                   tagword(TAG_NORMAL, a.stream), key);
+            bm[2 * h] = box_muller_parts(w.x, w.y);
+            bm[2 * h + 1] = box_muller_parts(w.z, w.w);
+        }
+        __syncwarp();
+        float areg[NREG];
+#pragma unroll
+        for (int r = 0; r < NREG; ++r) areg[r] = r < n_reg ? act[r] : 0.0f;
+        const float Vf = POP ? (float)V : 1.0f;
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) {
+            float reg = cneg[i];
+#pragma unroll
+            for (int r = 0; r < NREG; ++r) reg = fmaf(W[i][r], areg[r], reg);
+            const int nab = na_range[i] >> 16, nac = na_range[i] & 0xFFFF;
+            for (int e = nab; e < nab + nac; ++e) {
+                const NonAdd na = sna[e];
+                float prod = 1.0f;
+                if (na.kind == 0) {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[sna_src[t]];
+                    reg = fmaf(na.coef, prod, reg);
+                } else {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[sna_src[t]];
+                    reg = fmaf(na.coef, 1.0f - prod, reg);
+                }
+            }
+            float tx = reg + beta[i];
+            if (POP) tx *= Vf;
+            if (!(on & (1u << i))) tx = 0.0f;
+            em_update(m[i], p[i], tx, bm[i], mu_m, mu_p, k_t, dt);
+        }
+        if (POP) V = __dmul_rn(V, a.growth_factor);
+        buf ^= 1;
+    }
+
+    // ---- epilogue (as cle_fused_kernel) ------------------------------------------------
+    if (POP && a.check) {
+        const bool divides = V > a.V_div;
+        const int ne = a.epoch + 1;
+        const int par = ne & 1;
+        if (divides) {
+            V = V * 0.5;
+            if (live && u == 0) {
+                const uint4 w = philox(gcell, (uint32_t)a.step_end, 0u, tagword(TAG_MORAN, a.stream), key);
+                int64_t r;
+                if (a.exclude_mother) {
+                    r = (int64_t)(((uint64_t)w.x * (uint64_t)(N - 1)) >> 32);
+                    if (r >= cidx) r += 1;
+                } else {
+                    r = (int64_t)(((uint64_t)w.x * (uint64_t)N) >> 32);
+                }
+                a.dV[par][cidx] = V;
+                atomicMax(&a.owner[par][r], ((unsigned long long)(uint32_t)ne << 32) | (unsigned long long)cidx);
+            }
+#pragma unroll
+            for (int i = 0; i < GPL; ++i) {
+                const int g = u * GPL + i;
+                if (!(live && valid[i])) continue;
+                float mm, dm, pm, dp;
+                if (a.partition == 1) {
+                    mm = dm = m[i] * 0.5f;
+                    pm = dp = p[i] * 0.5f;
+                } else {
+                    const int64_t mi = (int64_t)rintf(m[i]);
+                    const int64_t pi = (int64_t)rintf(p[i]);
+                    const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 0u);
+                    const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 1u);
+                    mm = (float)mk; dm = (float)(mi - mk);
+                    pm = (float)pk; dp = (float)(pi - pk);
+                }
+                m[i] = mm;
+                p[i] = pm;
+                const size_t idx = (size_t)g * N + cidx;
+                a.dM[par][idx] = dm;
+                a.dP[par][idx] = dp;
+                a.dprom[par][idx] = (on >> i) & 1u;
+            }
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int i = 0; i < GPL; ++i) {
+        const int g = u * GPL + i;
+        if (!valid[i]) continue;
+        const size_t idx = (size_t)g * N + cell;
+        a.M[idx] = m[i];
+        a.P[idx] = p[i];
+        a.prom[idx] = (on >> i) & 1u;
+        if (a.last && a.out) {
+            if (a.readout == 0) a.out[idx] = (double)m[i];
+            else if (a.readout == 1) a.out[idx] = (double)p[i];
+            else { a.out[idx] = (double)m[i]; a.out[(size_t)(G + g) * N + cell] = (double)p[i]; }
+        }
+    }
+    if (POP && u == 0) a.V[cell] = V;
+    if (a.last && a.counts) {
+        const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, a.stream), key);
+        const double z = box_muller_z0_f64(w.x, w.y);
+        double pe = exp(a.cap_mu_log + a.cap_sigma * z);
+        pe = fmin(fmax(pe, 0.0), 1.0);
+        if (u == 0 && a.eff) a.eff[cell] = pe;
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) {
+            const int g = u * GPL + i;
+            if (!valid[i]) continue;
+            const double x = rint((double)(a.capture_species == 0 ? m[i] : p[i]));
+            const int64_t n = x > 0.0 ? (int64_t)x : 0;
+            int64_t y = 0;
+            if (n > 0 && pe != 0.0) y = binomial_capture(n, pe, key, a.stream, gcell, (uint32_t)g);
+            a.counts[(size_t)g * N + cell] = (int32_t)y;
+        }
+    }
+}
+
+template <int GPL, int NREG, bool POP>
+cudaError_t warpcell_launch_t(const FusedArgs& a, const float* wdense, cudaStream_t st) {
+    auto k = cle_warpcell_kernel<GPL, NREG, POP>;
+    const size_t smem = warpcell_smem_bytes<NREG>(a.G, GPL, a.n_na, a.n_na_src);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
+    const unsigned blocks = (unsigned)((a.N + cpb - 1) / cpb);
+    k<<<blocks, 32 * kWarpcellWarps, smem, st>>>(a, wdense);
+    return cudaGetLastError();
+}
+
+}  // namespace scrna

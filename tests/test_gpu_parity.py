@@ -227,3 +227,33 @@ def test_gpu_vs_cpu_ensemble(pkg, orc):
     Yc = orc.simulate(net, kin, dt=0.1, T=200.0, cell_num=5000, seed=7)["P"][0]
     assert abs(Yg.mean() - Yc.mean()) / Yc.mean() < 0.05
     assert abs(Yg.var() - Yc.var()) / Yc.var() < 0.15
+
+
+@pytest.mark.parametrize("G,bursty,seed", [(1, False, 1), (2, True, 2), (3, True, 3), (5, False, 4),
+                                           (10, True, 5), (13, True, 6), (17, False, 7), (32, True, 8)])
+def test_warp_and_block_kernels_identical(pkg, G, bursty, seed):
+    """The warp-per-cell-group kernel and the block-tile kernel compute the same sums in
+    the same order on the same increments: their results are bit-identical."""
+    net = pkg.sample_network(G, seed=seed, bursty=bursty)
+    kin = pkg.WORKLOAD_KINETICS
+    N = 257
+    outs = []
+    for path in ("warp", "block"):
+        run = _device_run(pkg, net, kin, N=N, steps=150, seed=seed, path=path)
+        outs.append(run.read_raw())
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+@pytest.mark.parametrize("partition", ["halve", "binomial"])
+def test_warp_and_block_kernels_identical_population(pkg, partition):
+    net = pkg.sample_network(7, seed=9, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    pop = pkg.PopulationConfig(cell_num=300, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                               div_check_interval=10, partition=partition)
+    outs = []
+    for path in ("warp", "block"):
+        run = _device_run(pkg, net, kin, N=300, steps=250, seed=3, population=pop, path=path)
+        outs.append(run.read_raw())
+    for k in ("M", "P", "prom", "V"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
