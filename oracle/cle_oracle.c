@@ -19,6 +19,7 @@
  * xor'ed with the other counter words and the key; key bumped by the Weyl
  * constants between rounds.
  * ------------------------------------------------------------------------- */
+#define ORC_LN2 0.69314718055994530942
 #define PHILOX_M0 0xD2511F53u
 #define PHILOX_M1 0xCD9E8D57u
 #define PHILOX_W0 0x9E3779B9u
@@ -153,14 +154,51 @@ int64_t orc_binomial_half(int64_t n, uint64_t seed, uint32_t stream, uint32_t ce
 }
 
 /* ---------------------------------------------------------------------------
+ * Telegraph waiting times.  log2 by the atanh series (log2 m = (2/ln 2) atanh z,
+ * z = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2)), terms to z^11), every operation an
+ * explicitly rounded FP32 op so the device computes the identical value.
+ * ------------------------------------------------------------------------- */
+static inline float f_of_bits(uint32_t b) { float f; memcpy(&f, &b, 4); return f; }
+static inline uint32_t bits_of_f(float f) { uint32_t b; memcpy(&b, &f, 4); return b; }
+
+float orc_log2f(float u) {
+    uint32_t b = bits_of_f(u);
+    int e = (int)((b >> 23) & 0xFFu) - 127;
+    float m = f_of_bits((b & 0x7FFFFFu) | 0x3F800000u);
+    if (m > 1.41421353816986083984375f) { m = m * 0.5f; e += 1; }
+    float z = (m - 1.0f) / (m + 1.0f);
+    float z2 = z * z;
+    float q = fmaf(z2, 1.0f / 11.0f, 1.0f / 9.0f);
+    q = fmaf(z2, q, 1.0f / 7.0f);
+    q = fmaf(z2, q, 1.0f / 5.0f);
+    q = fmaf(z2, q, 1.0f / 3.0f);
+    q = fmaf(z2, q, 1.0f);
+    return fmaf(z * q, 2.88539008f, (float)e);
+}
+
+/* Geometric number of steps (>= 1) until the next switch for stay probability
+ * 2^(1/inv): 1 + floor(log2(u) * inv), u = ((w>>8)+1) 2^-24 in (0, 1]. */
+int32_t orc_geom_steps(uint32_t w, float inv) {
+    float u = (float)((w >> 8) + 1u) * 5.9604644775390625e-8f;
+    float t = orc_log2f(u) * inv;
+    if (!(t < 1.0e9f)) t = 1.0e9f;
+    return 1 + (int32_t)floorf(t);
+}
+
+static inline int32_t next_switch(int64_t step, uint32_t w, float inv) {
+    int64_t t = step + orc_geom_steps(w, inv);
+    return t > 2147483647 ? 2147483647 : (int32_t)t;
+}
+
+/* ---------------------------------------------------------------------------
  * CLE
  * ------------------------------------------------------------------------- */
 typedef struct {
     int G;
     double* Apos;  /* [G*G] row-major, precompute_hill_matrices (network.jl:206-219) */
     double* Aneg;
-    uint32_t* thr_on;
-    uint32_t* thr_off;
+    float* inv_on;      /* 1 / log2(stay probability OFF) = -ln2 / (k_on dt) */
+    float* inv_off;     /* 1 / log2(stay probability ON)  = -ln2 / (k_off dt) */
     uint32_t* thr_init;
     uint8_t* tel;       /* switching active: isfinite(k_on) (tauleap_binomial.jl:86) */
     uint8_t* init_rand; /* both rates finite: random initial state (tauleap_binomial.jl:69) */
@@ -179,8 +217,8 @@ static void prep_build(const orc_net* net, double dt, prep_t* pp) {
             pp->Apos[(size_t)i * G + j] = a > 0.0 ? a : 0.0;
             pp->Aneg[(size_t)i * G + j] = -a > 0.0 ? -a : 0.0;
         }
-    pp->thr_on = (uint32_t*)calloc(G, 4);
-    pp->thr_off = (uint32_t*)calloc(G, 4);
+    pp->inv_on = (float*)calloc(G, 4);
+    pp->inv_off = (float*)calloc(G, 4);
     pp->thr_init = (uint32_t*)calloc(G, 4);
     pp->tel = (uint8_t*)calloc(G, 1);
     pp->init_rand = (uint8_t*)calloc(G, 1);
@@ -190,14 +228,14 @@ static void prep_build(const orc_net* net, double dt, prep_t* pp) {
         if (isfinite(kon) || isfinite(koff)) pp->bursty = 1;
         pp->tel[g] = isfinite(kon) ? 1 : 0;
         pp->init_rand[g] = (isfinite(kon) && isfinite(koff)) ? 1 : 0;
-        pp->thr_on[g] = prob_threshold(1.0 - exp(-kon * dt));
-        pp->thr_off[g] = isfinite(koff) ? prob_threshold(1.0 - exp(-koff * dt)) : 0xFFFFFFFFu;
+        pp->inv_on[g] = (float)(-ORC_LN2 / (kon * dt));
+        pp->inv_off[g] = (float)(-ORC_LN2 / (koff * dt));
         if (pp->init_rand[g]) pp->thr_init[g] = prob_threshold(kon / (kon + koff));
     }
 }
 
 static void prep_free(prep_t* pp) {
-    free(pp->Apos); free(pp->Aneg); free(pp->thr_on); free(pp->thr_off);
+    free(pp->Apos); free(pp->Aneg); free(pp->inv_on); free(pp->inv_off);
     free(pp->thr_init); free(pp->tel); free(pp->init_rand);
 }
 
@@ -209,22 +247,18 @@ typedef struct {
  * when vol > 0).  m, p, on are this cell's G-vectors; act/rep/reg are scratch. */
 static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, uint64_t seed,
                       uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
-                      double* p, uint8_t* on, double* act, double* rep, double* reg) {
+                      double* p, uint8_t* on, int32_t* ns, double* act, double* rep, double* reg) {
     int G = net->G;
-    /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121) */
+    /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
+     * the per-step Bernoulli(1 - exp(-k dt)) switch is sampled as its geometric waiting
+     * time, redrawn only when the promoter switches. */
     if (pp->bursty) {
-        for (int g0 = 0; g0 < G; g0 += 4) {
-            int any = 0;
-            for (int g = g0; g < G && g < g0 + 4; ++g) any |= pp->tel[g];
-            if (!any) continue;
+        for (int g = 0; g < G; ++g) {
+            if (!pp->tel[g] || (int64_t)step != ns[g]) continue;
+            on[g] ^= 1;
             uint32_t w[4];
-            draw(seed, cell, step, (uint32_t)(g0 >> 2), ORC_TAG_SWITCH, stream, w);
-            for (int g = g0; g < G && g < g0 + 4; ++g) {
-                if (!pp->tel[g]) continue;
-                uint32_t x = w[g - g0];
-                if (on[g]) { if (x < pp->thr_off[g]) on[g] = 0; }
-                else { if (x < pp->thr_on[g]) on[g] = 1; }
-            }
+            draw(seed, cell, step, (uint32_t)g, ORC_TAG_SWITCH, stream, w);
+            ns[g] = next_switch(step, w[0], on[g] ? pp->inv_off[g] : pp->inv_on[g]);
         }
     }
     /* Hill fractions (cle.jl:79-82) */
@@ -285,8 +319,9 @@ static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, ui
     }
 }
 
+/* Initial promoter states (tauleap_binomial.jl:64-76) and first switch times. */
 static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uint32_t cell,
-                           uint8_t* on) {
+                           uint8_t* on, int32_t* ns) {
     int G = pp->G;
     for (int g0 = 0; g0 < G; g0 += 4) {
         uint32_t w[4];
@@ -295,6 +330,13 @@ static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uin
         if (any) draw(seed, cell, 0, (uint32_t)(g0 >> 2), ORC_TAG_PROMOTER, stream, w);
         for (int g = g0; g < G && g < g0 + 4; ++g)
             on[g] = pp->init_rand[g] ? (w[g - g0] < pp->thr_init[g]) : 1;
+    }
+    for (int g = 0; g < G; ++g) {
+        ns[g] = 2147483647;
+        if (!pp->tel[g]) continue;
+        uint32_t w[4];
+        draw(seed, cell, 0, (uint32_t)g, ORC_TAG_SWITCH, stream, w);
+        ns[g] = next_switch(0, w[0], on[g] ? pp->inv_off[g] : pp->inv_on[g]);
     }
 }
 
@@ -347,14 +389,15 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             double* rep = (double*)malloc(sizeof(double) * G);
             double* reg = (double*)malloc(sizeof(double) * G);
             uint8_t* on = (uint8_t*)malloc(G);
+            int32_t* ns = (int32_t*)malloc(sizeof(int32_t) * G);
 #pragma omp for schedule(static)
             for (int64_t c = 0; c < N; ++c) {
                 memcpy(m, m0, sizeof(double) * G);
                 memcpy(p, p0, sizeof(double) * G);
                 const uint32_t gc = (uint32_t)(opt->cell_offset + c);
-                init_promoters(&pp, seed, stream, gc, on);
+                init_promoters(&pp, seed, stream, gc, on, ns);
                 for (int64_t s = 1; s <= n_steps; ++s)
-                    cell_step(net, &pp, &cf, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, act,
+                    cell_step(net, &pp, &cf, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, ns, act,
                               rep, reg);
                 for (int g = 0; g < G; ++g) {
                     M[(size_t)g * N + c] = m[g];
@@ -362,19 +405,20 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                     if (prom) prom[(size_t)g * N + c] = on[g];
                 }
             }
-            free(m); free(p); free(act); free(rep); free(reg); free(on);
+            free(m); free(p); free(act); free(rep); free(reg); free(on); free(ns);
         }
     } else {
         /* population: cells in lockstep, state cell-major [c][g] for the step loop */
         double* Ms = (double*)malloc(sizeof(double) * G * N);
         double* Ps = (double*)malloc(sizeof(double) * G * N);
         uint8_t* On = (uint8_t*)malloc((size_t)G * N);
+        int32_t* Ns = (int32_t*)malloc(sizeof(int32_t) * G * N);
         double* Vs = (double*)malloc(sizeof(double) * N);
         double growth_factor = exp(pop->growth_rate * opt->dt);
         for (int64_t c = 0; c < N; ++c) {
             memcpy(Ms + c * G, m0, sizeof(double) * G);
             memcpy(Ps + c * G, p0, sizeof(double) * G);
-            init_promoters(&pp, seed, stream, (uint32_t)c, On + c * G);
+            init_promoters(&pp, seed, stream, (uint32_t)c, On + c * G, Ns + c * G);
             uint32_t w[4];
             draw(seed, (uint32_t)c, 0, 0, ORC_TAG_VOLUME, stream, w);
             Vs[c] = pop->V_lo + (pop->V_hi - pop->V_lo) * u53(w[0], w[1]); /* cle.jl:158-159 */
@@ -383,6 +427,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
         double* dM = (double*)malloc(sizeof(double) * G * N);
         double* dP = (double*)malloc(sizeof(double) * G * N);
         uint8_t* dOn = (uint8_t*)malloc((size_t)G * N);
+        int32_t* dNs = (int32_t*)malloc(sizeof(int32_t) * G * N);
         double* dV = (double*)malloc(sizeof(double) * N);
         for (int64_t s = 1; s <= n_steps; ++s) {
 #pragma omp parallel
@@ -393,7 +438,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
 #pragma omp for schedule(static)
                 for (int64_t c = 0; c < N; ++c) {
                     cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, Vs[c],
-                              Ms + c * G, Ps + c * G, On + c * G, act, rep, reg);
+                              Ms + c * G, Ps + c * G, On + c * G, Ns + c * G, act, rep, reg);
                     Vs[c] = Vs[c] * growth_factor; /* cle.jl:237 */
                 }
                 free(act); free(rep); free(reg);
@@ -423,6 +468,13 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                         *pq = (double)pmth; dP[k * G + g] = (double)(pi - pmth);
                     }
                     dOn[k * G + g] = On[c * G + g];
+                    /* the daughter's switching is independent of the mother's: fresh waiting time */
+                    dNs[k * G + g] = 2147483647;
+                    if (pp.tel[g]) {
+                        uint32_t w[4];
+                        draw(seed, (uint32_t)c, (uint32_t)s, (uint32_t)g | 0x800000u, ORC_TAG_SWITCH, stream, w);
+                        dNs[k * G + g] = next_switch(s, w[0], dOn[k * G + g] ? pp.inv_off[g] : pp.inv_on[g]);
+                    }
                 }
                 Vs[c] = Vs[c] / 2.0;
                 dV[k] = Vs[c];
@@ -441,6 +493,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                 memcpy(Ms + r * G, dM + k * G, sizeof(double) * G);
                 memcpy(Ps + r * G, dP + k * G, sizeof(double) * G);
                 memcpy(On + r * G, dOn + k * G, (size_t)G);
+                memcpy(Ns + r * G, dNs + k * G, sizeof(int32_t) * G);
                 Vs[r] = dV[k];
             }
         }
@@ -452,7 +505,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             }
             if (V) V[c] = Vs[c];
         }
-        free(Ms); free(Ps); free(On); free(Vs); free(dividers); free(dM); free(dP);
+        free(Ms); free(Ps); free(On); free(Ns); free(dNs); free(Vs); free(dividers); free(dM); free(dP);
         free(dOn); free(dV);
     }
     free(m0); free(p0);

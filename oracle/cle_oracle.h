@@ -104,6 +104,11 @@ void orc_capture_counts(int64_t N, int32_t G, const double* X, const double* eff
 int64_t orc_binomial_invcdf(int64_t n, double p, uint64_t seed, uint32_t stream,
                             uint32_t cell, uint32_t gene);
 
+/* log2 of u in [2^-24, 1] by the explicitly rounded FP32 atanh series, and the
+ * geometric telegraph waiting time 1 + floor(log2(u(w)) * inv) (>= 1 steps). */
+float orc_log2f(float u);
+int32_t orc_geom_steps(uint32_t w, float inv);
+
 /* Binomial(n, 1/2) partition draw (popcount of n Philox bits). */
 int64_t orc_binomial_half(int64_t n, uint64_t seed, uint32_t stream, uint32_t cell,
                           uint32_t step, uint32_t gene, uint32_t species);

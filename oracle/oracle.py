@@ -183,3 +183,17 @@ def binomial_invcdf(n, p, seed, stream, cell, gene):
 def binomial_half(n, seed, stream, cell, step, gene, species):
     return lib().orc_binomial_half(int(n), int(seed), int(stream), int(cell), int(step),
                                    int(gene), int(species))
+
+
+def log2f(u):
+    L = lib()
+    L.orc_log2f.argtypes = [C.c_float]
+    L.orc_log2f.restype = C.c_float
+    return L.orc_log2f(float(u))
+
+
+def geom_steps(w, inv):
+    L = lib()
+    L.orc_geom_steps.argtypes = [C.c_uint32, C.c_float]
+    L.orc_geom_steps.restype = C.c_int32
+    return L.orc_geom_steps(int(w), float(inv))

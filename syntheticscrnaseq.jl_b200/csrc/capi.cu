@@ -25,8 +25,8 @@ int warpcell_pick_gpl(int G, bool bursty);
 cudaError_t warpcell_launch(const FusedArgs& a, const float* wdense, int gpl, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
-                              uint32_t key0, uint32_t key1, uint32_t stream, double* M, double* P,
-                              uint8_t* prom, cudaStream_t st);
+                              const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
+                              double* M, double* P, uint8_t* prom, int32_t* NS, cudaStream_t st);
 cudaError_t plain_readout_launch(int G, int64_t N, const double* M, const double* P, int readout,
                                  double* out, cudaStream_t st);
 cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* X, double mu_log,
@@ -114,8 +114,8 @@ struct scrna_state {
     int64_t N = 0;
     int32_t readout = 1;
     bool capture = false;
-    DevBuf M, P, prom, V, out, counts, eff;
-    DevBuf dM[2], dP[2], dprom[2], dV[2], owner[2];
+    DevBuf M, P, prom, NS, V, out, counts, eff;
+    DevBuf dM[2], dP[2], dprom[2], dNS[2], dV[2], owner[2];
     DevBuf M64, P64a, P64b;  // FP64 baseline state
     bool have_counts = false;
     bool last_plain = false;
@@ -124,6 +124,8 @@ struct scrna_state {
 };
 
 // ---- helpers ----------------------------------------------------------------------------------
+static constexpr double kLn2 = 0.69314718055994530942;
+
 static uint32_t prob_threshold(double p) {
     if (!(p > 0.0)) return 0u;
     double t = std::floor(p * 4294967296.0);
@@ -378,12 +380,12 @@ static int ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt
         const double kon = n->k_on[g], koff = n->k_off[g];
         const bool tel = std::isfinite(kon);
         if (tel) {
-            r.thr_on = prob_threshold(1.0 - std::exp(-kon * dt));
-            r.thr_off = std::isfinite(koff) ? prob_threshold(1.0 - std::exp(-koff * dt)) : 0xFFFFFFFFu;
+            // waiting-time parameters -ln2/(k dt): k = inf -> -0 (switch at once), k = 0 -> -inf (never)
+            r.inv_on = (float)(-kLn2 / (kon * dt));
+            r.inv_off = (float)(-kLn2 / (koff * dt));
             qt[g >> 2] = 1;
         } else {
-            r.thr_on = 0u;
-            r.thr_off = 0u;
+            r.inv_on = r.inv_off = std::nanf("");  // never switches
         }
         r.slot = n->reg_slot[g];
         r.in_begin = n->in_begin[g];
@@ -419,6 +421,7 @@ static int state_alloc(scrna_state* st, bool pop, bool plain) {
     CU(st->M.ensure(gn * 4));
     CU(st->P.ensure(gn * 4));
     CU(st->prom.ensure(gn));
+    CU(st->NS.ensure(gn * 4));
     CU(st->out.ensure(gn * outcols * 8));
     if (st->capture) {
         CU(st->counts.ensure(gn * 4));
@@ -430,6 +433,7 @@ static int state_alloc(scrna_state* st, bool pop, bool plain) {
             CU(st->dM[k].ensure(gn * 4));
             CU(st->dP[k].ensure(gn * 4));
             CU(st->dprom[k].ensure(gn));
+            CU(st->dNS[k].ensure(gn * 4));
             CU(st->dV[k].ensure((size_t)st->N * 8));
             CU(st->owner[k].ensure((size_t)st->N * 8));
         }
@@ -532,11 +536,13 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     a.in_edge = d.in_edge; a.na = d.na; a.na_src = d.na_src;
     a.quad_tel = net->b_quad_tel.as<uint8_t>();
     a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>();
+    a.NS = st->NS.as<int32_t>();
     if (pop) {
         a.V = st->V.as<double>();
         for (int k = 0; k < 2; ++k) {
             a.dM[k] = st->dM[k].as<float>(); a.dP[k] = st->dP[k].as<float>();
             a.dprom[k] = st->dprom[k].as<uint8_t>(); a.dV[k] = st->dV[k].as<double>();
+            a.dNS[k] = st->dNS[k].as<int32_t>();
             a.owner[k] = st->owner[k].as<unsigned long long>();
         }
     }
@@ -608,8 +614,8 @@ static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     double* M = st->M64.as<double>();
     double* Pa = st->P64a.as<double>();
     double* Pb = st->P64b.as<double>();
-    CU(plain_init_launch(d.G, st->N, o->cell_offset, net->b_ginit.as<GeneInit>(), k0, k1, sid, M, Pa,
-                         st->prom.as<uint8_t>(), s));
+    CU(plain_init_launch(d.G, st->N, o->cell_offset, net->b_ginit.as<GeneInit>(), net->b_genes.as<GeneRec>(),
+                         k0, k1, sid, M, Pa, st->prom.as<uint8_t>(), st->NS.as<int32_t>(), s));
     ctx->launches++;
     PlainArgs a{};
     a.G = d.G; a.n_quads = d.n_quads; a.N = st->N; a.cell_offset = o->cell_offset;
@@ -621,7 +627,7 @@ static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     a.in_edge = d.in_edge; a.in_w64 = d.in_w64; a.na = d.na; a.na_coef64 = d.na_coef64;
     a.na_src = d.na_src; a.reg_gene = d.reg_gene; a.quad_tel = net->b_quad_tel.as<uint8_t>();
     a.beta64 = d.beta64;
-    a.M = M; a.prom = st->prom.as<uint8_t>();
+    a.M = M; a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int32_t>();
     for (int64_t step = 1; step <= n_steps; ++step) {
         a.step = (int)step;
         a.Pold = (step & 1) ? Pa : Pb;
@@ -845,12 +851,11 @@ void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, 
         r.cneg = (float)n->cneg64[g];
         const double kon = n->k_on[g], koff = n->k_off[g];
         if (std::isfinite(kon)) {
-            r.thr_on = prob_threshold(1.0 - std::exp(-kon * dt));
-            r.thr_off = std::isfinite(koff) ? prob_threshold(1.0 - std::exp(-koff * dt)) : 0xFFFFFFFFu;
+            r.inv_on = (float)(-kLn2 / (kon * dt));
+            r.inv_off = (float)(-kLn2 / (koff * dt));
             qt[g >> 2] = 1;
         } else {
-            r.thr_on = 0u;
-            r.thr_off = 0u;
+            r.inv_on = r.inv_off = std::nanf("");
         }
         r.slot = n->reg_slot[g];
         r.in_begin = n->in_begin[g];

@@ -159,6 +159,44 @@ __device__ __forceinline__ float fsqrt_approx(float x) {
     return r;
 }
 
+// ---- telegraph waiting times ----------------------------------------------------------------
+// The reference switches a promoter with probability 1 - exp(-k dt) at every step; the
+// number of steps to the next switch is then geometric with stay probability
+// exp(-k dt) = 2^(1/inv), inv = -ln2 / (k dt).  It is drawn once per switch as
+// 1 + floor(log2(u) inv), u = ((w>>8)+1) 2^-24.  log2 is this library's own: the atanh
+// series log2 m = (2/ln 2) atanh z, z = (m-1)/(m+1), m in [sqrt(1/2), sqrt(2)), terms to
+// z^11, with every operation explicitly rounded so the CPU oracle reproduces it bit for bit.
+__device__ __forceinline__ float own_log2f(float u) {
+    const uint32_t b = __float_as_uint(u);
+    int e = (int)((b >> 23) & 0xFFu) - 127;
+    float m = __uint_as_float((b & 0x7FFFFFu) | 0x3F800000u);
+    if (m > 1.41421353816986083984375f) { m = __fmul_rn(m, 0.5f); e += 1; }
+    const float z = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float z2 = __fmul_rn(z, z);
+    float q = __fmaf_rn(z2, 1.0f / 11.0f, 1.0f / 9.0f);
+    q = __fmaf_rn(z2, q, 1.0f / 7.0f);
+    q = __fmaf_rn(z2, q, 1.0f / 5.0f);
+    q = __fmaf_rn(z2, q, 1.0f / 3.0f);
+    q = __fmaf_rn(z2, q, 1.0f);
+    return __fmaf_rn(__fmul_rn(z, q), 2.88539008f, (float)e);
+}
+
+__device__ __forceinline__ int32_t geom_steps(uint32_t w, float inv) {
+    const float u = __fmul_rn(__uint2float_rn((w >> 8) + 1u), 5.9604644775390625e-8f);
+    float t = __fmul_rn(own_log2f(u), inv);
+    if (!(t < 1.0e9f)) t = 1.0e9f;
+    return 1 + (int32_t)floorf(t);
+}
+
+// Step of the next switch after `step` (saturating), for stay-probability parameter inv.
+__device__ __forceinline__ int32_t next_switch(int64_t step, uint32_t w, float inv) {
+    const int64_t t = step + geom_steps(w, inv);
+    return t > 2147483647 ? 2147483647 : (int32_t)t;
+}
+
+constexpr int32_t kNever = 2147483647;
+constexpr uint32_t kDaughterSwitch = 0x800000u;  // counter flag: a daughter's fresh waiting time
+
 __device__ __forceinline__ float frcp_approx(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));

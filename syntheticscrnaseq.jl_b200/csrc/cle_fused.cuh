@@ -78,6 +78,7 @@ cle_fused_kernel(const FusedArgs a) {
     const bool has_reg = a.n_reg > 0;
 
     float m[UPT][4], p[UPT][4];
+    int32_t ns[UPT][4];         // step of the next promoter switch of each gene
     uint32_t on = 0xFFFFFFFFu;  // bit 4j+i: promoter of gene 4q_j+i is ON
     double V = 0.0;
 
@@ -110,6 +111,18 @@ cle_fused_kernel(const FusedArgs a) {
                     }
                 }
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {  // first waiting times (NaN parameter: gene never switches)
+                const int g = 4 * q + i;
+                ns[j][i] = kNever;
+                if (q < a.n_quads && g < G) {
+                    const GeneRec gr = sm.genes[g];
+                    if (gr.inv_off == gr.inv_off) {
+                        const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+                        ns[j][i] = next_switch(0, w.x, (on >> (4 * j + i)) & 1u ? gr.inv_off : gr.inv_on);
+                    }
+                }
+            }
         }
         if (POP) {
             const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
@@ -130,6 +143,7 @@ cle_fused_kernel(const FusedArgs a) {
         const float* Ms = from_daughter ? a.dM[par] : a.M;
         const float* Ps = from_daughter ? a.dP[par] : a.P;
         const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
+        const int32_t* Ns = from_daughter ? a.dNS[par] : a.NS;
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
@@ -139,6 +153,7 @@ cle_fused_kernel(const FusedArgs a) {
                 const bool ok = q < a.n_quads && g < G;
                 m[j][i] = ok ? Ms[(size_t)g * N + src] : 0.0f;
                 p[j][i] = ok ? Ps[(size_t)g * N + src] : 0.0f;
+                ns[j][i] = ok ? Ns[(size_t)g * N + src] : kNever;
                 if (ok && !Os[(size_t)g * N + src]) on &= ~(1u << (4 * j + i));
             }
         }
@@ -149,22 +164,19 @@ cle_fused_kernel(const FusedArgs a) {
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     int buf = 0;
     for (int s = a.step_begin; s <= a.step_end; ++s) {
-        // telegraph switching before the transcription update (tauleap_binomial.jl:111-121)
+        // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
+        // a gene switches when its waiting time runs out, then draws the next one
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
-            if (q < a.n_quads && sm.quad_tel[q]) {
-                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)q, tagword(TAG_SWITCH, a.stream), key);
-                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < 4; ++i) {
+                if (s == ns[j][i]) {
                     const int g = 4 * q + i;
-                    if (g < G) {
-                        const uint32_t bit = 1u << (4 * j + i);
-                        const bool is_on = on & bit;
-                        const uint32_t thr = is_on ? sm.genes[g].thr_off : sm.genes[g].thr_on;
-                        if (ws[i] < thr) on ^= bit;
-                    }
+                    const uint32_t bit = 1u << (4 * j + i);
+                    on ^= bit;
+                    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+                    ns[j][i] = next_switch(s, w.x, (on & bit) ? sm.genes[g].inv_off : sm.genes[g].inv_on);
                 }
             }
         }
@@ -279,7 +291,17 @@ cle_fused_kernel(const FusedArgs a) {
                     const size_t idx = (size_t)g * N + cidx;
                     a.dM[par][idx] = dm;
                     a.dP[par][idx] = dp;
-                    a.dprom[par][idx] = (on >> (4 * j + i)) & 1u;
+                    const uint32_t bon = (on >> (4 * j + i)) & 1u;
+                    a.dprom[par][idx] = bon;
+                    // the daughter's promoter switches independently of the mother's
+                    int32_t dns = kNever;
+                    const GeneRec gr = sm.genes[g];
+                    if (gr.inv_off == gr.inv_off) {
+                        const uint4 w = philox(gcell, (uint32_t)a.step_end, (uint32_t)g | kDaughterSwitch,
+                                               tagword(TAG_SWITCH, a.stream), key);
+                        dns = next_switch(a.step_end, w.x, bon ? gr.inv_off : gr.inv_on);
+                    }
+                    a.dNS[par][idx] = dns;
                 }
             }
         }
@@ -298,6 +320,7 @@ cle_fused_kernel(const FusedArgs a) {
                 a.M[idx] = m[j][i];
                 a.P[idx] = p[j][i];
                 a.prom[idx] = (on >> (4 * j + i)) & 1u;
+                a.NS[idx] = ns[j][i];
             }
             if (a.last && a.out) {
                 if (a.readout == 0) a.out[idx] = (double)m[j][i];

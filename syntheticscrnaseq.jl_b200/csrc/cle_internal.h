@@ -10,8 +10,8 @@ namespace scrna {
 struct GeneRec {
     float beta;        // basal rate beta_g
     float cneg;        // sum_j max(-A_eff[g,j], 0): the repression constant of the one-GEMM form
-    uint32_t thr_on;   // OFF->ON fires when the switch word < thr_on  (1-exp(-k_on dt))
-    uint32_t thr_off;  // ON->OFF fires when the switch word < thr_off (1-exp(-k_off dt)); 0 if no switching
+    float inv_on;      // -ln2 / (k_on dt): waiting-time parameter while OFF (-0: switch next step)
+    float inv_off;     // -ln2 / (k_off dt): waiting-time parameter while ON (-inf: never)
     int32_t slot;      // regulator slot of this gene (-1 when no edge reads its protein)
     int32_t in_begin;  // additive in-edges [in_begin, in_end) in the edge table
     int32_t in_end;
@@ -74,16 +74,18 @@ struct FusedArgs {
     const float2* in_edge;
     const NonAdd* na;
     const int32_t* na_src;
-    const uint8_t* quad_tel;     // per quad: any gene switches
+    const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
     // state [G][N]
     float* M;
     float* P;
     uint8_t* prom;
+    int32_t* NS;            // step of the next promoter switch
     double* V;
     // division scratch (two parities)
     float* dM[2];
     float* dP[2];
     uint8_t* dprom[2];
+    int32_t* dNS[2];
     double* dV[2];
     unsigned long long* owner[2];
     // outputs
@@ -123,6 +125,7 @@ struct PlainArgs {
     const double* Pold;
     double* Pnew;
     uint8_t* prom;
+    int32_t* NS;
 };
 
 }  // namespace scrna

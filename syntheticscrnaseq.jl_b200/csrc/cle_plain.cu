@@ -26,15 +26,12 @@ __global__ void __launch_bounds__(128) cle_plain_step_kernel(const PlainArgs a) 
     const GeneRec gr = a.genes[g];
     const int s = a.step;
 
-    // telegraph switching
+    // telegraph switching: the promoter switches when its waiting time runs out
     bool on = a.prom[idx];
-    const int q = g >> 2;
-    if (a.quad_tel[q]) {
-        const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)q, tagword(TAG_SWITCH, a.stream), key);
-        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-        const uint32_t x = ws[g & 3];
-        if (on) { if (x < gr.thr_off) on = false; }
-        else { if (x < gr.thr_on) on = true; }
+    if (s == a.NS[idx]) {
+        on = !on;
+        const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+        a.NS[idx] = next_switch(s, w.x, on ? gr.inv_off : gr.inv_on);
         a.prom[idx] = on;
     }
     // reg = A_pos*act + A_neg*rep over the in-edges, from the previous step's proteins
@@ -94,8 +91,8 @@ cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st) {
 
 // Initial FP64 state: ceil(steady state) and the initial promoter draws.
 __global__ void plain_init_kernel(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
-                                  uint32_t key0, uint32_t key1, uint32_t stream, double* M,
-                                  double* P, uint8_t* prom) {
+                                  const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
+                                  double* M, double* P, uint8_t* prom, int32_t* NS) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y;
     if (c >= N) return;
@@ -110,13 +107,20 @@ __global__ void plain_init_kernel(int G, int64_t N, int64_t cell_offset, const G
         on = ws[g & 3] < gi[g].thr_init;
     }
     prom[idx] = on;
+    int32_t ns = kNever;
+    if (gr[g].inv_off == gr[g].inv_off) {
+        const uint4 w = philox((uint32_t)(cell_offset + c), 0u, (uint32_t)g, tagword(TAG_SWITCH, stream),
+                               Key{key0, key1});
+        ns = next_switch(0, w.x, on ? gr[g].inv_off : gr[g].inv_on);
+    }
+    NS[idx] = ns;
 }
 
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
-                              uint32_t key0, uint32_t key1, uint32_t stream, double* M, double* P,
-                              uint8_t* prom, cudaStream_t st) {
+                              const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
+                              double* M, double* P, uint8_t* prom, int32_t* NS, cudaStream_t st) {
     dim3 grid((unsigned)((N + 127) / 128), (unsigned)G);
-    plain_init_kernel<<<grid, 128, 0, st>>>(G, N, cell_offset, gi, key0, key1, stream, M, P, prom);
+    plain_init_kernel<<<grid, 128, 0, st>>>(G, N, cell_offset, gi, gr, key0, key1, stream, M, P, prom, NS);
     return cudaGetLastError();
 }
 

@@ -72,7 +72,7 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
 
     // per-lane gene constants
     float beta[GPL], cneg[GPL], W[GPL][NREG];
-    uint32_t thr_on[GPL], thr_off[GPL];
+    float inv_on[GPL], inv_off[GPL];
     int slot[GPL], na_range[GPL];
     bool valid[GPL];
 #pragma unroll
@@ -83,17 +83,17 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
         const GeneRec gr = a.genes[gg];
         beta[i] = gr.beta;
         cneg[i] = gr.cneg;
-        thr_on[i] = gr.thr_on;
-        thr_off[i] = valid[i] ? gr.thr_off : 0u;
+        inv_on[i] = gr.inv_on;
+        inv_off[i] = valid[i] ? gr.inv_off : __int_as_float(0x7FC00000);  // NaN: never switches
         slot[i] = valid[i] ? gr.slot : -1;
         na_range[i] = valid[i] ? gr.na_range : 0;
 #pragma unroll
         for (int r = 0; r < NREG; ++r) W[i][r] = (valid[i] && r < n_reg) ? wdense[(size_t)gg * n_reg + r] : 0.0f;
     }
     const int quad = GPL == 4 ? u : (u >> 1);
-    const bool tel = quad * 4 < G && a.quad_tel[quad];
 
     float m[GPL], p[GPL];
+    int32_t ns[GPL];  // step of the next promoter switch
     uint32_t on = 0xFFFFFFFFu;  // bit i: promoter of gene u*GPL+i is ON
     double V = 0.0;
 
@@ -117,6 +117,14 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
                     on &= ~(1u << i);
             }
         }
+#pragma unroll
+        for (int i = 0; i < GPL; ++i) {
+            ns[i] = kNever;
+            if (inv_off[i] == inv_off[i]) {
+                const uint4 w = philox(gcell, 0u, (uint32_t)(u * GPL + i), tagword(TAG_SWITCH, a.stream), key);
+                ns[i] = next_switch(0, w.x, (on >> i) & 1u ? inv_off[i] : inv_on[i]);
+            }
+        }
         if (POP) {
             const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
             V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
@@ -135,11 +143,13 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
         const float* Ms = from_daughter ? a.dM[par] : a.M;
         const float* Ps = from_daughter ? a.dP[par] : a.P;
         const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
+        const int32_t* Ns = from_daughter ? a.dNS[par] : a.NS;
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
             const int g = u * GPL + i;
             m[i] = valid[i] ? Ms[(size_t)g * N + src] : 0.0f;
             p[i] = valid[i] ? Ps[(size_t)g * N + src] : 0.0f;
+            ns[i] = valid[i] ? Ns[(size_t)g * N + src] : kNever;
             if (valid[i] && !Os[(size_t)g * N + src]) on &= ~(1u << i);
         }
         if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
@@ -149,14 +159,13 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     int buf = 0;
     for (int s = a.step_begin; s <= a.step_end; ++s) {
-        if (tel) {
-            const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)quad, tagword(TAG_SWITCH, a.stream), key);
 #pragma unroll
-            for (int i = 0; i < GPL; ++i) {
-                const uint32_t x = quad_word<GPL>(w, u, i);
+        for (int i = 0; i < GPL; ++i) {  // telegraph: switch when the waiting time runs out
+            if (s == ns[i]) {
                 const uint32_t bit = 1u << i;
-                const uint32_t thr = (on & bit) ? thr_off[i] : thr_on[i];
-                if (x < thr) on ^= bit;
+                on ^= bit;
+                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(u * GPL + i), tagword(TAG_SWITCH, a.stream), key);
+                ns[i] = next_switch(s, w.x, (on & bit) ? inv_off[i] : inv_on[i]);
             }
         }
         float* act = act_w + (size_t)buf * (cpw + 1) * ld + (size_t)cl * ld;
@@ -244,7 +253,15 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
                 const size_t idx = (size_t)g * N + cidx;
                 a.dM[par][idx] = dm;
                 a.dP[par][idx] = dp;
-                a.dprom[par][idx] = (on >> i) & 1u;
+                const uint32_t bon = (on >> i) & 1u;
+                a.dprom[par][idx] = bon;
+                int32_t dns = kNever;  // the daughter's promoter switches independently
+                if (inv_off[i] == inv_off[i]) {
+                    const uint4 w = philox(gcell, (uint32_t)a.step_end, (uint32_t)g | kDaughterSwitch,
+                                           tagword(TAG_SWITCH, a.stream), key);
+                    dns = next_switch(a.step_end, w.x, bon ? inv_off[i] : inv_on[i]);
+                }
+                a.dNS[par][idx] = dns;
             }
         }
     }
@@ -257,6 +274,7 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
         a.M[idx] = m[i];
         a.P[idx] = p[i];
         a.prom[idx] = (on >> i) & 1u;
+        a.NS[idx] = ns[i];
         if (a.last && a.out) {
             if (a.readout == 0) a.out[idx] = (double)m[i];
             else if (a.readout == 1) a.out[idx] = (double)p[i];
