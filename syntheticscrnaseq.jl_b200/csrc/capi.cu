@@ -80,6 +80,8 @@ struct scrna_ctx {
     bool own_stream = false;
     std::atomic<int64_t> launches{0};
     int sm_count = 0;
+    // states reused by the synchronous simulate calls (most recent last)
+    std::vector<scrna_state*> state_cache;
 };
 
 struct scrna_net {
@@ -166,10 +168,13 @@ extern "C" int scrna_ctx_create(int device, scrna_ctx** out) {
     return SCRNA_OK;
 }
 
+extern "C" int scrna_state_destroy(scrna_state* st);
+
 extern "C" int scrna_ctx_destroy(scrna_ctx* ctx) {
     if (!ctx) return SCRNA_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (scrna_state* st : ctx->state_cache) scrna_state_destroy(st);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SCRNA_OK;
@@ -720,9 +725,26 @@ extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const sc
     if (cap && !counts) return fail(SCRNA_EINVAL, "counts is NULL but capture was requested");
     const int64_t N = pop ? pop->cell_num : o->cell_num;
     if (N <= 0) return fail(SCRNA_EINVAL, "cell_num must be positive");
+    // reuse a cached state of the same shape, so repeated calls allocate nothing
     scrna_state* st = nullptr;
-    if (int r = scrna_state_create(ctx, net, N, o->readout, cap != nullptr, &st)) return r;
-    std::unique_ptr<scrna_state, int (*)(scrna_state*)> guard(st, scrna_state_destroy);
+    auto& cache = ctx->state_cache;
+    for (size_t i = 0; i < cache.size(); ++i) {
+        scrna_state* c = cache[i];
+        if (c->G == net->G && c->N == N && c->readout == o->readout && c->capture == (cap != nullptr)) {
+            st = c;
+            cache.erase(cache.begin() + i);
+            cache.push_back(st);
+            break;
+        }
+    }
+    if (!st) {
+        if (int r = scrna_state_create(ctx, net, N, o->readout, cap != nullptr, &st)) return r;
+        if (cache.size() >= 4) {
+            scrna_state_destroy(cache.front());
+            cache.erase(cache.begin());
+        }
+        cache.push_back(st);
+    }
     if (int r = scrna_cle_run_device(ctx, net, kin, pop, cap, o, st)) return r;
     return scrna_state_read(ctx, st, out, cap ? counts : nullptr, cap ? eff : nullptr);
 }

@@ -41,7 +41,7 @@ __device__ __forceinline__ uint32_t quad_word(const uint4& w, int u, int i) {
 }
 
 template <int GPL, int NREG, bool POP>
-__global__ void __launch_bounds__(32 * kWarpcellWarps)
+__global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
 cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int G = a.G;
