@@ -48,9 +48,12 @@ enum scrna_readout { SCRNA_READOUT_MRNA = 0, SCRNA_READOUT_PROTEIN = 1, SCRNA_RE
  * or deterministic halving (src/algorithms/cle.jl:249-261). */
 enum scrna_partition { SCRNA_PARTITION_BINOMIAL = 0, SCRNA_PARTITION_HALVE = 1 };
 
-/* Arithmetic of a run: the fused FP32 path (tensor-core contraction at large dense G), or the
- * plain FP64 one-kernel-per-step path kept as the comparison baseline. */
-enum scrna_precision { SCRNA_PRECISION_FP32 = 0, SCRNA_PRECISION_FP64_PLAIN = 1 };
+/* Arithmetic of a run: the FP32 path (its tensor-core contraction at large dense G takes
+ * BF16 inputs, or FP16 inputs with SCRNA_PRECISION_FP32_F16), or the plain FP64
+ * one-kernel-per-step path kept as the comparison baseline. */
+enum scrna_precision {
+    SCRNA_PRECISION_FP32 = 0, SCRNA_PRECISION_FP64_PLAIN = 1, SCRNA_PRECISION_FP32_F16 = 2
+};
 
 /* Kernel family for the FP32 precision.  AUTO picks the register path for sparse
  * networks (the warp-per-cell-group kernel when G <= 32 with <= 16 regulator genes,

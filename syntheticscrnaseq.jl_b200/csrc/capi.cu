@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/scrna_cle.h"
+#include "capi_internal.h"
 #include "cle_internal.h"
 
 namespace scrna {
@@ -35,6 +36,8 @@ cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* 
 cudaError_t philox_check_launch(int n, const uint32_t* d_ctr, uint32_t k0, uint32_t k1,
                                 uint32_t* d_out, cudaStream_t st);
 cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStream_t st);
+int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
+               const scrna_cle_opts* o, scrna_state* st, int dtype);
 }  // namespace scrna
 
 using namespace scrna;
@@ -42,7 +45,7 @@ using namespace scrna;
 // ---- errors ------------------------------------------------------------------------------------
 static thread_local std::string g_err;
 
-static int fail(int code, const char* fmt, ...) {
+int scrna::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -51,79 +54,6 @@ static int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
-
-#define CU(call)                                                                          \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(SCRNA_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));     \
-    } while (0)
-
-// ---- device buffers -----------------------------------------------------------------------
-struct DevBuf {
-    void* p = nullptr;
-    size_t n = 0;
-    ~DevBuf() { if (p) cudaFree(p); }
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= n) return cudaSuccess;
-        if (p) { cudaFree(p); p = nullptr; n = 0; }
-        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
-        if (e == cudaSuccess) n = bytes;
-        return e;
-    }
-    template <class T> T* as() const { return static_cast<T*>(p); }
-};
-
-struct scrna_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    std::atomic<int64_t> launches{0};
-    int sm_count = 0;
-    // states reused by the synchronous simulate calls (most recent last)
-    std::vector<scrna_state*> state_cache;
-};
-
-struct scrna_net {
-    scrna_ctx* ctx = nullptr;
-    int32_t G = 0;
-    std::vector<double> basals;
-    std::vector<double> A;  // row-major A[i*G+j]
-    std::vector<double> k_on, k_off;
-    // host tables
-    std::vector<int32_t> reg_slot;   // gene -> slot or -1
-    std::vector<int32_t> reg_gene;   // slot -> gene
-    std::vector<int32_t> in_begin, in_end;
-    std::vector<float2> in_edge;
-    std::vector<double> in_w64;
-    std::vector<double> cneg64;
-    std::vector<int32_t> na_begin, na_count;
-    std::vector<NonAdd> na;
-    std::vector<double> na_coef64;
-    std::vector<int32_t> na_src;
-    NetDev dev;
-    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_wdense;
-    // per-run tables cached for the last (kinetics, dt, population mode)
-    DevBuf b_genes, b_ginit, b_quad_tel;
-    bool cache_valid = false;
-    double c_dt = 0, c_kin[6] = {0};
-    bool c_pop = false;
-};
-
-struct scrna_state {
-    scrna_ctx* ctx = nullptr;
-    int32_t G = 0;
-    int64_t N = 0;
-    int32_t readout = 1;
-    bool capture = false;
-    DevBuf M, P, prom, NS, V, out, counts, eff;
-    DevBuf dM[2], dP[2], dprom[2], dNS[2], dV[2], owner[2];
-    DevBuf M64, P64a, P64b;  // FP64 baseline state
-    bool have_counts = false;
-    bool last_plain = false;
-    bool last_pop = false;
-    const double* p64_final = nullptr;
-};
 
 // ---- helpers ----------------------------------------------------------------------------------
 static constexpr double kLn2 = 0.69314718055994530942;
@@ -670,9 +600,25 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
     if (o->cell_offset < 0 || o->cell_offset + N > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
     const bool plain = o->precision == SCRNA_PRECISION_FP64_PLAIN;
     if (plain && pop) return fail(SCRNA_ENOTSUP, "the FP64 baseline path has no population dynamics");
-    if (o->precision != SCRNA_PRECISION_FP32 && !plain) return fail(SCRNA_EINVAL, "unknown precision");
+    if (o->precision != SCRNA_PRECISION_FP32 && o->precision != SCRNA_PRECISION_FP32_F16 && !plain)
+        return fail(SCRNA_EINVAL, "unknown precision");
     if (int r = set_device(ctx)) return r;
     if (int r = ensure_gene_tables(net, kin, o->dt, pop != nullptr)) return r;
+    // kernel family: tensor cores for large dense networks (or when asked), else the register path
+    const NetDev& nd = net->dev;
+    const double density = (double)nd.n_in / ((double)net->G * net->G);
+    const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR ||
+                                   (o->path == SCRNA_PATH_AUTO &&
+                                    (nd.n_quads > fused_max_quads() || (net->G >= 256 && density >= 0.05))));
+    if (tensor) {
+        if (pop) return fail(SCRNA_ENOTSUP, "the tensor-core path has no population dynamics");
+        st->have_counts = cap != nullptr;
+        st->last_plain = false;
+        st->last_pop = false;
+        st->last_tensor = true;
+        return tensor_run(ctx, net, kin, cap, o, st, o->precision == SCRNA_PRECISION_FP32_F16 ? 1 : 0);
+    }
+    st->last_tensor = false;
     if (int r = state_alloc(st, pop != nullptr, plain)) return r;
     st->have_counts = cap != nullptr;
     st->last_plain = plain;
@@ -701,6 +647,23 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
     if (!st) return fail(SCRNA_EINVAL, "state is NULL");
     if (int r = set_device(ctx)) return r;
     const size_t gn = (size_t)st->G * st->N;
+    if (st->last_tensor) {  // cell-major state: transpose to [G][N] on the host
+        std::vector<float> tm(gn), tp(gn);
+        std::vector<uint8_t> tpr(gn);
+        CU(cudaMemcpyAsync(tm.data(), st->tM.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tp.data(), st->tP.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tpr.data(), st->tprom.p, gn, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        for (int64_t c = 0; c < st->N; ++c)
+            for (int g = 0; g < st->G; ++g) {
+                const size_t src = (size_t)c * st->G + g, dst = (size_t)g * st->N + c;
+                if (mrna) static_cast<float*>(mrna)[dst] = tm[src];
+                if (protein) static_cast<float*>(protein)[dst] = tp[src];
+                if (promoter) promoter[dst] = tpr[src];
+            }
+        if (volume) return fail(SCRNA_EINVAL, "the last run had no population");
+        return SCRNA_OK;
+    }
     const size_t esz = st->last_plain ? 8 : 4;
     const void* dm = st->last_plain ? st->M64.p : st->M.p;
     const void* dp = st->last_plain ? (const void*)st->p64_final : st->P.p;

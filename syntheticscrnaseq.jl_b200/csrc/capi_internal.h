@@ -1,0 +1,107 @@
+// Host-side objects behind the C ABI handles (scrna_ctx, scrna_net, scrna_state),
+// shared by the translation units of the library.  Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/scrna_cle.h"
+#include "cle_internal.h"
+
+struct cublasLtContext;
+
+namespace scrna {
+int fail(int code, const char* fmt, ...);
+}  // namespace scrna
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return scrna::fail(SCRNA_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---- device buffers -----------------------------------------------------------------------
+namespace scrna {
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; n = 0; }
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+}  // namespace scrna
+using scrna::DevBuf;
+using scrna::NetDev;
+using scrna::NonAdd;
+
+struct scrna_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::atomic<int64_t> launches{0};
+    int sm_count = 0;
+    // states reused by the synchronous simulate calls (most recent last)
+    std::vector<scrna_state*> state_cache;
+    // cuBLASLt handle and workspace of the tensor-core path (created on first use)
+    void* lt_handle = nullptr;
+    scrna::DevBuf lt_workspace;
+};
+
+struct scrna_net {
+    scrna_ctx* ctx = nullptr;
+    int32_t G = 0;
+    std::vector<double> basals;
+    std::vector<double> A;  // row-major A[i*G+j]
+    std::vector<double> k_on, k_off;
+    // host tables
+    std::vector<int32_t> reg_slot;   // gene -> slot or -1
+    std::vector<int32_t> reg_gene;   // slot -> gene
+    std::vector<int32_t> in_begin, in_end;
+    std::vector<float2> in_edge;
+    std::vector<double> in_w64;
+    std::vector<double> cneg64;
+    std::vector<int32_t> na_begin, na_count;
+    std::vector<NonAdd> na;
+    std::vector<double> na_coef64;
+    std::vector<int32_t> na_src;
+    NetDev dev;
+    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_wdense;
+    // per-run tables cached for the last (kinetics, dt, population mode)
+    DevBuf b_genes, b_ginit, b_quad_tel;
+    // tensor-core path: W = A_eff as 16-bit [G][Kp] (K-major), nonadd sources compacted
+    int32_t t_kp = 0;
+    int32_t t_dtype = -1;              // 0 bf16, 1 fp16
+    int32_t t_n_src = 0;               // distinct genes read by cooperative/redundant edges
+    DevBuf t_w16, t_na, t_na_src, t_src_gene, t_src_of_gene;
+    bool cache_valid = false;
+    double c_dt = 0, c_kin[6] = {0};
+    bool c_pop = false;
+};
+
+struct scrna_state {
+    scrna_ctx* ctx = nullptr;
+    int32_t G = 0;
+    int64_t N = 0;
+    int32_t readout = 1;
+    bool capture = false;
+    DevBuf M, P, prom, NS, V, out, counts, eff;
+    DevBuf dM[2], dP[2], dprom[2], dNS[2], dV[2], owner[2];
+    DevBuf M64, P64a, P64b;  // FP64 baseline state
+    // tensor-core path state, cell-major [N][G]
+    DevBuf tM, tP, tprom, tNS, tact16, tact32[2], treg;
+    bool last_tensor = false;
+    bool have_counts = false;
+    bool last_plain = false;
+    bool last_pop = false;
+    const double* p64_final = nullptr;
+};
+

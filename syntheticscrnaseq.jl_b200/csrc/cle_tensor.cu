@@ -1,0 +1,364 @@
+// Tensor-core path for large dense networks.
+//
+// For G in the thousands with ~10 % dense regulation, the additive term
+// reg = sum_j A_eff[i,j] act_j (the one-GEMM form of A_pos act + A_neg rep,
+// network.jl:206-219, cle.jl:84-86) is a real dense GEMM per Euler step:
+//     REG[N x G] = ACT[N x K] * W^T,  W = A_eff as 16-bit [G][K], ACT 16-bit [N][K]
+// with FP32 accumulation.  Each step is the GEMM (cuBLASLt, BF16 or FP16 inputs) followed
+// by one fused FP32 kernel that adds the repression constant and the cooperative /
+// redundant terms, applies telegraph switching, draws the Philox increments, updates
+// M and P (cle.jl:109-120) and writes the next step's 16-bit activations.  State is
+// cell-major [N][G] so that both kernels stream it with unit stride.
+#include <cublasLt.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "capi_internal.h"
+#include "cle_device.cuh"
+
+namespace scrna {
+
+template <class T> __device__ __forceinline__ T to16(float x);
+template <> __device__ __forceinline__ __nv_bfloat16 to16<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+template <> __device__ __forceinline__ __half to16<__half>(float x) { return __float2half_rn(x); }
+
+struct TensorArgs {
+    int32_t G, Kp, n_src;
+    int64_t N, cell_offset;
+    int32_t step;
+    float k_t, Kn, hill_n, mu_m, mu_p, dt;
+    int32_t hill_int;
+    uint32_t key0, key1, stream;
+    const GeneRec* genes;
+    const GeneInit* ginit;
+    const NonAdd* na;        // sources are compact source indices
+    const int32_t* na_src;
+    const int32_t* src_of_gene;  // gene -> compact source index or -1
+    const float* reg;        // [N][G] GEMM output of this step
+    float* M;
+    float* P;
+    uint8_t* prom;
+    int32_t* NS;
+    void* act16;             // [N][Kp]
+    const float* act32_cur;  // [N][n_src]
+    float* act32_next;
+};
+
+// Initial state (cle.jl:49-53), promoter draws and first activations; thread per (cell, gene).
+template <class T>
+__global__ void tensor_init_kernel(const TensorArgs a) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.N * a.G) return;
+    const int64_t c = idx / a.G;
+    const int g = (int)(idx - c * a.G);
+    const Key key{a.key0, a.key1};
+    const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+    const GeneInit gi = a.ginit[g];
+    const GeneRec gr = a.genes[g];
+    const float p0 = gi.p0;
+    a.M[idx] = gi.m0;
+    a.P[idx] = p0;
+    bool on = true;
+    if (gi.init_rand) {
+        const uint4 w = philox(gcell, 0u, (uint32_t)(g >> 2), tagword(TAG_PROMOTER, a.stream), key);
+        const uint32_t x = (g & 3) == 0 ? w.x : (g & 3) == 1 ? w.y : (g & 3) == 2 ? w.z : w.w;
+        on = x < gi.thr_init;
+    }
+    a.prom[idx] = on;
+    int32_t ns = kNever;
+    if (gr.inv_off == gr.inv_off) {
+        const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+        ns = next_switch(0, w.x, on ? gr.inv_off : gr.inv_on);
+    }
+    a.NS[idx] = ns;
+    const float act = hill_act(p0, a.Kn, a.hill_n, a.hill_int);
+    reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
+    const int src = a.src_of_gene[g];
+    if (src >= 0) a.act32_next[c * a.n_src + src] = act;
+}
+
+// One Euler-Maruyama step after the GEMM; thread per (cell, gene pair), one Philox block each.
+template <class T>
+__global__ void __launch_bounds__(256) tensor_step_kernel(const TensorArgs a) {
+    const int pairs = (a.G + 1) >> 1;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.N * pairs) return;
+    const int64_t c = idx / pairs;
+    const int k = (int)(idx - c * pairs);
+    const Key key{a.key0, a.key1};
+    const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+    const int s = a.step;
+    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)k, tagword(TAG_NORMAL, a.stream), key);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int g = 2 * k + h;
+        if (g >= a.G) break;
+        const int64_t e = c * a.G + g;
+        const GeneRec gr = a.genes[g];
+        bool on = a.prom[e];
+        int32_t ns = a.NS[e];
+        if (s == ns) {
+            on = !on;
+            const uint4 ws = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+            ns = next_switch(s, ws.x, on ? gr.inv_off : gr.inv_on);
+            a.prom[e] = on;
+            a.NS[e] = ns;
+        }
+        float reg = a.reg[e] + gr.cneg;
+        const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
+        for (int q = nab; q < nab + nac; ++q) {
+            const NonAdd na = a.na[q];
+            float prod = 1.0f;
+            if (na.kind == 0) {
+                for (int t = na.src_begin; t < na.src_end; ++t) prod *= a.act32_cur[c * a.n_src + a.na_src[t]];
+                reg = fmaf(na.coef, prod, reg);
+            } else {
+                for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - a.act32_cur[c * a.n_src + a.na_src[t]];
+                reg = fmaf(na.coef, 1.0f - prod, reg);
+            }
+        }
+        float tx = reg + gr.beta;
+        if (!on) tx = 0.0f;
+        const BM bm = h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+        float m = a.M[e], p = a.P[e];
+        em_update(m, p, tx, bm, a.mu_m, a.mu_p, a.k_t, a.dt);
+        a.M[e] = m;
+        a.P[e] = p;
+        const float act = hill_act(p, a.Kn, a.hill_n, a.hill_int);
+        reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
+        const int src = a.src_of_gene[g];
+        if (src >= 0) a.act32_next[c * a.n_src + src] = act;
+    }
+}
+
+// Readout: cell-major FP32 state -> cells x G (x2) column-major Float64, through a
+// shared-memory tile so both the reads and the writes are coalesced.
+__global__ void tensor_readout_kernel(int G, int64_t N, const float* M, const float* P, int readout,
+                                      double* out) {
+    __shared__ float tile[2][32][33];
+    const int64_t c0 = (int64_t)blockIdx.x * 32;
+    const int g0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int64_t c = c0 + r;
+        const int g = g0 + threadIdx.x;
+        const bool ok = c < N && g < G;
+        tile[0][r][threadIdx.x] = ok ? M[c * G + g] : 0.0f;
+        tile[1][r][threadIdx.x] = ok ? P[c * G + g] : 0.0f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int g = g0 + r;
+        const int64_t c = c0 + threadIdx.x;
+        if (g >= G || c >= N) continue;
+        const float mv = tile[0][threadIdx.x][r], pv = tile[1][threadIdx.x][r];
+        if (readout == 0) out[(size_t)g * N + c] = mv;
+        else if (readout == 1) out[(size_t)g * N + c] = pv;
+        else { out[(size_t)g * N + c] = mv; out[(size_t)(G + g) * N + c] = pv; }
+    }
+}
+
+// Capture on the cell-major state (capture.jl:30-44), thread per (cell, gene).
+__global__ void tensor_capture_kernel(int G, int64_t N, int64_t cell_offset, const float* X, double mu_log,
+                                      double sigma, uint32_t key0, uint32_t key1, uint32_t stream,
+                                      double* eff, int32_t* Y) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= N * G) return;
+    const int64_t c = idx / G;
+    const int g = (int)(idx - c * G);
+    const Key key{key0, key1};
+    const uint32_t gcell = (uint32_t)(cell_offset + c);
+    const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, stream), key);
+    double pe = exp(mu_log + sigma * box_muller_z0_f64(w.x, w.y));
+    pe = fmin(fmax(pe, 0.0), 1.0);
+    if (g == 0 && eff) eff[c] = pe;
+    const double x = rint((double)X[idx]);
+    const int64_t n = x > 0.0 ? (int64_t)x : 0;
+    int64_t y = 0;
+    if (n > 0 && pe != 0.0) y = binomial_capture(n, pe, key, stream, gcell, (uint32_t)g);
+    Y[(size_t)g * N + c] = (int32_t)y;
+}
+
+template <class T>
+__global__ void tensor_fill_w_kernel(int G, int Kp, const float* wdense_rowmajor, T* w16) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)G * Kp) return;
+    const int i = (int)(idx / Kp), j = (int)(idx - (int64_t)i * Kp);
+    w16[idx] = to16<T>(j < G ? wdense_rowmajor[(size_t)i * G + j] : 0.0f);
+}
+
+// ---- host side -------------------------------------------------------------------------------
+// Build the 16-bit weight matrix and the compact cooperative/redundant source tables.
+int tensor_prepare_net(scrna_net* n, int dtype) {
+    if (n->t_dtype == dtype) return SCRNA_OK;
+    const int G = n->G;
+    const int Kp = (G + 63) / 64 * 64;
+    std::vector<float> w((size_t)G * G, 0.0f);
+    for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j)
+            if (i != j) w[(size_t)i * G + j] = (float)(n->A[(size_t)i * G + j] * n->basals[i]);
+    // compact source indices of the cooperative / redundant edges
+    std::vector<int32_t> src_of_gene(G, -1), src_gene;
+    std::vector<int32_t> na_src(n->na_src.size());
+    for (size_t t = 0; t < n->na_src.size(); ++t) {
+        const int gene = n->reg_gene[n->na_src[t]];
+        if (src_of_gene[gene] < 0) { src_of_gene[gene] = (int)src_gene.size(); src_gene.push_back(gene); }
+        na_src[t] = src_of_gene[gene];
+    }
+    DevBuf wf;
+    CU(wf.ensure(w.size() * 4));
+    CU(cudaMemcpy(wf.p, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+    CU(n->t_w16.ensure((size_t)G * Kp * 2));
+    const int64_t tot = (int64_t)G * Kp;
+    if (dtype == 0) tensor_fill_w_kernel<__nv_bfloat16><<<(unsigned)((tot + 255) / 256), 256>>>(G, Kp, wf.as<float>(), n->t_w16.as<__nv_bfloat16>());
+    else tensor_fill_w_kernel<__half><<<(unsigned)((tot + 255) / 256), 256>>>(G, Kp, wf.as<float>(), n->t_w16.as<__half>());
+    CU(cudaGetLastError());
+    CU(cudaDeviceSynchronize());
+    CU(n->t_na_src.ensure(std::max<size_t>(na_src.size(), 1) * 4));
+    if (!na_src.empty()) CU(cudaMemcpy(n->t_na_src.p, na_src.data(), na_src.size() * 4, cudaMemcpyHostToDevice));
+    CU(n->t_src_of_gene.ensure((size_t)G * 4));
+    CU(cudaMemcpy(n->t_src_of_gene.p, src_of_gene.data(), (size_t)G * 4, cudaMemcpyHostToDevice));
+    n->t_kp = Kp;
+    n->t_n_src = (int)src_gene.size();
+    n->t_dtype = dtype;
+    return SCRNA_OK;
+}
+
+static int lt_fail(cublasStatus_t st, const char* what) {
+    return fail(SCRNA_ECUDA, "%s failed (cuBLAS status %d)", what, (int)st);
+}
+
+// REG[N][G] = ACT[N][Kp] * W[G][Kp]^T in column-major terms: C (G x N, ldc G) =
+// op(A) (G x Kp) * B (Kp x N) with A = W stored as Kp x G (lda Kp) transposed.
+struct LtGemm {
+    cublasLtMatmulDesc_t op = nullptr;
+    cublasLtMatrixLayout_t la = nullptr, lb = nullptr, lc = nullptr;
+    cublasLtMatmulAlgo_t algo{};
+    bool ok = false;
+    ~LtGemm() {
+        if (lc) cublasLtMatrixLayoutDestroy(lc);
+        if (lb) cublasLtMatrixLayoutDestroy(lb);
+        if (la) cublasLtMatrixLayoutDestroy(la);
+        if (op) cublasLtMatmulDescDestroy(op);
+    }
+};
+
+static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int Kp, int64_t N) {
+    cublasStatus_t st;
+    if (!ctx->lt_handle) {
+        cublasLtHandle_t h;
+        if ((st = cublasLtCreate(&h)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "cublasLtCreate");
+        ctx->lt_handle = h;
+    }
+    const size_t ws = 64u << 20;
+    CU(ctx->lt_workspace.ensure(ws));
+    const cudaDataType_t t16 = dtype == 0 ? CUDA_R_16BF : CUDA_R_16F;
+    if ((st = cublasLtMatmulDescCreate(&g.op, CUBLAS_COMPUTE_32F, CUDA_R_32F)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "MatmulDescCreate");
+    const cublasOperation_t ta = CUBLAS_OP_T, tb = CUBLAS_OP_N;
+    cublasLtMatmulDescSetAttribute(g.op, CUBLASLT_MATMUL_DESC_TRANSA, &ta, sizeof ta);
+    cublasLtMatmulDescSetAttribute(g.op, CUBLASLT_MATMUL_DESC_TRANSB, &tb, sizeof tb);
+    if ((st = cublasLtMatrixLayoutCreate(&g.la, t16, Kp, G, Kp)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutA");
+    if ((st = cublasLtMatrixLayoutCreate(&g.lb, t16, Kp, N, Kp)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutB");
+    if ((st = cublasLtMatrixLayoutCreate(&g.lc, CUDA_R_32F, G, N, G)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutC");
+    cublasLtMatmulPreference_t pref;
+    cublasLtMatmulPreferenceCreate(&pref);
+    cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ws, sizeof ws);
+    cublasLtMatmulHeuristicResult_t res{};
+    int nres = 0;
+    st = cublasLtMatmulAlgoGetHeuristic((cublasLtHandle_t)ctx->lt_handle, g.op, g.la, g.lb, g.lc, g.lc, pref, 1, &res, &nres);
+    cublasLtMatmulPreferenceDestroy(pref);
+    if (st != CUBLAS_STATUS_SUCCESS || nres == 0) return lt_fail(st, "AlgoGetHeuristic");
+    g.algo = res.algo;
+    g.ok = true;
+    return SCRNA_OK;
+}
+
+int64_t run_steps(const scrna_cle_opts* o);
+
+int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
+               const scrna_cle_opts* o, scrna_state* st, int dtype) {
+    if (int r = tensor_prepare_net(n, dtype)) return r;
+    const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src;
+    const int64_t N = st->N;
+    const size_t gn = (size_t)G * N;
+    CU(st->tM.ensure(gn * 4));
+    CU(st->tP.ensure(gn * 4));
+    CU(st->tprom.ensure(gn));
+    CU(st->tNS.ensure(gn * 4));
+    CU(st->treg.ensure(gn * 4));
+    CU(st->tact16.ensure((size_t)N * Kp * 2));
+    for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
+    CU(st->out.ensure(gn * (st->readout == SCRNA_READOUT_BOTH ? 2 : 1) * 8));
+    if (cap) {
+        CU(st->counts.ensure(gn * 4));
+        CU(st->eff.ensure((size_t)N * 8));
+    }
+    cudaStream_t s = ctx->stream;
+    CU(cudaMemsetAsync(st->tact16.p, 0, (size_t)N * Kp * 2, s));  // zero K padding
+    TensorArgs a{};
+    a.G = G; a.Kp = Kp; a.n_src = n_src; a.N = N; a.cell_offset = o->cell_offset;
+    a.k_t = (float)kin->k_t;
+    a.Kn = (float)std::pow(kin->K_d, kin->n);
+    a.hill_n = (float)kin->n;
+    a.hill_int = (kin->n == std::floor(kin->n) && kin->n >= 1.0 && kin->n <= 16.0) ? (int)kin->n : 0;
+    a.mu_m = (float)(kin->mu_m + kin->dilution);
+    a.mu_p = (float)(kin->mu_p + kin->dilution);
+    a.dt = (float)o->dt;
+    a.key0 = (uint32_t)o->seed; a.key1 = (uint32_t)(o->seed >> 32); a.stream = o->stream & 0xFFFFFFu;
+    a.genes = n->b_genes.as<GeneRec>();
+    a.ginit = n->b_ginit.as<GeneInit>();
+    a.na = n->dev.na;
+    a.na_src = n->t_na_src.as<int32_t>();
+    a.src_of_gene = n->t_src_of_gene.as<int32_t>();
+    a.reg = st->treg.as<float>();
+    a.M = st->tM.as<float>(); a.P = st->tP.as<float>();
+    a.prom = st->tprom.as<uint8_t>(); a.NS = st->tNS.as<int32_t>();
+    a.act16 = st->tact16.p;
+    a.act32_cur = st->tact32[1].as<float>();
+    a.act32_next = st->tact32[0].as<float>();
+    const unsigned b_init = (unsigned)((gn + 255) / 256);
+    if (dtype == 0) tensor_init_kernel<__nv_bfloat16><<<b_init, 256, 0, s>>>(a);
+    else tensor_init_kernel<__half><<<b_init, 256, 0, s>>>(a);
+    CU(cudaGetLastError());
+    ctx->launches++;
+
+    LtGemm gemm;
+    if (int r = lt_setup(ctx, gemm, dtype, G, Kp, N)) return r;
+    const float alpha = 1.0f, beta = 0.0f;
+    const int64_t n_steps = run_steps(o);
+    const int pairs = (G + 1) / 2;
+    const unsigned b_step = (unsigned)(((int64_t)N * pairs + 255) / 256);
+    for (int64_t step = 1; step <= n_steps; ++step) {
+        cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,
+                                            st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
+                                            &gemm.algo, ctx->lt_workspace.p, ctx->lt_workspace.n, s);
+        if (stt != CUBLAS_STATUS_SUCCESS) return lt_fail(stt, "cublasLtMatmul");
+        a.step = (int)step;
+        a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
+        a.act32_next = st->tact32[step & 1].as<float>();
+        if (dtype == 0) tensor_step_kernel<__nv_bfloat16><<<b_step, 256, 0, s>>>(a);
+        else tensor_step_kernel<__half><<<b_step, 256, 0, s>>>(a);
+        CU(cudaGetLastError());
+        ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
+    }
+    dim3 rgrid((unsigned)((N + 31) / 32), (unsigned)((G + 31) / 32));
+    tensor_readout_kernel<<<rgrid, dim3(32, 8), 0, s>>>(G, N, st->tM.as<float>(), st->tP.as<float>(), st->readout,
+                                                        st->out.as<double>());
+    CU(cudaGetLastError());
+    ctx->launches++;
+    if (cap) {
+        const double mu_log = std::log(cap->efficiency) -
+                              (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
+        const float* X = cap->readout == SCRNA_READOUT_MRNA ? st->tM.as<float>() : st->tP.as<float>();
+        tensor_capture_kernel<<<b_init, 256, 0, s>>>(G, N, o->cell_offset, X, mu_log, cap->efficiency_std, a.key0,
+                                                     a.key1, a.stream, st->eff.as<double>(), st->counts.as<int32_t>());
+        CU(cudaGetLastError());
+        ctx->launches++;
+    }
+    return SCRNA_OK;
+}
+
+}  // namespace scrna

@@ -1,0 +1,80 @@
+"""GPU tests of the tensor-core path (dense regulation, 16-bit GEMM inputs, FP32 state).
+
+Tolerances: the GEMM rounds W = A_eff and the Hill activations to BF16 (8-bit mantissa) or
+FP16 (11-bit), so trajectories are compared against the FP32 register path with
+|tensor - register| <= TOL * max(|register|, 1): TOL = 5e-2 (BF16), 1e-2 (FP16) after 150 steps;
+per-gene ensemble means against the FP64 oracle on the same increments within 2 %.
+Promoter states and capture counts (given the path's own X and efficiencies) are exact.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(pkg, G, seed, density=0.3, bursty=False):
+    net = pkg.dense_network(G, seed=seed, density=density, n_coop=4, n_redun=4)
+    if bursty:
+        rng = np.random.default_rng(seed)
+        net = pkg.GeneNetwork(G, net.basals, net.interactions, net.cooperative, net.redundant,
+                              k_on=np.exp(rng.uniform(np.log(0.1), np.log(1.0), G)),
+                              k_off=np.exp(rng.uniform(np.log(1.0), np.log(10.0), G)))
+    return net
+
+
+def _run(pkg, net, kin, path, precision="fp32", N=300, steps=150, seed=3, **kw):
+    run = pkg.DeviceRun(net, pkg.CLE(0.01), kin, cell_num=N, T=0.0, n_steps=steps, readout="both",
+                        seed=seed, path=path, precision=precision, **kw)
+    run.launch()
+    return run
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1.0)))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 5e-2), ("fp32_f16", 1e-2)])
+@pytest.mark.parametrize("bursty", [False, True])
+def test_tensor_matches_register_path(pkg, precision, tol, bursty):
+    net = _dense(pkg, 64, seed=1, bursty=bursty)
+    kin = pkg.WORKLOAD_KINETICS
+    ref = _run(pkg, net, kin, "block").read_raw()
+    got = _run(pkg, net, kin, "tensor", precision=precision).read_raw()
+    assert np.array_equal(got["prom"], ref["prom"])
+    assert _rel(got["M"], ref["M"].astype(np.float64)) < tol
+    assert _rel(got["P"], ref["P"].astype(np.float64)) < tol
+
+
+def test_tensor_per_gene_means_vs_oracle(pkg, orc):
+    net = _dense(pkg, 200, seed=5, density=0.1)
+    kin = pkg.WORKLOAD_KINETICS
+    N, steps = 2048, 300
+    got = _run(pkg, net, kin, "tensor", N=N, steps=steps, seed=11).read_raw()
+    ref = orc.simulate(net, kin, dt=0.01, cell_num=N, n_steps=steps, seed=11)
+    for key in ("M", "P"):
+        mg = got[key].astype(np.float64).mean(1)
+        mr = ref[key].mean(1)
+        err = np.abs(mg - mr) / np.maximum(np.abs(mr), 1.0)
+        assert err.max() < 0.02, (key, err.max())
+
+
+def test_tensor_readout_and_capture(pkg, orc):
+    net = _dense(pkg, 96, seed=7)
+    kin = pkg.WORKLOAD_KINETICS
+    cap = pkg.CaptureModel(efficiency=0.2, efficiency_std=0.5, readout="protein")
+    X, counts, eff = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=333, T=1.0, readout="protein", seed=4,
+                                  capture=cap, path="tensor")
+    raw = pkg.DeviceRun(net, pkg.CLE(0.01), kin, cell_num=333, T=1.0, readout="both", seed=4, path="tensor")
+    raw.launch()
+    both = raw.read()
+    assert np.array_equal(both[:, 96:], X)
+    want = orc.capture_counts(np.ascontiguousarray(X.T), eff, seed=4)
+    assert np.array_equal(counts.T, want)
+
+
+def test_auto_picks_tensor_for_large_dense(pkg):
+    net = _dense(pkg, 600, seed=2, density=0.1)
+    kin = pkg.WORKLOAD_KINETICS
+    a = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=128, T=0.2, seed=1)
+    b = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=128, T=0.2, seed=1, path="tensor")
+    assert np.array_equal(a, b)
