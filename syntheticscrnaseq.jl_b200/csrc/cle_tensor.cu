@@ -81,57 +81,74 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
     if (src >= 0) a.act32_next[c * a.n_src + src] = act;
 }
 
-// One Euler-Maruyama step after the GEMM; thread per (cell, gene pair), one Philox block each.
-template <class T>
-__global__ void __launch_bounds__(256) tensor_step_kernel(const TensorArgs a) {
+// One Euler-Maruyama step after the GEMM.  Thread = one gene pair (blockIdx.y, x) for a chunk
+// of kTensorCellsPerThread cells (blockIdx.x); per-gene constants stay in registers across the
+// chunk, consecutive threads touch consecutive genes of one cell (unit-stride rows).
+constexpr int kTensorCellsPerThread = 16;
+constexpr int kTensorPairsPerBlock = 128;
+
+template <class T, bool BURSTY>
+__global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const TensorArgs a) {
     const int pairs = (a.G + 1) >> 1;
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= a.N * pairs) return;
-    const int64_t c = idx / pairs;
-    const int k = (int)(idx - c * pairs);
+    const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
+    if (k >= pairs) return;
     const Key key{a.key0, a.key1};
-    const uint32_t gcell = (uint32_t)(a.cell_offset + c);
     const int s = a.step;
-    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)k, tagword(TAG_NORMAL, a.stream), key);
+    GeneRec gr[2];
+    int src[2];
+    bool valid[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int g = 2 * k + h;
-        if (g >= a.G) break;
-        const int64_t e = c * a.G + g;
-        const GeneRec gr = a.genes[g];
-        bool on = a.prom[e];
-        int32_t ns = a.NS[e];
-        if (s == ns) {
-            on = !on;
-            const uint4 ws = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-            ns = next_switch(s, ws.x, on ? gr.inv_off : gr.inv_on);
-            a.prom[e] = on;
-            a.NS[e] = ns;
-        }
-        float reg = a.reg[e] + gr.cneg;
-        const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
-        for (int q = nab; q < nab + nac; ++q) {
-            const NonAdd na = a.na[q];
-            float prod = 1.0f;
-            if (na.kind == 0) {
-                for (int t = na.src_begin; t < na.src_end; ++t) prod *= a.act32_cur[c * a.n_src + a.na_src[t]];
-                reg = fmaf(na.coef, prod, reg);
-            } else {
-                for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - a.act32_cur[c * a.n_src + a.na_src[t]];
-                reg = fmaf(na.coef, 1.0f - prod, reg);
+        valid[h] = g < a.G;
+        gr[h] = a.genes[valid[h] ? g : 0];
+        src[h] = valid[h] ? a.src_of_gene[g] : -1;
+    }
+    const int64_t c_begin = (int64_t)blockIdx.x * kTensorCellsPerThread;
+    const int64_t c_end = c_begin + kTensorCellsPerThread < a.N ? c_begin + kTensorCellsPerThread : a.N;
+    T* act16 = reinterpret_cast<T*>(a.act16);
+    for (int64_t c = c_begin; c < c_end; ++c) {
+        const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+        const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)k, tagword(TAG_NORMAL, a.stream), key);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!valid[h]) continue;
+            const int g = 2 * k + h;
+            const int64_t e = c * a.G + g;
+            bool on = true;
+            if (BURSTY) {
+                on = a.prom[e];
+                if (s == a.NS[e]) {
+                    on = !on;
+                    const uint4 ws = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
+                    a.NS[e] = next_switch(s, ws.x, on ? gr[h].inv_off : gr[h].inv_on);
+                    a.prom[e] = on;
+                }
             }
+            float reg = a.reg[e] + gr[h].cneg;
+            const int nab = gr[h].na_range >> 16, nac = gr[h].na_range & 0xFFFF;
+            for (int q = nab; q < nab + nac; ++q) {
+                const NonAdd na = a.na[q];
+                float prod = 1.0f;
+                if (na.kind == 0) {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= a.act32_cur[c * a.n_src + a.na_src[t]];
+                    reg = fmaf(na.coef, prod, reg);
+                } else {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - a.act32_cur[c * a.n_src + a.na_src[t]];
+                    reg = fmaf(na.coef, 1.0f - prod, reg);
+                }
+            }
+            float tx = reg + gr[h].beta;
+            if (!on) tx = 0.0f;
+            const BM bm = h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+            float m = a.M[e], p = a.P[e];
+            em_update(m, p, tx, bm, a.mu_m, a.mu_p, a.k_t, a.dt);
+            a.M[e] = m;
+            a.P[e] = p;
+            const float act = hill_act(p, a.Kn, a.hill_n, a.hill_int);
+            act16[c * a.Kp + g] = to16<T>(act);
+            if (src[h] >= 0) a.act32_next[c * a.n_src + src[h]] = act;
         }
-        float tx = reg + gr.beta;
-        if (!on) tx = 0.0f;
-        const BM bm = h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
-        float m = a.M[e], p = a.P[e];
-        em_update(m, p, tx, bm, a.mu_m, a.mu_p, a.k_t, a.dt);
-        a.M[e] = m;
-        a.P[e] = p;
-        const float act = hill_act(p, a.Kn, a.hill_n, a.hill_int);
-        reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
-        const int src = a.src_of_gene[g];
-        if (src >= 0) a.act32_next[c * a.n_src + src] = act;
     }
 }
 
@@ -330,7 +347,9 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     const float alpha = 1.0f, beta = 0.0f;
     const int64_t n_steps = run_steps(o);
     const int pairs = (G + 1) / 2;
-    const unsigned b_step = (unsigned)(((int64_t)N * pairs + 255) / 256);
+    const dim3 g_step((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
+                      (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
+    if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");
     for (int64_t step = 1; step <= n_steps; ++step) {
         cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,
                                             st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
@@ -339,8 +358,13 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         a.step = (int)step;
         a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
         a.act32_next = st->tact32[step & 1].as<float>();
-        if (dtype == 0) tensor_step_kernel<__nv_bfloat16><<<b_step, 256, 0, s>>>(a);
-        else tensor_step_kernel<__half><<<b_step, 256, 0, s>>>(a);
+        if (dtype == 0) {
+            if (n->dev.bursty) tensor_step_kernel<__nv_bfloat16, true><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
+            else tensor_step_kernel<__nv_bfloat16, false><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
+        } else {
+            if (n->dev.bursty) tensor_step_kernel<__half, true><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
+            else tensor_step_kernel<__half, false><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
+        }
         CU(cudaGetLastError());
         ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
     }
