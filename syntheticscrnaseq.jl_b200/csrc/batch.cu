@@ -1,0 +1,247 @@
+// Batched CLE over many networks of uneven size (scrna_cle_simulate_batch).
+//
+// Networks are grouped by register-path kernel variant (warp-per-cell-group kernel with
+// its genes-per-lane and regulator class, or block tiles with their quads per thread) and
+// by population mode.  Each group runs as ONE persistent launch whose blocks pull
+// (network, cell tile, step range) items from a device work queue, largest items first,
+// so small and large networks share the GPU without per-network launches.  Groups run on
+// their own streams so they overlap.  Population groups advance chunk by chunk (a chunk
+// ends at a division check, the division itself happens in the chunk's epilogue); the
+// chunk launches of a group are captured once into a CUDA graph and replayed.
+// Large dense networks go to the tensor-core path one after another.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace scrna {
+
+namespace {
+
+struct BatchNet {
+    int b = 0;
+    scrna_net* net = nullptr;
+    const scrna_kinetics* kin = nullptr;
+    const scrna_population* pop = nullptr;
+    scrna_cle_opts o{};
+    scrna_state* st = nullptr;
+    KernelChoice kc{};
+    int64_t n_steps = 0;
+    bool tensor = false;
+};
+
+struct GroupKey {
+    int warp, gpl, nreg, upt, pop, interval;
+    int64_t n_steps;
+    bool operator<(const GroupKey& r) const {
+        return std::tie(warp, gpl, nreg, upt, pop, interval, n_steps) <
+               std::tie(r.warp, r.gpl, r.nreg, r.upt, r.pop, r.interval, r.n_steps);
+    }
+};
+
+struct Group {
+    GroupKey key{};
+    std::vector<BatchNet*> nets;
+    DevBuf args, items, counters;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    ~Group() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (done) cudaEventDestroy(done);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+int64_t cells_per_tile(const BatchNet& bn) {
+    if (bn.kc.warp) {
+        const int lpc = (bn.net->G + bn.kc.gpl - 1) / bn.kc.gpl;
+        return (int64_t)(32 / lpc) * 4;  // cells per warp x warps per block
+    }
+    return 32;
+}
+
+}  // namespace
+
+int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* cap);
+
+int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,
+                   int32_t n_kins, const int64_t* cell_nums, const scrna_population* const* pops,
+                   const scrna_capture* cap, const scrna_cle_opts* opts, double* const* outs,
+                   int32_t* const* counts) {
+    std::vector<BatchNet> bn(B);
+    std::vector<std::unique_ptr<scrna_state, int (*)(scrna_state*)>> owned;
+    for (int b = 0; b < B; ++b) {
+        BatchNet& x = bn[b];
+        x.b = b;
+        x.net = const_cast<scrna_net*>(nets[b]);
+        x.kin = &kins[n_kins == 1 ? 0 : b];
+        x.pop = pops ? pops[b] : nullptr;
+        x.o = *opts;
+        x.o.stream = (opts->stream + (uint32_t)b) & 0xFFFFFFu;
+        if (!x.pop) {
+            if (!cell_nums) return fail(SCRNA_EINVAL, "cell_nums is NULL");
+            x.o.cell_num = cell_nums[b];
+        }
+        if (!x.net) return fail(SCRNA_EINVAL, "network %d is NULL", b);
+        if (int r = validate_run(x.net, x.kin, x.pop, cap, &x.o)) return r;
+        const int64_t N = x.pop ? x.pop->cell_num : x.o.cell_num;
+        if (N <= 0) return fail(SCRNA_EINVAL, "network %d has no cells", b);
+        if (x.o.cell_offset < 0 || x.o.cell_offset + N > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
+        x.n_steps = n_steps_of(&x.o);
+        if (x.n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
+        scrna_state* st = nullptr;
+        if (int r = scrna_state_create(ctx, x.net, N, x.o.readout, cap != nullptr, &st)) return r;
+        owned.emplace_back(st, scrna_state_destroy);
+        x.st = st;
+        if (int r = ensure_gene_tables(x.net, x.kin, x.o.dt, x.pop != nullptr)) return r;
+        const NetDev& d = x.net->dev;
+        const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
+        x.tensor = !x.pop && (d.n_quads > fused_max_quads() || (x.net->G >= 256 && density >= 0.05));
+        if (!x.tensor) {
+            x.kc = choose_kernel(x.net, x.o.path);
+            if (x.kc.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
+            if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
+            x.st->have_counts = cap != nullptr;
+        }
+    }
+    std::vector<BatchNet*> ptrs;
+    for (auto& x : bn) ptrs.push_back(&x);
+    if (int r = run_batch(ctx, ptrs, cap)) return r;
+    for (int b = 0; b < B; ++b)
+        if (int r = scrna_state_read(ctx, bn[b].st, outs[b], (cap && counts) ? counts[b] : nullptr, nullptr)) return r;
+    return SCRNA_OK;
+}
+
+int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* cap) {
+    // dense networks: tensor-core path, one after another on the context stream
+    for (BatchNet* x : all)
+        if (x->tensor) {
+            x->st->last_tensor = true;
+            x->st->have_counts = cap != nullptr;
+            if (int r = tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)) return r;
+        }
+    // register-path networks: one persistent launch (or one captured chunk sequence) per group
+    std::map<GroupKey, std::unique_ptr<Group>> groups;
+    for (BatchNet* x : all) {
+        if (x->tensor) continue;
+        GroupKey k{};
+        k.warp = x->kc.warp;
+        k.gpl = x->kc.warp ? x->kc.gpl : 0;
+        k.nreg = x->kc.warp ? x->kc.nreg : 0;
+        k.upt = x->kc.warp ? 0 : x->kc.block.upt;
+        k.pop = x->pop != nullptr;
+        k.interval = x->pop ? x->pop->div_check_interval : 0;
+        k.n_steps = x->pop ? x->n_steps : 0;
+        auto& g = groups[k];
+        if (!g) { g.reset(new Group()); g->key = k; }
+        g->nets.push_back(x);
+    }
+    cudaEvent_t start;
+    CU(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    CU(cudaEventRecord(start, ctx->stream));
+    for (auto& kv : groups) {
+        Group& g = *kv.second;
+        const GroupKey& k = g.key;
+        CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+        CU(cudaStreamWaitEvent(g.stream, start, 0));
+        // kernel arguments of every network of the group, and its work items
+        std::vector<FusedArgs> args(g.nets.size());
+        std::vector<TileWork> items;
+        int nw = 1;
+        size_t smem = 0;
+        for (size_t i = 0; i < g.nets.size(); ++i) {
+            BatchNet* x = g.nets[i];
+            fill_fused_args(x->net, x->kin, x->pop, cap, &x->o, x->st, &args[i]);
+            nw = std::max(nw, x->kc.block.nw);
+            smem = std::max(smem, x->kc.smem);
+            const int64_t cpt = cells_per_tile(*x);
+            const int64_t tiles = (x->st->N + cpt - 1) / cpt;
+            for (int64_t t = 0; t < tiles; ++t) {
+                TileWork w{};
+                w.arg = (int32_t)i;
+                w.tile = (int32_t)t;
+                w.ctl = TileCtl{1, (int32_t)x->n_steps, 1, 1, 0, 0};
+                items.push_back(w);
+            }
+            if (x->pop)
+                for (int q = 0; q < 2; ++q) CU(cudaMemsetAsync(x->st->owner[q].p, 0, (size_t)x->st->N * 8, g.stream));
+        }
+        // longest items first: cost ~ genes x steps of the item's network
+        std::stable_sort(items.begin(), items.end(), [&](const TileWork& a, const TileWork& b) {
+            const BatchNet* xa = g.nets[a.arg];
+            const BatchNet* xb = g.nets[b.arg];
+            return (double)xa->net->G * xa->n_steps > (double)xb->net->G * xb->n_steps;
+        });
+        CU(g.args.ensure(args.size() * sizeof(FusedArgs)));
+        CU(g.items.ensure(items.size() * sizeof(TileWork)));
+        CU(cudaMemcpyAsync(g.args.p, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice, g.stream));
+        CU(cudaMemcpyAsync(g.items.p, items.data(), items.size() * sizeof(TileWork), cudaMemcpyHostToDevice, g.stream));
+        const int n_items = (int)items.size();
+        const int grid = std::max(1, std::min(n_items, ctx->sm_count * (k.warp ? 6 : 8)));
+        auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
+            if (k.warp)
+                return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
+                                             k.nreg, k.pop != 0, smem, grid, ctl, use_shared, g.stream);
+            return fused_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
+                                      smem, k.pop != 0, grid, ctl, use_shared, g.stream);
+        };
+        if (!k.pop) {
+            CU(g.counters.ensure(sizeof(int)));
+            CU(cudaMemsetAsync(g.counters.p, 0, sizeof(int), g.stream));
+            CU(launch(g.counters.as<int>(), TileCtl{}, 0));
+            ctx->launches++;
+        } else {
+            // chunk schedule shared by every network of the group
+            std::vector<TileCtl> chunks;
+            const int64_t I = k.interval, n_steps = k.n_steps;
+            int64_t s0 = 1;
+            int epoch = 0;
+            bool first = true;
+            while (true) {
+                const int64_t s1 = n_steps == 0 ? 0 : std::min(n_steps, ((s0 - 1) / I + 1) * I);
+                const bool check = s1 >= s0 && (s1 % I == 0);
+                const bool final_chunk = s1 >= n_steps;
+                chunks.push_back(TileCtl{(int32_t)s0, (int32_t)s1, first ? 1 : 0, (final_chunk && !check) ? 1 : 0,
+                                         check ? 1 : 0, epoch});
+                first = false;
+                if (check) epoch += 1;
+                if (final_chunk) {
+                    if (check) chunks.push_back(TileCtl{(int32_t)s1 + 1, (int32_t)s1, 0, 1, 0, epoch});
+                    break;
+                }
+                s0 = s1 + 1;
+            }
+            CU(g.counters.ensure(chunks.size() * sizeof(int)));
+            CU(cudaMemsetAsync(g.counters.p, 0, chunks.size() * sizeof(int), g.stream));
+            // capture the chunk launches once and replay them as one graph
+            cudaGraph_t graph;
+            CU(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeRelaxed));
+            cudaError_t le = cudaSuccess;
+            for (size_t c = 0; c < chunks.size() && le == cudaSuccess; ++c)
+                le = launch(g.counters.as<int>() + c, chunks[c], 1);
+            cudaError_t ce = cudaStreamEndCapture(g.stream, &graph);
+            if (le != cudaSuccess) { if (ce == cudaSuccess) cudaGraphDestroy(graph); CU(le); }
+            CU(ce);
+            cudaError_t ie = cudaGraphInstantiate(&g.graph, graph, 0);
+            cudaGraphDestroy(graph);
+            CU(ie);
+            CU(cudaGraphLaunch(g.graph, g.stream));
+            ctx->launches += (int64_t)chunks.size();
+        }
+        CU(cudaEventRecord(g.done, g.stream));
+        CU(cudaStreamWaitEvent(ctx->stream, g.done, 0));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    cudaEventDestroy(start);
+    return SCRNA_OK;
+}
+
+}  // namespace scrna

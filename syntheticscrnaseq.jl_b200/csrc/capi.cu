@@ -23,6 +23,8 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 int warpcell_max_genes();
 int warpcell_max_regs();
 int warpcell_pick_gpl(int G, bool bursty);
+int warpcell_nreg_class(int n_reg);
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_na, int n_na_src);
 cudaError_t warpcell_launch(const FusedArgs& a, const float* wdense, int gpl, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
@@ -70,7 +72,7 @@ static int check_ctx(scrna_ctx* ctx) {
     return SCRNA_OK;
 }
 
-static int set_device(scrna_ctx* ctx) {
+int scrna::set_device(scrna_ctx* ctx) {
     CU(cudaSetDevice(ctx->device));
     return SCRNA_OK;
 }
@@ -299,7 +301,7 @@ extern "C" int scrna_net_destroy(scrna_net* net) {
 extern "C" int32_t scrna_net_genes(const scrna_net* net) { return net ? net->G : -1; }
 
 // Per-run gene tables (thresholds depend on dt, initial values on the kinetics).
-static int ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt, bool pop) {
+int scrna::ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt, bool pop) {
     const double kv[6] = {kin->k_t, kin->K_d, kin->n, kin->mu_m, kin->mu_p, kin->dilution};
     if (n->cache_valid && n->c_dt == dt && n->c_pop == pop && std::memcmp(kv, n->c_kin, sizeof kv) == 0)
         return SCRNA_OK;
@@ -350,7 +352,7 @@ static int ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt
 }
 
 // ---- states ------------------------------------------------------------------------------------
-static int state_alloc(scrna_state* st, bool pop, bool plain) {
+int scrna::state_alloc(scrna_state* st, bool pop, bool plain) {
     const size_t gn = (size_t)st->G * st->N;
     const int outcols = st->readout == SCRNA_READOUT_BOTH ? 2 : 1;
     CU(st->M.ensure(gn * 4));
@@ -413,7 +415,7 @@ extern "C" int scrna_state_device_ptrs(scrna_state* st, void** m, void** p) {
 }
 
 // ---- run planning ---------------------------------------------------------------------------
-static int validate_run(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+int scrna::validate_run(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
                         const scrna_capture* cap, const scrna_cle_opts* o) {
     if (!net || !kin || !o) return fail(SCRNA_EINVAL, "net, kinetics and opts are required");
     if (!(o->dt > 0.0) || !std::isfinite(o->dt)) return fail(SCRNA_EINVAL, "dt must be positive and finite");
@@ -437,18 +439,15 @@ static int validate_run(const scrna_net* net, const scrna_kinetics* kin, const s
     return SCRNA_OK;
 }
 
-static int64_t n_steps_of(const scrna_cle_opts* o) {
+int64_t scrna::n_steps_of(const scrna_cle_opts* o) {
     if (o->n_steps > 0) return o->n_steps;
     return (int64_t)std::ceil(o->T / o->dt);  // cle.jl:56
 }
 
-static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
-                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st) {
+// Kernel arguments of one network's run (everything but the step range and flags).
+void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                            const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, FusedArgs* out) {
     const NetDev& d = net->dev;
-    if (d.n_quads > fused_max_quads())
-        return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
-    const int64_t n_steps = n_steps_of(o);
-    if (n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
     FusedArgs a{};
     a.G = d.G; a.n_quads = d.n_quads; a.n_reg = d.n_reg; a.n_in = d.n_in; a.n_na = d.n_na; a.n_na_src = d.n_na_src;
     a.N = st->N;
@@ -490,6 +489,32 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         a.cap_mu_log = std::log(cap->efficiency) - (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
         a.cap_sigma = cap->efficiency_std;
     }
+    a.wdense = d.wdense;
+    *out = a;
+}
+
+// Register-path kernel of a network: warp-per-cell-group (gpl, nreg class) or block tiles.
+scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
+    const NetDev& d = net->dev;
+    KernelChoice k{};
+    const bool warp_ok = d.wdense != nullptr;
+    k.warp = path == SCRNA_PATH_WARP ? true : path == SCRNA_PATH_BLOCK ? false : warp_ok;
+    k.gpl = warpcell_pick_gpl(d.G, d.bursty);
+    k.nreg = warpcell_nreg_class(d.n_reg);
+    k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
+    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na, d.n_na_src) : k.block.smem;
+    return k;
+}
+
+static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st) {
+    const NetDev& d = net->dev;
+    if (d.n_quads > fused_max_quads())
+        return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
+    const int64_t n_steps = n_steps_of(o);
+    if (n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
+    FusedArgs a{};
+    fill_fused_args(net, kin, pop, cap, o, st, &a);
     const FusedLaunch L = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
     if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
     cudaStream_t s = ctx->stream;
@@ -719,24 +744,9 @@ extern "C" int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_n
     if (int r = check_ctx(ctx)) return r;
     if (B <= 0 || !nets || !kins || !opts || !outs) return fail(SCRNA_EINVAL, "bad batch arguments");
     if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
-    std::vector<scrna_state*> states(B, nullptr);
-    int rc = SCRNA_OK;
-    for (int b = 0; b < B && rc == SCRNA_OK; ++b) {
-        const scrna_population* pop = pops ? pops[b] : nullptr;
-        scrna_cle_opts o = *opts;
-        o.stream = (opts->stream + (uint32_t)b) & 0xFFFFFFu;
-        if (!pop) {
-            if (!cell_nums) { rc = fail(SCRNA_EINVAL, "cell_nums is NULL"); break; }
-            o.cell_num = cell_nums[b];
-        }
-        const int64_t N = pop ? pop->cell_num : o.cell_num;
-        rc = scrna_state_create(ctx, nets[b], N, o.readout, cap != nullptr, &states[b]);
-        if (rc == SCRNA_OK) rc = scrna_cle_run_device(ctx, nets[b], &kins[n_kins == 1 ? 0 : b], pop, cap, &o, states[b]);
-    }
-    for (int b = 0; b < B && rc == SCRNA_OK; ++b)
-        rc = scrna_state_read(ctx, states[b], outs[b], (cap && counts) ? counts[b] : nullptr, nullptr);
-    for (auto* st : states) scrna_state_destroy(st);
-    return rc;
+    if (opts->precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "batches run the FP32 path");
+    if (int r = set_device(ctx)) return r;
+    return batch_simulate(ctx, B, nets, kins, n_kins, cell_nums, pops, cap, opts, outs, counts);
 }
 
 extern "C" int scrna_apply_capture(scrna_ctx* ctx, int64_t N, int32_t G, const double* X, const scrna_capture* cap,

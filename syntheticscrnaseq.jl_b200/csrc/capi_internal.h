@@ -16,6 +16,10 @@ namespace scrna {
 int fail(int code, const char* fmt, ...);
 }  // namespace scrna
 
+struct scrna_net;
+struct scrna_state;
+struct scrna_ctx;
+
 #define CU(call)                                                                          \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
@@ -105,3 +109,35 @@ struct scrna_state {
     const double* p64_final = nullptr;
 };
 
+
+namespace scrna {
+// Register-path kernel chosen for a network.
+struct KernelChoice {
+    bool warp;
+    int gpl, nreg;
+    FusedLaunch block;
+    size_t smem;
+};
+int set_device(scrna_ctx* ctx);
+int ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt, bool pop);
+int validate_run(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                 const scrna_capture* cap, const scrna_cle_opts* o);
+int64_t n_steps_of(const scrna_cle_opts* o);
+int state_alloc(scrna_state* st, bool pop, bool plain);
+void fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, FusedArgs* out);
+KernelChoice choose_kernel(const scrna_net* net, int path);
+int fused_max_quads();
+cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
+                               int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
+                               cudaStream_t st);
+cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
+                                  int nreg, bool pop, size_t smem, int grid, TileCtl shared_ctl, int use_shared,
+                                  cudaStream_t st);
+int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
+               const scrna_cle_opts* o, scrna_state* st, int dtype);
+int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,
+                   int32_t n_kins, const int64_t* cell_nums, const scrna_population* const* pops,
+                   const scrna_capture* cap, const scrna_cle_opts* opts, double* const* outs,
+                   int32_t* const* counts);
+}  // namespace scrna

@@ -42,10 +42,10 @@ __host__ __device__ inline size_t fused_smem_bytes(int G, int n_reg, int n_in, i
     return (b + 15) & ~(size_t)15;
 }
 
+// One cell tile (32 cells) of one network through the step range of `ctl`.
 template <int UPT, bool POP>
-__global__ void __launch_bounds__(UPT <= 2 ? 256 : 512)
-cle_fused_kernel(const FusedArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
+                                           unsigned char* smem_raw) {
     Smem sm;
     {
         unsigned char* p = smem_raw;
@@ -69,7 +69,7 @@ cle_fused_kernel(const FusedArgs a) {
     const int warp = tid >> 5;
     const int NW = nthr >> 5;
     const int64_t N = a.N;
-    const int64_t cell = (int64_t)blockIdx.x * 32 + lane;
+    const int64_t cell = tile * 32 + lane;
     const bool live = cell < N;
     const int64_t cidx = live ? cell : N - 1;  // dead lanes shadow the last cell, never store
     const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
@@ -83,7 +83,7 @@ cle_fused_kernel(const FusedArgs a) {
     double V = 0.0;
 
     // ---- prologue: initial condition or state of the previous chunk -------------
-    if (a.first) {
+    if (ctl.first) {
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
@@ -132,10 +132,10 @@ cle_fused_kernel(const FusedArgs a) {
         // A cell replaced at the previous division takes the daughter of its new owner.
         int64_t src = cidx;
         bool from_daughter = false;
-        const int par = a.epoch & 1;
-        if (POP && a.epoch > 0) {
+        const int par = ctl.epoch & 1;
+        if (POP && ctl.epoch > 0) {
             const unsigned long long o = a.owner[par][cidx];
-            if ((uint32_t)(o >> 32) == (uint32_t)a.epoch) {
+            if ((uint32_t)(o >> 32) == (uint32_t)ctl.epoch) {
                 src = (int64_t)(o & 0xFFFFFFFFull);
                 from_daughter = true;
             }
@@ -163,7 +163,7 @@ cle_fused_kernel(const FusedArgs a) {
     // ---- fused step loop ---------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     int buf = 0;
-    for (int s = a.step_begin; s <= a.step_end; ++s) {
+    for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
         // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
         // a gene switches when its waiting time runs out, then draws the next one
 #pragma unroll
@@ -246,16 +246,16 @@ cle_fused_kernel(const FusedArgs a) {
     }
 
     // ---- epilogue --------------------------------------------------------------------
-    if (POP && a.check) {
+    if (POP && ctl.check) {
         // division (cle.jl:240-273): partition in registers, daughters to the
         // next-epoch buffers, replaced slot claimed with a last-writer-wins max.
         const bool divides = V > a.V_div;
-        const int ne = a.epoch + 1;
+        const int ne = ctl.epoch + 1;
         const int par = ne & 1;
         if (divides) {
             V = V * 0.5;
             if (live && warp == 0) {
-                const uint4 w = philox((uint32_t)(a.cell_offset + cidx), (uint32_t)a.step_end, 0u,
+                const uint4 w = philox((uint32_t)(a.cell_offset + cidx), (uint32_t)ctl.step_end, 0u,
                                        tagword(TAG_MORAN, a.stream), key);
                 int64_t r;
                 if (a.exclude_mother) {
@@ -281,8 +281,8 @@ cle_fused_kernel(const FusedArgs a) {
                     } else {  // binomial split of rounded counts
                         const int64_t mi = (int64_t)rintf(m[j][i]);
                         const int64_t pi = (int64_t)rintf(p[j][i]);
-                        const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 0u);
-                        const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 1u);
+                        const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)ctl.step_end, (uint32_t)g, 0u);
+                        const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)ctl.step_end, (uint32_t)g, 1u);
                         mm = (float)mk; dm = (float)(mi - mk);
                         pm = (float)pk; dp = (float)(pi - pk);
                     }
@@ -297,9 +297,9 @@ cle_fused_kernel(const FusedArgs a) {
                     int32_t dns = kNever;
                     const GeneRec gr = sm.genes[g];
                     if (gr.inv_off == gr.inv_off) {
-                        const uint4 w = philox(gcell, (uint32_t)a.step_end, (uint32_t)g | kDaughterSwitch,
+                        const uint4 w = philox(gcell, (uint32_t)ctl.step_end, (uint32_t)g | kDaughterSwitch,
                                                tagword(TAG_SWITCH, a.stream), key);
-                        dns = next_switch(a.step_end, w.x, bon ? gr.inv_off : gr.inv_on);
+                        dns = next_switch(ctl.step_end, w.x, bon ? gr.inv_off : gr.inv_on);
                     }
                     a.dNS[par][idx] = dns;
                 }
@@ -307,7 +307,7 @@ cle_fused_kernel(const FusedArgs a) {
         }
     }
     if (!live) return;
-    const bool write_state = !a.last || POP;
+    const bool write_state = !ctl.last || POP;
 #pragma unroll
     for (int j = 0; j < UPT; ++j) {
         const int q = warp + j * NW;
@@ -316,13 +316,13 @@ cle_fused_kernel(const FusedArgs a) {
             const int g = 4 * q + i;
             if (!(q < a.n_quads && g < G)) continue;
             const size_t idx = (size_t)g * N + cell;
-            if (write_state || a.last) {
+            if (write_state || ctl.last) {
                 a.M[idx] = m[j][i];
                 a.P[idx] = p[j][i];
                 a.prom[idx] = (on >> (4 * j + i)) & 1u;
                 a.NS[idx] = ns[j][i];
             }
-            if (a.last && a.out) {
+            if (ctl.last && a.out) {
                 if (a.readout == 0) a.out[idx] = (double)m[j][i];
                 else if (a.readout == 1) a.out[idx] = (double)p[j][i];
                 else { a.out[idx] = (double)m[j][i]; a.out[(size_t)(G + g) * N + cell] = (double)p[j][i]; }
@@ -330,7 +330,7 @@ cle_fused_kernel(const FusedArgs a) {
         }
     }
     if (POP && warp == 0) a.V[cell] = V;
-    if (a.last && a.counts) {
+    if (ctl.last && a.counts) {
         // capture (capture.jl:30-44): per-cell LogNormal efficiency, then inverse-CDF binomials
         const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, a.stream), key);
         const double z = box_muller_z0_f64(w.x, w.y);
@@ -355,12 +355,49 @@ cle_fused_kernel(const FusedArgs a) {
 }
 
 template <int UPT, bool POP>
+__global__ void __launch_bounds__(UPT <= 2 ? 256 : 512) cle_fused_kernel(const FusedArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
+    fused_tile<UPT, POP>(a, blockIdx.x, ctl, smem_raw);
+}
+
+// Persistent form: blocks pull (network, tile, step range) items from a device work queue
+// until it is empty; items of different networks and sizes share one launch.
+template <int UPT, bool POP>
+__global__ void __launch_bounds__(UPT <= 2 ? 256 : 512)
+cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
+                       TileCtl shared_ctl, int use_shared) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int next;
+    while (true) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = next;
+        __syncthreads();
+        if (it >= n_items) return;
+        const TileWork w = items[it];
+        fused_tile<UPT, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        __syncthreads();
+    }
+}
+
+template <int UPT, bool POP>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st) {
     auto k = cle_fused_kernel<UPT, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)((a.N + 31) / 32);
     k<<<blocks, nw * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int UPT, bool POP>
+cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
+                                 int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
+    auto k = cle_fused_queue_kernel<UPT, POP>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, nw * 32, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
     return cudaGetLastError();
 }
 

@@ -75,6 +75,7 @@ struct FusedArgs {
     const NonAdd* na;
     const int32_t* na_src;
     const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
+    const float* wdense;         // [G][n_reg] dense regulation rows (warp kernel), or null
     // state [G][N]
     float* M;
     float* P;
@@ -95,6 +96,19 @@ struct FusedArgs {
     double* eff;            // cells, nullable
     int32_t capture_species;
     double cap_mu_log, cap_sigma;
+};
+
+// Step range and division flags of one launch (or one queued work item).
+struct TileCtl {
+    int32_t step_begin, step_end, first, last, check, epoch;
+};
+
+// One item of a persistent launch's work queue: a cell tile of network `arg` (index into
+// the launch's FusedArgs array) advanced through a step range.
+struct TileWork {
+    int32_t arg;
+    int32_t tile;
+    TileCtl ctl;
 };
 
 // Launch shape of the fused kernel chosen for a network: quads per thread (UPT),

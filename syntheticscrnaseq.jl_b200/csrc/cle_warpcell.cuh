@@ -40,10 +40,11 @@ __device__ __forceinline__ uint32_t quad_word(const uint4& w, int u, int i) {
     return i == 0 ? (hi ? w.z : w.x) : (hi ? w.w : w.y);
 }
 
+// One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
 template <int GPL, int NREG, bool POP>
-__global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
-cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
+                                              unsigned char* smem_raw) {
+    const float* __restrict__ wdense = a.wdense;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
     const int cpw = 32 / lpc;
@@ -62,7 +63,7 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     const bool lane_ok = cl < cpw;
     if (!lane_ok) cl = cpw;  // spare lanes work on a private dummy row
     const int64_t N = a.N;
-    const int64_t cell = ((int64_t)blockIdx.x * kWarpcellWarps + warp) * cpw + (lane_ok ? cl : 0);
+    const int64_t cell = (tile * kWarpcellWarps + warp) * cpw + (lane_ok ? cl : 0);
     const bool live = lane_ok && cell < N;
     const int64_t cidx = cell < N ? cell : N - 1;
     const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
@@ -98,7 +99,7 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     double V = 0.0;
 
     // ---- prologue (as cle_fused_kernel) ----------------------------------------------
-    if (a.first) {
+    if (ctl.first) {
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
             const int g = u * GPL + i;
@@ -132,10 +133,10 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     } else {
         int64_t src = cidx;
         bool from_daughter = false;
-        const int par = a.epoch & 1;
-        if (POP && a.epoch > 0) {
+        const int par = ctl.epoch & 1;
+        if (POP && ctl.epoch > 0) {
             const unsigned long long o = a.owner[par][cidx];
-            if ((uint32_t)(o >> 32) == (uint32_t)a.epoch) {
+            if ((uint32_t)(o >> 32) == (uint32_t)ctl.epoch) {
                 src = (int64_t)(o & 0xFFFFFFFFull);
                 from_daughter = true;
             }
@@ -158,7 +159,7 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     // ---- fused step loop --------------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     int buf = 0;
-    for (int s = a.step_begin; s <= a.step_end; ++s) {
+    for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {  // telegraph: switch when the waiting time runs out
             if (s == ns[i]) {
@@ -214,14 +215,14 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
     }
 
     // ---- epilogue (as cle_fused_kernel) ------------------------------------------------
-    if (POP && a.check) {
+    if (POP && ctl.check) {
         const bool divides = V > a.V_div;
-        const int ne = a.epoch + 1;
+        const int ne = ctl.epoch + 1;
         const int par = ne & 1;
         if (divides) {
             V = V * 0.5;
             if (live && u == 0) {
-                const uint4 w = philox(gcell, (uint32_t)a.step_end, 0u, tagword(TAG_MORAN, a.stream), key);
+                const uint4 w = philox(gcell, (uint32_t)ctl.step_end, 0u, tagword(TAG_MORAN, a.stream), key);
                 int64_t r;
                 if (a.exclude_mother) {
                     r = (int64_t)(((uint64_t)w.x * (uint64_t)(N - 1)) >> 32);
@@ -243,8 +244,8 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
                 } else {
                     const int64_t mi = (int64_t)rintf(m[i]);
                     const int64_t pi = (int64_t)rintf(p[i]);
-                    const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 0u);
-                    const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)a.step_end, (uint32_t)g, 1u);
+                    const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)ctl.step_end, (uint32_t)g, 0u);
+                    const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)ctl.step_end, (uint32_t)g, 1u);
                     mm = (float)mk; dm = (float)(mi - mk);
                     pm = (float)pk; dp = (float)(pi - pk);
                 }
@@ -257,9 +258,9 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
                 a.dprom[par][idx] = bon;
                 int32_t dns = kNever;  // the daughter's promoter switches independently
                 if (inv_off[i] == inv_off[i]) {
-                    const uint4 w = philox(gcell, (uint32_t)a.step_end, (uint32_t)g | kDaughterSwitch,
+                    const uint4 w = philox(gcell, (uint32_t)ctl.step_end, (uint32_t)g | kDaughterSwitch,
                                            tagword(TAG_SWITCH, a.stream), key);
-                    dns = next_switch(a.step_end, w.x, bon ? inv_off[i] : inv_on[i]);
+                    dns = next_switch(ctl.step_end, w.x, bon ? inv_off[i] : inv_on[i]);
                 }
                 a.dNS[par][idx] = dns;
             }
@@ -275,14 +276,14 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
         a.P[idx] = p[i];
         a.prom[idx] = (on >> i) & 1u;
         a.NS[idx] = ns[i];
-        if (a.last && a.out) {
+        if (ctl.last && a.out) {
             if (a.readout == 0) a.out[idx] = (double)m[i];
             else if (a.readout == 1) a.out[idx] = (double)p[i];
             else { a.out[idx] = (double)m[i]; a.out[(size_t)(G + g) * N + cell] = (double)p[i]; }
         }
     }
     if (POP && u == 0) a.V[cell] = V;
-    if (a.last && a.counts) {
+    if (ctl.last && a.counts) {
         const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, a.stream), key);
         const double z = box_muller_z0_f64(w.x, w.y);
         double pe = exp(a.cap_mu_log + a.cap_sigma * z);
@@ -302,14 +303,49 @@ cle_warpcell_kernel(const FusedArgs a, const float* __restrict__ wdense) {
 }
 
 template <int GPL, int NREG, bool POP>
-cudaError_t warpcell_launch_t(const FusedArgs& a, const float* wdense, cudaStream_t st) {
+__global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
+    warpcell_tile<GPL, NREG, POP>(a, blockIdx.x, ctl, smem_raw);
+}
+
+template <int GPL, int NREG, bool POP>
+__global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
+cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
+                       TileCtl shared_ctl, int use_shared) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int next;
+    while (true) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = next;
+        __syncthreads();
+        if (it >= n_items) return;
+        const TileWork w = items[it];
+        warpcell_tile<GPL, NREG, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        __syncthreads();
+    }
+}
+
+template <int GPL, int NREG, bool POP>
+cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     auto k = cle_warpcell_kernel<GPL, NREG, POP>;
     const size_t smem = warpcell_smem_bytes<NREG>(a.G, GPL, a.n_na, a.n_na_src);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
     const unsigned blocks = (unsigned)((a.N + cpb - 1) / cpb);
-    k<<<blocks, 32 * kWarpcellWarps, smem, st>>>(a, wdense);
+    k<<<blocks, 32 * kWarpcellWarps, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int GPL, int NREG, bool POP>
+cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
+                                    size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
+    auto k = cle_warpcell_queue_kernel<GPL, NREG, POP>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, 32 * kWarpcellWarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
     return cudaGetLastError();
 }
 

@@ -2,10 +2,22 @@
 #include "cle_warpcell.cuh"
 
 namespace scrna {
-template cudaError_t warpcell_launch_t<4, 4, false>(const FusedArgs&, const float*, cudaStream_t);
-template cudaError_t warpcell_launch_t<4, 4, true>(const FusedArgs&, const float*, cudaStream_t);
-template cudaError_t warpcell_launch_t<4, 8, false>(const FusedArgs&, const float*, cudaStream_t);
-template cudaError_t warpcell_launch_t<4, 8, true>(const FusedArgs&, const float*, cudaStream_t);
-template cudaError_t warpcell_launch_t<4, 16, false>(const FusedArgs&, const float*, cudaStream_t);
-template cudaError_t warpcell_launch_t<4, 16, true>(const FusedArgs&, const float*, cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 4, false>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 4, false>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 4, true>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 4, true>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 8, false>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 8, false>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 8, true>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 8, true>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 16, false>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 16, false>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
+template cudaError_t warpcell_launch_t<4, 16, true>(const FusedArgs&, cudaStream_t);
+template cudaError_t warpcell_queue_launch_t<4, 16, true>(const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int,
+                                                              cudaStream_t);
 }  // namespace scrna

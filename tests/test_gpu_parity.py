@@ -257,3 +257,24 @@ def test_warp_and_block_kernels_identical_population(pkg, partition):
         outs.append(run.read_raw())
     for k in ("M", "P", "prom", "V"):
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_batch_mixed_population_equals_single_runs(pkg):
+    """Uneven networks, some with Moran populations, in one batch call (persistent launches
+    per kernel group, captured population chunks) give the same results as single runs."""
+    rng = np.random.default_rng(0)
+    kin = pkg.WORKLOAD_KINETICS
+    nets, cells, pops = [], [], []
+    for b in range(14):
+        G = int(rng.choice([2, 5, 9, 16, 31, 40, 77]))
+        nets.append(pkg.sample_network(G, seed=100 + b, bursty=bool(b % 3 == 0)))
+        N = int(rng.integers(40, 900))
+        cells.append(N)
+        pops.append(pkg.PopulationConfig(cell_num=N, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                                         div_check_interval=10) if b % 2 else None)
+    outs = pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=1.25, readout="both", seed=9,
+                                  stream=3, populations=pops)
+    for b in range(len(nets)):
+        single = pkg.simulate(nets[b], pkg.CLE(0.01), kin, population=pops[b], cell_num=cells[b], T=1.25,
+                              readout="both", seed=9, stream=3 + b)
+        assert np.array_equal(outs[b], single), b
