@@ -193,6 +193,52 @@ int scrna_state_device_ptrs(scrna_state* st, void** d_mrna, void** d_protein);
 int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* protein,
                          uint8_t* promoter, double* volume);
 
+/* ---- serving loop ---------------------------------------------------------------------
+ * A request server with continuous batching (no counterpart in the reference, which runs
+ * one simulate call at a time).  Submitted requests wait in a FIFO queue until their device
+ * footprint fits the HBM budget, then join the running set at the next chunk boundary: every
+ * chunk advances all running requests by up to `chunk_steps` Euler steps in shared
+ * persistent launches.  Requests keep their state on the device between chunks; results are
+ * identical to scrna_cle_simulate on the same inputs, alone or in any mix.  Population
+ * dynamics are not served (SCRNA_ENOTSUP). */
+typedef struct scrna_server scrna_server;
+
+typedef struct {
+    const scrna_net* net;
+    scrna_kinetics kin;
+    scrna_cle_opts opts;      /* cell_num, T or n_steps, readout, seed, stream, dt */
+    int32_t with_capture;
+    int32_t reserved;
+    scrna_capture capture;
+} scrna_request;
+
+enum scrna_request_state {
+    SCRNA_REQ_QUEUED = 0, SCRNA_REQ_RUNNING = 1, SCRNA_REQ_DONE = 2, SCRNA_REQ_FAILED = 3,
+    SCRNA_REQ_CANCELLED = 4
+};
+
+typedef struct {
+    int64_t submitted, completed, failed, queued, running;
+    int64_t units_done;       /* cell-gene-steps of completed requests */
+    int64_t bytes_in_use;     /* device footprint of admitted requests */
+    double busy_s;            /* wall time the worker spent with work in flight */
+    int64_t chunks;           /* chunk launches issued */
+} scrna_server_stats;
+
+/* hbm_budget_bytes <= 0: 80 % of the free device memory at creation. */
+int scrna_server_create(scrna_ctx* ctx, int64_t hbm_budget_bytes, int32_t chunk_steps, scrna_server** out);
+int scrna_server_destroy(scrna_server* srv);
+/* Non-blocking.  The network handle must stay alive until the request completes. */
+int scrna_submit(scrna_server* srv, const scrna_request* req, uint64_t* ticket);
+int scrna_poll(scrna_server* srv, uint64_t ticket, int32_t* state);
+/* Waits up to timeout_ms (< 0: forever) for the request, copies its results to the host
+ * (out: cells x G (x2) column-major; counts/efficiencies with capture, nullable) and
+ * releases it.  Returns SCRNA_ETIMEOUT if it is not done in time (the request stays). */
+int scrna_wait(scrna_server* srv, uint64_t ticket, int32_t timeout_ms, double* out, int32_t* counts,
+               double* efficiencies, double* latency_s);
+int scrna_cancel(scrna_server* srv, uint64_t ticket);
+int scrna_server_get_stats(scrna_server* srv, scrna_server_stats* stats);
+
 /* ---- scratch-free run ---------------------------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers that
  * cannot allocate device memory when they run a simulation (the allocator is owned

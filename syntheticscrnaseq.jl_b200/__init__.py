@@ -11,7 +11,7 @@ from .model import (CLE, INF, CaptureModel, CoopEdge, GeneNetwork, KineticParams
                     precompute_hill_matrices, steady_state)
 from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
                       dense_network, sample_network)
-from .api import (Context, DeviceRun, NetHandle, apply_capture, debug_philox, default_context,
+from .api import (Context, DeviceRun, NetHandle, Server, apply_capture, debug_philox, default_context,
                   measure_pipe_peaks, simulate, simulate_gpu_batch)
 from ._lib import ScrnaError
 
@@ -20,6 +20,6 @@ __all__ = [
     "default_algorithm", "hill_activation", "hill_repression", "is_bursty", "n_steps",
     "precompute_hill_matrices", "steady_state", "sample_network", "dense_network", "config0", "config1",
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
-    "NetHandle", "apply_capture", "debug_philox", "default_context", "measure_pipe_peaks", "simulate",
+    "NetHandle", "Server", "apply_capture", "debug_philox", "default_context", "measure_pipe_peaks", "simulate",
     "simulate_gpu_batch", "ScrnaError", "INF",
 ]

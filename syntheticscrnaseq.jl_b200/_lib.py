@@ -47,6 +47,17 @@ class Opts(C.Structure):
                 ("cell_offset", C.c_int64)]
 
 
+class Request(C.Structure):
+    _fields_ = [("net", C.c_void_p), ("kin", Kinetics), ("opts", Opts), ("with_capture", C.c_int32),
+                ("reserved", C.c_int32), ("capture", Capture)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "queued", "running",
+                                          "units_done", "bytes_in_use")] + \
+               [("busy_s", C.c_double), ("chunks", C.c_int64)]
+
+
 P = C.c_void_p
 I32, I64, U32, U64, DBL = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
 
@@ -73,6 +84,13 @@ SIGNATURES = {
     "scrna_state_device_ptrs": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "scrna_state_read_raw": (C.c_int, [P, P, P, P, P, P]),
     "scrna_cle_simulate_noalloc": (C.c_int, [P, P, P, P, P, P, P, P, P]),
+    "scrna_server_create": (C.c_int, [P, I64, I32, C.POINTER(P)]),
+    "scrna_server_destroy": (C.c_int, [P]),
+    "scrna_submit": (C.c_int, [P, P, C.POINTER(U64)]),
+    "scrna_poll": (C.c_int, [P, U64, C.POINTER(I32)]),
+    "scrna_wait": (C.c_int, [P, U64, I32, P, P, P, C.POINTER(DBL)]),
+    "scrna_cancel": (C.c_int, [P, U64]),
+    "scrna_server_get_stats": (C.c_int, [P, P]),
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),
 }

@@ -316,3 +316,71 @@ def measure_pipe_peaks(ctx: Optional[Context] = None):
     a, b, c = C.c_double(), C.c_double(), C.c_double()
     check(ctx.lib.scrna_measure_pipe_peaks(ctx.h, C.byref(a), C.byref(b), C.byref(c)))
     return a.value, b.value, c.value
+
+
+class Server:
+    """Request server with continuous batching (scrna_server_*): requests are admitted by
+    device footprint, keep their state on the GPU and advance in shared chunks of
+    `chunk_steps` Euler steps; `wait` returns the same results `simulate` gives."""
+
+    STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+    def __init__(self, ctx: Optional[Context] = None, *, hbm_budget_bytes: int = 0, chunk_steps: int = 250):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(self.ctx.lib.scrna_server_create(self.ctx.h, int(hbm_budget_bytes), int(chunk_steps), C.byref(h)))
+        self.h = h
+        self._meta = {}
+
+    def submit(self, handle: NetHandle, alg: CLE, kin: KineticParams, *, cell_num: int, T: float = 50.0,
+               readout: str = "protein", seed: int = 0, stream: int = 0, capture: Optional[CaptureModel] = None,
+               n_steps: int = 0, cell_offset: int = 0) -> int:
+        req = _lib.Request()
+        req.net = handle.h
+        req.kin = _kin(kin)
+        req.opts = _opts(alg, T=T, cell_num=cell_num, readout=readout, seed=seed, stream=stream, precision="fp32",
+                         path="auto", n_steps=n_steps, cell_offset=cell_offset)
+        if capture is not None:
+            req.with_capture = 1
+            req.capture = _cap(capture)
+        t = C.c_uint64()
+        check(self.ctx.lib.scrna_submit(self.h, C.byref(req), C.byref(t)))
+        self._meta[t.value] = (handle, int(cell_num), handle.G * (2 if readout == "both" else 1), capture is not None)
+        return t.value
+
+    def poll(self, ticket: int) -> str:
+        st = C.c_int32()
+        check(self.ctx.lib.scrna_poll(self.h, int(ticket), C.byref(st)))
+        return self.STATES[st.value]
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(readout, counts, efficiencies, latency_s); counts/efficiencies are None without capture."""
+        handle, N, cols, cap = self._meta[ticket]
+        out = np.empty((N, cols), dtype=np.float64, order="F")
+        counts = np.empty((N, handle.G), dtype=np.int32, order="F") if cap else None
+        eff = np.empty(N, dtype=np.float64) if cap else None
+        lat = C.c_double()
+        check(self.ctx.lib.scrna_wait(self.h, int(ticket), int(timeout_ms), out.ctypes.data,
+                                      None if counts is None else counts.ctypes.data,
+                                      None if eff is None else eff.ctypes.data, C.byref(lat)))
+        del self._meta[ticket]
+        return out, counts, eff, lat.value
+
+    def cancel(self, ticket: int):
+        check(self.ctx.lib.scrna_cancel(self.h, int(ticket)))
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        check(self.ctx.lib.scrna_server_get_stats(self.h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.scrna_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

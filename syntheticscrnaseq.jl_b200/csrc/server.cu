@@ -1,0 +1,391 @@
+// Serving loop with continuous batching (scrna_server_*).
+//
+// A worker thread owns the device side.  Submitted requests queue FIFO; at every chunk
+// boundary the worker admits queued requests while their device footprint fits the HBM
+// budget, then advances every running request by up to chunk_steps Euler steps with one
+// persistent work-queue launch per register-path kernel group (the same kernels as
+// scrna_cle_simulate).  State stays on the device between chunks, so a request's result
+// does not depend on what else runs beside it.  Finished requests keep their outputs on
+// the device until scrna_wait copies them out and releases the memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace scrna {
+void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr, GeneInit* gi,
+                      uint8_t* qt);
+}
+
+using namespace scrna;
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct SrvRequest {
+    uint64_t ticket = 0;
+    scrna_request req{};
+    scrna_net* net = nullptr;
+    int64_t N = 0, n_steps = 0, next = 1;
+    scrna_state* st = nullptr;
+    DevBuf genes, ginit, qtel;
+    FusedArgs args{};
+    KernelChoice kc{};
+    int state = SCRNA_REQ_QUEUED;
+    int64_t footprint = 0;
+    double t_submit = 0, t_done = 0;
+    std::string error;
+    int64_t s0 = 0, s1 = 0;  // step range of the chunk in flight
+    bool admitted = false;   // counted in the server's bytes in use
+    bool cancel = false;     // cancellation requested while running (applied between chunks)
+};
+
+int64_t footprint_of(const scrna_net* n, int64_t N, int readout, bool cap) {
+    const int64_t gn = (int64_t)n->G * N;
+    int64_t b = gn * (4 + 4 + 1 + 4);                     // M, P, promoter, next switch
+    b += gn * 8 * (readout == SCRNA_READOUT_BOTH ? 2 : 1);  // readout
+    if (cap) b += gn * 4 + N * 8;
+    return b + (1 << 16);
+}
+
+}  // namespace
+
+struct scrna_server {
+    scrna_ctx* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<SrvRequest*> queue;
+    std::vector<SrvRequest*> active;
+    std::map<uint64_t, SrvRequest*> reqs;
+    int64_t budget = 0, used = 0;
+    int chunk_steps = 250;
+    bool stop = false;
+    uint64_t next_ticket = 1;
+    scrna_server_stats stats{};
+    DevBuf args_dev, items_dev, counters_dev;
+    void run();
+};
+
+static void release(SrvRequest* r) {
+    if (r->st) scrna_state_destroy(r->st);
+    delete r;
+}
+
+// Device setup of an admitted request (worker thread).
+static int setup_request(scrna_server* s, SrvRequest* r) {
+    const scrna_net* n = r->net;
+    if (int rr = scrna_state_create(s->ctx, n, r->N, r->req.opts.readout, r->req.with_capture, &r->st)) return rr;
+    if (int rr = state_alloc(r->st, false, false)) return rr;
+    r->st->have_counts = r->req.with_capture != 0;
+    const int G = n->G;
+    std::vector<GeneRec> gr(G);
+    std::vector<GeneInit> gi(G);
+    std::vector<uint8_t> qt((G + 3) / 4);
+    gene_tables_host(n, &r->req.kin, r->req.opts.dt, gr.data(), gi.data(), qt.data());
+    CU(r->genes.ensure(G * sizeof(GeneRec)));
+    CU(r->ginit.ensure(G * sizeof(GeneInit)));
+    CU(r->qtel.ensure(qt.size()));
+    CU(cudaMemcpy(r->genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(r->ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(r->qtel.p, qt.data(), qt.size(), cudaMemcpyHostToDevice));
+    r->kc = choose_kernel(n, r->req.opts.path);
+    fill_fused_args(r->net, &r->req.kin, nullptr, r->req.with_capture ? &r->req.capture : nullptr, &r->req.opts,
+                    r->st, &r->args);
+    r->args.genes = r->genes.as<GeneRec>();
+    r->args.ginit = r->ginit.as<GeneInit>();
+    r->args.quad_tel = r->qtel.as<uint8_t>();
+    return SCRNA_OK;
+}
+
+void scrna_server::run() {
+    cudaSetDevice(ctx->device);
+    std::vector<FusedArgs> h_args;
+    std::vector<TileWork> h_items;
+    for (;;) {
+        std::vector<SrvRequest*> admitted;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_work.wait(lk, [&] { return stop || !queue.empty() || !active.empty(); });
+            if (stop) break;
+            // cancellations of running requests take effect between chunks
+            for (size_t i = 0; i < active.size();) {
+                if (active[i]->cancel) {
+                    active[i]->state = SCRNA_REQ_CANCELLED;
+                    active.erase(active.begin() + i);
+                    cv_done.notify_all();
+                } else {
+                    ++i;
+                }
+            }
+            // FIFO admission by device footprint
+            while (!queue.empty()) {
+                SrvRequest* r = queue.front();
+                if (r->state == SCRNA_REQ_CANCELLED) { queue.pop_front(); continue; }
+                if (r->footprint > budget) {
+                    r->state = SCRNA_REQ_FAILED;
+                    r->error = "request does not fit the device memory budget";
+                    queue.pop_front();
+                    stats.failed++;
+                    cv_done.notify_all();
+                    continue;
+                }
+                if (used + r->footprint > budget) break;
+                used += r->footprint;
+                r->admitted = true;
+                queue.pop_front();
+                admitted.push_back(r);
+            }
+        }
+        for (SrvRequest* r : admitted) {
+            const int rc = setup_request(this, r);
+            std::lock_guard<std::mutex> lk(mu);
+            if (rc != SCRNA_OK) {
+                r->state = SCRNA_REQ_FAILED;
+                r->error = scrna_last_error();
+                stats.failed++;
+                cv_done.notify_all();
+            } else {
+                r->state = SCRNA_REQ_RUNNING;
+                active.push_back(r);
+            }
+        }
+        std::vector<SrvRequest*> run_set;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            run_set = active;
+        }
+        if (run_set.empty()) continue;
+        const double t_chunk = now_s();
+        // one persistent launch per kernel group over the running requests' tiles
+        h_args.clear();
+        std::map<std::tuple<int, int, int, int>, std::vector<TileWork>> groups;
+        std::map<std::tuple<int, int, int, int>, std::pair<int, size_t>> shape;  // nw, smem
+        for (size_t i = 0; i < run_set.size(); ++i) {
+            SrvRequest* r = run_set[i];
+            h_args.push_back(r->args);
+            r->s0 = r->next;
+            r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps - 1);
+            const KernelChoice& kc = r->kc;
+            auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.nreg : 0, kc.warp ? 0 : kc.block.upt);
+            int64_t cpt = 32;
+            if (kc.warp) cpt = (int64_t)(32 / ((r->net->G + kc.gpl - 1) / kc.gpl)) * 4;
+            const int64_t tiles = (r->N + cpt - 1) / cpt;
+            TileCtl ctl{(int32_t)r->s0, (int32_t)r->s1, r->s0 == 1 ? 1 : 0, r->s1 >= r->n_steps ? 1 : 0, 0, 0};
+            auto& items = groups[key];
+            for (int64_t t = 0; t < tiles; ++t) items.push_back(TileWork{(int32_t)i, (int32_t)t, ctl});
+            auto& sh = shape[key];
+            sh.first = std::max(sh.first, kc.warp ? 1 : kc.block.nw);
+            sh.second = std::max(sh.second, kc.smem);
+        }
+        h_items.clear();
+        std::vector<size_t> offsets;
+        for (auto& kv : groups) {
+            offsets.push_back(h_items.size());
+            h_items.insert(h_items.end(), kv.second.begin(), kv.second.end());
+        }
+        int rc = SCRNA_OK;
+        cudaError_t e = cudaSuccess;
+        if ((e = args_dev.ensure(h_args.size() * sizeof(FusedArgs))) != cudaSuccess ||
+            (e = items_dev.ensure(h_items.size() * sizeof(TileWork))) != cudaSuccess ||
+            (e = counters_dev.ensure(groups.size() * sizeof(int))) != cudaSuccess ||
+            (e = cudaMemcpyAsync(args_dev.p, h_args.data(), h_args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(items_dev.p, h_items.data(), h_items.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(counters_dev.p, 0, groups.size() * sizeof(int), stream)) != cudaSuccess)
+            rc = SCRNA_ECUDA;
+        size_t gi = 0;
+        for (auto& kv : groups) {
+            if (rc != SCRNA_OK) break;
+            const auto& key = kv.first;
+            const int n_items = (int)kv.second.size();
+            const TileWork* items = items_dev.as<TileWork>() + offsets[gi];
+            int* counter = counters_dev.as<int>() + gi;
+            const auto& sh = shape[key];
+            const int grid = std::max(1, std::min(n_items, ctx->sm_count * (std::get<0>(key) ? 6 : 8)));
+            if (std::get<0>(key))
+                e = warpcell_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<1>(key),
+                                          std::get<2>(key), false, sh.second, grid, TileCtl{}, 0, stream);
+            else
+                e = fused_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<3>(key), sh.first,
+                                       sh.second, false, grid, TileCtl{}, 0, stream);
+            if (e != cudaSuccess) rc = SCRNA_ECUDA;
+            ++gi;
+        }
+        if (rc == SCRNA_OK && (e = cudaStreamSynchronize(stream)) != cudaSuccess) rc = SCRNA_ECUDA;
+        const double t_end = now_s();
+        std::lock_guard<std::mutex> lk(mu);
+        stats.busy_s += t_end - t_chunk;
+        stats.chunks += (int64_t)groups.size();
+        ctx->launches += (int64_t)groups.size();
+        for (SrvRequest* r : run_set) {
+            if (r->state != SCRNA_REQ_RUNNING) continue;
+            if (rc != SCRNA_OK) {
+                r->state = SCRNA_REQ_FAILED;
+                r->error = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+                stats.failed++;
+            } else {
+                r->next = r->s1 + 1;
+                if (r->s1 >= r->n_steps) {
+                    r->state = SCRNA_REQ_DONE;
+                    r->t_done = t_end;
+                    stats.completed++;
+                    stats.units_done += (int64_t)r->net->G * r->N * r->n_steps;
+                }
+            }
+        }
+        for (size_t i = 0; i < active.size();) {
+            if (active[i]->state != SCRNA_REQ_RUNNING) active.erase(active.begin() + i);
+            else ++i;
+        }
+        cv_done.notify_all();
+    }
+}
+
+extern "C" int scrna_server_create(scrna_ctx* ctx, int64_t budget, int32_t chunk_steps, scrna_server** out) {
+    if (!ctx || !out) return fail(SCRNA_EINVAL, "ctx/out is NULL");
+    if (chunk_steps <= 0) return fail(SCRNA_EINVAL, "chunk_steps must be positive");
+    if (int r = set_device(ctx)) return r;
+    auto* s = new scrna_server();
+    s->ctx = ctx;
+    s->chunk_steps = chunk_steps;
+    if (budget <= 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        budget = (int64_t)(0.8 * (double)fr);
+    }
+    s->budget = budget;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete s; return fail(SCRNA_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_server_destroy(scrna_server* s) {
+    if (!s) return SCRNA_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto& kv : s->reqs) release(kv.second);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_submit(scrna_server* s, const scrna_request* q, uint64_t* ticket) {
+    if (!s || !q || !ticket) return fail(SCRNA_EINVAL, "bad arguments");
+    const scrna_capture* cap = q->with_capture ? &q->capture : nullptr;
+    if (int r = validate_run(q->net, &q->kin, nullptr, cap, &q->opts)) return r;
+    if (q->opts.precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "the server runs the FP32 path");
+    const scrna_net* n = q->net;
+    if (n->dev.n_quads > fused_max_quads()) return fail(SCRNA_ENOTSUP, "the server runs register-path networks (G <= 512)");
+    if (q->opts.cell_num <= 0) return fail(SCRNA_EINVAL, "cell_num must be positive");
+    if (q->opts.cell_offset < 0 || q->opts.cell_offset + q->opts.cell_num > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
+    auto* r = new SrvRequest();
+    r->req = *q;
+    r->net = const_cast<scrna_net*>(n);
+    r->N = q->opts.cell_num;
+    r->n_steps = n_steps_of(&q->opts);
+    if (r->n_steps >= (1ll << 31)) { delete r; return fail(SCRNA_EINVAL, "too many steps"); }
+    r->footprint = footprint_of(n, r->N, q->opts.readout, cap != nullptr);
+    r->t_submit = now_s();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->ticket = s->next_ticket++;
+        s->reqs[r->ticket] = r;
+        s->queue.push_back(r);
+        s->stats.submitted++;
+    }
+    s->cv_work.notify_all();
+    *ticket = r->ticket;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_poll(scrna_server* s, uint64_t ticket, int32_t* state) {
+    if (!s || !state) return fail(SCRNA_EINVAL, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return fail(SCRNA_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+    *state = it->second->state;
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_wait(scrna_server* s, uint64_t ticket, int32_t timeout_ms, double* out, int32_t* counts,
+                          double* eff, double* latency_s) {
+    if (!s) return fail(SCRNA_EINVAL, "server is NULL");
+    SrvRequest* r = nullptr;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return fail(SCRNA_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+        r = it->second;
+        auto finished = [&] { return r->state >= SCRNA_REQ_DONE; };
+        if (timeout_ms < 0) s->cv_done.wait(lk, finished);
+        else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished))
+            return fail(SCRNA_ETIMEOUT, "request %llu not done within %d ms", (unsigned long long)ticket, timeout_ms);
+        s->reqs.erase(it);
+    }
+    int rc = SCRNA_OK;
+    if (r->state == SCRNA_REQ_DONE) {
+        if (latency_s) *latency_s = r->t_done - r->t_submit;
+        if (out || counts || eff)
+            rc = scrna_state_read(s->ctx, r->st, out, r->req.with_capture ? counts : nullptr,
+                                  r->req.with_capture ? eff : nullptr);
+    } else if (r->state == SCRNA_REQ_CANCELLED) {
+        rc = fail(SCRNA_ECANCELED, "request %llu was cancelled", (unsigned long long)ticket);
+    } else {
+        rc = fail(SCRNA_ECUDA, "request %llu failed: %s", (unsigned long long)ticket, r->error.c_str());
+    }
+    const bool admitted = r->admitted;
+    const int64_t fp = r->footprint;
+    release(r);
+    if (admitted) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->used -= fp;
+    }
+    s->cv_work.notify_all();
+    return rc;
+}
+
+extern "C" int scrna_cancel(scrna_server* s, uint64_t ticket) {
+    if (!s) return fail(SCRNA_EINVAL, "server is NULL");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return fail(SCRNA_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+    SrvRequest* r = it->second;
+    if (r->state == SCRNA_REQ_QUEUED) r->state = SCRNA_REQ_CANCELLED;  // never on the device
+    else if (r->state == SCRNA_REQ_RUNNING) r->cancel = true;         // dropped at the next chunk boundary
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_server_get_stats(scrna_server* s, scrna_server_stats* out) {
+    if (!s || !out) return fail(SCRNA_EINVAL, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
+    out->queued = (int64_t)s->queue.size();
+    out->running = (int64_t)s->active.size();
+    out->bytes_in_use = s->used;
+    return SCRNA_OK;
+}
