@@ -46,6 +46,11 @@ def _args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="telegraph", choices=["telegraph", "dense", "batch", "serve"],
+                    help="telegraph: the headline workload; the others are reported in DESIGN.md")
+    ap.add_argument("--requests", type=int, default=60, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="serve: Poisson arrival rate (1/s)")
+    ap.add_argument("--batch-networks", type=int, default=256, help="batch: number of networks")
     ap.add_argument("--cpu-sample-cells", type=int, default=20000)
     ap.add_argument("--cpu-sample-steps", type=int, default=1000)
     ap.add_argument("--ref-sample-steps", type=int, default=250)
@@ -303,10 +308,133 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def _event_time(fn, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def run_dense(args):
+    """Dense regulation, G=2000, 65,536 cells, dt=0.005, T=40 (8,000 steps): tensor-core path."""
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    wl = pkg.config2()
+    ctx = pkg.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    steps = pkg.n_steps(wl.T, wl.dt) if args.steps > 0 else 0
+    n_steps = steps if args.steps >= 1 else 100
+    G, N = wl.net.G, wl.cell_num
+    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout="protein", seed=7, ctx=ctx)
+    run.launch()
+    torch.cuda.synchronize()
+    el = [_event_time(run.launch, stream) for _ in range(max(1, args.steps))]
+    per = sum(el) / len(el)
+    units = G * N * n_steps
+    Kp = (G + 63) // 64 * 64
+    flops = 2.0 * G * Kp * N * n_steps
+    algo_bytes = 18.0 * units  # M, P read + write (FP32), 16-bit activations written
+    peaks = _measured_peaks()
+    line = {"workload": wl.name, "value": units / per, "unit": "cell·gene·steps/s", "s_per_run": per,
+            "euler_steps": n_steps, "gemm_tflops": flops / per / 1e12, "tensor_frac": flops / per / 1e12 / peaks["bf16_tflops"],
+            "hbm_gbs_algorithmic": algo_bytes / per / 1e9, "hbm_frac": algo_bytes / per / 1e9 / peaks["hbm_gbs"],
+            "peaks": peaks}
+    print(json.dumps(line), flush=True)
+
+
+def _measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def run_batch_workload(args):
+    """256 networks, G ~ LogUniform(5, 500), cells ~ LogUniform(1k, 50k), half with a Moran
+    population, dt=0.01, T=50: one simulate_gpu_batch call (persistent launches per group)."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    wls = pkg.config3(n_networks=args.batch_networks)
+    nets = [w.net for w in wls]
+    cells = [w.cell_num for w in wls]
+    pops = [w.population for w in wls]
+    units = sum(w.net.G * w.cell_num * pkg.n_steps(w.T, w.dt) for w in wls)
+    kin = wls[0].kin
+    t0 = time.perf_counter()
+    pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=50.0, populations=pops, seed=1)
+    warm = time.perf_counter() - t0
+    els = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=50.0, populations=pops, seed=1)
+        els.append(time.perf_counter() - t0)
+    per = sum(els) / len(els)
+    print(json.dumps({"workload": "batch-%d-uneven" % len(wls), "value": units / per, "unit": "cell·gene·steps/s",
+                      "s_per_run": per, "first_run_s": warm, "units_per_run": units,
+                      "networks_with_population": sum(p is not None for p in pops),
+                      "note": "host wall clock around the whole batch call, results copied to host"}), flush=True)
+
+
+def run_serve(args):
+    """Poisson request stream (rate --rate), G ~ LogUniform(5, 500), cells ~ LogUniform(1k, 100k),
+    T ~ U(20, 60) h, bursty / constitutive mix, capture on: continuous-batching server."""
+    import threading
+    import numpy as np
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    reqs = pkg.config4_requests(n_requests=args.requests, rate_per_s=args.rate)
+    ctx = pkg.default_context()
+    handles = [pkg.NetHandle(w.net, ctx) for _, w in reqs]
+    srv = pkg.Server(ctx, chunk_steps=500)
+    tickets = [None] * len(reqs)
+    t_start = time.perf_counter()
+
+    def submitter():
+        for i, (t_arr, w) in enumerate(reqs):
+            delay = t_start + t_arr - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = srv.submit(handles[i], pkg.CLE(w.dt), w.kin, cell_num=w.cell_num, T=w.T,
+                                    readout="mrna", seed=i, capture=w.capture)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lats = []
+    for i in range(len(reqs)):
+        while tickets[i] is None:
+            time.sleep(0.001)
+        lats.append(srv.wait(tickets[i], -1)[3])
+    th.join()
+    makespan = time.perf_counter() - t_start
+    st = srv.stats()
+    srv.close()
+    units = st["units_done"]
+    offered = sum(w.net.G * w.cell_num * pkg.n_steps(w.T, w.dt) for _, w in reqs) / reqs[-1][0]
+    print(json.dumps({"workload": "serve-poisson", "requests": len(reqs), "rate_per_s": args.rate,
+                      "value": units / makespan, "unit": "cell·gene·steps/s", "p50_latency_s": float(np.percentile(lats, 50)),
+                      "p99_latency_s": float(np.percentile(lats, 99)), "makespan_s": makespan,
+                      "busy_s": st["busy_s"], "offered_load": offered,
+                      "max_stable_rate_per_s": (units / st["busy_s"]) / (units / len(reqs)) if st["busy_s"] > 0 else None,
+                      "chunks": st["chunks"]}), flush=True)
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "dense":
+        run_dense(args)
+    elif args.workload == "batch":
+        run_batch_workload(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 
