@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import glob
 import os
+import re
 import shutil
 import subprocess
 from concurrent.futures import ThreadPoolExecutor
@@ -26,9 +27,23 @@ def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def _deps():
-    d = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-    return d + glob.glob(os.path.join(INCLUDE, "*.h"))
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src):
+    """Local headers that src includes, directly or through other local headers."""
+    seen, todo = set(), [src]
+    while todo:
+        with open(todo.pop()) as f:
+            text = f.read()
+        for name in _INCLUDE_RE.findall(text):
+            for d in (CSRC, INCLUDE):
+                path = os.path.join(d, name)
+                if os.path.exists(path) and path not in seen:
+                    seen.add(path)
+                    todo.append(path)
+                    break
+    return sorted(seen)
 
 
 def _stale(target, srcs) -> bool:
@@ -56,13 +71,12 @@ def _run(cmd, verbose):
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    deps = _deps()
     jobs = []
     objs = []
     for src in sources():
         obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + deps):
+        if force or _stale(obj, [src] + _deps(src)):
             cmd = [nvcc()] + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")

@@ -24,8 +24,8 @@ int warpcell_max_genes();
 int warpcell_max_regs();
 int warpcell_pick_gpl(int G, bool bursty);
 int warpcell_nreg_class(int n_reg);
-size_t warpcell_smem(int G, int gpl, int n_reg, int n_na, int n_na_src);
-cudaError_t warpcell_launch(const FusedArgs& a, const float* wdense, int gpl, bool pop, cudaStream_t st);
+size_t warpcell_smem(int G, int gpl, int n_reg);
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int kmax, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
@@ -274,7 +274,37 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     d.na_coef64 = n->b_na_coef64.as<double>();
     d.beta64 = n->b_beta64.as<double>();
     for (int g = 0; g < G; ++g) d.bursty = d.bursty || std::isfinite(n->k_on[g]);
-    if (G <= warpcell_max_genes() && d.n_reg <= warpcell_max_regs()) {
+    bool lane_ok = G <= warpcell_max_genes() && d.n_reg <= warpcell_max_regs();
+    int kmax = 0;
+    for (int g = 0; g < G && lane_ok; ++g) {
+        kmax = std::max(kmax, n->na_count[g]);
+        for (int e = n->na_begin[g]; e < n->na_begin[g] + n->na_count[g]; ++e)
+            lane_ok = lane_ok && n->na[e].src_end - n->na[e].src_begin <= kLaneSrc;
+    }
+    lane_ok = lane_ok && kmax <= kLaneTerms;
+    if (lane_ok) {
+        // padded non-additive terms per gene, in the order of the na table (bit-identical sums)
+        const int nreg = warpcell_nreg_class(d.n_reg);
+        const int zero_slot = nreg, one_slot = nreg + 1;  // constant slots of the kernel's rows
+        std::vector<LaneTerm> ln((size_t)G * kLaneTerms);
+        for (int g = 0; g < G; ++g)
+            for (int k = 0; k < kLaneTerms; ++k) {
+                LaneTerm t{};
+                for (int q = 0; q < kLaneSrc; ++q) t.src[q] = one_slot;
+                if (k < n->na_count[g]) {
+                    const NonAdd& na = n->na[n->na_begin[g] + k];
+                    t.coef = na.coef;
+                    t.kind = na.kind;
+                    for (int q = 0; q < kLaneSrc; ++q) {
+                        const int si = na.src_begin + q;
+                        t.src[q] = si < na.src_end ? n->na_src[si] : (na.kind == 0 ? one_slot : zero_slot);
+                    }
+                }
+                ln[(size_t)g * kLaneTerms + k] = t;
+            }
+        CU(up(n->b_lane_na, ln.data(), ln.size() * sizeof(LaneTerm)));
+        d.lane_na = n->b_lane_na.as<LaneTerm>();
+        d.lane_kmax = kmax <= 2 ? kmax : 4;
         // dense rows W[g][slot] = A_eff[g, reg_gene[slot]] for the warp-per-cell-group kernel
         std::vector<float> wd((size_t)G * std::max(d.n_reg, 1), 0.0f);
         for (int g = 0; g < G; ++g)
@@ -490,19 +520,22 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
         a.cap_sigma = cap->efficiency_std;
     }
     a.wdense = d.wdense;
+    a.lane_na = d.lane_na;
     *out = a;
 }
 
-// Register-path kernel of a network: warp-per-cell-group (gpl, nreg class) or block tiles.
+// Register-path kernel of a network: warp-per-cell-group (gpl, nreg class, terms per gene)
+// or block tiles.
 scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     const NetDev& d = net->dev;
     KernelChoice k{};
     const bool warp_ok = d.wdense != nullptr;
-    k.warp = path == SCRNA_PATH_WARP ? true : path == SCRNA_PATH_BLOCK ? false : warp_ok;
+    k.warp = path == SCRNA_PATH_BLOCK ? false : warp_ok;
     k.gpl = warpcell_pick_gpl(d.G, d.bursty);
     k.nreg = warpcell_nreg_class(d.n_reg);
+    k.kmax = d.lane_kmax;
     k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
-    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na, d.n_na_src) : k.block.smem;
+    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg) : k.block.smem;
     return k;
 }
 
@@ -521,10 +554,12 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     // kernel choice: warp-per-cell-group for small networks, block tiles otherwise
     const bool warp_ok = d.wdense != nullptr;
     const bool use_warp = o->path == SCRNA_PATH_WARP ? true : o->path == SCRNA_PATH_BLOCK ? false : warp_ok;
-    if (use_warp && !warp_ok) return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d and <= %d regulators", warpcell_max_genes(), warpcell_max_regs());
+    if (use_warp && !warp_ok)
+        return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d regulators and <= %d cooperative/redundant "
+                    "terms of <= %d sources per gene", warpcell_max_genes(), warpcell_max_regs(), kLaneTerms, kLaneSrc);
     const int gpl = warpcell_pick_gpl(d.G, d.bursty);
     auto launch = [&](bool is_pop) -> cudaError_t {
-        return use_warp ? warpcell_launch(a, d.wdense, gpl, is_pop, s) : fused_launch(a, L, is_pop, s);
+        return use_warp ? warpcell_launch(a, gpl, d.lane_kmax, is_pop, s) : fused_launch(a, L, is_pop, s);
     };
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;

@@ -1,6 +1,8 @@
 // Launch planning and dispatch of the fused register-path kernel (the kernel
 // template is in cle_fused.cuh; each quads-per-thread variant is compiled in its
 // own translation unit).
+#include <type_traits>
+
 #include "cle_internal.h"
 #include <cuda_runtime.h>
 
@@ -46,9 +48,9 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 }
 
 // ---- warp-per-cell-group variant for small networks ---------------------------------------
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st);
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 template <int UPT, bool POP>
@@ -75,48 +77,61 @@ int warpcell_pick_gpl(int G, bool bursty) {
     return pick;
 }
 
-size_t warpcell_smem(int G, int gpl, int n_reg, int n_na, int n_na_src) {
+size_t warpcell_smem(int G, int gpl, int n_reg) {
     const int lpc = (G + gpl - 1) / gpl;
     const int cpw = 32 / lpc;
-    const int nreg = warpcell_nreg_class(n_reg);
-    size_t b = (size_t)4 * 2 * (cpw + 1) * (nreg + 1) * sizeof(float);
-    b += (size_t)n_na * sizeof(NonAdd) + (size_t)n_na_src * sizeof(int32_t);
+    const int ld = warpcell_nreg_class(n_reg) + 3;  // slots + constants 0 and 1, odd row length
+    const size_t b = (size_t)4 * 2 * (cpw + 1) * ld * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
-#define SCRNA_WARP_DISPATCH(CALL)                                        \
-    switch ((gpl == 4 ? 100 : 0) + nreg * 2 + (pop ? 1 : 0)) {           \
-        case 8: return CALL(2, 4, false);                                \
-        case 9: return CALL(2, 4, true);                                 \
-        case 16: return CALL(2, 8, false);                               \
-        case 17: return CALL(2, 8, true);                                \
-        case 32: return CALL(2, 16, false);                              \
-        case 33: return CALL(2, 16, true);                               \
-        case 108: return CALL(4, 4, false);                              \
-        case 109: return CALL(4, 4, true);                               \
-        case 116: return CALL(4, 8, false);                              \
-        case 117: return CALL(4, 8, true);                               \
-        case 132: return CALL(4, 16, false);                             \
-        case 133: return CALL(4, 16, true);                              \
-        default: return cudaErrorInvalidValue;                           \
-    }
+template <int V>
+using IntC = std::integral_constant<int, V>;
 
-cudaError_t warpcell_launch(const FusedArgs& a0, const float* wdense, int gpl, bool pop, cudaStream_t st) {
-    FusedArgs a = a0;
-    a.wdense = wdense;
-    const int nreg = warpcell_nreg_class(a.n_reg);
-#define CALL(G_, R_, P_) warpcell_launch_t<G_, R_, P_>(a, st)
-    SCRNA_WARP_DISPATCH(CALL)
-#undef CALL
+// Calls f(IntC<GPL>, IntC<NREG>, IntC<KMAX>, bool_constant<POP>) for the runtime shape.
+template <class F>
+static cudaError_t warpcell_dispatch(int gpl, int nreg, int kmax, bool pop, F&& f) {
+    auto by_k = [&](auto g, auto r) -> cudaError_t {
+        switch (kmax * 2 + (pop ? 1 : 0)) {
+            case 0: return f(g, r, IntC<0>{}, std::false_type{});
+            case 1: return f(g, r, IntC<0>{}, std::true_type{});
+            case 2: return f(g, r, IntC<1>{}, std::false_type{});
+            case 3: return f(g, r, IntC<1>{}, std::true_type{});
+            case 4: return f(g, r, IntC<2>{}, std::false_type{});
+            case 5: return f(g, r, IntC<2>{}, std::true_type{});
+            case 8: return f(g, r, IntC<4>{}, std::false_type{});
+            case 9: return f(g, r, IntC<4>{}, std::true_type{});
+            default: return cudaErrorInvalidValue;
+        }
+    };
+    auto by_r = [&](auto g) -> cudaError_t {
+        switch (nreg) {
+            case 4: return by_k(g, IntC<4>{});
+            case 8: return by_k(g, IntC<8>{});
+            case 16: return by_k(g, IntC<16>{});
+            default: return cudaErrorInvalidValue;
+        }
+    };
+    switch (gpl) {
+        case 2: return by_r(IntC<2>{});
+        case 4: return by_r(IntC<4>{});
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int kmax, bool pop, cudaStream_t st) {
+    return warpcell_dispatch(gpl, warpcell_nreg_class(a.n_reg), kmax, pop, [&](auto g, auto r, auto k, auto p) {
+        return warpcell_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(a, st);
+    });
 }
 
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int nreg, bool pop, size_t smem, int grid, TileCtl shared_ctl, int use_shared,
-                                  cudaStream_t st) {
-#define CALL(G_, R_, P_) \
-    warpcell_queue_launch_t<G_, R_, P_>(args, items, n_items, counter, smem, grid, shared_ctl, use_shared, st)
-    SCRNA_WARP_DISPATCH(CALL)
-#undef CALL
+                                  int nreg, int kmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
+                                  int use_shared, cudaStream_t st) {
+    return warpcell_dispatch(gpl, nreg, kmax, pop, [&](auto g, auto r, auto k, auto p) {
+        return warpcell_queue_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(
+            args, items, n_items, counter, smem, grid, shared_ctl, use_shared, st);
+    });
 }
 
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,

@@ -32,6 +32,18 @@ struct NonAdd {
     int32_t src_end;
 };
 
+// Cooperative / redundant term of one target gene in the warp kernel's padded per-gene
+// list: sources are regulator slots; a padded source names a constant slot (1 for a
+// cooperative term, 0 for a redundant one) and a padded term has coef 0.
+constexpr int kLaneTerms = 4;  // terms per gene
+constexpr int kLaneSrc = 3;    // sources per term
+struct LaneTerm {
+    float coef;
+    int32_t kind;
+    int32_t src[kLaneSrc];
+    int32_t pad[3];
+};
+
 // Device-resident network tables (owned by scrna_net).
 struct NetDev {
     int32_t G = 0;
@@ -48,6 +60,8 @@ struct NetDev {
     double* na_coef64 = nullptr; // FP64 s*beta_target (baseline path)
     double* beta64 = nullptr;    // FP64 basals (baseline path)
     float* wdense = nullptr;     // [G][n_reg] dense regulation rows (small networks), or null
+    LaneTerm* lane_na = nullptr; // [G][kLaneTerms] padded non-additive terms (with wdense)
+    int32_t lane_kmax = 0;       // terms per gene the warp kernel runs (0, 1, 2 or 4)
     bool bursty = false;         // any gene switches (finite k_on)
 };
 
@@ -76,6 +90,7 @@ struct FusedArgs {
     const int32_t* na_src;
     const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
     const float* wdense;         // [G][n_reg] dense regulation rows (warp kernel), or null
+    const LaneTerm* lane_na;     // [G][kLaneTerms] padded non-additive terms (warp kernel)
     // state [G][N]
     float* M;
     float* P;

@@ -1,17 +1,22 @@
 // Warp-per-cell-group register-path CLE kernel for small networks (sm_100a).
 //
-// For G <= 32 genes with at most 16 regulator genes, a whole cell lives inside one
-// warp: lane = (cell, unit) where a unit is GPL consecutive genes (a gene pair or a
-// gene quad).  All lanes of a warp run the same instruction stream; what differs per
-// lane (basal rate, telegraph thresholds, the dense row of regulation weights over the
-// regulator slots) sits in registers, loaded once.  Per Euler step:
+// For G <= 32 genes with at most 16 regulator genes and at most kLaneTerms cooperative
+// / redundant terms per gene (each over at most kLaneSrc sources), a whole cell lives
+// inside one warp: lane = (cell, unit) where a unit is GPL consecutive genes (a gene
+// pair or a gene quad).  All lanes of a warp run the same instruction stream; what
+// differs per lane (basal rate, telegraph thresholds, the dense row of additive weights
+// over the regulator slots, the padded list of non-additive terms) sits in registers,
+// loaded once.  Per Euler step:
 //   telegraph switch -> Hill of the lane's regulator genes into a per-warp shared slot
 //   table -> Philox + Box-Muller for the lane's genes -> __syncwarp -> read the cell's
-//   regulator activations -> reg = cneg + W_row . act (+ cooperative / redundant terms)
+//   regulator activations -> reg = cneg + W_row . act + sum of KMAX padded terms
 //   -> M, P update.
-// There is no block-wide barrier: warps are independent.  The arithmetic and the
-// Philox streams are those of cle_fused_kernel (same sums in the same order: the
-// dense row adds exact zeros for absent edges), so both kernels give identical results.
+// There is no block-wide barrier: warps are independent, and no lane branches on the
+// network's structure.  The arithmetic and the Philox streams are those of
+// cle_fused_kernel (same sums in the same order: the dense row adds exact zeros for
+// absent edges; a padded term has coefficient 0 and a padded source reads a constant
+// slot holding 1 (cooperative) or 0 (redundant), which leave the product unchanged), so
+// both kernels give identical results.
 #pragma once
 #include "cle_device.cuh"
 #include "cle_internal.h"
@@ -23,11 +28,14 @@ constexpr int kWarpcellWarps = 4;  // warps per block
 __host__ __device__ inline int warpcell_lanes_per_cell(int G, int gpl) { return (G + gpl - 1) / gpl; }
 __host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 32 / warpcell_lanes_per_cell(G, gpl); }
 
+// Row of one cell's regulator activations: NREG slots, then the constants 0 and 1 read
+// by padded term sources; odd length so the rows of a warp's cells fall in different banks.
+__host__ __device__ constexpr int warpcell_ld(int nreg) { return nreg + 3; }
+
 template <int NREG>
-__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_na, int n_na_src) {
+__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl) {
     const int cpw = warpcell_cells_per_warp(G, gpl);
-    size_t b = (size_t)kWarpcellWarps * 2 * (cpw + 1) * (NREG + 1) * sizeof(float);
-    b += (size_t)n_na * sizeof(NonAdd) + (size_t)n_na_src * sizeof(int32_t);
+    const size_t b = (size_t)kWarpcellWarps * 2 * (cpw + 1) * warpcell_ld(NREG) * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
@@ -41,20 +49,15 @@ __device__ __forceinline__ uint32_t quad_word(const uint4& w, int u, int i) {
 }
 
 // One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
     const float* __restrict__ wdense = a.wdense;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
     const int cpw = 32 / lpc;
-    const int ld = NREG + 1;
+    constexpr int ld = warpcell_ld(NREG);
     float* act_all = reinterpret_cast<float*>(smem_raw);
-    NonAdd* sna = reinterpret_cast<NonAdd*>(act_all + (size_t)kWarpcellWarps * 2 * (cpw + 1) * ld);
-    int32_t* sna_src = reinterpret_cast<int32_t*>(sna + a.n_na);
-    for (int i = threadIdx.x; i < a.n_na; i += blockDim.x) sna[i] = a.na[i];
-    for (int i = threadIdx.x; i < a.n_na_src; i += blockDim.x) sna_src[i] = a.na_src[i];
-    __syncthreads();
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -70,12 +73,21 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     const Key key{a.key0, a.key1};
     const int n_reg = a.n_reg;
     float* act_w = act_all + (size_t)warp * 2 * (cpw + 1) * ld;
+    for (int r = lane; r < 2 * (cpw + 1); r += 32) {  // constant slots of every row
+        act_w[(size_t)r * ld + NREG] = 0.0f;
+        act_w[(size_t)r * ld + NREG + 1] = 1.0f;
+    }
+    __syncwarp();
 
     // per-lane gene constants
     float beta[GPL], cneg[GPL], W[GPL][NREG];
     float inv_on[GPL], inv_off[GPL];
-    int slot[GPL], na_range[GPL];
+    int slot[GPL];
     bool valid[GPL];
+    // padded non-additive terms: reg += coef * (off + sgn * prod_q (off + sgn * act[src_q]))
+    // with (sgn, off) = (1, 0) cooperative, (-1, 1) redundant
+    float tc[GPL][KMAX > 0 ? KMAX : 1], tsg[GPL][KMAX > 0 ? KMAX : 1], tof[GPL][KMAX > 0 ? KMAX : 1];
+    int ts[GPL][KMAX > 0 ? KMAX : 1][kLaneSrc];
 #pragma unroll
     for (int i = 0; i < GPL; ++i) {
         const int g = u * GPL + i;
@@ -87,9 +99,18 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         inv_on[i] = gr.inv_on;
         inv_off[i] = valid[i] ? gr.inv_off : __int_as_float(0x7FC00000);  // NaN: never switches
         slot[i] = valid[i] ? gr.slot : -1;
-        na_range[i] = valid[i] ? gr.na_range : 0;
 #pragma unroll
         for (int r = 0; r < NREG; ++r) W[i][r] = (valid[i] && r < n_reg) ? wdense[(size_t)gg * n_reg + r] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            const LaneTerm t = a.lane_na[(size_t)gg * kLaneTerms + k];
+            const bool on_k = valid[i];
+            tc[i][k] = on_k ? t.coef : 0.0f;
+            tsg[i][k] = t.kind == 0 ? 1.0f : -1.0f;
+            tof[i][k] = t.kind == 0 ? 0.0f : 1.0f;
+#pragma unroll
+            for (int q = 0; q < kLaneSrc; ++q) ts[i][k][q] = t.src[q];
+        }
     }
     const int quad = GPL == 4 ? u : (u >> 1);
 
@@ -193,17 +214,12 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             float reg = cneg[i];
 #pragma unroll
             for (int r = 0; r < NREG; ++r) reg = fmaf(W[i][r], areg[r], reg);
-            const int nab = na_range[i] >> 16, nac = na_range[i] & 0xFFFF;
-            for (int e = nab; e < nab + nac; ++e) {
-                const NonAdd na = sna[e];
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {  // x and 1-x are exact as fmaf(+-1, x, 0 or 1)
                 float prod = 1.0f;
-                if (na.kind == 0) {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[sna_src[t]];
-                    reg = fmaf(na.coef, prod, reg);
-                } else {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[sna_src[t]];
-                    reg = fmaf(na.coef, 1.0f - prod, reg);
-                }
+#pragma unroll
+                for (int q = 0; q < kLaneSrc; ++q) prod *= fmaf(tsg[i][k], act[ts[i][k][q]], tof[i][k]);
+                reg = fmaf(tc[i][k], fmaf(tsg[i][k], prod, tof[i][k]), reg);
             }
             float tx = reg + beta[i];
             if (POP) tx *= Vf;
@@ -302,14 +318,14 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     }
 }
 
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    warpcell_tile<GPL, NREG, POP>(a, blockIdx.x, ctl, smem_raw);
+    warpcell_tile<GPL, NREG, KMAX, POP>(a, blockIdx.x, ctl, smem_raw);
 }
 
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
 cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
@@ -322,15 +338,15 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         __syncthreads();
         if (it >= n_items) return;
         const TileWork w = items[it];
-        warpcell_tile<GPL, NREG, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        warpcell_tile<GPL, NREG, KMAX, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
         __syncthreads();
     }
 }
 
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
-    auto k = cle_warpcell_kernel<GPL, NREG, POP>;
-    const size_t smem = warpcell_smem_bytes<NREG>(a.G, GPL, a.n_na, a.n_na_src);
+    auto k = cle_warpcell_kernel<GPL, NREG, KMAX, POP>;
+    const size_t smem = warpcell_smem_bytes<NREG>(a.G, GPL);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
@@ -339,10 +355,10 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int GPL, int NREG, bool POP>
+template <int GPL, int NREG, int KMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    auto k = cle_warpcell_queue_kernel<GPL, NREG, POP>;
+    auto k = cle_warpcell_queue_kernel<GPL, NREG, KMAX, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, 32 * kWarpcellWarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
@@ -350,3 +366,19 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
 }
 
 }  // namespace scrna
+
+// Explicit instantiation of both launchers of one kernel variant (one .cu file per
+// (GPL, NREG) pair keeps the parallel build balanced).
+#define SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, KMAX, POP)                                                        \
+    template cudaError_t scrna::warpcell_launch_t<GPL, NREG, KMAX, POP>(const FusedArgs&, cudaStream_t);         \
+    template cudaError_t scrna::warpcell_queue_launch_t<GPL, NREG, KMAX, POP>(                                   \
+        const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int, cudaStream_t);
+#define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, NREG)       \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 0, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 0, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 1, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 1, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 2, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 2, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 4, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 4, true)

@@ -1,0 +1,4 @@
+// Instantiations of the warp-per-cell-group kernel: 2 genes per lane, up to 4 regulator slots.
+#include "cle_warpcell.cuh"
+
+SCRNA_WARPCELL_INSTANTIATE_ALL(2, 4)

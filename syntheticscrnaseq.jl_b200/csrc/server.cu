@@ -174,15 +174,16 @@ void scrna_server::run() {
         const double t_chunk = now_s();
         // one persistent launch per kernel group over the running requests' tiles
         h_args.clear();
-        std::map<std::tuple<int, int, int, int>, std::vector<TileWork>> groups;
-        std::map<std::tuple<int, int, int, int>, std::pair<int, size_t>> shape;  // nw, smem
+        std::map<std::tuple<int, int, int, int, int>, std::vector<TileWork>> groups;
+        std::map<std::tuple<int, int, int, int, int>, std::pair<int, size_t>> shape;  // nw, smem
         for (size_t i = 0; i < run_set.size(); ++i) {
             SrvRequest* r = run_set[i];
             h_args.push_back(r->args);
             r->s0 = r->next;
             r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps - 1);
             const KernelChoice& kc = r->kc;
-            auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.nreg : 0, kc.warp ? 0 : kc.block.upt);
+            auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.nreg : 0, kc.warp ? 0 : kc.block.upt,
+                                       kc.warp ? kc.kmax : 0);
             int64_t cpt = 32;
             if (kc.warp) cpt = (int64_t)(32 / ((r->net->G + kc.gpl - 1) / kc.gpl)) * 4;
             const int64_t tiles = (r->N + cpt - 1) / cpt;
@@ -219,7 +220,7 @@ void scrna_server::run() {
             const int grid = std::max(1, std::min(n_items, ctx->sm_count * (std::get<0>(key) ? 6 : 8)));
             if (std::get<0>(key))
                 e = warpcell_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<1>(key),
-                                          std::get<2>(key), false, sh.second, grid, TileCtl{}, 0, stream);
+                                          std::get<2>(key), std::get<4>(key), false, sh.second, grid, TileCtl{}, 0, stream);
             else
                 e = fused_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<3>(key), sh.first,
                                        sh.second, false, grid, TileCtl{}, 0, stream);

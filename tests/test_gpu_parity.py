@@ -245,6 +245,43 @@ def test_warp_and_block_kernels_identical(pkg, G, bursty, seed):
         assert np.array_equal(outs[0][k], outs[1][k]), k
 
 
+def _terms_per_target(net):
+    cnt = {}
+    for e in list(net.cooperative) + list(net.redundant):
+        cnt[e.target] = cnt.get(e.target, 0) + 1
+    return max(cnt.values()) if cnt else 0
+
+
+@pytest.mark.parametrize("G,seed,n_coop,n_redun,n_src", [(12, 21, (3, 4), (3, 4), (2, 3)),   # 1 term, 3 sources
+                                                         (8, 0, (2, 3), (2, 3), (2, 3)),      # 2 terms
+                                                         (10, 1, (3, 3), (3, 3), (2, 3)),     # 2 terms
+                                                         (14, 1, (5, 6), (5, 6), (2, 3))])    # 3 terms
+def test_warp_kernel_padded_terms_identical(pkg, G, seed, n_coop, n_redun, n_src):
+    """Networks with several cooperative / redundant terms per gene over 2-3 sources: the
+    warp kernel's padded per-lane terms (coefficient 0, constant 0/1 sources) give the
+    block kernel's sums bit for bit."""
+    net = pkg.sample_network(G, seed=seed, bursty=True, n_coop_range=n_coop, n_redun_range=n_redun,
+                             n_sources_range=n_src)
+    assert 1 <= _terms_per_target(net) <= 4
+    kin = pkg.WORKLOAD_KINETICS
+    outs = [_device_run(pkg, net, kin, N=301, steps=120, seed=seed, path=p).read_raw() for p in ("warp", "block")]
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_warp_kernel_rejects_long_terms(pkg):
+    """A cooperative term over 4 sources is beyond the warp kernel's padded lists: asking
+    for that kernel fails with a clear error, the automatic choice runs the block kernel."""
+    net = pkg.sample_network(8, seed=3, n_coop_range=(1, 1), n_redun_range=(0, 0), n_sources_range=(4, 4))
+    assert any(len(e.sources) == 4 for e in net.cooperative)
+    kin = pkg.WORKLOAD_KINETICS
+    with pytest.raises(pkg.ScrnaError):
+        _device_run(pkg, net, kin, N=64, steps=10, seed=1, path="warp")
+    a = _device_run(pkg, net, kin, N=64, steps=10, seed=1, path="auto").read_raw()
+    b = _device_run(pkg, net, kin, N=64, steps=10, seed=1, path="block").read_raw()
+    assert np.array_equal(a["P"], b["P"])
+
+
 @pytest.mark.parametrize("partition", ["halve", "binomial"])
 def test_warp_and_block_kernels_identical_population(pkg, partition):
     net = pkg.sample_network(7, seed=9, bursty=True)
