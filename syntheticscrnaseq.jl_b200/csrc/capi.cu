@@ -21,11 +21,10 @@ FusedLaunch fused_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int n
 int fused_max_quads();
 cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st);
 int warpcell_max_genes();
-int warpcell_max_regs();
-int warpcell_pick_gpl(int G, bool bursty);
-int warpcell_nreg_class(int n_reg);
+int warpcell_emax_class(int max_in);
+int warpcell_pick_gpl(int G, bool bursty, int emax);
 size_t warpcell_smem(int G, int gpl, int n_reg);
-cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int kmax, bool pop, cudaStream_t st);
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int kmax, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
@@ -274,20 +273,28 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     d.na_coef64 = n->b_na_coef64.as<double>();
     d.beta64 = n->b_beta64.as<double>();
     for (int g = 0; g < G; ++g) d.bursty = d.bursty || std::isfinite(n->k_on[g]);
-    bool lane_ok = G <= warpcell_max_genes() && d.n_reg <= warpcell_max_regs();
-    int kmax = 0;
+    // padded per-gene lists of the warp-per-cell-group kernel (small networks)
+    bool lane_ok = G <= warpcell_max_genes();
+    int emax = 0, kmax = 0;
     for (int g = 0; g < G && lane_ok; ++g) {
+        emax = std::max(emax, n->in_end[g] - n->in_begin[g]);
         kmax = std::max(kmax, n->na_count[g]);
         for (int e = n->na_begin[g]; e < n->na_begin[g] + n->na_count[g]; ++e)
             lane_ok = lane_ok && n->na[e].src_end - n->na[e].src_begin <= kLaneSrc;
     }
-    lane_ok = lane_ok && kmax <= kLaneTerms;
+    lane_ok = lane_ok && emax <= kLaneEdges && kmax <= kLaneTerms;
     if (lane_ok) {
-        // padded non-additive terms per gene, in the order of the na table (bit-identical sums)
-        const int nreg = warpcell_nreg_class(d.n_reg);
-        const int zero_slot = nreg, one_slot = nreg + 1;  // constant slots of the kernel's rows
+        // same order as the edge tables (bit-identical sums with the block kernel)
+        const int zero_slot = d.n_reg, one_slot = d.n_reg + 1;  // constant slots of the kernel's rows
+        std::vector<int2> li((size_t)G * kLaneEdges, make_int2(zero_slot, 0));
         std::vector<LaneTerm> ln((size_t)G * kLaneTerms);
-        for (int g = 0; g < G; ++g)
+        for (int g = 0; g < G; ++g) {
+            for (int e = n->in_begin[g], k = 0; e < n->in_end[g]; ++e, ++k) {
+                int32_t slot, wbits;
+                std::memcpy(&slot, &n->in_edge[e].y, 4);
+                std::memcpy(&wbits, &n->in_edge[e].x, 4);
+                li[(size_t)g * kLaneEdges + k] = make_int2(slot, wbits);
+            }
             for (int k = 0; k < kLaneTerms; ++k) {
                 LaneTerm t{};
                 for (int q = 0; q < kLaneSrc; ++q) t.src[q] = one_slot;
@@ -302,19 +309,13 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
                 }
                 ln[(size_t)g * kLaneTerms + k] = t;
             }
+        }
+        CU(up(n->b_lane_in, li.data(), li.size() * sizeof(int2)));
         CU(up(n->b_lane_na, ln.data(), ln.size() * sizeof(LaneTerm)));
+        d.lane_in = n->b_lane_in.as<int2>();
         d.lane_na = n->b_lane_na.as<LaneTerm>();
+        d.lane_emax = warpcell_emax_class(emax);
         d.lane_kmax = kmax <= 2 ? kmax : 4;
-        // dense rows W[g][slot] = A_eff[g, reg_gene[slot]] for the warp-per-cell-group kernel
-        std::vector<float> wd((size_t)G * std::max(d.n_reg, 1), 0.0f);
-        for (int g = 0; g < G; ++g)
-            for (int e = n->in_begin[g]; e < n->in_end[g]; ++e) {
-                int32_t slot;
-                std::memcpy(&slot, &n->in_edge[e].y, 4);
-                wd[(size_t)g * d.n_reg + slot] = n->in_edge[e].x;
-            }
-        CU(up(n->b_wdense, wd.data(), wd.size() * sizeof(float)));
-        d.wdense = n->b_wdense.as<float>();
     }
     *out = n.release();
     return SCRNA_OK;
@@ -519,20 +520,24 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
         a.cap_mu_log = std::log(cap->efficiency) - (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
         a.cap_sigma = cap->efficiency_std;
     }
-    a.wdense = d.wdense;
+    a.lane_in = d.lane_in;
     a.lane_na = d.lane_na;
+    for (int r = 0; r < 10; ++r) {
+        a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
+        a.rk1[r] = a.key1 + (uint32_t)r * 0xBB67AE85u;
+    }
     *out = a;
 }
 
-// Register-path kernel of a network: warp-per-cell-group (gpl, nreg class, terms per gene)
-// or block tiles.
+// Register-path kernel of a network: warp-per-cell-group (genes per lane, in-edges and
+// terms per gene) or block tiles.
 scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     const NetDev& d = net->dev;
     KernelChoice k{};
-    const bool warp_ok = d.wdense != nullptr;
+    const bool warp_ok = d.lane_in != nullptr;
     k.warp = path == SCRNA_PATH_BLOCK ? false : warp_ok;
-    k.gpl = warpcell_pick_gpl(d.G, d.bursty);
-    k.nreg = warpcell_nreg_class(d.n_reg);
+    k.gpl = warpcell_pick_gpl(d.G, d.bursty, d.lane_emax);
+    k.emax = d.lane_emax;
     k.kmax = d.lane_kmax;
     k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
     k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg) : k.block.smem;
@@ -552,14 +557,14 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
     cudaStream_t s = ctx->stream;
     // kernel choice: warp-per-cell-group for small networks, block tiles otherwise
-    const bool warp_ok = d.wdense != nullptr;
+    const bool warp_ok = d.lane_in != nullptr;
     const bool use_warp = o->path == SCRNA_PATH_WARP ? true : o->path == SCRNA_PATH_BLOCK ? false : warp_ok;
     if (use_warp && !warp_ok)
-        return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d regulators and <= %d cooperative/redundant "
-                    "terms of <= %d sources per gene", warpcell_max_genes(), warpcell_max_regs(), kLaneTerms, kLaneSrc);
-    const int gpl = warpcell_pick_gpl(d.G, d.bursty);
+        return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d in-edges and <= %d cooperative/redundant "
+                    "terms of <= %d sources per gene", warpcell_max_genes(), kLaneEdges, kLaneTerms, kLaneSrc);
+    const int gpl = warpcell_pick_gpl(d.G, d.bursty, d.lane_emax);
     auto launch = [&](bool is_pop) -> cudaError_t {
-        return use_warp ? warpcell_launch(a, gpl, d.lane_kmax, is_pop, s) : fused_launch(a, L, is_pop, s);
+        return use_warp ? warpcell_launch(a, gpl, d.lane_emax, d.lane_kmax, is_pop, s) : fused_launch(a, L, is_pop, s);
     };
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;

@@ -42,6 +42,22 @@ __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, u
     return make_uint4(c0, c1, c2, c3);
 }
 
+// Philox4x32-10 with its ten round keys given (round r: key + r (0x9E3779B9, 0xBB67AE85),
+// precomputed on the host).  Identical output to philox(); when rk0 / rk1 live in kernel
+// parameter space the rounds read them as constant operands instead of recomputing them.
+__device__ __forceinline__ uint4 philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                           const uint32_t* rk0, const uint32_t* rk1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ rk0[r];
+        const uint32_t n2 = hi0 ^ c3 ^ rk1[r];
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
 __device__ __forceinline__ uint32_t tagword(uint32_t tag, uint32_t stream) {
     return (tag << 24) | (stream & 0xFFFFFFu);
 }

@@ -48,9 +48,9 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 }
 
 // ---- warp-per-cell-group variant for small networks ---------------------------------------
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st);
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 template <int UPT, bool POP>
@@ -58,12 +58,12 @@ cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, i
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 
 int warpcell_max_genes() { return 32; }
-int warpcell_max_regs() { return 16; }
-int warpcell_nreg_class(int n_reg) { return n_reg <= 4 ? 4 : n_reg <= 8 ? 8 : 16; }
+int warpcell_emax_class(int max_in) { return max_in <= 2 ? 2 : max_in <= 4 ? 4 : 8; }
 
 // Genes per lane for a network: a cost model of issue slots per cell-gene-step
 // (Philox calls per gene, plus lanes left idle by the cell packing).
-int warpcell_pick_gpl(int G, bool bursty) {
+int warpcell_pick_gpl(int G, bool bursty, int emax) {
+    if (emax > 4) return 2;  // 8 padded in-edges per gene: only gene pairs fit in registers
     double best = 1e30;
     int pick = 2;
     for (int gpl : {2, 4}) {
@@ -80,17 +80,18 @@ int warpcell_pick_gpl(int G, bool bursty) {
 size_t warpcell_smem(int G, int gpl, int n_reg) {
     const int lpc = (G + gpl - 1) / gpl;
     const int cpw = 32 / lpc;
-    const int ld = warpcell_nreg_class(n_reg) + 3;  // slots + constants 0 and 1, odd row length
-    const size_t b = (size_t)4 * 2 * (cpw + 1) * ld * sizeof(float);
+    const int ld = (n_reg + 3) | 1;  // slots, constants 0 and 1, a write-only slot; odd row length
+    const size_t b = (size_t)4 * (cpw + 1) * ld * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
 template <int V>
 using IntC = std::integral_constant<int, V>;
 
-// Calls f(IntC<GPL>, IntC<NREG>, IntC<KMAX>, bool_constant<POP>) for the runtime shape.
+// Calls f(IntC<GPL>, IntC<EMAX>, IntC<KMAX>, bool_constant<POP>) for the runtime shape
+// (gene quads take at most 4 in-edges per gene).
 template <class F>
-static cudaError_t warpcell_dispatch(int gpl, int nreg, int kmax, bool pop, F&& f) {
+static cudaError_t warpcell_dispatch(int gpl, int emax, int kmax, bool pop, F&& f) {
     auto by_k = [&](auto g, auto r) -> cudaError_t {
         switch (kmax * 2 + (pop ? 1 : 0)) {
             case 0: return f(g, r, IntC<0>{}, std::false_type{});
@@ -104,31 +105,26 @@ static cudaError_t warpcell_dispatch(int gpl, int nreg, int kmax, bool pop, F&& 
             default: return cudaErrorInvalidValue;
         }
     };
-    auto by_r = [&](auto g) -> cudaError_t {
-        switch (nreg) {
-            case 4: return by_k(g, IntC<4>{});
-            case 8: return by_k(g, IntC<8>{});
-            case 16: return by_k(g, IntC<16>{});
-            default: return cudaErrorInvalidValue;
-        }
-    };
-    switch (gpl) {
-        case 2: return by_r(IntC<2>{});
-        case 4: return by_r(IntC<4>{});
+    switch (gpl * 16 + emax) {
+        case 34: return by_k(IntC<2>{}, IntC<2>{});
+        case 36: return by_k(IntC<2>{}, IntC<4>{});
+        case 40: return by_k(IntC<2>{}, IntC<8>{});
+        case 66: return by_k(IntC<4>{}, IntC<2>{});
+        case 68: return by_k(IntC<4>{}, IntC<4>{});
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int kmax, bool pop, cudaStream_t st) {
-    return warpcell_dispatch(gpl, warpcell_nreg_class(a.n_reg), kmax, pop, [&](auto g, auto r, auto k, auto p) {
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int kmax, bool pop, cudaStream_t st) {
+    return warpcell_dispatch(gpl, emax, kmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(a, st);
     });
 }
 
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int nreg, int kmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
+                                  int emax, int kmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
                                   int use_shared, cudaStream_t st) {
-    return warpcell_dispatch(gpl, nreg, kmax, pop, [&](auto g, auto r, auto k, auto p) {
+    return warpcell_dispatch(gpl, emax, kmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_queue_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(
             args, items, n_items, counter, smem, grid, shared_ctl, use_shared, st);
     });

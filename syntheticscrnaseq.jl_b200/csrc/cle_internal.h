@@ -32,9 +32,12 @@ struct NonAdd {
     int32_t src_end;
 };
 
-// Cooperative / redundant term of one target gene in the warp kernel's padded per-gene
-// list: sources are regulator slots; a padded source names a constant slot (1 for a
-// cooperative term, 0 for a redundant one) and a padded term has coef 0.
+// Padded per-gene lists of the warp kernel.  An in-edge is {source slot, weight bits};
+// padding is {slot n_reg (constant 0), weight 0}.  A cooperative / redundant term names
+// regulator slots as sources; a padded source names a constant slot (n_reg + 1 holding 1
+// for a cooperative term, n_reg holding 0 for a redundant one) and a padded term has
+// coef 0.
+constexpr int kLaneEdges = 8;  // in-edges per gene
 constexpr int kLaneTerms = 4;  // terms per gene
 constexpr int kLaneSrc = 3;    // sources per term
 struct LaneTerm {
@@ -59,8 +62,9 @@ struct NetDev {
     double* in_w64 = nullptr;    // FP64 additive weights (baseline path)
     double* na_coef64 = nullptr; // FP64 s*beta_target (baseline path)
     double* beta64 = nullptr;    // FP64 basals (baseline path)
-    float* wdense = nullptr;     // [G][n_reg] dense regulation rows (small networks), or null
-    LaneTerm* lane_na = nullptr; // [G][kLaneTerms] padded non-additive terms (with wdense)
+    int2* lane_in = nullptr;     // [G][kLaneEdges] padded in-edges (small networks), or null
+    LaneTerm* lane_na = nullptr; // [G][kLaneTerms] padded non-additive terms (with lane_in)
+    int32_t lane_emax = 0;       // in-edges per gene the warp kernel runs (2, 4 or 8)
     int32_t lane_kmax = 0;       // terms per gene the warp kernel runs (0, 1, 2 or 4)
     bool bursty = false;         // any gene switches (finite k_on)
 };
@@ -79,6 +83,7 @@ struct FusedArgs {
     float k_t, Kn, hill_n, mu_m, mu_p, dt;
     int32_t hill_int;       // >0: integer Hill exponent (repeated products)
     uint32_t key0, key1, stream;
+    uint32_t rk0[10], rk1[10];  // Philox round keys of (key0, key1)
     // population
     double growth_factor, V_div, V_lo, V_hi;
     int32_t partition, exclude_mother;
@@ -89,7 +94,7 @@ struct FusedArgs {
     const NonAdd* na;
     const int32_t* na_src;
     const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
-    const float* wdense;         // [G][n_reg] dense regulation rows (warp kernel), or null
+    const int2* lane_in;         // [G][kLaneEdges] padded in-edges (warp kernel)
     const LaneTerm* lane_na;     // [G][kLaneTerms] padded non-additive terms (warp kernel)
     // state [G][N]
     float* M;

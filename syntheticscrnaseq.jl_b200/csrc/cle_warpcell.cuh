@@ -1,22 +1,21 @@
 // Warp-per-cell-group register-path CLE kernel for small networks (sm_100a).
 //
-// For G <= 32 genes with at most 16 regulator genes and at most kLaneTerms cooperative
-// / redundant terms per gene (each over at most kLaneSrc sources), a whole cell lives
-// inside one warp: lane = (cell, unit) where a unit is GPL consecutive genes (a gene
-// pair or a gene quad).  All lanes of a warp run the same instruction stream; what
-// differs per lane (basal rate, telegraph thresholds, the dense row of additive weights
-// over the regulator slots, the padded list of non-additive terms) sits in registers,
-// loaded once.  Per Euler step:
-//   telegraph switch -> Hill of the lane's regulator genes into a per-warp shared slot
-//   table -> Philox + Box-Muller for the lane's genes -> __syncwarp -> read the cell's
-//   regulator activations -> reg = cneg + W_row . act + sum of KMAX padded terms
-//   -> M, P update.
-// There is no block-wide barrier: warps are independent, and no lane branches on the
-// network's structure.  The arithmetic and the Philox streams are those of
-// cle_fused_kernel (same sums in the same order: the dense row adds exact zeros for
-// absent edges; a padded term has coefficient 0 and a padded source reads a constant
-// slot holding 1 (cooperative) or 0 (redundant), which leave the product unchanged), so
-// both kernels give identical results.
+// For G <= 32 genes with at most kLaneEdges additive in-edges and kLaneTerms
+// cooperative / redundant terms (each over at most kLaneSrc sources) per gene, a whole
+// cell lives inside one warp: lane = (cell, unit) where a unit is GPL consecutive genes
+// (a gene pair or a gene quad).  All lanes of a warp run the same instruction stream;
+// what differs per lane sits in registers, loaded once: basal rate, telegraph
+// parameters, and the gene's padded lists of EMAX in-edges (weight, shared-memory
+// address of the source's activation) and KMAX non-additive terms.  Per Euler step:
+//   telegraph switch -> Hill of the lane's genes into the cell's activation row in
+//   shared memory -> Philox + Box-Muller -> __syncwarp -> reg = cneg + sum of EMAX
+//   padded edges + sum of KMAX padded terms -> M, P update -> __syncwarp.
+// No lane branches on the network's structure and there is no block-wide barrier.
+// The arithmetic and the Philox streams are those of cle_fused_kernel (same sums in the
+// same order: a padded edge has weight 0 and reads the constant-0 slot; a padded term
+// has coefficient 0 and a padded source reads a constant slot holding 1 (cooperative)
+// or 0 (redundant), which leave the product unchanged), so both kernels give
+// identical results.
 #pragma once
 #include "cle_device.cuh"
 #include "cle_internal.h"
@@ -28,14 +27,14 @@ constexpr int kWarpcellWarps = 4;  // warps per block
 __host__ __device__ inline int warpcell_lanes_per_cell(int G, int gpl) { return (G + gpl - 1) / gpl; }
 __host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 32 / warpcell_lanes_per_cell(G, gpl); }
 
-// Row of one cell's regulator activations: NREG slots, then the constants 0 and 1 read
-// by padded term sources; odd length so the rows of a warp's cells fall in different banks.
-__host__ __device__ constexpr int warpcell_ld(int nreg) { return nreg + 3; }
+// Activation row of one cell: n_reg regulator slots, the constants 0 (slot n_reg) and 1
+// (slot n_reg + 1), a write-only slot for genes that regulate nothing (n_reg + 2); odd
+// length so the rows of a warp's cells start in different banks.
+__host__ __device__ inline int warpcell_ld(int n_reg) { return (n_reg + 3) | 1; }
 
-template <int NREG>
-__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl) {
+__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg) {
     const int cpw = warpcell_cells_per_warp(G, gpl);
-    const size_t b = (size_t)kWarpcellWarps * 2 * (cpw + 1) * warpcell_ld(NREG) * sizeof(float);
+    const size_t b = (size_t)kWarpcellWarps * (cpw + 1) * warpcell_ld(n_reg) * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
@@ -48,16 +47,21 @@ __device__ __forceinline__ uint32_t quad_word(const uint4& w, int u, int i) {
     return i == 0 ? (hi ? w.z : w.x) : (hi ? w.w : w.y);
 }
 
+__device__ __forceinline__ float& smem_f32(unsigned char* base, uint32_t off) {
+    return *reinterpret_cast<float*>(base + off);
+}
+
 // One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
-template <int GPL, int NREG, int KMAX, bool POP>
+// RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
+template <int GPL, int EMAX, int KMAX, bool POP, bool RK>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
-    const float* __restrict__ wdense = a.wdense;
+    constexpr int KM = KMAX > 0 ? KMAX : 1;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
     const int cpw = 32 / lpc;
-    constexpr int ld = warpcell_ld(NREG);
-    float* act_all = reinterpret_cast<float*>(smem_raw);
+    const int n_reg = a.n_reg;
+    const int ld = warpcell_ld(n_reg);
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -71,23 +75,28 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     const int64_t cidx = cell < N ? cell : N - 1;
     const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
     const Key key{a.key0, a.key1};
-    const int n_reg = a.n_reg;
-    float* act_w = act_all + (size_t)warp * 2 * (cpw + 1) * ld;
-    for (int r = lane; r < 2 * (cpw + 1); r += 32) {  // constant slots of every row
-        act_w[(size_t)r * ld + NREG] = 0.0f;
-        act_w[(size_t)r * ld + NREG + 1] = 1.0f;
+
+    // constant slots of this warp's rows (written once; Hill stores never touch them)
+    float* rows = reinterpret_cast<float*>(smem_raw) + (size_t)warp * (cpw + 1) * ld;
+    for (int r = lane; r < cpw + 1; r += 32) {
+        rows[(size_t)r * ld + n_reg] = 0.0f;
+        rows[(size_t)r * ld + n_reg + 1] = 1.0f;
     }
     __syncwarp();
+    const uint32_t row = (uint32_t)(((size_t)warp * (cpw + 1) + cl) * ld * sizeof(float));
+    auto slot_addr = [&](int slot) { return row + (uint32_t)slot * (uint32_t)sizeof(float); };
 
     // per-lane gene constants
-    float beta[GPL], cneg[GPL], W[GPL][NREG];
+    float beta[GPL], cneg[GPL];
     float inv_on[GPL], inv_off[GPL];
-    int slot[GPL];
-    bool valid[GPL];
-    // padded non-additive terms: reg += coef * (off + sgn * prod_q (off + sgn * act[src_q]))
+    uint32_t hill_at[GPL];         // where this gene's activation is stored
+    float ew[GPL][EMAX];           // padded in-edges: weight, source address
+    uint32_t ea[GPL][EMAX];
+    // padded terms: reg += coef * (off + sgn * prod_q (off + sgn * act[src_q]))
     // with (sgn, off) = (1, 0) cooperative, (-1, 1) redundant
-    float tc[GPL][KMAX > 0 ? KMAX : 1], tsg[GPL][KMAX > 0 ? KMAX : 1], tof[GPL][KMAX > 0 ? KMAX : 1];
-    int ts[GPL][KMAX > 0 ? KMAX : 1][kLaneSrc];
+    float tc[GPL][KM], tsg[GPL][KM], tof[GPL][KM];
+    uint32_t ta[GPL][KM][kLaneSrc];
+    bool valid[GPL];
 #pragma unroll
     for (int i = 0; i < GPL; ++i) {
         const int g = u * GPL + i;
@@ -98,18 +107,21 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         cneg[i] = gr.cneg;
         inv_on[i] = gr.inv_on;
         inv_off[i] = valid[i] ? gr.inv_off : __int_as_float(0x7FC00000);  // NaN: never switches
-        slot[i] = valid[i] ? gr.slot : -1;
+        hill_at[i] = slot_addr(valid[i] && gr.slot >= 0 ? gr.slot : n_reg + 2);
 #pragma unroll
-        for (int r = 0; r < NREG; ++r) W[i][r] = (valid[i] && r < n_reg) ? wdense[(size_t)gg * n_reg + r] : 0.0f;
+        for (int e = 0; e < EMAX; ++e) {
+            const int2 ed = a.lane_in[(size_t)gg * kLaneEdges + e];
+            ew[i][e] = valid[i] ? __int_as_float(ed.y) : 0.0f;
+            ea[i][e] = slot_addr(ed.x);
+        }
 #pragma unroll
         for (int k = 0; k < KMAX; ++k) {
             const LaneTerm t = a.lane_na[(size_t)gg * kLaneTerms + k];
-            const bool on_k = valid[i];
-            tc[i][k] = on_k ? t.coef : 0.0f;
+            tc[i][k] = valid[i] ? t.coef : 0.0f;
             tsg[i][k] = t.kind == 0 ? 1.0f : -1.0f;
             tof[i][k] = t.kind == 0 ? 0.0f : 1.0f;
 #pragma unroll
-            for (int q = 0; q < kLaneSrc; ++q) ts[i][k][q] = t.src[q];
+            for (int q = 0; q < kLaneSrc; ++q) ta[i][k][q] = slot_addr(t.src[q]);
         }
     }
     const int quad = GPL == 4 ? u : (u >> 1);
@@ -179,7 +191,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 
     // ---- fused step loop --------------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
-    int buf = 0;
+    const bool any_reg = n_reg > 0;
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {  // telegraph: switch when the waiting time runs out
@@ -190,35 +202,33 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
                 ns[i] = next_switch(s, w.x, (on & bit) ? inv_off[i] : inv_on[i]);
             }
         }
-        float* act = act_w + (size_t)buf * (cpw + 1) * ld + (size_t)cl * ld;
-        if (n_reg > 0) {
+        __syncwarp();  // every lane has read the row of the previous step
+        if (any_reg) {
 #pragma unroll
-            for (int i = 0; i < GPL; ++i)
-                if (slot[i] >= 0) act[slot[i]] = hill_act(p[i], a.Kn, a.hill_n, a.hill_int);
+            for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = hill_act(p[i], a.Kn, a.hill_n, a.hill_int);
         }
         BM bm[GPL];
 #pragma unroll
         for (int h = 0; h < GPL / 2; ++h) {
-            const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(u * (GPL / 2) + h),
-                                   tagword(TAG_NORMAL, a.stream), key);
+            const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
+            const uint4 w = RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1)
+                               : philox(gcell, (uint32_t)s, c2, c3, key);
             bm[2 * h] = box_muller_parts(w.x, w.y);
             bm[2 * h + 1] = box_muller_parts(w.z, w.w);
         }
-        __syncwarp();
-        float areg[NREG];
-#pragma unroll
-        for (int r = 0; r < NREG; ++r) areg[r] = r < n_reg ? act[r] : 0.0f;
+        __syncwarp();  // the cell's row is complete
         const float Vf = POP ? (float)V : 1.0f;
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
             float reg = cneg[i];
 #pragma unroll
-            for (int r = 0; r < NREG; ++r) reg = fmaf(W[i][r], areg[r], reg);
+            for (int e = 0; e < EMAX; ++e) reg = fmaf(ew[i][e], smem_f32(smem_raw, ea[i][e]), reg);
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {  // x and 1-x are exact as fmaf(+-1, x, 0 or 1)
                 float prod = 1.0f;
 #pragma unroll
-                for (int q = 0; q < kLaneSrc; ++q) prod *= fmaf(tsg[i][k], act[ts[i][k][q]], tof[i][k]);
+                for (int q = 0; q < kLaneSrc; ++q)
+                    prod *= fmaf(tsg[i][k], smem_f32(smem_raw, ta[i][k][q]), tof[i][k]);
                 reg = fmaf(tc[i][k], fmaf(tsg[i][k], prod, tof[i][k]), reg);
             }
             float tx = reg + beta[i];
@@ -227,7 +237,6 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             em_update(m[i], p[i], tx, bm[i], mu_m, mu_p, k_t, dt);
         }
         if (POP) V = __dmul_rn(V, a.growth_factor);
-        buf ^= 1;
     }
 
     // ---- epilogue (as cle_fused_kernel) ------------------------------------------------
@@ -318,14 +327,14 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     }
 }
 
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    warpcell_tile<GPL, NREG, KMAX, POP>(a, blockIdx.x, ctl, smem_raw);
+    warpcell_tile<GPL, EMAX, KMAX, POP, true>(a, blockIdx.x, ctl, smem_raw);
 }
 
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
 cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
@@ -338,15 +347,15 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         __syncthreads();
         if (it >= n_items) return;
         const TileWork w = items[it];
-        warpcell_tile<GPL, NREG, KMAX, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        warpcell_tile<GPL, EMAX, KMAX, POP, false>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
         __syncthreads();
     }
 }
 
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
-    auto k = cle_warpcell_kernel<GPL, NREG, KMAX, POP>;
-    const size_t smem = warpcell_smem_bytes<NREG>(a.G, GPL);
+    auto k = cle_warpcell_kernel<GPL, EMAX, KMAX, POP>;
+    const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
@@ -355,10 +364,10 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int GPL, int NREG, int KMAX, bool POP>
+template <int GPL, int EMAX, int KMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    auto k = cle_warpcell_queue_kernel<GPL, NREG, KMAX, POP>;
+    auto k = cle_warpcell_queue_kernel<GPL, EMAX, KMAX, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, 32 * kWarpcellWarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
@@ -368,17 +377,17 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
 }  // namespace scrna
 
 // Explicit instantiation of both launchers of one kernel variant (one .cu file per
-// (GPL, NREG) pair keeps the parallel build balanced).
-#define SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, KMAX, POP)                                                        \
-    template cudaError_t scrna::warpcell_launch_t<GPL, NREG, KMAX, POP>(const FusedArgs&, cudaStream_t);         \
-    template cudaError_t scrna::warpcell_queue_launch_t<GPL, NREG, KMAX, POP>(                                   \
+// (GPL, EMAX) pair keeps the parallel build balanced).
+#define SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, KMAX, POP)                                                        \
+    template cudaError_t scrna::warpcell_launch_t<GPL, EMAX, KMAX, POP>(const FusedArgs&, cudaStream_t);         \
+    template cudaError_t scrna::warpcell_queue_launch_t<GPL, EMAX, KMAX, POP>(                                   \
         const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int, cudaStream_t);
-#define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, NREG)       \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 0, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 0, true)      \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 1, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 1, true)      \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 2, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 2, true)      \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 4, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, NREG, 4, true)
+#define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, EMAX)       \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 1, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 1, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 2, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 2, true)      \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 4, false)     \
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 4, true)
