@@ -177,17 +177,30 @@ float orc_log2f(float u) {
 }
 
 /* Geometric number of steps (>= 1) until the next switch for stay probability
- * 2^(1/inv): 1 + floor(log2(u) * inv), u = ((w>>8)+1) 2^-24 in (0, 1]. */
-int32_t orc_geom_steps(uint32_t w, float inv) {
-    float u = (float)((w >> 8) + 1u) * 5.9604644775390625e-8f;
+ * 2^(1/inv): 1 + floor(log2(u) * inv) for a uniform u in (0, 1]. */
+int32_t orc_geom_steps_u(float u, float inv) {
     float t = orc_log2f(u) * inv;
     if (!(t < 1.0e9f)) t = 1.0e9f;
     return 1 + (int32_t)floorf(t);
 }
 
+/* Initial and daughter waiting times: u = ((w>>8)+1) 2^-24 from a dedicated switch word. */
+int32_t orc_geom_steps(uint32_t w, float inv) {
+    return orc_geom_steps_u((float)((w >> 8) + 1u) * 5.9604644775390625e-8f, inv);
+}
+
+/* Waiting time drawn when a promoter switches at a step: the 9 low bits of each of the
+ * gene's two normal words of that step (Box-Muller reads only their top 23 bits),
+ * u = (((w0 & 511) << 9 | (w1 & 511)) + 1) 2^-18. */
+float orc_switch_uniform(uint32_t w0, uint32_t w1) {
+    uint32_t b = ((w0 & 0x1FFu) << 9) | (w1 & 0x1FFu);
+    return (float)(b + 1u) * 3.814697265625e-06f;
+}
+
+static inline int32_t clamp_step(int64_t t) { return t > 2147483647 ? 2147483647 : (int32_t)t; }
+
 static inline int32_t next_switch(int64_t step, uint32_t w, float inv) {
-    int64_t t = step + orc_geom_steps(w, inv);
-    return t > 2147483647 ? 2147483647 : (int32_t)t;
+    return clamp_step(step + orc_geom_steps(w, inv));
 }
 
 /* ---------------------------------------------------------------------------
@@ -251,14 +264,16 @@ static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, ui
     int G = net->G;
     /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
      * the per-step Bernoulli(1 - exp(-k dt)) switch is sampled as its geometric waiting
-     * time, redrawn only when the promoter switches. */
+     * time, redrawn only when the promoter switches, from the spare bits of the gene's
+     * normal words of this step. */
     if (pp->bursty) {
         for (int g = 0; g < G; ++g) {
             if (!pp->tel[g] || (int64_t)step != ns[g]) continue;
             on[g] ^= 1;
             uint32_t w[4];
-            draw(seed, cell, step, (uint32_t)g, ORC_TAG_SWITCH, stream, w);
-            ns[g] = next_switch(step, w[0], on[g] ? pp->inv_off[g] : pp->inv_on[g]);
+            draw(seed, cell, step, (uint32_t)(g >> 1), ORC_TAG_NORMAL, stream, w);
+            float u = (g & 1) ? orc_switch_uniform(w[2], w[3]) : orc_switch_uniform(w[0], w[1]);
+            ns[g] = clamp_step((int64_t)step + orc_geom_steps_u(u, on[g] ? pp->inv_off[g] : pp->inv_on[g]));
         }
     }
     /* Hill fractions (cle.jl:79-82) */

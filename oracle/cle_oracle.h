@@ -105,9 +105,13 @@ int64_t orc_binomial_invcdf(int64_t n, double p, uint64_t seed, uint32_t stream,
                             uint32_t cell, uint32_t gene);
 
 /* log2 of u in [2^-24, 1] by the explicitly rounded FP32 atanh series, and the
- * geometric telegraph waiting time 1 + floor(log2(u(w)) * inv) (>= 1 steps). */
+ * geometric telegraph waiting time 1 + floor(log2(u) * inv) (>= 1 steps) for a uniform
+ * u in (0, 1]: from a switch word, u = ((w>>8)+1) 2^-24 (initial and daughter waiting
+ * times); at a switch step, u = orc_switch_uniform of the gene's two normal words. */
 float orc_log2f(float u);
+int32_t orc_geom_steps_u(float u, float inv);
 int32_t orc_geom_steps(uint32_t w, float inv);
+float orc_switch_uniform(uint32_t w0, uint32_t w1);
 
 /* Binomial(n, 1/2) partition draw (popcount of n Philox bits). */
 int64_t orc_binomial_half(int64_t n, uint64_t seed, uint32_t stream, uint32_t cell,

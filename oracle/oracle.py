@@ -197,3 +197,17 @@ def geom_steps(w, inv):
     L.orc_geom_steps.argtypes = [C.c_uint32, C.c_float]
     L.orc_geom_steps.restype = C.c_int32
     return L.orc_geom_steps(int(w), float(inv))
+
+
+def geom_steps_u(u, inv):
+    L = lib()
+    L.orc_geom_steps_u.argtypes = [C.c_float, C.c_float]
+    L.orc_geom_steps_u.restype = C.c_int32
+    return L.orc_geom_steps_u(float(u), float(inv))
+
+
+def switch_uniform(w0, w1):
+    L = lib()
+    L.orc_switch_uniform.argtypes = [C.c_uint32, C.c_uint32]
+    L.orc_switch_uniform.restype = C.c_float
+    return L.orc_switch_uniform(int(w0), int(w1))

@@ -11,7 +11,8 @@ namespace scrna {
 // the library's reproducibility contract: a run is a pure function of (seed, stream).
 enum : uint32_t {
     TAG_NORMAL = 1,      // (cell, step, gene_pair)    -> Box-Muller pairs for genes 2k, 2k+1
-    TAG_SWITCH = 2,      // (cell, step, gene_quad)    -> one telegraph word per gene
+    TAG_SWITCH = 2,      // (cell, 0, gene), (cell, division step, gene | kDaughterSwitch)
+                         //   -> initial / daughter waiting time of a promoter
     TAG_PROMOTER = 3,    // (cell, 0, gene_quad)       -> initial promoter state
     TAG_VOLUME = 4,      // (cell, 0, 0)               -> initial volume
     TAG_MORAN = 5,       // (mother, step, 0)          -> replaced slot
@@ -197,17 +198,31 @@ __device__ __forceinline__ float own_log2f(float u) {
     return __fmaf_rn(__fmul_rn(z, q), 2.88539008f, (float)e);
 }
 
-__device__ __forceinline__ int32_t geom_steps(uint32_t w, float inv) {
-    const float u = __fmul_rn(__uint2float_rn((w >> 8) + 1u), 5.9604644775390625e-8f);
+__device__ __forceinline__ int32_t geom_steps_u(float u, float inv) {
     float t = __fmul_rn(own_log2f(u), inv);
     if (!(t < 1.0e9f)) t = 1.0e9f;
     return 1 + (int32_t)floorf(t);
 }
 
-// Step of the next switch after `step` (saturating), for stay-probability parameter inv.
-__device__ __forceinline__ int32_t next_switch(int64_t step, uint32_t w, float inv) {
-    const int64_t t = step + geom_steps(w, inv);
+// Step of the next switch after `step` (saturating), for stay-probability parameter inv
+// and a uniform u in (0, 1].
+__device__ __forceinline__ int32_t next_switch_u(int64_t step, float u, float inv) {
+    const int64_t t = step + geom_steps_u(u, inv);
     return t > 2147483647 ? 2147483647 : (int32_t)t;
+}
+
+// Initial and daughter waiting times come from a dedicated switch word w:
+// u = ((w>>8)+1) 2^-24.
+__device__ __forceinline__ int32_t next_switch(int64_t step, uint32_t w, float inv) {
+    return next_switch_u(step, __fmul_rn(__uint2float_rn((w >> 8) + 1u), 5.9604644775390625e-8f), inv);
+}
+
+// A promoter that switches at a step draws its next waiting time from the spare bits of
+// the gene's two normal words of that step (Box-Muller reads only their top 23 bits):
+// u = (((w0 & 511) << 9 | (w1 & 511)) + 1) 2^-18, so a switch costs no Philox call.
+__device__ __forceinline__ float switch_uniform(uint32_t w0, uint32_t w1) {
+    const uint32_t b = ((w0 & 0x1FFu) << 9) | (w1 & 0x1FFu);
+    return __fmul_rn(__uint2float_rn(b + 1u), 3.814697265625e-06f);
 }
 
 constexpr int32_t kNever = 2147483647;

@@ -164,22 +164,6 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     int buf = 0;
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
-        // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
-        // a gene switches when its waiting time runs out, then draws the next one
-#pragma unroll
-        for (int j = 0; j < UPT; ++j) {
-            const int q = warp + j * NW;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                if (s == ns[j][i]) {
-                    const int g = 4 * q + i;
-                    const uint32_t bit = 1u << (4 * j + i);
-                    on ^= bit;
-                    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-                    ns[j][i] = next_switch(s, w.x, (on & bit) ? sm.genes[g].inv_off : sm.genes[g].inv_on);
-                }
-            }
-        }
         // Hill activations of regulator genes -> slot table
         float* act = sm.act + (size_t)buf * a.n_reg * 32;
         if (has_reg) {
@@ -215,6 +199,15 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                     const int i = 2 * h + k;
                     const int g = g0 + k;
                     if (g >= G) continue;
+                    // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
+                    // a gene switches when its waiting time runs out and draws the next one
+                    // from the spare bits of its normal words
+                    if (s == ns[j][i]) {
+                        const uint32_t bit = 1u << (4 * j + i);
+                        on ^= bit;
+                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                        ns[j][i] = next_switch_u(s, us, (on & bit) ? sm.genes[g].inv_off : sm.genes[g].inv_on);
+                    }
                     const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
                     const GeneRec gr = sm.genes[g];
                     float reg = gr.cneg;

@@ -26,12 +26,15 @@ __global__ void __launch_bounds__(128) cle_plain_step_kernel(const PlainArgs a) 
     const GeneRec gr = a.genes[g];
     const int s = a.step;
 
-    // telegraph switching: the promoter switches when its waiting time runs out
+    // normals of this (cell, step, gene)
+    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(g >> 1), tagword(TAG_NORMAL, a.stream), key);
+    const uint32_t w0 = (g & 1) ? w.z : w.x, w1 = (g & 1) ? w.w : w.y;
+    // telegraph switching: the promoter switches when its waiting time runs out and draws
+    // the next one from the spare bits of its normal words
     bool on = a.prom[idx];
     if (s == a.NS[idx]) {
         on = !on;
-        const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-        a.NS[idx] = next_switch(s, w.x, on ? gr.inv_off : gr.inv_on);
+        a.NS[idx] = next_switch_u(s, switch_uniform(w0, w1), on ? gr.inv_off : gr.inv_on);
         a.prom[idx] = on;
     }
     // reg = A_pos*act + A_neg*rep over the in-edges, from the previous step's proteins
@@ -59,11 +62,8 @@ __global__ void __launch_bounds__(128) cle_plain_step_kernel(const PlainArgs a) 
         const double val = na.kind == 0 ? prod : __dadd_rn(1.0, -prod);
         reg = __dadd_rn(reg, __dmul_rn(a.na_coef64[e], val));
     }
-    // normals of this (cell, step, gene)
-    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(g >> 1), tagword(TAG_NORMAL, a.stream), key);
     double zm, zp;
-    if (g & 1) box_muller_f64(w.z, w.w, &zm, &zp);
-    else box_muller_f64(w.x, w.y, &zm, &zp);
+    box_muller_f64(w0, w1, &zm, &zp);
 
     double tx = __dadd_rn(reg, a.beta64[g]);
     if (!on) tx = 0.0;

@@ -118,10 +118,10 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
             bool on = true;
             if (BURSTY) {
                 on = a.prom[e];
-                if (s == a.NS[e]) {
+                if (s == a.NS[e]) {  // next waiting time from the spare bits of the normal words
                     on = !on;
-                    const uint4 ws = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-                    a.NS[e] = next_switch(s, ws.x, on ? gr[h].inv_off : gr[h].inv_on);
+                    const float us = h == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                    a.NS[e] = next_switch_u(s, us, on ? gr[h].inv_off : gr[h].inv_on);
                     a.prom[e] = on;
                 }
             }

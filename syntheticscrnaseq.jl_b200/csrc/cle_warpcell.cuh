@@ -51,9 +51,20 @@ __device__ __forceinline__ float& smem_f32(unsigned char* base, uint32_t off) {
     return *reinterpret_cast<float*>(base + off);
 }
 
+// Hill activation p^n / (p^n + K^n); HN == 2 is the square without the exponent dispatch.
+template <int HN>
+__device__ __forceinline__ float warpcell_hill(float p, const FusedArgs& a) {
+    if (HN == 2) {
+        const float pn = p * p;
+        return fminf(pn * frcp_approx(pn + a.Kn), 1.0f);  // as hill_act with hill_int == 2
+    }
+    return hill_act(p, a.Kn, a.hill_n, a.hill_int);
+}
+
 // One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
 // RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
-template <int GPL, int EMAX, int KMAX, bool POP, bool RK>
+// HN: 2 for a Hill exponent of exactly 2, else 0 (any exponent).
+template <int GPL, int EMAX, int KMAX, bool POP, bool RK, int HN>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
     constexpr int KM = KMAX > 0 ? KMAX : 1;
@@ -192,20 +203,14 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     // ---- fused step loop --------------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     const bool any_reg = n_reg > 0;
-    for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
+    int32_t ns_min = ns[0];  // earliest switch of the lane's genes
 #pragma unroll
-        for (int i = 0; i < GPL; ++i) {  // telegraph: switch when the waiting time runs out
-            if (s == ns[i]) {
-                const uint32_t bit = 1u << i;
-                on ^= bit;
-                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(u * GPL + i), tagword(TAG_SWITCH, a.stream), key);
-                ns[i] = next_switch(s, w.x, (on & bit) ? inv_off[i] : inv_on[i]);
-            }
-        }
+    for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
+    for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
         __syncwarp();  // every lane has read the row of the previous step
         if (any_reg) {
 #pragma unroll
-            for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = hill_act(p[i], a.Kn, a.hill_n, a.hill_int);
+            for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = warpcell_hill<HN>(p[i], a);
         }
         BM bm[GPL];
 #pragma unroll
@@ -213,8 +218,25 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
             const uint4 w = RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1)
                                : philox(gcell, (uint32_t)s, c2, c3, key);
+            if (s == ns_min) {  // telegraph: a promoter switches when its waiting time runs out
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int i = 2 * h + k;
+                    if (s == ns[i]) {
+                        const uint32_t bit = 1u << i;
+                        on ^= bit;
+                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                        ns[i] = next_switch_u(s, us, (on & bit) ? inv_off[i] : inv_on[i]);
+                    }
+                }
+            }
             bm[2 * h] = box_muller_parts(w.x, w.y);
             bm[2 * h + 1] = box_muller_parts(w.z, w.w);
+        }
+        if (s == ns_min) {
+            ns_min = ns[0];
+#pragma unroll
+            for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
         }
         __syncwarp();  // the cell's row is complete
         const float Vf = POP ? (float)V : 1.0f;
@@ -331,7 +353,8 @@ template <int GPL, int EMAX, int KMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    warpcell_tile<GPL, EMAX, KMAX, POP, true>(a, blockIdx.x, ctl, smem_raw);
+    if (a.hill_int == 2) warpcell_tile<GPL, EMAX, KMAX, POP, true, 2>(a, blockIdx.x, ctl, smem_raw);
+    else warpcell_tile<GPL, EMAX, KMAX, POP, true, 0>(a, blockIdx.x, ctl, smem_raw);
 }
 
 template <int GPL, int EMAX, int KMAX, bool POP>
@@ -347,7 +370,10 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         __syncthreads();
         if (it >= n_items) return;
         const TileWork w = items[it];
-        warpcell_tile<GPL, EMAX, KMAX, POP, false>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        const FusedArgs& a = args[w.arg];
+        const TileCtl& ctl = use_shared ? shared_ctl : w.ctl;
+        if (a.hill_int == 2) warpcell_tile<GPL, EMAX, KMAX, POP, false, 2>(a, w.tile, ctl, smem_raw);
+        else warpcell_tile<GPL, EMAX, KMAX, POP, false, 0>(a, w.tile, ctl, smem_raw);
         __syncthreads();
     }
 }

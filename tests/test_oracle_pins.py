@@ -106,6 +106,27 @@ def test_telegraph_mean(pkg, orc):
     assert abs(frac_on - k_on / (k_on + k_off)) < 0.02
 
 
+def test_switch_waiting_time_is_geometric(orc):
+    """A promoter switching at a step draws its next waiting time from the 18 spare bits
+    of its normal words: over all 2^18 uniforms, P(K > k) = q^k (q = exp(-k_sw dt)) to
+    within the grid spacing, i.e. the per-step Bernoulli switching of
+    tauleap_binomial.jl:111-121."""
+    rng = np.random.default_rng(1)
+    for w0, w1 in rng.integers(0, 2**32, size=(50, 2), dtype=np.uint64):
+        w0, w1 = int(w0), int(w1)
+        want = ((((w0 & 511) << 9) | (w1 & 511)) + 1) / 2.0**18
+        assert orc.switch_uniform(w0, w1) == np.float32(want)
+    for rate, dt in ((0.5, 0.01), (7.0, 0.01), (2.0, 0.1)):
+        inv = np.float32(-math.log(2.0) / (rate * dt))
+        q = math.exp(-rate * dt)
+        u = (np.arange(2**18, dtype=np.float64) + 1.0) / 2.0**18
+        K = np.array([orc.geom_steps_u(x, inv) for x in u])
+        assert K.min() >= 1
+        mean_wait = 1.0 / (1.0 - q)
+        for k in np.unique(np.linspace(0, 5 * mean_wait, 40).astype(int)):
+            assert abs(np.mean(K > k) - q ** k) < 2.0**-16, (rate, dt, k)
+
+
 def test_capture_bands(orc):
     """test/test_capture.jl:1-31 on the inverse-CDF capture sampler."""
     rng = np.random.default_rng(42)
