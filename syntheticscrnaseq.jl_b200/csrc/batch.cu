@@ -37,11 +37,11 @@ struct BatchNet {
 };
 
 struct GroupKey {
-    int warp, gpl, emax, kmax, upt, pop, interval;
+    int warp, gpl, emax, tmax, upt, pop, interval;
     int64_t n_steps;
     bool operator<(const GroupKey& r) const {
-        return std::tie(warp, gpl, emax, kmax, upt, pop, interval, n_steps) <
-               std::tie(r.warp, r.gpl, r.emax, r.kmax, r.upt, r.pop, r.interval, r.n_steps);
+        return std::tie(warp, gpl, emax, tmax, upt, pop, interval, n_steps) <
+               std::tie(r.warp, r.gpl, r.emax, r.tmax, r.upt, r.pop, r.interval, r.n_steps);
     }
 };
 
@@ -135,7 +135,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         k.warp = x->kc.warp;
         k.gpl = x->kc.warp ? x->kc.gpl : 0;
         k.emax = x->kc.warp ? x->kc.emax : 0;
-        k.kmax = x->kc.warp ? x->kc.kmax : 0;
+        k.tmax = x->kc.warp ? x->kc.tmax : 0;
         k.upt = x->kc.warp ? 0 : x->kc.block.upt;
         k.pop = x->pop != nullptr;
         k.interval = x->pop ? x->pop->div_check_interval : 0;
@@ -190,7 +190,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
             if (k.warp)
                 return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
-                                             k.emax, k.kmax, k.pop != 0, smem, grid, ctl, use_shared, g.stream);
+                                             k.emax, k.tmax, k.pop != 0, smem, grid, ctl, use_shared, g.stream);
             return fused_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
                                       smem, k.pop != 0, grid, ctl, use_shared, g.stream);
         };

@@ -23,8 +23,8 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 int warpcell_max_genes();
 int warpcell_emax_class(int max_in);
 int warpcell_pick_gpl(int G, bool bursty, int emax);
-size_t warpcell_smem(int G, int gpl, int n_reg);
-cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int kmax, bool pop, cudaStream_t st);
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms);
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
@@ -273,49 +273,57 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     d.na_coef64 = n->b_na_coef64.as<double>();
     d.beta64 = n->b_beta64.as<double>();
     for (int g = 0; g < G; ++g) d.bursty = d.bursty || std::isfinite(n->k_on[g]);
-    // padded per-gene lists of the warp-per-cell-group kernel (small networks)
+    // tables of the warp-per-cell-group kernel (small networks): per gene its additive
+    // edges then one edge per term targeting it (term j's value sits in slot n_reg+3+j)
     bool lane_ok = G <= warpcell_max_genes();
-    int emax = 0, kmax = 0;
+    int max_in = 0;
     for (int g = 0; g < G && lane_ok; ++g) {
-        emax = std::max(emax, n->in_end[g] - n->in_begin[g]);
-        kmax = std::max(kmax, n->na_count[g]);
+        max_in = std::max(max_in, n->in_end[g] - n->in_begin[g] + n->na_count[g]);
         for (int e = n->na_begin[g]; e < n->na_begin[g] + n->na_count[g]; ++e)
             lane_ok = lane_ok && n->na[e].src_end - n->na[e].src_begin <= kLaneSrc;
     }
-    lane_ok = lane_ok && emax <= kLaneEdges && kmax <= kLaneTerms;
+    lane_ok = lane_ok && max_in <= kLaneEdges;
+    const int emax = warpcell_emax_class(max_in);
+    const int gpl = warpcell_pick_gpl(G, d.bursty, emax);
+    const int lpc = (G + gpl - 1) / gpl;
+    const int tmax = (d.n_na + lpc - 1) / lpc;
+    lane_ok = lane_ok && tmax <= kLaneTerms;
     if (lane_ok) {
-        // same order as the edge tables (bit-identical sums with the block kernel)
         const int zero_slot = d.n_reg, one_slot = d.n_reg + 1;  // constant slots of the kernel's rows
         std::vector<int2> li((size_t)G * kLaneEdges, make_int2(zero_slot, 0));
-        std::vector<LaneTerm> ln((size_t)G * kLaneTerms);
         for (int g = 0; g < G; ++g) {
-            for (int e = n->in_begin[g], k = 0; e < n->in_end[g]; ++e, ++k) {
+            int k = 0;
+            for (int e = n->in_begin[g]; e < n->in_end[g]; ++e, ++k) {
                 int32_t slot, wbits;
                 std::memcpy(&slot, &n->in_edge[e].y, 4);
                 std::memcpy(&wbits, &n->in_edge[e].x, 4);
                 li[(size_t)g * kLaneEdges + k] = make_int2(slot, wbits);
             }
-            for (int k = 0; k < kLaneTerms; ++k) {
-                LaneTerm t{};
-                for (int q = 0; q < kLaneSrc; ++q) t.src[q] = one_slot;
-                if (k < n->na_count[g]) {
-                    const NonAdd& na = n->na[n->na_begin[g] + k];
-                    t.coef = na.coef;
-                    t.kind = na.kind;
-                    for (int q = 0; q < kLaneSrc; ++q) {
-                        const int si = na.src_begin + q;
-                        t.src[q] = si < na.src_end ? n->na_src[si] : (na.kind == 0 ? one_slot : zero_slot);
-                    }
-                }
-                ln[(size_t)g * kLaneTerms + k] = t;
+            for (int e = n->na_begin[g]; e < n->na_begin[g] + n->na_count[g]; ++e, ++k) {
+                int32_t wbits;
+                std::memcpy(&wbits, &n->na[e].coef, 4);
+                li[(size_t)g * kLaneEdges + k] = make_int2(d.n_reg + 3 + e, wbits);
             }
         }
+        std::vector<LaneTerm> lt(std::max<size_t>(n->na.size(), 1));
+        for (size_t e = 0; e < n->na.size(); ++e) {
+            const NonAdd& na = n->na[e];
+            LaneTerm t{};
+            t.coef = na.coef;
+            t.kind = na.kind;
+            for (int q = 0; q < kLaneSrc; ++q) {
+                const int si = na.src_begin + q;
+                t.src[q] = si < na.src_end ? n->na_src[si] : (na.kind == 0 ? one_slot : zero_slot);
+            }
+            lt[e] = t;
+        }
         CU(up(n->b_lane_in, li.data(), li.size() * sizeof(int2)));
-        CU(up(n->b_lane_na, ln.data(), ln.size() * sizeof(LaneTerm)));
+        CU(up(n->b_lane_term, lt.data(), lt.size() * sizeof(LaneTerm)));
         d.lane_in = n->b_lane_in.as<int2>();
-        d.lane_na = n->b_lane_na.as<LaneTerm>();
-        d.lane_emax = warpcell_emax_class(emax);
-        d.lane_kmax = kmax <= 2 ? kmax : 4;
+        d.lane_term = n->b_lane_term.as<LaneTerm>();
+        d.lane_gpl = gpl;
+        d.lane_emax = emax;
+        d.lane_tmax = tmax;
     }
     *out = n.release();
     return SCRNA_OK;
@@ -521,7 +529,7 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
         a.cap_sigma = cap->efficiency_std;
     }
     a.lane_in = d.lane_in;
-    a.lane_na = d.lane_na;
+    a.lane_term = d.lane_term;
     for (int r = 0; r < 10; ++r) {
         a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
         a.rk1[r] = a.key1 + (uint32_t)r * 0xBB67AE85u;
@@ -536,11 +544,11 @@ scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     KernelChoice k{};
     const bool warp_ok = d.lane_in != nullptr;
     k.warp = path == SCRNA_PATH_BLOCK ? false : warp_ok;
-    k.gpl = warpcell_pick_gpl(d.G, d.bursty, d.lane_emax);
+    k.gpl = d.lane_gpl;
     k.emax = d.lane_emax;
-    k.kmax = d.lane_kmax;
+    k.tmax = d.lane_tmax;
     k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
-    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg) : k.block.smem;
+    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na) : k.block.smem;
     return k;
 }
 
@@ -560,11 +568,11 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     const bool warp_ok = d.lane_in != nullptr;
     const bool use_warp = o->path == SCRNA_PATH_WARP ? true : o->path == SCRNA_PATH_BLOCK ? false : warp_ok;
     if (use_warp && !warp_ok)
-        return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d in-edges and <= %d cooperative/redundant "
-                    "terms of <= %d sources per gene", warpcell_max_genes(), kLaneEdges, kLaneTerms, kLaneSrc);
-    const int gpl = warpcell_pick_gpl(d.G, d.bursty, d.lane_emax);
+        return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d in-edges (additive and cooperative/redundant) "
+                    "per gene, terms of <= %d sources and <= %d terms per lane", warpcell_max_genes(), kLaneEdges,
+                    kLaneSrc, kLaneTerms);
     auto launch = [&](bool is_pop) -> cudaError_t {
-        return use_warp ? warpcell_launch(a, gpl, d.lane_emax, d.lane_kmax, is_pop, s) : fused_launch(a, L, is_pop, s);
+        return use_warp ? warpcell_launch(a, d.lane_gpl, d.lane_emax, d.lane_tmax, is_pop, s) : fused_launch(a, L, is_pop, s);
     };
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;

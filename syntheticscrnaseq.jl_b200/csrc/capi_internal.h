@@ -78,7 +78,7 @@ struct scrna_net {
     std::vector<double> na_coef64;
     std::vector<int32_t> na_src;
     NetDev dev;
-    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_lane_in, b_lane_na;
+    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_lane_in, b_lane_term;
     // per-run tables cached for the last (kinetics, dt, population mode)
     DevBuf b_genes, b_ginit, b_quad_tel;
     // tensor-core path: W = A_eff as 16-bit [G][Kp] (K-major), nonadd sources compacted
@@ -114,7 +114,7 @@ namespace scrna {
 // Register-path kernel chosen for a network.
 struct KernelChoice {
     bool warp;
-    int gpl, emax, kmax;
+    int gpl, emax, tmax;
     FusedLaunch block;
     size_t smem;
 };
@@ -132,7 +132,7 @@ cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
                                cudaStream_t st);
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int emax, int kmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
+                                  int emax, int tmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
                                   int use_shared, cudaStream_t st);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype);

@@ -48,9 +48,9 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 }
 
 // ---- warp-per-cell-group variant for small networks ---------------------------------------
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st);
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 template <int UPT, bool POP>
@@ -77,10 +77,10 @@ int warpcell_pick_gpl(int G, bool bursty, int emax) {
     return pick;
 }
 
-size_t warpcell_smem(int G, int gpl, int n_reg) {
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms) {
     const int lpc = (G + gpl - 1) / gpl;
     const int cpw = 32 / lpc;
-    const int ld = (n_reg + 3) | 1;  // slots, constants 0 and 1, a write-only slot; odd row length
+    const int ld = (n_reg + 3 + n_terms) | 1;  // slots, constants 0 and 1, a write-only slot, terms
     const size_t b = (size_t)4 * (cpw + 1) * ld * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
@@ -88,20 +88,18 @@ size_t warpcell_smem(int G, int gpl, int n_reg) {
 template <int V>
 using IntC = std::integral_constant<int, V>;
 
-// Calls f(IntC<GPL>, IntC<EMAX>, IntC<KMAX>, bool_constant<POP>) for the runtime shape
+// Calls f(IntC<GPL>, IntC<EMAX>, IntC<TMAX>, bool_constant<POP>) for the runtime shape
 // (gene quads take at most 4 in-edges per gene).
 template <class F>
-static cudaError_t warpcell_dispatch(int gpl, int emax, int kmax, bool pop, F&& f) {
+static cudaError_t warpcell_dispatch(int gpl, int emax, int tmax, bool pop, F&& f) {
     auto by_k = [&](auto g, auto r) -> cudaError_t {
-        switch (kmax * 2 + (pop ? 1 : 0)) {
+        switch (tmax * 2 + (pop ? 1 : 0)) {
             case 0: return f(g, r, IntC<0>{}, std::false_type{});
             case 1: return f(g, r, IntC<0>{}, std::true_type{});
             case 2: return f(g, r, IntC<1>{}, std::false_type{});
             case 3: return f(g, r, IntC<1>{}, std::true_type{});
             case 4: return f(g, r, IntC<2>{}, std::false_type{});
             case 5: return f(g, r, IntC<2>{}, std::true_type{});
-            case 8: return f(g, r, IntC<4>{}, std::false_type{});
-            case 9: return f(g, r, IntC<4>{}, std::true_type{});
             default: return cudaErrorInvalidValue;
         }
     };
@@ -115,16 +113,16 @@ static cudaError_t warpcell_dispatch(int gpl, int emax, int kmax, bool pop, F&& 
     }
 }
 
-cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int kmax, bool pop, cudaStream_t st) {
-    return warpcell_dispatch(gpl, emax, kmax, pop, [&](auto g, auto r, auto k, auto p) {
+cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, bool pop, cudaStream_t st) {
+    return warpcell_dispatch(gpl, emax, tmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(a, st);
     });
 }
 
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int emax, int kmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
+                                  int emax, int tmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
                                   int use_shared, cudaStream_t st) {
-    return warpcell_dispatch(gpl, emax, kmax, pop, [&](auto g, auto r, auto k, auto p) {
+    return warpcell_dispatch(gpl, emax, tmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_queue_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(
             args, items, n_items, counter, smem, grid, shared_ctl, use_shared, st);
     });

@@ -32,13 +32,13 @@ struct NonAdd {
     int32_t src_end;
 };
 
-// Padded per-gene lists of the warp kernel.  An in-edge is {source slot, weight bits};
-// padding is {slot n_reg (constant 0), weight 0}.  A cooperative / redundant term names
-// regulator slots as sources; a padded source names a constant slot (n_reg + 1 holding 1
-// for a cooperative term, n_reg holding 0 for a redundant one) and a padded term has
-// coef 0.
-constexpr int kLaneEdges = 8;  // in-edges per gene
-constexpr int kLaneTerms = 4;  // terms per gene
+// Tables of the warp kernel.  A gene's in-edges are {source slot, weight bits}: its
+// additive edges, then one edge {n_reg + 3 + j, coef_j} per cooperative / redundant term
+// j targeting it; padding is {slot n_reg (constant 0), weight 0}.  A term names regulator
+// slots as sources; a padded source names a constant slot (n_reg + 1 holding 1 for a
+// cooperative term, n_reg holding 0 for a redundant one).
+constexpr int kLaneEdges = 8;  // in-edges per gene (additive + terms)
+constexpr int kLaneTerms = 2;  // terms evaluated per lane
 constexpr int kLaneSrc = 3;    // sources per term
 struct LaneTerm {
     float coef;
@@ -63,9 +63,10 @@ struct NetDev {
     double* na_coef64 = nullptr; // FP64 s*beta_target (baseline path)
     double* beta64 = nullptr;    // FP64 basals (baseline path)
     int2* lane_in = nullptr;     // [G][kLaneEdges] padded in-edges (small networks), or null
-    LaneTerm* lane_na = nullptr; // [G][kLaneTerms] padded non-additive terms (with lane_in)
+    LaneTerm* lane_term = nullptr;  // [n_na] terms with padded sources (with lane_in)
+    int32_t lane_gpl = 0;        // genes per lane of the warp kernel (2 or 4)
     int32_t lane_emax = 0;       // in-edges per gene the warp kernel runs (2, 4 or 8)
-    int32_t lane_kmax = 0;       // terms per gene the warp kernel runs (0, 1, 2 or 4)
+    int32_t lane_tmax = 0;       // terms per lane the warp kernel evaluates (0, 1 or 2)
     bool bursty = false;         // any gene switches (finite k_on)
 };
 
@@ -95,7 +96,7 @@ struct FusedArgs {
     const int32_t* na_src;
     const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
     const int2* lane_in;         // [G][kLaneEdges] padded in-edges (warp kernel)
-    const LaneTerm* lane_na;     // [G][kLaneTerms] padded non-additive terms (warp kernel)
+    const LaneTerm* lane_term;   // [n_na] terms with padded sources (warp kernel)
     // state [G][N]
     float* M;
     float* P;

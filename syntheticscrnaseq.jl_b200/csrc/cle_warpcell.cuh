@@ -1,21 +1,22 @@
 // Warp-per-cell-group register-path CLE kernel for small networks (sm_100a).
 //
-// For G <= 32 genes with at most kLaneEdges additive in-edges and kLaneTerms
-// cooperative / redundant terms (each over at most kLaneSrc sources) per gene, a whole
-// cell lives inside one warp: lane = (cell, unit) where a unit is GPL consecutive genes
-// (a gene pair or a gene quad).  All lanes of a warp run the same instruction stream;
-// what differs per lane sits in registers, loaded once: basal rate, telegraph
-// parameters, and the gene's padded lists of EMAX in-edges (weight, shared-memory
-// address of the source's activation) and KMAX non-additive terms.  Per Euler step:
-//   telegraph switch -> Hill of the lane's genes into the cell's activation row in
-//   shared memory -> Philox + Box-Muller -> __syncwarp -> reg = cneg + sum of EMAX
-//   padded edges + sum of KMAX padded terms -> M, P update -> __syncwarp.
+// For G <= 32 genes, a whole cell lives inside one warp: lane = (cell, unit) where a
+// unit is GPL consecutive genes (a gene pair or a gene quad).  A cell's regulator
+// activations live in one shared-memory row: the regulator slots, the constants 0 and 1,
+// a write-only slot, then one slot per cooperative / redundant term holding that term's
+// value (the product over its sources), so a term enters its target's regulation as one
+// more in-edge.  Each lane keeps in registers its genes' constants and padded lists of
+// EMAX in-edges (weight, shared-memory address of the source slot), and the TMAX terms
+// of the cell that it evaluates.  Per Euler step:
+//   Hill of the lane's genes into the row -> Philox (+ telegraph switch) + Box-Muller
+//   -> __syncwarp -> term values into the row -> __syncwarp -> reg = cneg + sum of EMAX
+//   padded edges -> M, P update.
 // No lane branches on the network's structure and there is no block-wide barrier.
 // The arithmetic and the Philox streams are those of cle_fused_kernel (same sums in the
-// same order: a padded edge has weight 0 and reads the constant-0 slot; a padded term
-// has coefficient 0 and a padded source reads a constant slot holding 1 (cooperative)
-// or 0 (redundant), which leave the product unchanged), so both kernels give
-// identical results.
+// same order: a gene's edges are sorted by slot, so its additive edges come first, then
+// its terms in table order; a padded edge has weight 0 and reads the constant-0 slot; a
+// padded term source reads the constant 1 (cooperative) or 0 (redundant), which leave
+// the product unchanged), so both kernels give identical results.
 #pragma once
 #include "cle_device.cuh"
 #include "cle_internal.h"
@@ -28,13 +29,13 @@ __host__ __device__ inline int warpcell_lanes_per_cell(int G, int gpl) { return 
 __host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 32 / warpcell_lanes_per_cell(G, gpl); }
 
 // Activation row of one cell: n_reg regulator slots, the constants 0 (slot n_reg) and 1
-// (slot n_reg + 1), a write-only slot for genes that regulate nothing (n_reg + 2); odd
-// length so the rows of a warp's cells start in different banks.
-__host__ __device__ inline int warpcell_ld(int n_reg) { return (n_reg + 3) | 1; }
+// (slot n_reg + 1), a write-only slot (n_reg + 2) for values nobody reads, then the
+// n_terms term values; odd length so the rows of a warp's cells start in different banks.
+__host__ __device__ inline int warpcell_ld(int n_reg, int n_terms) { return (n_reg + 3 + n_terms) | 1; }
 
-__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg) {
+__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg, int n_terms) {
     const int cpw = warpcell_cells_per_warp(G, gpl);
-    const size_t b = (size_t)kWarpcellWarps * (cpw + 1) * warpcell_ld(n_reg) * sizeof(float);
+    const size_t b = (size_t)kWarpcellWarps * (cpw + 1) * warpcell_ld(n_reg, n_terms) * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
@@ -64,15 +65,16 @@ __device__ __forceinline__ float warpcell_hill(float p, const FusedArgs& a) {
 // One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
 // RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
 // HN: 2 for a Hill exponent of exactly 2, else 0 (any exponent).
-template <int GPL, int EMAX, int KMAX, bool POP, bool RK, int HN>
+template <int GPL, int EMAX, int TMAX, bool POP, bool RK, int HN>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
-    constexpr int KM = KMAX > 0 ? KMAX : 1;
+    constexpr int TM = TMAX > 0 ? TMAX : 1;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
     const int cpw = 32 / lpc;
     const int n_reg = a.n_reg;
-    const int ld = warpcell_ld(n_reg);
+    const int n_terms = a.n_na;
+    const int ld = warpcell_ld(n_reg, n_terms);
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -103,10 +105,21 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     uint32_t hill_at[GPL];         // where this gene's activation is stored
     float ew[GPL][EMAX];           // padded in-edges: weight, source address
     uint32_t ea[GPL][EMAX];
-    // padded terms: reg += coef * (off + sgn * prod_q (off + sgn * act[src_q]))
-    // with (sgn, off) = (1, 0) cooperative, (-1, 1) redundant
-    float tc[GPL][KM], tsg[GPL][KM], tof[GPL][KM];
-    uint32_t ta[GPL][KM][kLaneSrc];
+    // terms this lane evaluates (term u + k lpc): value = off + sgn * prod_q (off + sgn * act[src_q])
+    // with (sgn, off) = (1, 0) cooperative, (-1, 1) redundant, stored at tout
+    float tsg[TM], tof[TM];
+    uint32_t ta[TM][kLaneSrc], tout[TM];
+#pragma unroll
+    for (int k = 0; k < TMAX; ++k) {
+        const int j = u + k * lpc;
+        const bool has = lane_ok && j < n_terms;
+        const LaneTerm t = a.lane_term[has ? j : 0];
+        tsg[k] = t.kind == 0 ? 1.0f : -1.0f;
+        tof[k] = t.kind == 0 ? 0.0f : 1.0f;
+#pragma unroll
+        for (int q = 0; q < kLaneSrc; ++q) ta[k][q] = slot_addr(t.src[q]);
+        tout[k] = slot_addr(has ? n_reg + 3 + j : n_reg + 2);
+    }
     bool valid[GPL];
 #pragma unroll
     for (int i = 0; i < GPL; ++i) {
@@ -124,15 +137,6 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             const int2 ed = a.lane_in[(size_t)gg * kLaneEdges + e];
             ew[i][e] = valid[i] ? __int_as_float(ed.y) : 0.0f;
             ea[i][e] = slot_addr(ed.x);
-        }
-#pragma unroll
-        for (int k = 0; k < KMAX; ++k) {
-            const LaneTerm t = a.lane_na[(size_t)gg * kLaneTerms + k];
-            tc[i][k] = valid[i] ? t.coef : 0.0f;
-            tsg[i][k] = t.kind == 0 ? 1.0f : -1.0f;
-            tof[i][k] = t.kind == 0 ? 0.0f : 1.0f;
-#pragma unroll
-            for (int q = 0; q < kLaneSrc; ++q) ta[i][k][q] = slot_addr(t.src[q]);
         }
     }
     const int quad = GPL == 4 ? u : (u >> 1);
@@ -238,21 +242,23 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 #pragma unroll
             for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
         }
-        __syncwarp();  // the cell's row is complete
+        __syncwarp();  // the cell's activations are complete
+        if (TMAX > 0) {
+#pragma unroll
+            for (int k = 0; k < TMAX; ++k) {  // x and 1-x are exact as fmaf(+-1, x, 0 or 1)
+                float prod = 1.0f;
+#pragma unroll
+                for (int q = 0; q < kLaneSrc; ++q) prod *= fmaf(tsg[k], smem_f32(smem_raw, ta[k][q]), tof[k]);
+                smem_f32(smem_raw, tout[k]) = fmaf(tsg[k], prod, tof[k]);
+            }
+            __syncwarp();  // the cell's term values are complete
+        }
         const float Vf = POP ? (float)V : 1.0f;
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
             float reg = cneg[i];
 #pragma unroll
             for (int e = 0; e < EMAX; ++e) reg = fmaf(ew[i][e], smem_f32(smem_raw, ea[i][e]), reg);
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) {  // x and 1-x are exact as fmaf(+-1, x, 0 or 1)
-                float prod = 1.0f;
-#pragma unroll
-                for (int q = 0; q < kLaneSrc; ++q)
-                    prod *= fmaf(tsg[i][k], smem_f32(smem_raw, ta[i][k][q]), tof[i][k]);
-                reg = fmaf(tc[i][k], fmaf(tsg[i][k], prod, tof[i][k]), reg);
-            }
             float tx = reg + beta[i];
             if (POP) tx *= Vf;
             if (!(on & (1u << i))) tx = 0.0f;
@@ -349,15 +355,15 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     }
 }
 
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    if (a.hill_int == 2) warpcell_tile<GPL, EMAX, KMAX, POP, true, 2>(a, blockIdx.x, ctl, smem_raw);
-    else warpcell_tile<GPL, EMAX, KMAX, POP, true, 0>(a, blockIdx.x, ctl, smem_raw);
+    if (a.hill_int == 2) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2>(a, blockIdx.x, ctl, smem_raw);
+    else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0>(a, blockIdx.x, ctl, smem_raw);
 }
 
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 __global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
 cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
@@ -372,16 +378,16 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         const TileWork w = items[it];
         const FusedArgs& a = args[w.arg];
         const TileCtl& ctl = use_shared ? shared_ctl : w.ctl;
-        if (a.hill_int == 2) warpcell_tile<GPL, EMAX, KMAX, POP, false, 2>(a, w.tile, ctl, smem_raw);
-        else warpcell_tile<GPL, EMAX, KMAX, POP, false, 0>(a, w.tile, ctl, smem_raw);
+        if (a.hill_int == 2) warpcell_tile<GPL, EMAX, TMAX, POP, false, 2>(a, w.tile, ctl, smem_raw);
+        else warpcell_tile<GPL, EMAX, TMAX, POP, false, 0>(a, w.tile, ctl, smem_raw);
         __syncthreads();
     }
 }
 
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
-    auto k = cle_warpcell_kernel<GPL, EMAX, KMAX, POP>;
-    const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg);
+    auto k = cle_warpcell_kernel<GPL, EMAX, TMAX, POP>;
+    const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg, a.n_na);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
@@ -390,10 +396,10 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int GPL, int EMAX, int KMAX, bool POP>
+template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    auto k = cle_warpcell_queue_kernel<GPL, EMAX, KMAX, POP>;
+    auto k = cle_warpcell_queue_kernel<GPL, EMAX, TMAX, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, 32 * kWarpcellWarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
@@ -404,9 +410,9 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
 
 // Explicit instantiation of both launchers of one kernel variant (one .cu file per
 // (GPL, EMAX) pair keeps the parallel build balanced).
-#define SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, KMAX, POP)                                                        \
-    template cudaError_t scrna::warpcell_launch_t<GPL, EMAX, KMAX, POP>(const FusedArgs&, cudaStream_t);         \
-    template cudaError_t scrna::warpcell_queue_launch_t<GPL, EMAX, KMAX, POP>(                                   \
+#define SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, TMAX, POP)                                                        \
+    template cudaError_t scrna::warpcell_launch_t<GPL, EMAX, TMAX, POP>(const FusedArgs&, cudaStream_t);         \
+    template cudaError_t scrna::warpcell_queue_launch_t<GPL, EMAX, TMAX, POP>(                                   \
         const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int, cudaStream_t);
 #define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, EMAX)       \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, false)     \
@@ -414,6 +420,4 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 1, false)     \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 1, true)      \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 2, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 2, true)      \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 4, false)     \
-    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 4, true)
+    SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 2, true)

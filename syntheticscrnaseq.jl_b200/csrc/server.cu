@@ -183,7 +183,7 @@ void scrna_server::run() {
             r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps - 1);
             const KernelChoice& kc = r->kc;
             auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.emax : 0, kc.warp ? 0 : kc.block.upt,
-                                       kc.warp ? kc.kmax : 0);
+                                       kc.warp ? kc.tmax : 0);
             int64_t cpt = 32;
             if (kc.warp) cpt = (int64_t)(32 / ((r->net->G + kc.gpl - 1) / kc.gpl)) * 4;
             const int64_t tiles = (r->N + cpt - 1) / cpt;

@@ -258,8 +258,9 @@ def _terms_per_target(net):
                                                          (14, 1, (5, 6), (5, 6), (2, 3))])    # 3 terms
 def test_warp_kernel_padded_terms_identical(pkg, G, seed, n_coop, n_redun, n_src):
     """Networks with several cooperative / redundant terms per gene over 2-3 sources: the
-    warp kernel's padded per-lane terms (coefficient 0, constant 0/1 sources) give the
-    block kernel's sums bit for bit."""
+    warp kernel evaluates each term once per cell into its own activation slot (padded
+    sources read constant 0/1 slots) and adds it as an in-edge of its target; the sums
+    equal the block kernel's bit for bit."""
     net = pkg.sample_network(G, seed=seed, bursty=True, n_coop_range=n_coop, n_redun_range=n_redun,
                              n_sources_range=n_src)
     assert 1 <= _terms_per_target(net) <= 4
@@ -270,8 +271,9 @@ def test_warp_kernel_padded_terms_identical(pkg, G, seed, n_coop, n_redun, n_src
 
 
 def test_warp_kernel_rejects_long_terms(pkg):
-    """A cooperative term over 4 sources is beyond the warp kernel's padded lists: asking
-    for that kernel fails with a clear error, the automatic choice runs the block kernel."""
+    """A cooperative term over 4 sources is beyond the warp kernel's term evaluation:
+    asking for that kernel fails with a clear error, the automatic choice runs the block
+    kernel."""
     net = pkg.sample_network(8, seed=3, n_coop_range=(1, 1), n_redun_range=(0, 0), n_sources_range=(4, 4))
     assert any(len(e.sources) == 4 for e in net.cooperative)
     kin = pkg.WORKLOAD_KINETICS
