@@ -246,7 +246,7 @@ int scrna_server_get_stats(scrna_server* srv, scrna_server_stats* stats);
  * or device memory is budgeted up front).  It runs the fused FP32 kernel of
  * scrna_cle_run_device, optionally with population and capture, and calls no
  * cudaMalloc, cudaFree or other allocating routine: all working memory comes from
- * one array of about 12.9 MB that the library reserves on every GPU it is loaded on,
+ * one array of about 16.0 MB that the library reserves on every GPU it is loaded on,
  * held until the process exits.  Limits per call: 65,536 cells, 512 genes and
  * 262,144 cell-genes; larger runs are rejected with SCRNA_EINVAL.
  *   d_out    device pointer, cells x G (x2 for SCRNA_READOUT_BOTH) float64, column-major

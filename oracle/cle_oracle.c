@@ -199,8 +199,17 @@ float orc_switch_uniform(uint32_t w0, uint32_t w1) {
 
 static inline int32_t clamp_step(int64_t t) { return t > 2147483647 ? 2147483647 : (int32_t)t; }
 
-static inline int32_t next_switch(int64_t step, uint32_t w, float inv) {
-    return clamp_step(step + orc_geom_steps(w, inv));
+/* Switching state of one gene: the step of the next switch and the waiting time that
+ * follows it.  Waiting times are drawn one switch ahead: a promoter switching at step s
+ * enters state X, stays kn steps (drawn earlier, for X) and draws the waiting time after
+ * its next switch (for !X) from the spare bits of step s.  A fresh promoter (initial state
+ * or a daughter) draws both from one switch word pair.  Never switching: both INT32_MAX. */
+typedef struct { int32_t ns, kn; } sw_t;
+
+static inline void fresh_switch(sw_t* sw, int64_t step, const uint32_t w[4], int on, float inv_on,
+                                float inv_off) {
+    sw->ns = clamp_step(step + orc_geom_steps(w[0], on ? inv_off : inv_on));
+    sw->kn = orc_geom_steps(w[1], on ? inv_on : inv_off);
 }
 
 /* ---------------------------------------------------------------------------
@@ -260,20 +269,21 @@ typedef struct {
  * when vol > 0).  m, p, on are this cell's G-vectors; act/rep/reg are scratch. */
 static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, uint64_t seed,
                       uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
-                      double* p, uint8_t* on, int32_t* ns, double* act, double* rep, double* reg) {
+                      double* p, uint8_t* on, sw_t* sw, double* act, double* rep, double* reg) {
     int G = net->G;
     /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
      * the per-step Bernoulli(1 - exp(-k dt)) switch is sampled as its geometric waiting
-     * time, redrawn only when the promoter switches, from the spare bits of the gene's
-     * normal words of this step. */
+     * time (one switch ahead, see sw_t), from the spare bits of the gene's normal words
+     * of the switch step. */
     if (pp->bursty) {
         for (int g = 0; g < G; ++g) {
-            if (!pp->tel[g] || (int64_t)step != ns[g]) continue;
+            if (!pp->tel[g] || (int64_t)step != sw[g].ns) continue;
             on[g] ^= 1;
             uint32_t w[4];
             draw(seed, cell, step, (uint32_t)(g >> 1), ORC_TAG_NORMAL, stream, w);
             float u = (g & 1) ? orc_switch_uniform(w[2], w[3]) : orc_switch_uniform(w[0], w[1]);
-            ns[g] = clamp_step((int64_t)step + orc_geom_steps_u(u, on[g] ? pp->inv_off[g] : pp->inv_on[g]));
+            sw[g].ns = clamp_step((int64_t)step + sw[g].kn);
+            sw[g].kn = orc_geom_steps_u(u, on[g] ? pp->inv_on[g] : pp->inv_off[g]);
         }
     }
     /* Hill fractions (cle.jl:79-82) */
@@ -336,7 +346,7 @@ static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, ui
 
 /* Initial promoter states (tauleap_binomial.jl:64-76) and first switch times. */
 static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uint32_t cell,
-                           uint8_t* on, int32_t* ns) {
+                           uint8_t* on, sw_t* sw) {
     int G = pp->G;
     for (int g0 = 0; g0 < G; g0 += 4) {
         uint32_t w[4];
@@ -347,11 +357,11 @@ static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uin
             on[g] = pp->init_rand[g] ? (w[g - g0] < pp->thr_init[g]) : 1;
     }
     for (int g = 0; g < G; ++g) {
-        ns[g] = 2147483647;
+        sw[g].ns = sw[g].kn = 2147483647;
         if (!pp->tel[g]) continue;
         uint32_t w[4];
         draw(seed, cell, 0, (uint32_t)g, ORC_TAG_SWITCH, stream, w);
-        ns[g] = next_switch(0, w[0], on[g] ? pp->inv_off[g] : pp->inv_on[g]);
+        fresh_switch(&sw[g], 0, w, on[g], pp->inv_on[g], pp->inv_off[g]);
     }
 }
 
@@ -404,7 +414,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             double* rep = (double*)malloc(sizeof(double) * G);
             double* reg = (double*)malloc(sizeof(double) * G);
             uint8_t* on = (uint8_t*)malloc(G);
-            int32_t* ns = (int32_t*)malloc(sizeof(int32_t) * G);
+            sw_t* ns = (sw_t*)malloc(sizeof(sw_t) * G);
 #pragma omp for schedule(static)
             for (int64_t c = 0; c < N; ++c) {
                 memcpy(m, m0, sizeof(double) * G);
@@ -427,7 +437,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
         double* Ms = (double*)malloc(sizeof(double) * G * N);
         double* Ps = (double*)malloc(sizeof(double) * G * N);
         uint8_t* On = (uint8_t*)malloc((size_t)G * N);
-        int32_t* Ns = (int32_t*)malloc(sizeof(int32_t) * G * N);
+        sw_t* Ns = (sw_t*)malloc(sizeof(sw_t) * G * N);
         double* Vs = (double*)malloc(sizeof(double) * N);
         double growth_factor = exp(pop->growth_rate * opt->dt);
         for (int64_t c = 0; c < N; ++c) {
@@ -442,7 +452,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
         double* dM = (double*)malloc(sizeof(double) * G * N);
         double* dP = (double*)malloc(sizeof(double) * G * N);
         uint8_t* dOn = (uint8_t*)malloc((size_t)G * N);
-        int32_t* dNs = (int32_t*)malloc(sizeof(int32_t) * G * N);
+        sw_t* dNs = (sw_t*)malloc(sizeof(sw_t) * G * N);
         double* dV = (double*)malloc(sizeof(double) * N);
         for (int64_t s = 1; s <= n_steps; ++s) {
 #pragma omp parallel
@@ -484,11 +494,11 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                     }
                     dOn[k * G + g] = On[c * G + g];
                     /* the daughter's switching is independent of the mother's: fresh waiting time */
-                    dNs[k * G + g] = 2147483647;
+                    dNs[k * G + g].ns = dNs[k * G + g].kn = 2147483647;
                     if (pp.tel[g]) {
                         uint32_t w[4];
                         draw(seed, (uint32_t)c, (uint32_t)s, (uint32_t)g | 0x800000u, ORC_TAG_SWITCH, stream, w);
-                        dNs[k * G + g] = next_switch(s, w[0], dOn[k * G + g] ? pp.inv_off[g] : pp.inv_on[g]);
+                        fresh_switch(&dNs[k * G + g], s, w, dOn[k * G + g], pp.inv_on[g], pp.inv_off[g]);
                     }
                 }
                 Vs[c] = Vs[c] / 2.0;
@@ -508,7 +518,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                 memcpy(Ms + r * G, dM + k * G, sizeof(double) * G);
                 memcpy(Ps + r * G, dP + k * G, sizeof(double) * G);
                 memcpy(On + r * G, dOn + k * G, (size_t)G);
-                memcpy(Ns + r * G, dNs + k * G, sizeof(int32_t) * G);
+                memcpy(Ns + r * G, dNs + k * G, sizeof(sw_t) * G);
                 Vs[r] = dV[k];
             }
         }

@@ -28,7 +28,7 @@ cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, boo
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
-                              double* M, double* P, uint8_t* prom, int32_t* NS, cudaStream_t st);
+                              double* M, double* P, uint8_t* prom, int2* NS, cudaStream_t st);
 cudaError_t plain_readout_launch(int G, int64_t N, const double* M, const double* P, int readout,
                                  double* out, cudaStream_t st);
 cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* X, double mu_log,
@@ -397,7 +397,7 @@ int scrna::state_alloc(scrna_state* st, bool pop, bool plain) {
     CU(st->M.ensure(gn * 4));
     CU(st->P.ensure(gn * 4));
     CU(st->prom.ensure(gn));
-    CU(st->NS.ensure(gn * 4));
+    CU(st->NS.ensure(gn * sizeof(int2)));
     CU(st->out.ensure(gn * outcols * 8));
     if (st->capture) {
         CU(st->counts.ensure(gn * 4));
@@ -409,7 +409,7 @@ int scrna::state_alloc(scrna_state* st, bool pop, bool plain) {
             CU(st->dM[k].ensure(gn * 4));
             CU(st->dP[k].ensure(gn * 4));
             CU(st->dprom[k].ensure(gn));
-            CU(st->dNS[k].ensure(gn * 4));
+            CU(st->dNS[k].ensure(gn * sizeof(int2)));
             CU(st->dV[k].ensure((size_t)st->N * 8));
             CU(st->owner[k].ensure((size_t)st->N * 8));
         }
@@ -509,13 +509,13 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
     a.in_edge = d.in_edge; a.na = d.na; a.na_src = d.na_src;
     a.quad_tel = net->b_quad_tel.as<uint8_t>();
     a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>();
-    a.NS = st->NS.as<int32_t>();
+    a.NS = st->NS.as<int2>();
     if (pop) {
         a.V = st->V.as<double>();
         for (int k = 0; k < 2; ++k) {
             a.dM[k] = st->dM[k].as<float>(); a.dP[k] = st->dP[k].as<float>();
             a.dprom[k] = st->dprom[k].as<uint8_t>(); a.dV[k] = st->dV[k].as<double>();
-            a.dNS[k] = st->dNS[k].as<int32_t>();
+            a.dNS[k] = st->dNS[k].as<int2>();
             a.owner[k] = st->owner[k].as<unsigned long long>();
         }
     }
@@ -623,7 +623,7 @@ static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     double* Pa = st->P64a.as<double>();
     double* Pb = st->P64b.as<double>();
     CU(plain_init_launch(d.G, st->N, o->cell_offset, net->b_ginit.as<GeneInit>(), net->b_genes.as<GeneRec>(),
-                         k0, k1, sid, M, Pa, st->prom.as<uint8_t>(), st->NS.as<int32_t>(), s));
+                         k0, k1, sid, M, Pa, st->prom.as<uint8_t>(), st->NS.as<int2>(), s));
     ctx->launches++;
     PlainArgs a{};
     a.G = d.G; a.n_quads = d.n_quads; a.N = st->N; a.cell_offset = o->cell_offset;
@@ -635,7 +635,7 @@ static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     a.in_edge = d.in_edge; a.in_w64 = d.in_w64; a.na = d.na; a.na_coef64 = d.na_coef64;
     a.na_src = d.na_src; a.reg_gene = d.reg_gene; a.quad_tel = net->b_quad_tel.as<uint8_t>();
     a.beta64 = d.beta64;
-    a.M = M; a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int32_t>();
+    a.M = M; a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int2>();
     for (int64_t step = 1; step <= n_steps; ++step) {
         a.step = (int)step;
         a.Pold = (step & 1) ? Pa : Pb;

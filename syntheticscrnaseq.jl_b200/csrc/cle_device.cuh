@@ -217,12 +217,35 @@ __device__ __forceinline__ int32_t next_switch(int64_t step, uint32_t w, float i
     return next_switch_u(step, __fmul_rn(__uint2float_rn((w >> 8) + 1u), 5.9604644775390625e-8f), inv);
 }
 
-// A promoter that switches at a step draws its next waiting time from the spare bits of
-// the gene's two normal words of that step (Box-Muller reads only their top 23 bits):
-// u = (((w0 & 511) << 9 | (w1 & 511)) + 1) 2^-18, so a switch costs no Philox call.
-__device__ __forceinline__ float switch_uniform(uint32_t w0, uint32_t w1) {
-    const uint32_t b = ((w0 & 0x1FFu) << 9) | (w1 & 0x1FFu);
+// A promoter that switches at a step draws a waiting time from the spare bits of the
+// gene's two normal words of that step (Box-Muller reads only their top 23 bits):
+// b = (w0 & 511) << 9 | (w1 & 511), u = (b + 1) 2^-18, so a switch costs no Philox call.
+__device__ __forceinline__ uint32_t switch_bits(uint32_t w0, uint32_t w1) {
+    return ((w0 & 0x1FFu) << 9) | (w1 & 0x1FFu);
+}
+__device__ __forceinline__ float switch_uniform_bits(uint32_t b) {
     return __fmul_rn(__uint2float_rn(b + 1u), 3.814697265625e-06f);
+}
+__device__ __forceinline__ float switch_uniform(uint32_t w0, uint32_t w1) {
+    return switch_uniform_bits(switch_bits(w0, w1));
+}
+
+__device__ __forceinline__ int32_t sat_step(int64_t t) { return t > 2147483647 ? 2147483647 : (int32_t)t; }
+
+// Switching state of a gene, int2 {x: step of the next switch, y: the waiting time that
+// follows it}.  Waiting times are drawn one switch ahead: a promoter switching at step s
+// enters state X, stays y steps (drawn earlier, for X) and draws the waiting time after
+// its next switch (for !X) from the spare bits of step s.  inv_on parameterises the stay
+// while OFF, inv_off while ON.  A fresh promoter (initial state, or a daughter at
+// division) draws both from a switch word pair; a gene that never switches has both kNever.
+__device__ __forceinline__ int2 fresh_switch(int64_t step, uint32_t w0, uint32_t w1, bool on, float inv_on,
+                                             float inv_off) {
+    const float u1 = __fmul_rn(__uint2float_rn((w1 >> 8) + 1u), 5.9604644775390625e-8f);
+    return make_int2(next_switch(step, w0, on ? inv_off : inv_on), geom_steps_u(u1, on ? inv_on : inv_off));
+}
+// The switch itself: `on` is the state entered at step s.
+__device__ __forceinline__ int2 switch_at(int64_t step, int2 sw, float us, bool on, float inv_on, float inv_off) {
+    return make_int2(sat_step(step + sw.y), geom_steps_u(us, on ? inv_on : inv_off));
 }
 
 constexpr int32_t kNever = 2147483647;

@@ -78,7 +78,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     const bool has_reg = a.n_reg > 0;
 
     float m[UPT][4], p[UPT][4];
-    int32_t ns[UPT][4];         // step of the next promoter switch of each gene
+    int2 ns[UPT][4];            // switching state of each gene (fresh_switch in cle_device.cuh)
     uint32_t on = 0xFFFFFFFFu;  // bit 4j+i: promoter of gene 4q_j+i is ON
     double V = 0.0;
 
@@ -114,12 +114,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
 #pragma unroll
             for (int i = 0; i < 4; ++i) {  // first waiting times (NaN parameter: gene never switches)
                 const int g = 4 * q + i;
-                ns[j][i] = kNever;
+                ns[j][i] = make_int2(kNever, kNever);
                 if (q < a.n_quads && g < G) {
                     const GeneRec gr = sm.genes[g];
                     if (gr.inv_off == gr.inv_off) {
                         const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-                        ns[j][i] = next_switch(0, w.x, (on >> (4 * j + i)) & 1u ? gr.inv_off : gr.inv_on);
+                        ns[j][i] = fresh_switch(0, w.x, w.y, (on >> (4 * j + i)) & 1u, gr.inv_on, gr.inv_off);
                     }
                 }
             }
@@ -143,7 +143,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
         const float* Ms = from_daughter ? a.dM[par] : a.M;
         const float* Ps = from_daughter ? a.dP[par] : a.P;
         const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
-        const int32_t* Ns = from_daughter ? a.dNS[par] : a.NS;
+        const int2* Ns = from_daughter ? a.dNS[par] : a.NS;
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
@@ -153,7 +153,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                 const bool ok = q < a.n_quads && g < G;
                 m[j][i] = ok ? Ms[(size_t)g * N + src] : 0.0f;
                 p[j][i] = ok ? Ps[(size_t)g * N + src] : 0.0f;
-                ns[j][i] = ok ? Ns[(size_t)g * N + src] : kNever;
+                ns[j][i] = ok ? Ns[(size_t)g * N + src] : make_int2(kNever, kNever);
                 if (ok && !Os[(size_t)g * N + src]) on &= ~(1u << (4 * j + i));
             }
         }
@@ -202,11 +202,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                     // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
                     // a gene switches when its waiting time runs out and draws the next one
                     // from the spare bits of its normal words
-                    if (s == ns[j][i]) {
+                    if (s == ns[j][i].x) {
                         const uint32_t bit = 1u << (4 * j + i);
                         on ^= bit;
                         const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
-                        ns[j][i] = next_switch_u(s, us, (on & bit) ? sm.genes[g].inv_off : sm.genes[g].inv_on);
+                        ns[j][i] = switch_at(s, ns[j][i], us, on & bit, sm.genes[g].inv_on, sm.genes[g].inv_off);
                     }
                     const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
                     const GeneRec gr = sm.genes[g];
@@ -287,12 +287,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                     const uint32_t bon = (on >> (4 * j + i)) & 1u;
                     a.dprom[par][idx] = bon;
                     // the daughter's promoter switches independently of the mother's
-                    int32_t dns = kNever;
+                    int2 dns = make_int2(kNever, kNever);
                     const GeneRec gr = sm.genes[g];
                     if (gr.inv_off == gr.inv_off) {
                         const uint4 w = philox(gcell, (uint32_t)ctl.step_end, (uint32_t)g | kDaughterSwitch,
                                                tagword(TAG_SWITCH, a.stream), key);
-                        dns = next_switch(ctl.step_end, w.x, bon ? gr.inv_off : gr.inv_on);
+                        dns = fresh_switch(ctl.step_end, w.x, w.y, bon, gr.inv_on, gr.inv_off);
                     }
                     a.dNS[par][idx] = dns;
                 }

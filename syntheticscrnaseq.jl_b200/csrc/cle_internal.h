@@ -101,13 +101,13 @@ struct FusedArgs {
     float* M;
     float* P;
     uint8_t* prom;
-    int32_t* NS;            // step of the next promoter switch
+    int2* NS;               // switching state {next switch step, waiting time after it}
     double* V;
     // division scratch (two parities)
     float* dM[2];
     float* dP[2];
     uint8_t* dprom[2];
-    int32_t* dNS[2];
+    int2* dNS[2];
     double* dV[2];
     unsigned long long* owner[2];
     // outputs
@@ -160,7 +160,7 @@ struct PlainArgs {
     const double* Pold;
     double* Pnew;
     uint8_t* prom;
-    int32_t* NS;
+    int2* NS;
 };
 
 }  // namespace scrna

@@ -32,9 +32,10 @@ __global__ void __launch_bounds__(128) cle_plain_step_kernel(const PlainArgs a) 
     // telegraph switching: the promoter switches when its waiting time runs out and draws
     // the next one from the spare bits of its normal words
     bool on = a.prom[idx];
-    if (s == a.NS[idx]) {
+    const int2 sw = a.NS[idx];
+    if (s == sw.x) {
         on = !on;
-        a.NS[idx] = next_switch_u(s, switch_uniform(w0, w1), on ? gr.inv_off : gr.inv_on);
+        a.NS[idx] = switch_at(s, sw, switch_uniform(w0, w1), on, gr.inv_on, gr.inv_off);
         a.prom[idx] = on;
     }
     // reg = A_pos*act + A_neg*rep over the in-edges, from the previous step's proteins
@@ -92,7 +93,7 @@ cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st) {
 // Initial FP64 state: ceil(steady state) and the initial promoter draws.
 __global__ void plain_init_kernel(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                                   const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
-                                  double* M, double* P, uint8_t* prom, int32_t* NS) {
+                                  double* M, double* P, uint8_t* prom, int2* NS) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y;
     if (c >= N) return;
@@ -107,18 +108,18 @@ __global__ void plain_init_kernel(int G, int64_t N, int64_t cell_offset, const G
         on = ws[g & 3] < gi[g].thr_init;
     }
     prom[idx] = on;
-    int32_t ns = kNever;
+    int2 ns = make_int2(kNever, kNever);
     if (gr[g].inv_off == gr[g].inv_off) {
         const uint4 w = philox((uint32_t)(cell_offset + c), 0u, (uint32_t)g, tagword(TAG_SWITCH, stream),
                                Key{key0, key1});
-        ns = next_switch(0, w.x, on ? gr[g].inv_off : gr[g].inv_on);
+        ns = fresh_switch(0, w.x, w.y, on, gr[g].inv_on, gr[g].inv_off);
     }
     NS[idx] = ns;
 }
 
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
                               const GeneRec* gr, uint32_t key0, uint32_t key1, uint32_t stream,
-                              double* M, double* P, uint8_t* prom, int32_t* NS, cudaStream_t st) {
+                              double* M, double* P, uint8_t* prom, int2* NS, cudaStream_t st) {
     dim3 grid((unsigned)((N + 127) / 128), (unsigned)G);
     plain_init_kernel<<<grid, 128, 0, st>>>(G, N, cell_offset, gi, gr, key0, key1, stream, M, P, prom, NS);
     return cudaGetLastError();

@@ -42,7 +42,7 @@ struct TensorArgs {
     float* M;
     float* P;
     uint8_t* prom;
-    int32_t* NS;
+    int2* NS;
     void* act16;             // [N][Kp]
     const float* act32_cur;  // [N][n_src]
     float* act32_next;
@@ -69,10 +69,10 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
         on = x < gi.thr_init;
     }
     a.prom[idx] = on;
-    int32_t ns = kNever;
+    int2 ns = make_int2(kNever, kNever);
     if (gr.inv_off == gr.inv_off) {
         const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-        ns = next_switch(0, w.x, on ? gr.inv_off : gr.inv_on);
+        ns = fresh_switch(0, w.x, w.y, on, gr.inv_on, gr.inv_off);
     }
     a.NS[idx] = ns;
     const float act = hill_act(p0, a.Kn, a.hill_n, a.hill_int);
@@ -118,10 +118,11 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
             bool on = true;
             if (BURSTY) {
                 on = a.prom[e];
-                if (s == a.NS[e]) {  // next waiting time from the spare bits of the normal words
+                const int2 sw = a.NS[e];
+                if (s == sw.x) {  // waiting time from the spare bits of the normal words
                     on = !on;
                     const float us = h == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
-                    a.NS[e] = next_switch_u(s, us, on ? gr[h].inv_off : gr[h].inv_on);
+                    a.NS[e] = switch_at(s, sw, us, on, gr[h].inv_on, gr[h].inv_off);
                     a.prom[e] = on;
                 }
             }
@@ -304,7 +305,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     CU(st->tM.ensure(gn * 4));
     CU(st->tP.ensure(gn * 4));
     CU(st->tprom.ensure(gn));
-    CU(st->tNS.ensure(gn * 4));
+    CU(st->tNS.ensure(gn * sizeof(int2)));
     CU(st->treg.ensure(gn * 4));
     CU(st->tact16.ensure((size_t)N * Kp * 2));
     for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
@@ -332,7 +333,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.src_of_gene = n->t_src_of_gene.as<int32_t>();
     a.reg = st->treg.as<float>();
     a.M = st->tM.as<float>(); a.P = st->tP.as<float>();
-    a.prom = st->tprom.as<uint8_t>(); a.NS = st->tNS.as<int32_t>();
+    a.prom = st->tprom.as<uint8_t>(); a.NS = st->tNS.as<int2>();
     a.act16 = st->tact16.p;
     a.act32_cur = st->tact32[1].as<float>();
     a.act32_next = st->tact32[0].as<float>();

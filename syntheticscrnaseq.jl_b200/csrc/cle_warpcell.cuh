@@ -143,6 +143,8 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 
     float m[GPL], p[GPL];
     int32_t ns[GPL];  // step of the next promoter switch
+    int32_t kn[GPL];  // waiting time after it (fresh_switch); < 0: not drawn yet, -(b + 1) for the
+                      // spare bits b of the switch step that created it
     uint32_t on = 0xFFFFFFFFu;  // bit i: promoter of gene u*GPL+i is ON
     double V = 0.0;
 
@@ -168,10 +170,12 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         }
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
-            ns[i] = kNever;
+            ns[i] = kn[i] = kNever;
             if (inv_off[i] == inv_off[i]) {
                 const uint4 w = philox(gcell, 0u, (uint32_t)(u * GPL + i), tagword(TAG_SWITCH, a.stream), key);
-                ns[i] = next_switch(0, w.x, (on >> i) & 1u ? inv_off[i] : inv_on[i]);
+                const int2 f = fresh_switch(0, w.x, w.y, (on >> i) & 1u, inv_on[i], inv_off[i]);
+                ns[i] = f.x;
+                kn[i] = f.y;
             }
         }
         if (POP) {
@@ -192,13 +196,15 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         const float* Ms = from_daughter ? a.dM[par] : a.M;
         const float* Ps = from_daughter ? a.dP[par] : a.P;
         const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
-        const int32_t* Ns = from_daughter ? a.dNS[par] : a.NS;
+        const int2* Ns = from_daughter ? a.dNS[par] : a.NS;
 #pragma unroll
         for (int i = 0; i < GPL; ++i) {
             const int g = u * GPL + i;
             m[i] = valid[i] ? Ms[(size_t)g * N + src] : 0.0f;
             p[i] = valid[i] ? Ps[(size_t)g * N + src] : 0.0f;
-            ns[i] = valid[i] ? Ns[(size_t)g * N + src] : kNever;
+            const int2 sw = valid[i] ? Ns[(size_t)g * N + src] : make_int2(kNever, kNever);
+            ns[i] = sw.x;
+            kn[i] = sw.y;
             if (valid[i] && !Os[(size_t)g * N + src]) on &= ~(1u << i);
         }
         if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
@@ -207,6 +213,15 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     // ---- fused step loop --------------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
     const bool any_reg = n_reg > 0;
+    // Draw the pending waiting times of this lane (the state after the next switch is the
+    // opposite of the current one, which holds until that switch).
+    auto resolve_pending = [&]() {
+#pragma unroll
+        for (int i = 0; i < GPL; ++i)
+            if (kn[i] < 0)
+                kn[i] = geom_steps_u(switch_uniform_bits((uint32_t)(-kn[i] - 1)),
+                                     (on >> i) & 1u ? inv_on[i] : inv_off[i]);
+    };
     int32_t ns_min = ns[0];  // earliest switch of the lane's genes
 #pragma unroll
     for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
@@ -216,28 +231,38 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 #pragma unroll
             for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = warpcell_hill<HN>(p[i], a);
         }
+        // telegraph: a promoter switches when its waiting time runs out, and needs the waiting
+        // time drawn at its previous switch.  Those draws wait until some switching gene of the
+        // warp needs one; then every lane draws all of its pending ones together.
+        const bool due = s == ns_min;
+        const bool warp_due = __any_sync(0xFFFFFFFFu, due);
+        if (warp_due) {
+            bool need = false;
+#pragma unroll
+            for (int i = 0; i < GPL; ++i) need |= s == ns[i] && kn[i] < 0;
+            if (__any_sync(0xFFFFFFFFu, need)) resolve_pending();
+        }
         BM bm[GPL];
 #pragma unroll
         for (int h = 0; h < GPL / 2; ++h) {
             const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
             const uint4 w = RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1)
                                : philox(gcell, (uint32_t)s, c2, c3, key);
-            if (s == ns_min) {  // telegraph: a promoter switches when its waiting time runs out
+            if (warp_due && due) {
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const int i = 2 * h + k;
-                    if (s == ns[i]) {
-                        const uint32_t bit = 1u << i;
-                        on ^= bit;
-                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
-                        ns[i] = next_switch_u(s, us, (on & bit) ? inv_off[i] : inv_on[i]);
+                    if (s == ns[i]) {  // switch_at, with the next draw left pending
+                        on ^= 1u << i;
+                        ns[i] = sat_step((int64_t)s + kn[i]);
+                        kn[i] = -(int32_t)(k == 0 ? switch_bits(w.x, w.y) : switch_bits(w.z, w.w)) - 1;
                     }
                 }
             }
             bm[2 * h] = box_muller_parts(w.x, w.y);
             bm[2 * h + 1] = box_muller_parts(w.z, w.w);
         }
-        if (s == ns_min) {
+        if (warp_due && due) {
             ns_min = ns[0];
 #pragma unroll
             for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
@@ -268,6 +293,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     }
 
     // ---- epilogue (as cle_fused_kernel) ------------------------------------------------
+    resolve_pending();
     if (POP && ctl.check) {
         const bool divides = V > a.V_div;
         const int ne = ctl.epoch + 1;
@@ -309,11 +335,11 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
                 a.dP[par][idx] = dp;
                 const uint32_t bon = (on >> i) & 1u;
                 a.dprom[par][idx] = bon;
-                int32_t dns = kNever;  // the daughter's promoter switches independently
+                int2 dns = make_int2(kNever, kNever);  // the daughter's promoter switches independently
                 if (inv_off[i] == inv_off[i]) {
                     const uint4 w = philox(gcell, (uint32_t)ctl.step_end, (uint32_t)g | kDaughterSwitch,
                                            tagword(TAG_SWITCH, a.stream), key);
-                    dns = next_switch(ctl.step_end, w.x, bon ? inv_off[i] : inv_on[i]);
+                    dns = fresh_switch(ctl.step_end, w.x, w.y, bon, inv_on[i], inv_off[i]);
                 }
                 a.dNS[par][idx] = dns;
             }
@@ -328,7 +354,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         a.M[idx] = m[i];
         a.P[idx] = p[i];
         a.prom[idx] = (on >> i) & 1u;
-        a.NS[idx] = ns[i];
+        a.NS[idx] = make_int2(ns[i], kn[i]);
         if (ctl.last && a.out) {
             if (a.readout == 0) a.out[idx] = (double)m[i];
             else if (a.readout == 1) a.out[idx] = (double)p[i];

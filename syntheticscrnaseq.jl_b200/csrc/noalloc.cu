@@ -11,7 +11,7 @@
 // passes the network (created earlier) and device pointers for the outputs.
 //
 // Limits: at most kMaxCells cells, kMaxGenes genes and kMaxCellGenes cell-genes
-// per call.  The array (kScratchBytes, about 12.9 MB) is held on every GPU that
+// per call.  The array (kScratchBytes, about 16.0 MB) is held on every GPU that
 // loads the library until the process exits.
 #include <cuda_runtime.h>
 
@@ -55,12 +55,12 @@ constexpr size_t kOffM = 0;
 constexpr size_t kOffP = kOffM + align256(4 * kMaxCellGenes);
 constexpr size_t kOffProm = kOffP + align256(4 * kMaxCellGenes);
 constexpr size_t kOffNS = kOffProm + align256(kMaxCellGenes);
-constexpr size_t kOffV = kOffNS + align256(4 * kMaxCellGenes);
+constexpr size_t kOffV = kOffNS + align256(8 * kMaxCellGenes);
 constexpr size_t kOffDM = kOffV + align256(8 * kMaxCells);            // two parities each below
 constexpr size_t kOffDP = kOffDM + 2 * align256(4 * kMaxCellGenes);
 constexpr size_t kOffDProm = kOffDP + 2 * align256(4 * kMaxCellGenes);
 constexpr size_t kOffDNS = kOffDProm + 2 * align256(kMaxCellGenes);
-constexpr size_t kOffDV = kOffDNS + 2 * align256(4 * kMaxCellGenes);
+constexpr size_t kOffDV = kOffDNS + 2 * align256(8 * kMaxCellGenes);
 constexpr size_t kOffOwner = kOffDV + 2 * align256(8 * kMaxCells);
 constexpr size_t kOffGenes = kOffOwner + 2 * align256(8 * kMaxCells);
 constexpr size_t kOffGinit = kOffGenes + align256(sizeof(GeneRec) * kMaxGenes);
@@ -166,7 +166,7 @@ extern "C" int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, 
     a.M = reinterpret_cast<float*>(s + kOffM);
     a.P = reinterpret_cast<float*>(s + kOffP);
     a.prom = s + kOffProm;
-    a.NS = reinterpret_cast<int32_t*>(s + kOffNS);
+    a.NS = reinterpret_cast<int2*>(s + kOffNS);
     if (pop) {
         a.growth_factor = std::exp(pop->growth_rate * o->dt);
         a.V_div = pop->V_div; a.V_lo = pop->V_init_lo; a.V_hi = pop->V_init_hi;
@@ -176,7 +176,7 @@ extern "C" int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, 
             a.dM[k] = reinterpret_cast<float*>(s + kOffDM + k * align256(4 * kMaxCellGenes));
             a.dP[k] = reinterpret_cast<float*>(s + kOffDP + k * align256(4 * kMaxCellGenes));
             a.dprom[k] = s + kOffDProm + k * align256(kMaxCellGenes);
-            a.dNS[k] = reinterpret_cast<int32_t*>(s + kOffDNS + k * align256(4 * kMaxCellGenes));
+            a.dNS[k] = reinterpret_cast<int2*>(s + kOffDNS + k * align256(8 * kMaxCellGenes));
             a.dV[k] = reinterpret_cast<double*>(s + kOffDV + k * align256(8 * kMaxCells));
             a.owner[k] = reinterpret_cast<unsigned long long*>(s + kOffOwner + k * align256(8 * kMaxCells));
         }
