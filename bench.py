@@ -51,6 +51,8 @@ def _args():
     ap.add_argument("--requests", type=int, default=60, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--batch-networks", type=int, default=256, help="batch: number of networks")
+    ap.add_argument("--dense-steps", type=int, default=0,
+                    help="dense: Euler steps per run (default: the workload's T/dt = 8,000)")
     ap.add_argument("--cpu-sample-cells", type=int, default=20000)
     ap.add_argument("--cpu-sample-steps", type=int, default=1000)
     ap.add_argument("--ref-sample-steps", type=int, default=250)
@@ -328,10 +330,10 @@ def run_dense(args):
     ctx = pkg.Context(0)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    steps = pkg.n_steps(wl.T, wl.dt) if args.steps > 0 else 0
-    n_steps = steps if args.steps >= 1 else 100
+    n_steps = args.dense_steps if args.dense_steps > 0 else pkg.n_steps(wl.T, wl.dt)
     G, N = wl.net.G, wl.cell_num
-    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout="protein", seed=7, ctx=ctx)
+    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=0.0, n_steps=n_steps, readout="protein",
+                        seed=7, ctx=ctx)
     run.launch()
     torch.cuda.synchronize()
     el = [_event_time(run.launch, stream) for _ in range(max(1, args.steps))]

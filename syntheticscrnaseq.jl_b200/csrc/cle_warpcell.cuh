@@ -243,26 +243,27 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             if (__any_sync(0xFFFFFFFFu, need)) resolve_pending();
         }
         BM bm[GPL];
+        uint32_t sb[GPL];  // spare bits of each gene's normal words
 #pragma unroll
         for (int h = 0; h < GPL / 2; ++h) {
             const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
             const uint4 w = RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1)
                                : philox(gcell, (uint32_t)s, c2, c3, key);
-            if (warp_due && due) {
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int i = 2 * h + k;
-                    if (s == ns[i]) {  // switch_at, with the next draw left pending
-                        on ^= 1u << i;
-                        ns[i] = sat_step((int64_t)s + kn[i]);
-                        kn[i] = -(int32_t)(k == 0 ? switch_bits(w.x, w.y) : switch_bits(w.z, w.w)) - 1;
-                    }
-                }
-            }
+            sb[2 * h] = switch_bits(w.x, w.y);
+            sb[2 * h + 1] = switch_bits(w.z, w.w);
             bm[2 * h] = box_muller_parts(w.x, w.y);
             bm[2 * h + 1] = box_muller_parts(w.z, w.w);
         }
-        if (warp_due && due) {
+        if (warp_due) {  // switch_at for the genes due now, with the next draw left pending
+#pragma unroll
+            for (int i = 0; i < GPL; ++i) {
+                const bool sw = s == ns[i];
+                on ^= (uint32_t)sw << i;
+                // s + kn < 2^32 (both < 2^31): the unsigned sum saturates at kNever
+                const int32_t nn = (int32_t)min((uint32_t)s + (uint32_t)kn[i], (uint32_t)kNever);
+                ns[i] = sw ? nn : ns[i];
+                kn[i] = sw ? -(int32_t)sb[i] - 1 : kn[i];
+            }
             ns_min = ns[0];
 #pragma unroll
             for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
