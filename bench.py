@@ -339,8 +339,8 @@ def run_dense(args):
     el = [_event_time(run.launch, stream) for _ in range(max(1, args.steps))]
     per = sum(el) / len(el)
     units = G * N * n_steps
-    Kp = (G + 63) // 64 * 64
-    flops = 2.0 * G * Kp * N * n_steps
+    K = G + len(wl.net.cooperative) + len(wl.net.redundant)  # gene columns + one column per term
+    flops = 2.0 * G * K * N * n_steps
     algo_bytes = 18.0 * units  # M, P read + write (FP32), 16-bit activations written
     peaks = _measured_peaks()
     line = {"workload": wl.name, "value": units / per, "unit": "cell·gene·steps/s", "s_per_run": per,

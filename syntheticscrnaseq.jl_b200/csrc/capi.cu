@@ -720,16 +720,17 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
     if (!st) return fail(SCRNA_EINVAL, "state is NULL");
     if (int r = set_device(ctx)) return r;
     const size_t gn = (size_t)st->G * st->N;
-    if (st->last_tensor) {  // cell-major state: transpose to [G][N] on the host
-        std::vector<float> tm(gn), tp(gn);
-        std::vector<uint8_t> tpr(gn);
-        CU(cudaMemcpyAsync(tm.data(), st->tM.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaMemcpyAsync(tp.data(), st->tP.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaMemcpyAsync(tpr.data(), st->tprom.p, gn, cudaMemcpyDeviceToHost, ctx->stream));
+    if (st->last_tensor) {  // cell-major state [N][t_ld]: transpose to [G][N] on the host
+        const size_t ln = (size_t)st->t_ld * st->N;
+        std::vector<float> tm(ln), tp(ln);
+        std::vector<uint8_t> tpr(ln);
+        CU(cudaMemcpyAsync(tm.data(), st->tM.p, ln * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tp.data(), st->tP.p, ln * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tpr.data(), st->tprom.p, ln, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
         for (int64_t c = 0; c < st->N; ++c)
             for (int g = 0; g < st->G; ++g) {
-                const size_t src = (size_t)c * st->G + g, dst = (size_t)g * st->N + c;
+                const size_t src = (size_t)c * st->t_ld + g, dst = (size_t)g * st->N + c;
                 if (mrna) static_cast<float*>(mrna)[dst] = tm[src];
                 if (protein) static_cast<float*>(protein)[dst] = tp[src];
                 if (promoter) promoter[dst] = tpr[src];

@@ -102,6 +102,7 @@ struct scrna_state {
     DevBuf M64, P64a, P64b;  // FP64 baseline state
     // tensor-core path state, cell-major [N][G]
     DevBuf tM, tP, tprom, tNS, tact16, tact32[2], treg;
+    int t_ld = 0;  // row stride of the cell-major tensor-path state
     bool last_tensor = false;
     bool have_counts = false;
     bool last_plain = false;

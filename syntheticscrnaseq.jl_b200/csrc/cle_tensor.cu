@@ -4,11 +4,15 @@
 // reg = sum_j A_eff[i,j] act_j (the one-GEMM form of A_pos act + A_neg rep,
 // network.jl:206-219, cle.jl:84-86) is a real dense GEMM per Euler step:
 //     REG[N x G] = ACT[N x K] * W^T,  W = A_eff as 16-bit [G][K], ACT 16-bit [N][K]
-// with FP32 accumulation.  Each step is the GEMM (cuBLASLt, BF16 or FP16 inputs) followed
-// by one fused FP32 kernel that adds the repression constant and the cooperative /
-// redundant terms, applies telegraph switching, draws the Philox increments, updates
-// M and P (cle.jl:109-120) and writes the next step's 16-bit activations.  State is
-// cell-major [N][G] so that both kernels stream it with unit stride.
+// with FP32 accumulation.  The cooperative / redundant terms (cle.jl:89-106) are extra K
+// columns: column G + j of ACT holds the value of term j (the product over its sources,
+// from their FP32 activations) and W[target_j][G + j] its coefficient s_j beta_target.
+// Each step is a small kernel writing the term columns, the GEMM (cuBLASLt, BF16 or FP16
+// inputs) and one fused FP32 kernel that adds the repression constant, applies telegraph
+// switching, draws the Philox increments, updates M and P (cle.jl:109-120) and writes the
+// next step's 16-bit activations.  State is
+// cell-major [N][ld], ld = G rounded up to a whole gene pair, so that both kernels stream
+// it with unit stride and the step kernel moves each gene pair with one 8-byte access.
 #include <cublasLt.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -26,20 +30,25 @@ template <class T> __device__ __forceinline__ T to16(float x);
 template <> __device__ __forceinline__ __nv_bfloat16 to16<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
 template <> __device__ __forceinline__ __half to16<__half>(float x) { return __float2half_rn(x); }
 
+// Row stride of the cell-major state: G rounded up to a whole gene pair.
+inline int tensor_ld(int G) { return (G + 1) & ~1; }
+
 struct TensorArgs {
-    int32_t G, Kp, n_src;
+    int32_t G, ld, Kp, n_src;
     int64_t N, cell_offset;
     int32_t step;
     float k_t, Kn, hill_n, mu_m, mu_p, dt;
     int32_t hill_int;
     uint32_t key0, key1, stream;
+    uint32_t rk0[10], rk1[10];   // Philox round keys of (key0, key1)
     const GeneRec* genes;
     const GeneInit* ginit;
     const NonAdd* na;        // sources are compact source indices
     const int32_t* na_src;
     const int32_t* src_of_gene;  // gene -> compact source index or -1
-    const float* reg;        // [N][G] GEMM output of this step
-    float* M;
+    int32_t n_terms;         // cooperative / redundant terms = extra K columns G .. G + n_terms
+    float* reg;              // [N][ld] GEMM output of this step
+    float* M;                // [N][ld] (as P, prom, NS)
     float* P;
     uint8_t* prom;
     int2* NS;
@@ -58,23 +67,24 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
     const Key key{a.key0, a.key1};
     const uint32_t gcell = (uint32_t)(a.cell_offset + c);
     const GeneInit gi = a.ginit[g];
+    const int64_t sidx = c * a.ld + g;  // state index
     const GeneRec gr = a.genes[g];
     const float p0 = gi.p0;
-    a.M[idx] = gi.m0;
-    a.P[idx] = p0;
+    a.M[sidx] = gi.m0;
+    a.P[sidx] = p0;
     bool on = true;
     if (gi.init_rand) {
         const uint4 w = philox(gcell, 0u, (uint32_t)(g >> 2), tagword(TAG_PROMOTER, a.stream), key);
         const uint32_t x = (g & 3) == 0 ? w.x : (g & 3) == 1 ? w.y : (g & 3) == 2 ? w.z : w.w;
         on = x < gi.thr_init;
     }
-    a.prom[idx] = on;
+    a.prom[sidx] = on;
     int2 ns = make_int2(kNever, kNever);
     if (gr.inv_off == gr.inv_off) {
         const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
         ns = fresh_switch(0, w.x, w.y, on, gr.inv_on, gr.inv_off);
     }
-    a.NS[idx] = ns;
+    a.NS[sidx] = ns;
     const float act = hill_act(p0, a.Kn, a.hill_n, a.hill_int);
     reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
     const int src = a.src_of_gene[g];
@@ -83,79 +93,119 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
 
 // One Euler-Maruyama step after the GEMM.  Thread = one gene pair (blockIdx.y, x) for a chunk
 // of kTensorCellsPerThread cells (blockIdx.x); per-gene constants stay in registers across the
-// chunk, consecutive threads touch consecutive genes of one cell (unit-stride rows).
-constexpr int kTensorCellsPerThread = 16;
+// chunk, consecutive threads touch consecutive gene pairs of one cell (unit-stride rows, one
+// 8-byte access per pair).  The kernel is bound by HBM: every thread issues the loads of its
+// whole chunk (GEMM output, M, P) before computing, so enough bytes are in flight.
+constexpr int kTensorCellsPerThread = 8;
 constexpr int kTensorPairsPerBlock = 128;
 
-template <class T, bool BURSTY>
-__global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const TensorArgs a) {
-    const int pairs = (a.G + 1) >> 1;
-    const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
-    if (k >= pairs) return;
-    const Key key{a.key0, a.key1};
-    const int s = a.step;
-    GeneRec gr[2];
-    int src[2];
-    bool valid[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int g = 2 * k + h;
-        valid[h] = g < a.G;
-        gr[h] = a.genes[valid[h] ? g : 0];
-        src[h] = valid[h] ? a.src_of_gene[g] : -1;
+template <class T> struct Pair16;
+template <> struct Pair16<__nv_bfloat16> { using type = __nv_bfloat162; };
+template <> struct Pair16<__half> { using type = __half2; };
+
+// Term columns of the activation matrix: thread = (cell, term), value from the FP32
+// activations of the term's compact source genes written by the previous step.
+template <class T>
+__global__ void tensor_terms_kernel(const TensorArgs a) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.N * a.n_terms) return;
+    const int64_t c = idx / a.n_terms;
+    const int j = (int)(idx - c * a.n_terms);
+    const float* act = a.act32_cur + c * a.n_src;
+    const NonAdd na = a.na[j];
+    float prod = 1.0f;
+    if (na.kind == 0) {
+        for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[a.na_src[t]];
+    } else {
+        for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[a.na_src[t]];
+        prod = 1.0f - prod;
     }
+    reinterpret_cast<T*>(a.act16)[c * a.Kp + a.G + j] = to16<T>(prod);
+}
+
+template <int HN>
+__device__ __forceinline__ float tensor_hill(float p, const TensorArgs& a) {
+    if (HN == 2) {
+        const float pn = p * p;
+        return fminf(pn * frcp_approx(pn + a.Kn), 1.0f);  // as hill_act with hill_int == 2
+    }
+    return hill_act(p, a.Kn, a.hill_n, a.hill_int);
+}
+
+template <class T, bool BURSTY, int HN>
+__global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const TensorArgs a) {
+    using T2 = typename Pair16<T>::type;
+    const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
+    if (k >= (a.ld >> 1)) return;
+    const int g0 = 2 * k;
+    const bool has1 = g0 + 1 < a.G;  // the second gene of the pair exists (else: row padding)
+    const GeneRec r0 = a.genes[g0];
+    const GeneRec r1 = a.genes[has1 ? g0 + 1 : g0];
+    const int src0 = a.src_of_gene[g0];
+    const int src1 = has1 ? a.src_of_gene[g0 + 1] : -1;
+    const uint32_t c3 = tagword(TAG_NORMAL, a.stream);
+    const int s = a.step;
     const int64_t c_begin = (int64_t)blockIdx.x * kTensorCellsPerThread;
     const int64_t c_end = c_begin + kTensorCellsPerThread < a.N ? c_begin + kTensorCellsPerThread : a.N;
-    T* act16 = reinterpret_cast<T*>(a.act16);
-    for (int64_t c = c_begin; c < c_end; ++c) {
-        const uint32_t gcell = (uint32_t)(a.cell_offset + c);
-        const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)k, tagword(TAG_NORMAL, a.stream), key);
+    const size_t rs = (size_t)(a.ld >> 1);  // row stride in pairs
+    const float2* regp = reinterpret_cast<const float2*>(a.reg) + (size_t)c_begin * rs + k;
+    float2* Mp = reinterpret_cast<float2*>(a.M) + (size_t)c_begin * rs + k;
+    float2* Pp = reinterpret_cast<float2*>(a.P) + (size_t)c_begin * rs + k;
+    T2* actp = reinterpret_cast<T2*>(a.act16) + (size_t)c_begin * (a.Kp >> 1) + k;
+    constexpr int CPT = kTensorCellsPerThread;
+    const int nc = (int)(c_end - c_begin);
+    float2 rg[CPT], mm[CPT], pp[CPT];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (!valid[h]) continue;
-            const int g = 2 * k + h;
-            const int64_t e = c * a.G + g;
-            bool on = true;
-            if (BURSTY) {
-                on = a.prom[e];
-                const int2 sw = a.NS[e];
-                if (s == sw.x) {  // waiting time from the spare bits of the normal words
-                    on = !on;
-                    const float us = h == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
-                    a.NS[e] = switch_at(s, sw, us, on, gr[h].inv_on, gr[h].inv_off);
-                    a.prom[e] = on;
-                }
-            }
-            float reg = a.reg[e] + gr[h].cneg;
-            const int nab = gr[h].na_range >> 16, nac = gr[h].na_range & 0xFFFF;
-            for (int q = nab; q < nab + nac; ++q) {
-                const NonAdd na = a.na[q];
-                float prod = 1.0f;
-                if (na.kind == 0) {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= a.act32_cur[c * a.n_src + a.na_src[t]];
-                    reg = fmaf(na.coef, prod, reg);
-                } else {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - a.act32_cur[c * a.n_src + a.na_src[t]];
-                    reg = fmaf(na.coef, 1.0f - prod, reg);
-                }
-            }
-            float tx = reg + gr[h].beta;
-            if (!on) tx = 0.0f;
-            const BM bm = h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
-            float m = a.M[e], p = a.P[e];
-            em_update(m, p, tx, bm, a.mu_m, a.mu_p, a.k_t, a.dt);
-            a.M[e] = m;
-            a.P[e] = p;
-            const float act = hill_act(p, a.Kn, a.hill_n, a.hill_int);
-            act16[c * a.Kp + g] = to16<T>(act);
-            if (src[h] >= 0) a.act32_next[c * a.n_src + src[h]] = act;
+    for (int i = 0; i < CPT; ++i) {
+        if (i < nc) {
+            rg[i] = regp[i * rs];
+            mm[i] = Mp[i * rs];
+            pp[i] = Pp[i * rs];
         }
+    }
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+        if (i >= nc) break;
+        const int64_t c = c_begin + i;
+        const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+        const uint4 w = philox_rk(gcell, (uint32_t)s, (uint32_t)k, c3, a.rk0, a.rk1);
+        float tx0 = (rg[i].x + r0.cneg) + r0.beta, tx1 = (rg[i].y + r1.cneg) + r1.beta;
+        if (BURSTY) {
+            const size_t e = (size_t)c * a.ld + g0;
+            const uchar2 on = *reinterpret_cast<const uchar2*>(a.prom + e);
+            const int4 sw = *reinterpret_cast<const int4*>(a.NS + e);
+            bool on0 = on.x, on1 = on.y;
+            if (s == sw.x) {  // waiting time from the spare bits of the normal words
+                on0 = !on0;
+                a.NS[e] = switch_at(s, make_int2(sw.x, sw.y), switch_uniform(w.x, w.y), on0, r0.inv_on, r0.inv_off);
+                a.prom[e] = on0;
+            }
+            if (has1 && s == sw.z) {
+                on1 = !on1;
+                a.NS[e + 1] = switch_at(s, make_int2(sw.z, sw.w), switch_uniform(w.z, w.w), on1, r1.inv_on, r1.inv_off);
+                a.prom[e + 1] = on1;
+            }
+            if (!on0) tx0 = 0.0f;
+            if (!on1) tx1 = 0.0f;
+        }
+        float2 m2 = mm[i], p2 = pp[i];
+        em_update(m2.x, p2.x, tx0, box_muller_parts(w.x, w.y), a.mu_m, a.mu_p, a.k_t, a.dt);
+        em_update(m2.y, p2.y, tx1, box_muller_parts(w.z, w.w), a.mu_m, a.mu_p, a.k_t, a.dt);
+        Mp[i * rs] = m2;
+        Pp[i * rs] = p2;
+        const float a0 = tensor_hill<HN>(p2.x, a), a1 = tensor_hill<HN>(p2.y, a);
+        T2 act;
+        act.x = to16<T>(a0);
+        act.y = to16<T>(has1 ? a1 : 0.0f);  // the padding column of the activations stays 0
+        actp[(size_t)i * (a.Kp >> 1)] = act;
+        if (src0 >= 0) a.act32_next[c * a.n_src + src0] = a0;
+        if (src1 >= 0) a.act32_next[c * a.n_src + src1] = a1;
     }
 }
 
 // Readout: cell-major FP32 state -> cells x G (x2) column-major Float64, through a
 // shared-memory tile so both the reads and the writes are coalesced.
-__global__ void tensor_readout_kernel(int G, int64_t N, const float* M, const float* P, int readout,
+__global__ void tensor_readout_kernel(int G, int ld, int64_t N, const float* M, const float* P, int readout,
                                       double* out) {
     __shared__ float tile[2][32][33];
     const int64_t c0 = (int64_t)blockIdx.x * 32;
@@ -164,8 +214,8 @@ __global__ void tensor_readout_kernel(int G, int64_t N, const float* M, const fl
         const int64_t c = c0 + r;
         const int g = g0 + threadIdx.x;
         const bool ok = c < N && g < G;
-        tile[0][r][threadIdx.x] = ok ? M[c * G + g] : 0.0f;
-        tile[1][r][threadIdx.x] = ok ? P[c * G + g] : 0.0f;
+        tile[0][r][threadIdx.x] = ok ? M[c * ld + g] : 0.0f;
+        tile[1][r][threadIdx.x] = ok ? P[c * ld + g] : 0.0f;
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -180,7 +230,7 @@ __global__ void tensor_readout_kernel(int G, int64_t N, const float* M, const fl
 }
 
 // Capture on the cell-major state (capture.jl:30-44), thread per (cell, gene).
-__global__ void tensor_capture_kernel(int G, int64_t N, int64_t cell_offset, const float* X, double mu_log,
+__global__ void tensor_capture_kernel(int G, int ld, int64_t N, int64_t cell_offset, const float* X, double mu_log,
                                       double sigma, uint32_t key0, uint32_t key1, uint32_t stream,
                                       double* eff, int32_t* Y) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -193,7 +243,7 @@ __global__ void tensor_capture_kernel(int G, int64_t N, int64_t cell_offset, con
     double pe = exp(mu_log + sigma * box_muller_z0_f64(w.x, w.y));
     pe = fmin(fmax(pe, 0.0), 1.0);
     if (g == 0 && eff) eff[c] = pe;
-    const double x = rint((double)X[idx]);
+    const double x = rint((double)X[c * ld + g]);
     const int64_t n = x > 0.0 ? (int64_t)x : 0;
     int64_t y = 0;
     if (n > 0 && pe != 0.0) y = binomial_capture(n, pe, key, stream, gcell, (uint32_t)g);
@@ -201,11 +251,11 @@ __global__ void tensor_capture_kernel(int G, int64_t N, int64_t cell_offset, con
 }
 
 template <class T>
-__global__ void tensor_fill_w_kernel(int G, int Kp, const float* wdense_rowmajor, T* w16) {
+__global__ void tensor_fill_w_kernel(int G, int K, int Kp, const float* w_rowmajor, T* w16) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)G * Kp) return;
     const int i = (int)(idx / Kp), j = (int)(idx - (int64_t)i * Kp);
-    w16[idx] = to16<T>(j < G ? wdense_rowmajor[(size_t)i * G + j] : 0.0f);
+    w16[idx] = to16<T>(j < K ? w_rowmajor[(size_t)i * K + j] : 0.0f);
 }
 
 // ---- host side -------------------------------------------------------------------------------
@@ -213,11 +263,15 @@ __global__ void tensor_fill_w_kernel(int G, int Kp, const float* wdense_rowmajor
 int tensor_prepare_net(scrna_net* n, int dtype) {
     if (n->t_dtype == dtype) return SCRNA_OK;
     const int G = n->G;
-    const int Kp = (G + 63) / 64 * 64;
-    std::vector<float> w((size_t)G * G, 0.0f);
+    const int n_terms = (int)n->na.size();
+    const int K = G + n_terms;
+    const int Kp = (K + 63) / 64 * 64;
+    std::vector<float> w((size_t)G * K, 0.0f);
     for (int i = 0; i < G; ++i)
         for (int j = 0; j < G; ++j)
-            if (i != j) w[(size_t)i * G + j] = (float)(n->A[(size_t)i * G + j] * n->basals[i]);
+            if (i != j) w[(size_t)i * K + j] = (float)(n->A[(size_t)i * G + j] * n->basals[i]);
+    for (int i = 0; i < G; ++i)
+        for (int e = n->na_begin[i]; e < n->na_begin[i] + n->na_count[i]; ++e) w[(size_t)i * K + G + e] = n->na[e].coef;
     // compact source indices of the cooperative / redundant edges
     std::vector<int32_t> src_of_gene(G, -1), src_gene;
     std::vector<int32_t> na_src(n->na_src.size());
@@ -231,8 +285,8 @@ int tensor_prepare_net(scrna_net* n, int dtype) {
     CU(cudaMemcpy(wf.p, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
     CU(n->t_w16.ensure((size_t)G * Kp * 2));
     const int64_t tot = (int64_t)G * Kp;
-    if (dtype == 0) tensor_fill_w_kernel<__nv_bfloat16><<<(unsigned)((tot + 255) / 256), 256>>>(G, Kp, wf.as<float>(), n->t_w16.as<__nv_bfloat16>());
-    else tensor_fill_w_kernel<__half><<<(unsigned)((tot + 255) / 256), 256>>>(G, Kp, wf.as<float>(), n->t_w16.as<__half>());
+    if (dtype == 0) tensor_fill_w_kernel<__nv_bfloat16><<<(unsigned)((tot + 255) / 256), 256>>>(G, K, Kp, wf.as<float>(), n->t_w16.as<__nv_bfloat16>());
+    else tensor_fill_w_kernel<__half><<<(unsigned)((tot + 255) / 256), 256>>>(G, K, Kp, wf.as<float>(), n->t_w16.as<__half>());
     CU(cudaGetLastError());
     CU(cudaDeviceSynchronize());
     CU(n->t_na_src.ensure(std::max<size_t>(na_src.size(), 1) * 4));
@@ -249,7 +303,7 @@ static int lt_fail(cublasStatus_t st, const char* what) {
     return fail(SCRNA_ECUDA, "%s failed (cuBLAS status %d)", what, (int)st);
 }
 
-// REG[N][G] = ACT[N][Kp] * W[G][Kp]^T in column-major terms: C (G x N, ldc G) =
+// REG[N][ld] = ACT[N][Kp] * W[G][Kp]^T in column-major terms: C (G x N, ldc ld) =
 // op(A) (G x Kp) * B (Kp x N) with A = W stored as Kp x G (lda Kp) transposed.
 struct LtGemm {
     cublasLtMatmulDesc_t op = nullptr;
@@ -264,7 +318,7 @@ struct LtGemm {
     }
 };
 
-static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int Kp, int64_t N) {
+static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp, int64_t N) {
     cublasStatus_t st;
     if (!ctx->lt_handle) {
         cublasLtHandle_t h;
@@ -280,7 +334,7 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int Kp, int64_t
     cublasLtMatmulDescSetAttribute(g.op, CUBLASLT_MATMUL_DESC_TRANSB, &tb, sizeof tb);
     if ((st = cublasLtMatrixLayoutCreate(&g.la, t16, Kp, G, Kp)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutA");
     if ((st = cublasLtMatrixLayoutCreate(&g.lb, t16, Kp, N, Kp)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutB");
-    if ((st = cublasLtMatrixLayoutCreate(&g.lc, CUDA_R_32F, G, N, G)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutC");
+    if ((st = cublasLtMatrixLayoutCreate(&g.lc, CUDA_R_32F, G, N, ld)) != CUBLAS_STATUS_SUCCESS) return lt_fail(st, "LayoutC");
     cublasLtMatmulPreference_t pref;
     cublasLtMatmulPreferenceCreate(&pref);
     cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ws, sizeof ws);
@@ -299,14 +353,15 @@ int64_t run_steps(const scrna_cle_opts* o);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype) {
     if (int r = tensor_prepare_net(n, dtype)) return r;
-    const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src;
+    const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, ld = tensor_ld(G);
     const int64_t N = st->N;
-    const size_t gn = (size_t)G * N;
-    CU(st->tM.ensure(gn * 4));
-    CU(st->tP.ensure(gn * 4));
-    CU(st->tprom.ensure(gn));
-    CU(st->tNS.ensure(gn * sizeof(int2)));
-    CU(st->treg.ensure(gn * 4));
+    const size_t gn = (size_t)G * N, ln = (size_t)ld * N;
+    CU(st->tM.ensure(ln * 4));
+    CU(st->tP.ensure(ln * 4));
+    CU(st->tprom.ensure(ln));
+    CU(st->tNS.ensure(ln * sizeof(int2)));
+    CU(st->treg.ensure(ln * 4));
+    st->t_ld = ld;
     CU(st->tact16.ensure((size_t)N * Kp * 2));
     for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
     CU(st->out.ensure(gn * (st->readout == SCRNA_READOUT_BOTH ? 2 : 1) * 8));
@@ -317,7 +372,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     cudaStream_t s = ctx->stream;
     CU(cudaMemsetAsync(st->tact16.p, 0, (size_t)N * Kp * 2, s));  // zero K padding
     TensorArgs a{};
-    a.G = G; a.Kp = Kp; a.n_src = n_src; a.N = N; a.cell_offset = o->cell_offset;
+    a.G = G; a.ld = ld; a.Kp = Kp; a.n_src = n_src; a.N = N; a.cell_offset = o->cell_offset;
     a.k_t = (float)kin->k_t;
     a.Kn = (float)std::pow(kin->K_d, kin->n);
     a.hill_n = (float)kin->n;
@@ -326,11 +381,16 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.mu_p = (float)(kin->mu_p + kin->dilution);
     a.dt = (float)o->dt;
     a.key0 = (uint32_t)o->seed; a.key1 = (uint32_t)(o->seed >> 32); a.stream = o->stream & 0xFFFFFFu;
+    for (int r = 0; r < 10; ++r) {
+        a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
+        a.rk1[r] = a.key1 + (uint32_t)r * 0xBB67AE85u;
+    }
     a.genes = n->b_genes.as<GeneRec>();
     a.ginit = n->b_ginit.as<GeneInit>();
     a.na = n->dev.na;
     a.na_src = n->t_na_src.as<int32_t>();
     a.src_of_gene = n->t_src_of_gene.as<int32_t>();
+    a.n_terms = (int)n->na.size();
     a.reg = st->treg.as<float>();
     a.M = st->tM.as<float>(); a.P = st->tP.as<float>();
     a.prom = st->tprom.as<uint8_t>(); a.NS = st->tNS.as<int2>();
@@ -344,33 +404,41 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     ctx->launches++;
 
     LtGemm gemm;
-    if (int r = lt_setup(ctx, gemm, dtype, G, Kp, N)) return r;
+    if (int r = lt_setup(ctx, gemm, dtype, G, ld, Kp, N)) return r;
     const float alpha = 1.0f, beta = 0.0f;
     const int64_t n_steps = run_steps(o);
-    const int pairs = (G + 1) / 2;
+    const int pairs = ld / 2;
+    using StepFn = void (*)(TensorArgs);
+    const bool h2 = a.hill_int == 2, bursty = n->dev.bursty;
+    StepFn step_fn;
+    if (dtype == 0) step_fn = bursty ? (h2 ? tensor_step_kernel<__nv_bfloat16, true, 2> : tensor_step_kernel<__nv_bfloat16, true, 0>)
+                                     : (h2 ? tensor_step_kernel<__nv_bfloat16, false, 2> : tensor_step_kernel<__nv_bfloat16, false, 0>);
+    else step_fn = bursty ? (h2 ? tensor_step_kernel<__half, true, 2> : tensor_step_kernel<__half, true, 0>)
+                          : (h2 ? tensor_step_kernel<__half, false, 2> : tensor_step_kernel<__half, false, 0>);
     const dim3 g_step((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
                       (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
     if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");
     for (int64_t step = 1; step <= n_steps; ++step) {
+        a.step = (int)step;
+        a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
+        a.act32_next = st->tact32[step & 1].as<float>();
+        if (a.n_terms > 0) {  // term columns from the previous step's activations
+            const int64_t nt = N * a.n_terms;
+            if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a);
+            else tensor_terms_kernel<__half><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a);
+            CU(cudaGetLastError());
+            ctx->launches += 1;
+        }
         cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,
                                             st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
                                             &gemm.algo, ctx->lt_workspace.p, ctx->lt_workspace.n, s);
         if (stt != CUBLAS_STATUS_SUCCESS) return lt_fail(stt, "cublasLtMatmul");
-        a.step = (int)step;
-        a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
-        a.act32_next = st->tact32[step & 1].as<float>();
-        if (dtype == 0) {
-            if (n->dev.bursty) tensor_step_kernel<__nv_bfloat16, true><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
-            else tensor_step_kernel<__nv_bfloat16, false><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
-        } else {
-            if (n->dev.bursty) tensor_step_kernel<__half, true><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
-            else tensor_step_kernel<__half, false><<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
-        }
+        step_fn<<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
         CU(cudaGetLastError());
         ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
     }
     dim3 rgrid((unsigned)((N + 31) / 32), (unsigned)((G + 31) / 32));
-    tensor_readout_kernel<<<rgrid, dim3(32, 8), 0, s>>>(G, N, st->tM.as<float>(), st->tP.as<float>(), st->readout,
+    tensor_readout_kernel<<<rgrid, dim3(32, 8), 0, s>>>(G, ld, N, st->tM.as<float>(), st->tP.as<float>(), st->readout,
                                                         st->out.as<double>());
     CU(cudaGetLastError());
     ctx->launches++;
@@ -378,7 +446,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         const double mu_log = std::log(cap->efficiency) -
                               (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
         const float* X = cap->readout == SCRNA_READOUT_MRNA ? st->tM.as<float>() : st->tP.as<float>();
-        tensor_capture_kernel<<<b_init, 256, 0, s>>>(G, N, o->cell_offset, X, mu_log, cap->efficiency_std, a.key0,
+        tensor_capture_kernel<<<b_init, 256, 0, s>>>(G, ld, N, o->cell_offset, X, mu_log, cap->efficiency_std, a.key0,
                                                      a.key1, a.stream, st->eff.as<double>(), st->counts.as<int32_t>());
         CU(cudaGetLastError());
         ctx->launches++;
