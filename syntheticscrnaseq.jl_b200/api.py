@@ -108,8 +108,11 @@ class NetHandle:
         self.G = int(net.G)
 
     def close(self):
+        # after the context is closed (e.g. finalized first at interpreter exit) the handle
+        # must not be used; the context's teardown already released the device
         if getattr(self, "h", None):
-            self.ctx.lib.scrna_net_destroy(self.h)
+            if getattr(self.ctx, "h", None):
+                self.ctx.lib.scrna_net_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -291,7 +294,8 @@ class DeviceRun:
 
     def close(self):
         if getattr(self, "st", None):
-            self.ctx.lib.scrna_state_destroy(self.st)
+            if getattr(self.ctx, "h", None):
+                self.ctx.lib.scrna_state_destroy(self.st)
             self.st = None
 
     def __del__(self):
@@ -376,7 +380,8 @@ class Server:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.scrna_server_destroy(self.h)
+            if getattr(self.ctx, "h", None):
+                self.ctx.lib.scrna_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

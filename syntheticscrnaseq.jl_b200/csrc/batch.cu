@@ -37,11 +37,11 @@ struct BatchNet {
 };
 
 struct GroupKey {
-    int warp, gpl, emax, tmax, upt, pop, interval;
+    int warp, gpl, emax, tmax, nwarps, upt, pop, interval;
     int64_t n_steps;
     bool operator<(const GroupKey& r) const {
-        return std::tie(warp, gpl, emax, tmax, upt, pop, interval, n_steps) <
-               std::tie(r.warp, r.gpl, r.emax, r.tmax, r.upt, r.pop, r.interval, r.n_steps);
+        return std::tie(warp, gpl, emax, tmax, nwarps, upt, pop, interval, n_steps) <
+               std::tie(r.warp, r.gpl, r.emax, r.tmax, r.nwarps, r.upt, r.pop, r.interval, r.n_steps);
     }
 };
 
@@ -60,10 +60,7 @@ struct Group {
 };
 
 int64_t cells_per_tile(const BatchNet& bn) {
-    if (bn.kc.warp) {
-        const int lpc = (bn.net->G + bn.kc.gpl - 1) / bn.kc.gpl;
-        return (int64_t)(32 / lpc) * 4;  // cells per warp x warps per block
-    }
+    if (bn.kc.warp) return warpcell_cells_per_block_host(bn.net->G, bn.kc.gpl);
     return 32;
 }
 
@@ -136,6 +133,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         k.gpl = x->kc.warp ? x->kc.gpl : 0;
         k.emax = x->kc.warp ? x->kc.emax : 0;
         k.tmax = x->kc.warp ? x->kc.tmax : 0;
+        k.nwarps = x->kc.warp ? x->kc.nwarps : 0;
         k.upt = x->kc.warp ? 0 : x->kc.block.upt;
         k.pop = x->pop != nullptr;
         k.interval = x->pop ? x->pop->div_check_interval : 0;
@@ -186,11 +184,12 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         CU(cudaMemcpyAsync(g.args.p, args.data(), args.size() * sizeof(FusedArgs), cudaMemcpyHostToDevice, g.stream));
         CU(cudaMemcpyAsync(g.items.p, items.data(), items.size() * sizeof(TileWork), cudaMemcpyHostToDevice, g.stream));
         const int n_items = (int)items.size();
-        const int grid = std::max(1, std::min(n_items, ctx->sm_count * (k.warp ? 6 : 8)));
+        const int grid = std::max(1, std::min(n_items, ctx->sm_count * (k.warp ? std::max(1, 24 / k.nwarps) : 8)));
         auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
             if (k.warp)
                 return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
-                                             k.emax, k.tmax, k.pop != 0, smem, grid, ctl, use_shared, g.stream);
+                                             k.emax, k.tmax, k.pop != 0, smem, grid, k.nwarps, ctl, use_shared,
+                                             g.stream);
             return fused_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
                                       smem, k.pop != 0, grid, ctl, use_shared, g.stream);
         };

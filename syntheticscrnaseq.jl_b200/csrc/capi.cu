@@ -284,9 +284,11 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     }
     lane_ok = lane_ok && max_in <= kLaneEdges;
     const int emax = warpcell_emax_class(max_in);
-    const int gpl = warpcell_pick_gpl(G, d.bursty, emax);
-    const int lpc = (G + gpl - 1) / gpl;
-    const int tmax = (d.n_na + lpc - 1) / lpc;
+    // genes per lane: the cheaper of 2 and 4 that leaves <= kLaneTerms terms per lane
+    auto terms_per_lane = [&](int g) { const int lpc = (G + g - 1) / g; return (d.n_na + lpc - 1) / lpc; };
+    int gpl = warpcell_pick_gpl(G, d.bursty, emax);
+    if (terms_per_lane(gpl) > kLaneTerms && gpl == 4) gpl = 2;
+    const int tmax = terms_per_lane(gpl);
     lane_ok = lane_ok && tmax <= kLaneTerms;
     if (lane_ok) {
         const int zero_slot = d.n_reg, one_slot = d.n_reg + 1;  // constant slots of the kernel's rows
@@ -547,6 +549,7 @@ scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     k.gpl = d.lane_gpl;
     k.emax = d.lane_emax;
     k.tmax = d.lane_tmax;
+    k.nwarps = warp_ok ? warpcell_block_warps_host(d.G, d.lane_gpl) : 0;
     k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
     k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na) : k.block.smem;
     return k;

@@ -115,7 +115,7 @@ namespace scrna {
 // Register-path kernel chosen for a network.
 struct KernelChoice {
     bool warp;
-    int gpl, emax, tmax;
+    int gpl, emax, tmax, nwarps;
     FusedLaunch block;
     size_t smem;
 };
@@ -133,8 +133,10 @@ cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
                                cudaStream_t st);
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int emax, int tmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
-                                  int use_shared, cudaStream_t st);
+                                  int emax, int tmax, bool pop, size_t smem, int grid, int nwarps,
+                                  TileCtl shared_ctl, int use_shared, cudaStream_t st);
+int warpcell_cells_per_block_host(int G, int gpl);
+int warpcell_block_warps_host(int G, int gpl);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype);
 int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,

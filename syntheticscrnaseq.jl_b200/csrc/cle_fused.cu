@@ -4,6 +4,7 @@
 #include <type_traits>
 
 #include "cle_internal.h"
+#include "cle_warpcell.cuh"
 #include <cuda_runtime.h>
 
 namespace scrna {
@@ -47,43 +48,39 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
     }
 }
 
-// ---- warp-per-cell-group variant for small networks ---------------------------------------
+// ---- lane-per-gene-unit variant (networks up to 512 genes) ---------------------------------
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st);
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
-                                    size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
+                                    size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
+                                    cudaStream_t st);
 template <int UPT, bool POP>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 
-int warpcell_max_genes() { return 32; }
+int warpcell_max_genes() { return kWarpcellMaxGenes; }
 int warpcell_emax_class(int max_in) { return max_in <= 2 ? 2 : max_in <= 4 ? 4 : 8; }
 
-// Genes per lane for a network: a cost model of issue slots per cell-gene-step
-// (Philox calls per gene, plus lanes left idle by the cell packing).
+// Genes per lane for a network: a cost model of issue slots per cell-gene-step, ~20 per
+// lane and step plus ~80 per gene, over the lanes a cell occupies (idle lanes included).
 int warpcell_pick_gpl(int G, bool bursty, int emax) {
+    (void)bursty;
     if (emax > 4) return 2;  // 8 padded in-edges per gene: only gene pairs fit in registers
     double best = 1e30;
     int pick = 2;
     for (int gpl : {2, 4}) {
-        const int lpc = (G + gpl - 1) / gpl;
-        const int cpw = 32 / lpc;
-        const double philox = 0.5 + (bursty ? 0.02 : 0.0);
-        const double waste = 32.0 * gpl / ((double)G * cpw);
-        const double cost = (48.0 + 42.0 * philox) * waste;
+        const int w = warpcell_wpc(G, gpl);
+        const double lanes = w == 1 ? 32.0 / warpcell_cells_per_warp(G, gpl) : 32.0 * w;
+        const double cost = lanes * (20.0 + 80.0 * gpl) / G;
         if (cost < best) { best = cost; pick = gpl; }
     }
     return pick;
 }
 
-size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms) {
-    const int lpc = (G + gpl - 1) / gpl;
-    const int cpw = 32 / lpc;
-    const int ld = (n_reg + 3 + n_terms) | 1;  // slots, constants 0 and 1, a write-only slot, terms
-    const size_t b = (size_t)4 * (cpw + 1) * ld * sizeof(float);
-    return (b + 15) & ~(size_t)15;
-}
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms) { return warpcell_smem_bytes(G, gpl, n_reg, n_terms); }
+int warpcell_cells_per_block_host(int G, int gpl) { return warpcell_cells_per_block(G, gpl); }
+int warpcell_block_warps_host(int G, int gpl) { return warpcell_block_warps(G, gpl); }
 
 template <int V>
 using IntC = std::integral_constant<int, V>;
@@ -120,11 +117,11 @@ cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, boo
 }
 
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
-                                  int emax, int tmax, bool pop, size_t smem, int grid, TileCtl shared_ctl,
-                                  int use_shared, cudaStream_t st) {
+                                  int emax, int tmax, bool pop, size_t smem, int grid, int nwarps,
+                                  TileCtl shared_ctl, int use_shared, cudaStream_t st) {
     return warpcell_dispatch(gpl, emax, tmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_queue_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(
-            args, items, n_items, counter, smem, grid, shared_ctl, use_shared, st);
+            args, items, n_items, counter, smem, grid, nwarps, shared_ctl, use_shared, st);
     });
 }
 

@@ -1,7 +1,8 @@
-// Warp-per-cell-group register-path CLE kernel for small networks (sm_100a).
+// Lane-per-gene-unit register-path CLE kernel for networks up to 512 genes (sm_100a).
 //
-// For G <= 32 genes, a whole cell lives inside one warp: lane = (cell, unit) where a
-// unit is GPL consecutive genes (a gene pair or a gene quad).  A cell's regulator
+// lane = (cell, unit) where a unit is GPL consecutive genes (a gene pair or a gene quad).
+// A cell whose units fit in a warp shares the warp with other cells (no barrier at all);
+// a larger cell spans wpc <= 8 warps synchronised by a named barrier of its own.  A cell's regulator
 // activations live in one shared-memory row: the regulator slots, the constants 0 and 1,
 // a write-only slot, then one slot per cooperative / redundant term holding that term's
 // value (the product over its sources), so a term enters its target's regulation as one
@@ -9,8 +10,8 @@
 // EMAX in-edges (weight, shared-memory address of the source slot), and the TMAX terms
 // of the cell that it evaluates.  Per Euler step:
 //   Hill of the lane's genes into the row -> Philox (+ telegraph switch) + Box-Muller
-//   -> __syncwarp -> term values into the row -> __syncwarp -> reg = cneg + sum of EMAX
-//   padded edges -> M, P update.
+//   -> cell sync -> term values into the row -> cell sync -> reg = cneg + sum of EMAX
+//   padded edges -> M, P update -> cell sync.
 // No lane branches on the network's structure and there is no block-wide barrier.
 // The arithmetic and the Philox streams are those of cle_fused_kernel (same sums in the
 // same order: a gene's edges are sorted by slot, so its additive edges come first, then
@@ -23,10 +24,30 @@
 
 namespace scrna {
 
-constexpr int kWarpcellWarps = 4;  // warps per block
+constexpr int kWarpcellMaxGenes = 512;
 
+// Launch geometry of a network (host and device agree on it).
 __host__ __device__ inline int warpcell_lanes_per_cell(int G, int gpl) { return (G + gpl - 1) / gpl; }
-__host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 32 / warpcell_lanes_per_cell(G, gpl); }
+// warps per cell: 1 when a cell fits in a warp (then several cells share it)
+__host__ __device__ inline int warpcell_wpc(int G, int gpl) { return (warpcell_lanes_per_cell(G, gpl) + 31) / 32; }
+__host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) {
+    const int lpc = warpcell_lanes_per_cell(G, gpl);
+    return lpc <= 32 ? 32 / lpc : 1;
+}
+// warps per block: 4 independent warps of small cells, or whole multi-warp cells (<= 8 warps)
+__host__ __device__ inline int warpcell_block_warps(int G, int gpl) {
+    const int w = warpcell_wpc(G, gpl);
+    return w == 1 ? 4 : w * (8 / w);
+}
+__host__ __device__ inline int warpcell_cells_per_block(int G, int gpl) {
+    const int w = warpcell_wpc(G, gpl);
+    return w == 1 ? warpcell_block_warps(G, gpl) * warpcell_cells_per_warp(G, gpl) : warpcell_block_warps(G, gpl) / w;
+}
+// activation rows of a block: one per cell, plus a row per warp for the spare lanes of small cells
+__host__ __device__ inline int warpcell_rows_per_block(int G, int gpl) {
+    const int w = warpcell_wpc(G, gpl);
+    return w == 1 ? warpcell_block_warps(G, gpl) * (warpcell_cells_per_warp(G, gpl) + 1) : warpcell_block_warps(G, gpl) / w;
+}
 
 // Activation row of one cell: n_reg regulator slots, the constants 0 (slot n_reg) and 1
 // (slot n_reg + 1), a write-only slot (n_reg + 2) for values nobody reads, then the
@@ -34,9 +55,19 @@ __host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) { return 
 __host__ __device__ inline int warpcell_ld(int n_reg, int n_terms) { return (n_reg + 3 + n_terms) | 1; }
 
 __host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg, int n_terms) {
-    const int cpw = warpcell_cells_per_warp(G, gpl);
-    const size_t b = (size_t)kWarpcellWarps * (cpw + 1) * warpcell_ld(n_reg, n_terms) * sizeof(float);
+    const size_t b = (size_t)warpcell_rows_per_block(G, gpl) * warpcell_ld(n_reg, n_terms) * sizeof(float);
     return (b + 15) & ~(size_t)15;
+}
+
+// Barrier of the wpc warps of one cell: named barrier 1 + cell group of the block (a block
+// holds at most 4 multi-warp cells).  Literal ids keep the kernel's barrier count at 5.
+__device__ __forceinline__ void cell_barrier(int id, int nthreads) {
+    switch (id) {
+        case 1: asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); break;
+        case 2: asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory"); break;
+        case 3: asm volatile("bar.sync 3, %0;" ::"r"(nthreads) : "memory"); break;
+        default: asm volatile("bar.sync 4, %0;" ::"r"(nthreads) : "memory"); break;
+    }
 }
 
 // Word of gene u*GPL+i in the quad's Philox block (word index (u*GPL+i) mod 4), selected
@@ -62,41 +93,64 @@ __device__ __forceinline__ float warpcell_hill(float p, const FusedArgs& a) {
     return hill_act(p, a.Kn, a.hill_n, a.hill_int);
 }
 
-// One block tile (kWarpcellWarps warps of cells) of one network through ctl's step range.
+// One block tile (warpcell_cells_per_block cells) of one network through ctl's step range.
 // RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
 // HN: 2 for a Hill exponent of exactly 2, else 0 (any exponent).
-template <int GPL, int EMAX, int TMAX, bool POP, bool RK, int HN>
+// MW: cells span several warps (warpcell_wpc > 1), else several cells share a warp.
+template <int GPL, int EMAX, int TMAX, bool POP, bool RK, int HN, bool MW>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
     constexpr int TM = TMAX > 0 ? TMAX : 1;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
-    const int cpw = 32 / lpc;
+    const int wpc = MW ? warpcell_wpc(G, GPL) : 1;
     const int n_reg = a.n_reg;
     const int n_terms = a.n_na;
     const int ld = warpcell_ld(n_reg, n_terms);
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    int cl = lane / lpc;
-    const int u = lane - cl * lpc;
-    const bool lane_ok = cl < cpw;
-    if (!lane_ok) cl = cpw;  // spare lanes work on a private dummy row
+    const int nwarps = blockDim.x >> 5;
+    int u, row_idx, first_row, n_rows;
+    bool lane_ok;
+    int64_t cell;
+    if (!MW) {  // several cells per warp; spare lanes work on a private dummy row
+        const int cpw = 32 / lpc;
+        int cl = lane / lpc;
+        u = lane - cl * lpc;
+        lane_ok = cl < cpw;
+        if (!lane_ok) cl = cpw;
+        cell = (tile * nwarps + warp) * cpw + (lane_ok ? cl : 0);
+        first_row = warp * (cpw + 1);
+        n_rows = cpw + 1;
+        row_idx = first_row + cl;
+    } else {  // one cell per group of wpc warps; spare lanes of its last warp hold no gene
+        const int grp = warp / wpc;
+        u = (warp - grp * wpc) * 32 + lane;
+        lane_ok = u < lpc;
+        cell = tile * (nwarps / wpc) + grp;
+        first_row = row_idx = grp;
+        n_rows = (warp - grp * wpc) == 0 ? 1 : 0;  // the group's first warp sets up the row
+    }
+    const int bar_id = 1 + warp / wpc, bar_threads = 32 * wpc;
+    auto cell_sync = [&]() {
+        if (!MW) __syncwarp();
+        else cell_barrier(bar_id, bar_threads);
+    };
     const int64_t N = a.N;
-    const int64_t cell = (tile * kWarpcellWarps + warp) * cpw + (lane_ok ? cl : 0);
     const bool live = lane_ok && cell < N;
     const int64_t cidx = cell < N ? cell : N - 1;
     const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
     const Key key{a.key0, a.key1};
 
-    // constant slots of this warp's rows (written once; Hill stores never touch them)
-    float* rows = reinterpret_cast<float*>(smem_raw) + (size_t)warp * (cpw + 1) * ld;
-    for (int r = lane; r < cpw + 1; r += 32) {
+    // constant slots of the rows (written once; Hill stores never touch them)
+    float* rows = reinterpret_cast<float*>(smem_raw) + (size_t)first_row * ld;
+    for (int r = lane; r < n_rows; r += 32) {
         rows[(size_t)r * ld + n_reg] = 0.0f;
         rows[(size_t)r * ld + n_reg + 1] = 1.0f;
     }
-    __syncwarp();
-    const uint32_t row = (uint32_t)(((size_t)warp * (cpw + 1) + cl) * ld * sizeof(float));
+    cell_sync();
+    const uint32_t row = (uint32_t)((size_t)row_idx * ld * sizeof(float));
     auto slot_addr = [&](int slot) { return row + (uint32_t)slot * (uint32_t)sizeof(float); };
 
     // per-lane gene constants
@@ -226,7 +280,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 #pragma unroll
     for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
-        __syncwarp();  // every lane has read the row of the previous step
+        cell_sync();  // every lane has read the row of the previous step
         if (any_reg) {
 #pragma unroll
             for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = warpcell_hill<HN>(p[i], a);
@@ -268,7 +322,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 #pragma unroll
             for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
         }
-        __syncwarp();  // the cell's activations are complete
+        cell_sync();  // the cell's activations are complete
         if (TMAX > 0) {
 #pragma unroll
             for (int k = 0; k < TMAX; ++k) {  // x and 1-x are exact as fmaf(+-1, x, 0 or 1)
@@ -277,7 +331,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
                 for (int q = 0; q < kLaneSrc; ++q) prod *= fmaf(tsg[k], smem_f32(smem_raw, ta[k][q]), tof[k]);
                 smem_f32(smem_raw, tout[k]) = fmaf(tsg[k], prod, tof[k]);
             }
-            __syncwarp();  // the cell's term values are complete
+            cell_sync();  // the cell's term values are complete
         }
         const float Vf = POP ? (float)V : 1.0f;
 #pragma unroll
@@ -383,15 +437,21 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 }
 
 template <int GPL, int EMAX, int TMAX, bool POP>
-__global__ void __launch_bounds__(32 * kWarpcellWarps, 6) cle_warpcell_kernel(const FusedArgs a) {
+__global__ void __launch_bounds__(256, 3) cle_warpcell_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    if (a.hill_int == 2) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2>(a, blockIdx.x, ctl, smem_raw);
-    else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0>(a, blockIdx.x, ctl, smem_raw);
+    const bool mw = warpcell_wpc(a.G, GPL) > 1;
+    if (a.hill_int == 2) {
+        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, true>(a, blockIdx.x, ctl, smem_raw);
+        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, false>(a, blockIdx.x, ctl, smem_raw);
+    } else {
+        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, true>(a, blockIdx.x, ctl, smem_raw);
+        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, false>(a, blockIdx.x, ctl, smem_raw);
+    }
 }
 
 template <int GPL, int EMAX, int TMAX, bool POP>
-__global__ void __launch_bounds__(32 * kWarpcellWarps, 6)
+__global__ void __launch_bounds__(256, 3)
 cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -405,8 +465,14 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         const TileWork w = items[it];
         const FusedArgs& a = args[w.arg];
         const TileCtl& ctl = use_shared ? shared_ctl : w.ctl;
-        if (a.hill_int == 2) warpcell_tile<GPL, EMAX, TMAX, POP, false, 2>(a, w.tile, ctl, smem_raw);
-        else warpcell_tile<GPL, EMAX, TMAX, POP, false, 0>(a, w.tile, ctl, smem_raw);
+        const bool mw = warpcell_wpc(a.G, GPL) > 1;
+        if (a.hill_int == 2) {
+            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, true>(a, w.tile, ctl, smem_raw);
+            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, false>(a, w.tile, ctl, smem_raw);
+        } else {
+            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, true>(a, w.tile, ctl, smem_raw);
+            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, false>(a, w.tile, ctl, smem_raw);
+        }
         __syncthreads();
     }
 }
@@ -417,19 +483,21 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg, a.n_na);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int64_t cpb = (int64_t)warpcell_cells_per_warp(a.G, GPL) * kWarpcellWarps;
+    const int64_t cpb = warpcell_cells_per_block(a.G, GPL);
     const unsigned blocks = (unsigned)((a.N + cpb - 1) / cpb);
-    k<<<blocks, 32 * kWarpcellWarps, smem, st>>>(a);
+    k<<<blocks, 32 * warpcell_block_warps(a.G, GPL), smem, st>>>(a);
     return cudaGetLastError();
 }
 
+// Every network of one queue launch has the same warps per block (nwarps).
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
-                                    size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
+                                    size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
+                                    cudaStream_t st) {
     auto k = cle_warpcell_queue_kernel<GPL, EMAX, TMAX, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, 32 * kWarpcellWarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
+    k<<<grid, 32 * nwarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
     return cudaGetLastError();
 }
 
@@ -440,7 +508,7 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
 #define SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, TMAX, POP)                                                        \
     template cudaError_t scrna::warpcell_launch_t<GPL, EMAX, TMAX, POP>(const FusedArgs&, cudaStream_t);         \
     template cudaError_t scrna::warpcell_queue_launch_t<GPL, EMAX, TMAX, POP>(                                   \
-        const FusedArgs*, const TileWork*, int, int*, size_t, int, TileCtl, int, cudaStream_t);
+        const FusedArgs*, const TileWork*, int, int*, size_t, int, int, TileCtl, int, cudaStream_t);
 #define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, EMAX)       \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, false)     \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, true)      \

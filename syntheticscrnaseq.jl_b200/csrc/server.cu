@@ -182,10 +182,11 @@ void scrna_server::run() {
             r->s0 = r->next;
             r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps - 1);
             const KernelChoice& kc = r->kc;
-            auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.emax : 0, kc.warp ? 0 : kc.block.upt,
-                                       kc.warp ? kc.tmax : 0);
+            // (warp kernel, genes per lane, in-edges, warps per block or block-kernel quads per thread, terms)
+            auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.emax : 0,
+                                       kc.warp ? kc.nwarps : kc.block.upt, kc.warp ? kc.tmax : 0);
             int64_t cpt = 32;
-            if (kc.warp) cpt = (int64_t)(32 / ((r->net->G + kc.gpl - 1) / kc.gpl)) * 4;
+            if (kc.warp) cpt = warpcell_cells_per_block_host(r->net->G, kc.gpl);
             const int64_t tiles = (r->N + cpt - 1) / cpt;
             TileCtl ctl{(int32_t)r->s0, (int32_t)r->s1, r->s0 == 1 ? 1 : 0, r->s1 >= r->n_steps ? 1 : 0, 0, 0};
             auto& items = groups[key];
@@ -217,10 +218,12 @@ void scrna_server::run() {
             const TileWork* items = items_dev.as<TileWork>() + offsets[gi];
             int* counter = counters_dev.as<int>() + gi;
             const auto& sh = shape[key];
-            const int grid = std::max(1, std::min(n_items, ctx->sm_count * (std::get<0>(key) ? 6 : 8)));
+            const int per_sm = std::get<0>(key) ? std::max(1, 24 / std::get<3>(key)) : 8;
+            const int grid = std::max(1, std::min(n_items, ctx->sm_count * per_sm));
             if (std::get<0>(key))
                 e = warpcell_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<1>(key),
-                                          std::get<2>(key), std::get<4>(key), false, sh.second, grid, TileCtl{}, 0, stream);
+                                          std::get<2>(key), std::get<4>(key), false, sh.second, grid,
+                                          std::get<3>(key), TileCtl{}, 0, stream);
             else
                 e = fused_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<3>(key), sh.first,
                                        sh.second, false, grid, TileCtl{}, 0, stream);

@@ -230,10 +230,13 @@ def test_gpu_vs_cpu_ensemble(pkg, orc):
 
 
 @pytest.mark.parametrize("G,bursty,seed", [(1, False, 1), (2, True, 2), (3, True, 3), (5, False, 4),
-                                           (10, True, 5), (13, True, 6), (17, False, 7), (32, True, 8)])
+                                           (10, True, 5), (13, True, 6), (17, False, 7), (32, True, 8),
+                                           (40, True, 9), (77, False, 10), (150, True, 11), (300, False, 12),
+                                           (500, True, 13)])
 def test_warp_and_block_kernels_identical(pkg, G, bursty, seed):
-    """The warp-per-cell-group kernel and the block-tile kernel compute the same sums in
-    the same order on the same increments: their results are bit-identical."""
+    """The lane-per-gene-unit kernel (cells within a warp, or spanning up to 8 warps with a
+    named barrier) and the block-tile kernel compute the same sums in the same order on the
+    same increments: their results are bit-identical."""
     net = pkg.sample_network(G, seed=seed, bursty=bursty)
     kin = pkg.WORKLOAD_KINETICS
     N = 257
@@ -284,9 +287,9 @@ def test_warp_kernel_rejects_long_terms(pkg):
     assert np.array_equal(a["P"], b["P"])
 
 
-@pytest.mark.parametrize("partition", ["halve", "binomial"])
-def test_warp_and_block_kernels_identical_population(pkg, partition):
-    net = pkg.sample_network(7, seed=9, bursty=True)
+@pytest.mark.parametrize("partition,G", [("halve", 7), ("binomial", 7), ("binomial", 120)])
+def test_warp_and_block_kernels_identical_population(pkg, partition, G):
+    net = pkg.sample_network(G, seed=9, bursty=True)
     kin = pkg.WORKLOAD_KINETICS
     pop = pkg.PopulationConfig(cell_num=300, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
                                div_check_interval=10, partition=partition)
