@@ -113,7 +113,7 @@ class ClockSampler:
 
 def _traffic_per_launch():
     """DRAM bytes per launch of the fused kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "cle_fused_telegraph_capture_G10_N20000.md")
+    path = os.path.join(ROOT, "profiles", "cle_warpcell_telegraph_capture_G10_N20000.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
