@@ -56,12 +56,14 @@ enum scrna_precision {
 };
 
 /* Kernel family for the FP32 precision.  AUTO picks the register path for sparse
- * networks (the warp-per-cell-group kernel when G <= 32 with <= 16 regulator genes,
- * block tiles otherwise) and the tensor-core path for large dense ones.  BLOCK and
- * WARP force one register-path kernel (both give identical results). */
+ * networks (the lane-per-gene-unit kernel when the network fits it, G <= 512, block tiles
+ * otherwise) and the tensor-core path for large dense ones.  BLOCK and WARP force one
+ * register-path kernel (both give identical results).  TENSOR is the fused tcgen05
+ * contraction + Euler step; TENSOR_LIBRARY the same step with the contraction done by a
+ * library GEMM (cuBLASLt) and a separate update kernel, kept for comparison. */
 enum scrna_path {
     SCRNA_PATH_AUTO = 0, SCRNA_PATH_REGISTER = 1, SCRNA_PATH_TENSOR = 2,
-    SCRNA_PATH_BLOCK = 3, SCRNA_PATH_WARP = 4
+    SCRNA_PATH_BLOCK = 3, SCRNA_PATH_WARP = 4, SCRNA_PATH_TENSOR_LIBRARY = 5
 };
 
 typedef struct scrna_ctx scrna_ctx;
@@ -268,6 +270,12 @@ int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, const scrna
  * published known-answer vectors. */
 int scrna_debug_philox(scrna_ctx* ctx, int32_t n, const uint32_t* ctr, const uint32_t* key,
                        uint32_t* out);
+/* C[M x N] (FP32, row-major) = A[M x K] * B[N x K]^T on device pointers, A and B 16-bit
+ * (dtype 0 BF16, 1 FP16) row-major with K a multiple of 64, by the library's hand-written
+ * tcgen05 GEMM (the contraction of the dense path); synchronous.  No counterpart in the
+ * reference: it checks the tensor-core kernel against another GEMM. */
+int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
+                        int32_t K, int32_t dtype);
 /* Measures the sustained issue rate of the FP32 FMA pipe and of the special-function
  * unit (MUFU) pipe with two microkernels; results in operations per second. */
 int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma_ops_per_s, double* sfu_ops_per_s,

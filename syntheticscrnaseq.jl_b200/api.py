@@ -22,7 +22,7 @@ from .model import CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConf
 
 READOUT = {"mrna": 0, "protein": 1, "both": 2}
 PRECISION = {"fp32": 0, "fp64_plain": 1, "fp32_f16": 2}
-PATH = {"auto": 0, "register": 1, "tensor": 2, "block": 3, "warp": 4}
+PATH = {"auto": 0, "register": 1, "tensor": 2, "block": 3, "warp": 4, "tensor_library": 5}
 
 
 class Context:

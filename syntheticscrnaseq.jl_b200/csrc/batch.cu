@@ -119,10 +119,15 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
 int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* cap) {
     // dense networks: tensor-core path, one after another on the context stream
     for (BatchNet* x : all)
-        if (x->tensor) {
-            x->st->last_tensor = true;
+        if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
+            const bool fused = x->net->G <= 4096;
+            x->st->last_tensor = !fused;
+            x->st->last_plain = false;
+            x->st->last_pop = false;
             x->st->have_counts = cap != nullptr;
-            if (int r = tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)) return r;
+            if (int r = fused ? tc_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)
+                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0))
+                return r;
         }
     // register-path networks: one persistent launch (or one captured chunk sequence) per group
     std::map<GroupKey, std::unique_ptr<Group>> groups;

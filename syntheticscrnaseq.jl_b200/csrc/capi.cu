@@ -683,7 +683,7 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
     // kernel family: tensor cores for large dense networks (or when asked), else the register path
     const NetDev& nd = net->dev;
     const double density = (double)nd.n_in / ((double)net->G * net->G);
-    const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR ||
+    const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
                                    (o->path == SCRNA_PATH_AUTO &&
                                     (nd.n_quads > fused_max_quads() || (net->G >= 256 && density >= 0.05))));
     if (tensor) {
@@ -691,8 +691,13 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
         st->have_counts = cap != nullptr;
         st->last_plain = false;
         st->last_pop = false;
-        st->last_tensor = true;
-        return tensor_run(ctx, net, kin, cap, o, st, o->precision == SCRNA_PRECISION_FP32_F16 ? 1 : 0);
+        const int dtype = o->precision == SCRNA_PRECISION_FP32_F16 ? 1 : 0;
+        if (o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {  // library-GEMM variant, cell-major state
+            st->last_tensor = true;
+            return tensor_run(ctx, net, kin, cap, o, st, dtype);
+        }
+        st->last_tensor = false;  // the fused kernel keeps the register path's gene-major state
+        return tc_run(ctx, net, kin, cap, o, st, dtype);
     }
     st->last_tensor = false;
     if (int r = state_alloc(st, pop != nullptr, plain)) return r;

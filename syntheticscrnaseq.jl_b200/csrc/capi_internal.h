@@ -58,6 +58,7 @@ struct scrna_ctx {
     // cuBLASLt handle and workspace of the tensor-core path (created on first use)
     void* lt_handle = nullptr;
     scrna::DevBuf lt_workspace;
+    scrna::DevBuf tc_err;        // error flag of the tcgen05 kernels (one int)
 };
 
 struct scrna_net {
@@ -137,6 +138,11 @@ cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, 
                                   TileCtl shared_ctl, int use_shared, cudaStream_t st);
 int warpcell_cells_per_block_host(int G, int gpl);
 int warpcell_block_warps_host(int G, int gpl);
+int tensor_prepare_net(scrna_net* n, int dtype);
+cudaError_t tensor_terms_launch(int dtype, int64_t N, int G, int Kp, int n_terms, int n_src, const NonAdd* na,
+                                const int32_t* na_src, const float* act32, void* act16, cudaStream_t st);
+int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
+           const scrna_cle_opts* o, scrna_state* st, int dtype);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype);
 int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,

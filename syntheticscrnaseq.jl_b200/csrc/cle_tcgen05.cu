@@ -1,0 +1,685 @@
+// Hand-written tcgen05 kernels for sm_100a.
+//
+// tc_gemm_kernel: C[M x N] (FP32) = A[M x K] * B[N x K]^T with A and B 16-bit (BF16 or
+// FP16), both K-major — the shape of the dense path's per-step contraction REG = ACT * W^T.
+// tc_cle_step_kernel: the same contraction with one Euler-Maruyama step of the CLE fused
+// into its epilogue, so the regulation never leaves the chip.
+//
+// One persistent CTA per SM:
+//   warp 0      TMA producer: 128 x 64 tiles of A and 256 x 64 tiles of B into a 4-stage
+//               shared-memory ring (128-byte swizzle), one mbarrier per stage;
+//   warp 1      allocates 512 TMEM columns (two 128 x 256 FP32 accumulators); one thread
+//               issues tcgen05.mma (M=128, N=256, K=16, four per stage) and commits each
+//               stage back to the producer and each finished accumulator to the epilogue;
+//   epilogue    warps 2.. : warp w reads TMEM lanes 32 (w % 4) .. +31 (one row = one cell
+//               each) in 32-column loads.
+// The two accumulators let the epilogue of one tile overlap the MMAs of the next.  Every
+// wait is bounded (tc::mbar_wait); a timeout sets the error flag and the kernel leaves.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "capi_internal.h"
+#include "cle_device.cuh"
+#include "tc_sm100.cuh"
+
+namespace scrna {
+
+constexpr int kTcBM = 128, kTcBN = 256, kTcBK = 64, kTcStages = 4;
+constexpr int kTcThreads = 192;
+constexpr uint32_t kTcABytes = kTcBM * kTcBK * 2, kTcBBytes = kTcBN * kTcBK * 2;
+constexpr size_t kTcSmem = 1024 + (size_t)kTcStages * (kTcABytes + kTcBBytes) + 256;
+
+struct TcShared {
+    uint64_t full[kTcStages], empty[kTcStages], tmem_full[2], tmem_empty[2];
+    uint32_t tmem_base;
+};
+
+__device__ __forceinline__ void tc_fail(int* err, int code) { atomicCAS(err, 0, code); }
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, float* C,
+               int M, int N, int K, uint32_t idesc, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_dyn[];
+    // 1024-byte aligned stage buffers (128-byte swizzle atoms), control block after them
+    const uint32_t base = tc::smem_u32(smem_dyn);
+    unsigned char* stages = smem_dyn + ((1024 - (base & 1023)) & 1023);
+    unsigned char* a_s = stages;
+    unsigned char* b_s = stages + (size_t)kTcStages * kTcABytes;
+    TcShared* sh = reinterpret_cast<TcShared*>(b_s + (size_t)kTcStages * kTcBBytes);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_m = (M + kTcBM - 1) / kTcBM, tiles_n = (N + kTcBN - 1) / kTcBN;
+    const int n_tiles = tiles_m * tiles_n;
+    const int kb_n = (K + kTcBK - 1) / kTcBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            tc::mbar_init(&sh->full[s], 1);
+            tc::mbar_init(&sh->empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&sh->tmem_full[a], 1);
+            tc::mbar_init(&sh->tmem_empty[a], 4);  // one arrival per epilogue warp
+        }
+        tc::fence_mbar_init();
+        tc::prefetch_tensormap(&map_a);
+        tc::prefetch_tensormap(&map_b);
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(&sh->tmem_base, 2 * kTcBN);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh->tmem_base;
+
+    if (warp == 0 && lane == 0) {  // ---- TMA producer
+        int stage = 0;
+        uint32_t phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
+            for (int kb = 0; kb < kb_n; ++kb) {
+                if (!tc::mbar_wait(&sh->empty[stage], phase ^ 1u)) { tc_fail(err, 1); goto producer_done; }
+                tc::mbar_arrive_expect_tx(&sh->full[stage], kTcABytes + kTcBBytes);
+                tc::tma_load_2d(a_s + (size_t)stage * kTcABytes, &map_a, &sh->full[stage], kb * kTcBK, m * kTcBM);
+                tc::tma_load_2d(b_s + (size_t)stage * kTcBBytes, &map_b, &sh->full[stage], kb * kTcBK, n * kTcBN);
+                if (++stage == kTcStages) { stage = 0; phase ^= 1u; }
+            }
+        }
+    producer_done:;
+    } else if (warp == 1 && lane == 0) {  // ---- MMA issuer
+        int stage = 0, acc = 0;
+        uint32_t phase = 0, acc_phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            if (!tc::mbar_wait(&sh->tmem_empty[acc], acc_phase ^ 1u)) { tc_fail(err, 3); break; }
+            tc::tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(acc * kTcBN);
+            bool ok = true;
+            for (int kb = 0; kb < kb_n; ++kb) {
+                if (!tc::mbar_wait(&sh->full[stage], phase)) { tc_fail(err, 2); ok = false; break; }
+                tc::tc_fence_after();
+                const uint32_t a_addr = tc::smem_u32(a_s + (size_t)stage * kTcABytes);
+                const uint32_t b_addr = tc::smem_u32(b_s + (size_t)stage * kTcBBytes);
+#pragma unroll
+                for (int k = 0; k < kTcBK / 16; ++k)
+                    tc::umma_f16(d, tc::sw128_kmajor_desc(a_addr + 32u * k), tc::sw128_kmajor_desc(b_addr + 32u * k),
+                                 idesc, (kb | k) != 0 ? 1u : 0u);
+                tc::umma_commit(&sh->empty[stage]);  // the stage is free once these MMAs are done
+                if (++stage == kTcStages) { stage = 0; phase ^= 1u; }
+            }
+            if (!ok) break;
+            tc::umma_commit(&sh->tmem_full[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+        }
+    } else if (warp >= 2) {  // ---- epilogue
+        const int q = warp & 3;  // TMEM lane quadrant of this warp
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
+            if (!tc::mbar_wait(&sh->tmem_full[acc], acc_phase)) { tc_fail(err, 4); break; }
+            tc::tc_fence_after();
+            const int row = m * kTcBM + 32 * q + lane;
+            for (int c = 0; c < kTcBN / 32; ++c) {
+                float v[32];
+                tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTcBN + 32 * c), v);
+                const int col0 = n * kTcBN + 32 * c;
+                if (row < M) {
+                    float* dst = C + (size_t)row * N + col0;
+                    if (col0 + 32 <= N && (N & 3) == 0) {  // 16-byte stores
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4)
+                            *reinterpret_cast<float4*>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (col0 + j < N) dst[j] = v[j];
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&sh->tmem_empty[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 2 * kTcBN);
+    }
+}
+
+// ---- fused contraction + Euler-Maruyama step ---------------------------------------------
+// State is gene-major [G][N] (the register path's layout): for one gene the 32 cells of a
+// warp are 32 consecutive floats.  ACT is cell-major [N][Kp] 16-bit, two buffers: the MMAs of
+// step s read ACT[(s-1) & 1] (gene columns from step s-1, term columns written by the terms
+// kernel, zero padding) while the epilogue writes the gene columns of ACT[s & 1].
+struct TcStepArgs {
+    int32_t G, Kp, n_src, step, last, readout, hill_int, pad0;
+    int64_t N, cell_offset;
+    float k_t, Kn, hill_n, mu_m, mu_p, dt;
+    uint32_t stream;
+    uint32_t rk0[10], rk1[10];  // Philox round keys of the seed
+    const GeneRec* genes;
+    const int32_t* src_of_gene;  // gene -> compact source index of the terms, or -1
+    float* M;                    // [G][N]
+    float* P;
+    uint8_t* prom;
+    int2* NS;
+    void* act_next;              // [N][Kp], gene columns written
+    float* act32_next;           // [N][n_src]
+    double* out;                 // cells x G (x2) column-major, written by the last step (nullable)
+    int* err;
+};
+
+constexpr int kTcEpiWarps = 16;  // 4 per TMEM lane quadrant, 64 accumulator columns each
+constexpr int kTcMaxGenes = 4096; // gene table of the epilogue in shared memory (8 bytes a gene)
+constexpr int kTcStepThreads = 32 * (2 + kTcEpiWarps);
+
+template <class T> struct TcPack;
+template <> struct TcPack<__nv_bfloat16> {
+    static __device__ __forceinline__ uint32_t two(float a, float b) {
+        const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&v);
+    }
+    static __device__ __forceinline__ uint16_t one(float a) {
+        const __nv_bfloat16 v = __float2bfloat16_rn(a);
+        return *reinterpret_cast<const uint16_t*>(&v);
+    }
+};
+template <> struct TcPack<__half> {
+    static __device__ __forceinline__ uint32_t two(float a, float b) {
+        const __half2 v = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&v);
+    }
+    static __device__ __forceinline__ uint16_t one(float a) {
+        const __half v = __float2half_rn(a);
+        return *reinterpret_cast<const uint16_t*>(&v);
+    }
+};
+
+template <int HN>
+__device__ __forceinline__ float tc_hill(float p, const TcStepArgs& a) {
+    if (HN == 2) {
+        const float pn = p * p;
+        return fminf(pn * frcp_approx(pn + a.Kn), 1.0f);  // as hill_act with hill_int == 2
+    }
+    return hill_act(p, a.Kn, a.hill_n, a.hill_int);
+}
+
+// State of one cell x 8 genes g0 .. g0+7 (16 loads issued together).
+__device__ __forceinline__ void tc_load_group(const TcStepArgs& a, int64_t c, bool cell_ok, int g0, float (&m)[8],
+                                              float (&p)[8]) {
+    const int G = a.G;
+    const size_t N = (size_t)a.N;
+    const bool full = g0 + 8 <= G;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const size_t idx = (size_t)(g0 + j) * N + (size_t)c;
+        const bool ok = cell_ok && (full || g0 + j < G);
+        m[j] = ok ? a.M[idx] : 0.0f;
+        p[j] = ok ? a.P[idx] : 0.0f;
+    }
+}
+
+// One cell (this thread's accumulator row) x 8 genes g0 .. g0+7 of one tile, state already
+// loaded: four Philox blocks, eight updates, the stores and one 16-byte activation store.
+template <class T, bool BURSTY, int HN>
+__device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float2* gtab, const float (&v)[8], int64_t c,
+                                              bool cell_ok, int g0, float (&m)[8], float (&p)[8]) {
+    const uint32_t gcell = (uint32_t)(a.cell_offset + (cell_ok ? c : 0));
+    const uint32_t c3 = tagword(TAG_NORMAL, a.stream);
+    const int G = a.G;
+    const size_t N = (size_t)a.N;
+    const bool full = g0 + 8 <= G;  // uniform across the warp
+    uint32_t packed[4];
+#pragma unroll
+    for (int jp = 0; jp < 4; ++jp) {
+        const int g = g0 + 2 * jp;
+        packed[jp] = 0;
+        if (!full && g >= G) continue;  // uniform
+        const uint4 w = philox_rk(gcell, (uint32_t)a.step, (uint32_t)(g >> 1), c3, a.rk0, a.rk1);
+        float act2[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = 2 * jp + h, gene = g + h;
+            if (!full && gene >= G) continue;
+            const float2 gt = gtab[gene];  // {cneg + beta, compact source index bits}
+            const size_t idx = (size_t)gene * N + (size_t)c;
+            float tx = v[j] + gt.x;
+            if (BURSTY && cell_ok) {
+                bool on = a.prom[idx];
+                const int2 sw = a.NS[idx];
+                if ((int)a.step == sw.x) {  // waiting time from the spare bits of the normal words
+                    on = !on;
+                    const GeneRec gr = a.genes[gene];
+                    const float us = h == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                    a.NS[idx] = switch_at(a.step, sw, us, on, gr.inv_on, gr.inv_off);
+                    a.prom[idx] = on;
+                }
+                if (!on) tx = 0.0f;
+            }
+            em_update(m[j], p[j], tx, h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w), a.mu_m,
+                      a.mu_p, a.k_t, a.dt);
+            const float act = tc_hill<HN>(p[j], a);
+            act2[h] = act;
+            if (cell_ok) {
+                a.M[idx] = m[j];
+                a.P[idx] = p[j];
+                if (a.last && a.out) {
+                    if (a.readout == 0) a.out[idx] = (double)m[j];
+                    else if (a.readout == 1) a.out[idx] = (double)p[j];
+                    else { a.out[idx] = (double)m[j]; a.out[(size_t)(G + gene) * N + (size_t)c] = (double)p[j]; }
+                }
+                const int src = __float_as_int(gt.y);
+                if (src >= 0) a.act32_next[c * a.n_src + src] = act;
+            }
+        }
+        packed[jp] = TcPack<T>::two(act2[0], act2[1]);
+    }
+    if (!cell_ok) return;
+    // next activations: gene columns only (the term columns after G belong to the terms kernel)
+    T* row = reinterpret_cast<T*>(a.act_next) + (size_t)c * a.Kp + g0;
+    if (full) {
+        *reinterpret_cast<uint4*>(row) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+    } else {
+        for (int jp = 0; jp < 4; ++jp) {
+            const int g = g0 + 2 * jp;
+            if (g >= G) break;
+            if (g + 1 < G) *reinterpret_cast<uint32_t*>(row + 2 * jp) = packed[jp];
+            else *reinterpret_cast<uint16_t*>(row + 2 * jp) = (uint16_t)(packed[jp] & 0xFFFFu);
+        }
+    }
+}
+
+template <class T, bool BURSTY, int HN>
+__global__ void __launch_bounds__(kTcStepThreads, 1)
+tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                   const TcStepArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_dyn[];
+    const uint32_t base = tc::smem_u32(smem_dyn);
+    unsigned char* stages = smem_dyn + ((1024 - (base & 1023)) & 1023);
+    unsigned char* a_s = stages;
+    unsigned char* b_s = stages + (size_t)kTcStages * kTcABytes;
+    TcShared* sh = reinterpret_cast<TcShared*>(b_s + (size_t)kTcStages * kTcBBytes);
+    float2* gtab = reinterpret_cast<float2*>(reinterpret_cast<unsigned char*>(sh) + 256);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t N = a.N;
+    const int G = a.G;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) {  // per-gene constants of the epilogue
+        const GeneRec gr = a.genes[i];
+        gtab[i] = make_float2(gr.cneg + gr.beta, __int_as_float(a.src_of_gene[i]));
+    }
+    const int tiles_m = (int)((N + kTcBM - 1) / kTcBM), tiles_n = (G + kTcBN - 1) / kTcBN;
+    const int n_tiles = tiles_m * tiles_n;
+    const int kb_n = a.Kp / kTcBK;
+    constexpr uint32_t idesc = tc::umma_idesc_f16(std::is_same<T, __nv_bfloat16>::value, kTcBM, kTcBN);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            tc::mbar_init(&sh->full[s], 1);
+            tc::mbar_init(&sh->empty[s], 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            tc::mbar_init(&sh->tmem_full[k], 1);
+            tc::mbar_init(&sh->tmem_empty[k], kTcEpiWarps);
+        }
+        tc::fence_mbar_init();
+        tc::prefetch_tensormap(&map_a);
+        tc::prefetch_tensormap(&map_b);
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(&sh->tmem_base, 2 * kTcBN);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh->tmem_base;
+
+    if (warp == 0 && lane == 0) {  // ---- TMA producer
+        int stage = 0;
+        uint32_t phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
+            for (int kb = 0; kb < kb_n; ++kb) {
+                if (!tc::mbar_wait(&sh->empty[stage], phase ^ 1u)) { tc_fail(a.err, 1); goto producer_done; }
+                tc::mbar_arrive_expect_tx(&sh->full[stage], kTcABytes + kTcBBytes);
+                tc::tma_load_2d(a_s + (size_t)stage * kTcABytes, &map_a, &sh->full[stage], kb * kTcBK, m * kTcBM);
+                tc::tma_load_2d(b_s + (size_t)stage * kTcBBytes, &map_b, &sh->full[stage], kb * kTcBK, n * kTcBN);
+                if (++stage == kTcStages) { stage = 0; phase ^= 1u; }
+            }
+        }
+    producer_done:;
+    } else if (warp == 1 && lane == 0) {  // ---- MMA issuer
+        int stage = 0, acc = 0;
+        uint32_t phase = 0, acc_phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            if (!tc::mbar_wait(&sh->tmem_empty[acc], acc_phase ^ 1u)) { tc_fail(a.err, 3); break; }
+            tc::tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(acc * kTcBN);
+            bool ok = true;
+            for (int kb = 0; kb < kb_n; ++kb) {
+                if (!tc::mbar_wait(&sh->full[stage], phase)) { tc_fail(a.err, 2); ok = false; break; }
+                tc::tc_fence_after();
+                const uint32_t a_addr = tc::smem_u32(a_s + (size_t)stage * kTcABytes);
+                const uint32_t b_addr = tc::smem_u32(b_s + (size_t)stage * kTcBBytes);
+#pragma unroll
+                for (int k = 0; k < kTcBK / 16; ++k)
+                    tc::umma_f16(d, tc::sw128_kmajor_desc(a_addr + 32u * k), tc::sw128_kmajor_desc(b_addr + 32u * k),
+                                 idesc, (kb | k) != 0 ? 1u : 0u);
+                tc::umma_commit(&sh->empty[stage]);
+                if (++stage == kTcStages) { stage = 0; phase ^= 1u; }
+            }
+            if (!ok) break;
+            tc::umma_commit(&sh->tmem_full[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+        }
+    } else if (warp >= 2) {  // ---- epilogue: Euler-Maruyama step of the tile's cells x genes
+        const int q = warp & 3;             // TMEM lane quadrant
+        const int slice = (warp - 2) >> 2;  // 64-column slice of the accumulator
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
+            if (!tc::mbar_wait(&sh->tmem_full[acc], acc_phase)) { tc_fail(a.err, 4); break; }
+            tc::tc_fence_after();
+            const int64_t c = (int64_t)m * kTcBM + 32 * q + lane;
+            const bool cell_ok = c < N;
+            // groups of 8 genes, the next group's state loaded while this one is computed
+            const int gs = n * kTcBN + slice * 64;
+            float ms[8], ps[8];
+            if (gs < G) tc_load_group(a, c, cell_ok, gs, ms, ps);
+#pragma unroll 1
+            for (int grp = 0; grp < 8; ++grp) {
+                const int g0 = gs + grp * 8;
+                if (g0 >= G) break;  // uniform across the warp
+                float mn[8], pn[8];
+                if (grp + 1 < 8 && g0 + 8 < G) tc_load_group(a, c, cell_ok, g0 + 8, mn, pn);
+                float v[8];
+                tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTcBN + slice * 64 + grp * 8), v);
+                tc_step_group<T, BURSTY, HN>(a, gtab, v, c, cell_ok, g0, ms, ps);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) { ms[j] = mn[j]; ps[j] = pn[j]; }
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&sh->tmem_empty[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 2 * kTcBN);
+    }
+}
+
+// Initial state of the fused path (cle.jl:49-53, tauleap_binomial.jl:64-76): gene-major
+// M, P, promoter and switching state, the first activations and the term-source activations.
+template <class T>
+__global__ void tc_init_kernel(int G, int64_t N, int Kp, int n_src, int64_t cell_offset, const GeneInit* ginit,
+                               const GeneRec* genes, const int32_t* src_of_gene, float Kn, float hill_n, int hill_int,
+                               uint32_t key0, uint32_t key1, uint32_t stream, float* M, float* P, uint8_t* prom,
+                               int2* NS, T* act, float* act32) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)G * N) return;
+    const int g = (int)(idx / N);
+    const int64_t c = idx - (int64_t)g * N;
+    const Key key{key0, key1};
+    const uint32_t gcell = (uint32_t)(cell_offset + c);
+    const GeneInit gi = ginit[g];
+    const GeneRec gr = genes[g];
+    M[idx] = gi.m0;
+    P[idx] = gi.p0;
+    bool on = true;
+    if (gi.init_rand) {
+        const uint4 w = philox(gcell, 0u, (uint32_t)(g >> 2), tagword(TAG_PROMOTER, stream), key);
+        const uint32_t x = (g & 3) == 0 ? w.x : (g & 3) == 1 ? w.y : (g & 3) == 2 ? w.z : w.w;
+        on = x < gi.thr_init;
+    }
+    prom[idx] = on;
+    int2 ns = make_int2(kNever, kNever);
+    if (gr.inv_off == gr.inv_off) {
+        const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, stream), key);
+        ns = fresh_switch(0, w.x, w.y, on, gr.inv_on, gr.inv_off);
+    }
+    NS[idx] = ns;
+    const float a0 = hill_act(gi.p0, Kn, hill_n, hill_int);
+    const uint16_t bits = TcPack<T>::one(a0);
+    *reinterpret_cast<uint16_t*>(act + (size_t)c * Kp + g) = bits;
+    const int src = src_of_gene[g];
+    if (src >= 0) act32[c * n_src + src] = a0;
+}
+
+// Readout of a run with no step, and capture (capture.jl:30-44) on the gene-major state.
+__global__ void tc_readout_kernel(int G, int64_t N, const float* M, const float* P, int readout, double* out) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)G * N) return;
+    if (readout == 0) out[idx] = M[idx];
+    else if (readout == 1) out[idx] = P[idx];
+    else { out[idx] = M[idx]; out[idx + (int64_t)G * N] = P[idx]; }
+}
+
+__global__ void tc_capture_kernel(int G, int64_t N, int64_t cell_offset, const float* X, double mu_log, double sigma,
+                                  uint32_t key0, uint32_t key1, uint32_t stream, double* eff, int32_t* Y) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)G * N) return;
+    const int g = (int)(idx / N);
+    const int64_t c = idx - (int64_t)g * N;
+    const Key key{key0, key1};
+    const uint32_t gcell = (uint32_t)(cell_offset + c);
+    const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_EFFICIENCY, stream), key);
+    double pe = exp(mu_log + sigma * box_muller_z0_f64(w.x, w.y));
+    pe = fmin(fmax(pe, 0.0), 1.0);
+    if (g == 0 && eff) eff[c] = pe;
+    const double x = rint((double)X[idx]);
+    const int64_t n = x > 0.0 ? (int64_t)x : 0;
+    int64_t y = 0;
+    if (n > 0 && pe != 0.0) y = binomial_capture(n, pe, key, stream, gcell, (uint32_t)g);
+    Y[idx] = (int32_t)y;
+}
+
+// ---- host --------------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// Row-major [rows][k] 16-bit matrix, box = box_rows x 64 elements (128 bytes), 128-byte swizzle.
+int tc_make_map(CUtensorMap* map, const void* ptr, int64_t rows, int64_t k, int box_rows, bool bf16) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return fail(SCRNA_ECUDA, "cuTensorMapEncodeTiled is not available");
+    if (k % 8 != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0)
+        return fail(SCRNA_EINVAL, "tensor-core operands need 16-byte aligned rows");
+    const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)k * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kTcBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                           const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SCRNA_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SCRNA_OK;
+}
+
+int tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int N, int K, bool bf16, int* err_dev) {
+    CUtensorMap ma, mb;
+    if (int r = tc_make_map(&ma, A, M, K, kTcBM, bf16)) return r;
+    if (int r = tc_make_map(&mb, B, N, K, kTcBN, bf16)) return r;
+    if (M > (int64_t)1 << 30) return fail(SCRNA_ENOTSUP, "too many rows for the tensor-core GEMM");
+    CU(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    const int64_t tiles = ((M + kTcBM - 1) / kTcBM) * ((N + kTcBN - 1) / kTcBN);
+    const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
+    tc_gemm_kernel<<<grid, kTcThreads, kTcSmem, ctx->stream>>>(ma, mb, C, (int)M, N, K, tc::umma_idesc_f16(bf16, kTcBM, kTcBN),
+                                                                err_dev);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    return SCRNA_OK;
+}
+
+int64_t run_steps(const scrna_cle_opts* o);
+
+// The dense path with the fused kernel: per Euler step the term columns, then one
+// tc_cle_step_kernel launch.  Synchronous: it reads back the pipeline error flag.
+int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
+           const scrna_cle_opts* o, scrna_state* st, int dtype) {
+    if (int r = tensor_prepare_net(n, dtype)) return r;
+    const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, n_terms = (int)n->na.size();
+    const int64_t N = st->N;
+    if (N > (int64_t)1 << 30) return fail(SCRNA_ENOTSUP, "too many cells for the tensor-core path");
+    if (G > kTcMaxGenes) return fail(SCRNA_ENOTSUP, "the fused tensor-core kernel takes G <= %d", kTcMaxGenes);
+    const bool bf16 = dtype == 0;
+    if (int r = state_alloc(st, false, false)) return r;
+    const size_t act_elems = (size_t)N * Kp;
+    CU(st->tact16.ensure(2 * act_elems * 2));
+    for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
+    CU(ctx->tc_err.ensure(sizeof(int)));
+    cudaStream_t s = ctx->stream;
+    unsigned char* act[2] = {static_cast<unsigned char*>(st->tact16.p),
+                             static_cast<unsigned char*>(st->tact16.p) + act_elems * 2};
+    CU(cudaMemsetAsync(st->tact16.p, 0, 2 * act_elems * 2, s));  // padding columns stay 0
+    CU(cudaMemsetAsync(ctx->tc_err.p, 0, sizeof(int), s));
+
+    const uint32_t key0 = (uint32_t)o->seed, key1 = (uint32_t)(o->seed >> 32), sid = o->stream & 0xFFFFFFu;
+    const float Kn = (float)std::pow(kin->K_d, kin->n);
+    const int hill_int = (kin->n == std::floor(kin->n) && kin->n >= 1.0 && kin->n <= 16.0) ? (int)kin->n : 0;
+    const int64_t gn = (int64_t)G * N;
+    const unsigned b_all = (unsigned)((gn + 255) / 256);
+    const GeneRec* genes = n->b_genes.as<GeneRec>();
+    const int32_t* src_of_gene = n->t_src_of_gene.as<int32_t>();
+    if (bf16)
+        tc_init_kernel<__nv_bfloat16><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(),
+                                                            genes, src_of_gene, Kn, (float)kin->n, hill_int, key0, key1,
+                                                            sid, st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(),
+                                                            st->NS.as<int2>(), reinterpret_cast<__nv_bfloat16*>(act[0]),
+                                                            st->tact32[0].as<float>());
+    else
+        tc_init_kernel<__half><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(), genes,
+                                                     src_of_gene, Kn, (float)kin->n, hill_int, key0, key1, sid,
+                                                     st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(),
+                                                     st->NS.as<int2>(), reinterpret_cast<__half*>(act[0]),
+                                                     st->tact32[0].as<float>());
+    CU(cudaGetLastError());
+    ctx->launches++;
+
+    CUtensorMap map_a[2], map_b;
+    for (int k = 0; k < 2; ++k)
+        if (int r = tc_make_map(&map_a[k], act[k], N, Kp, kTcBM, bf16)) return r;
+    if (int r = tc_make_map(&map_b, n->t_w16.p, G, Kp, kTcBN, bf16)) return r;
+
+    TcStepArgs a{};
+    a.G = G; a.Kp = Kp; a.n_src = n_src; a.readout = st->readout; a.hill_int = hill_int;
+    a.N = N; a.cell_offset = o->cell_offset;
+    a.k_t = (float)kin->k_t; a.Kn = Kn; a.hill_n = (float)kin->n;
+    a.mu_m = (float)(kin->mu_m + kin->dilution);
+    a.mu_p = (float)(kin->mu_p + kin->dilution);
+    a.dt = (float)o->dt;
+    a.stream = sid;
+    for (int r = 0; r < 10; ++r) {
+        a.rk0[r] = key0 + (uint32_t)r * 0x9E3779B9u;
+        a.rk1[r] = key1 + (uint32_t)r * 0xBB67AE85u;
+    }
+    a.genes = genes; a.src_of_gene = src_of_gene;
+    a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int2>();
+    a.out = st->out.as<double>();
+    a.err = ctx->tc_err.as<int>();
+
+    using StepFn = void (*)(const CUtensorMap, const CUtensorMap, const TcStepArgs);
+    const bool h2 = hill_int == 2, bursty = n->dev.bursty;
+    StepFn fn;
+    if (bf16) fn = bursty ? (h2 ? tc_cle_step_kernel<__nv_bfloat16, true, 2> : tc_cle_step_kernel<__nv_bfloat16, true, 0>)
+                          : (h2 ? tc_cle_step_kernel<__nv_bfloat16, false, 2> : tc_cle_step_kernel<__nv_bfloat16, false, 0>);
+    else fn = bursty ? (h2 ? tc_cle_step_kernel<__half, true, 2> : tc_cle_step_kernel<__half, true, 0>)
+                     : (h2 ? tc_cle_step_kernel<__half, false, 2> : tc_cle_step_kernel<__half, false, 0>);
+    const size_t smem = kTcSmem + (size_t)G * sizeof(float2);  // + the epilogue's gene table
+    CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + kTcBN - 1) / kTcBN);
+    const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
+    const int64_t n_steps = run_steps(o);
+    for (int64_t step = 1; step <= n_steps; ++step) {
+        const int cur = (int)((step - 1) & 1), nxt = (int)(step & 1);
+        if (n_terms > 0) {  // term columns of ACT[cur] from the previous step's activations
+            CU(tensor_terms_launch(dtype, N, G, Kp, n_terms, n_src, n->dev.na, n->t_na_src.as<int32_t>(),
+                                   st->tact32[cur].as<float>(), act[cur], s));
+            ctx->launches++;
+        }
+        a.step = (int)step;
+        a.last = step == n_steps;
+        a.act_next = act[nxt];
+        a.act32_next = st->tact32[nxt].as<float>();
+        fn<<<grid, kTcStepThreads, smem, s>>>(map_a[cur], map_b, a);
+        CU(cudaGetLastError());
+        ctx->launches++;
+    }
+    if (n_steps == 0) {
+        tc_readout_kernel<<<b_all, 256, 0, s>>>(G, N, st->M.as<float>(), st->P.as<float>(), st->readout,
+                                                st->out.as<double>());
+        CU(cudaGetLastError());
+        ctx->launches++;
+    }
+    if (cap) {
+        const double mu_log = std::log(cap->efficiency) -
+                              (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);
+        const float* X = cap->readout == SCRNA_READOUT_MRNA ? st->M.as<float>() : st->P.as<float>();
+        tc_capture_kernel<<<b_all, 256, 0, s>>>(G, N, o->cell_offset, X, mu_log, cap->efficiency_std, key0, key1, sid,
+                                                st->eff.as<double>(), st->counts.as<int32_t>());
+        CU(cudaGetLastError());
+        ctx->launches++;
+    }
+    int h = 0;
+    CU(cudaMemcpyAsync(&h, ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (h != 0) return fail(SCRNA_ECUDA, "tensor-core step pipeline wait timed out (stage %d)", h);
+    return SCRNA_OK;
+}
+
+}  // namespace scrna
+
+using namespace scrna;
+
+// Diagnostic entry point (no counterpart in the reference): C = A * B^T on device pointers
+// with the hand-written tcgen05 GEMM, synchronous; fails if a pipeline wait timed out.
+extern "C" int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
+                                   int32_t K, int32_t dtype) {
+    if (!ctx || !A || !B || !C) return fail(SCRNA_EINVAL, "NULL argument");
+    if (M <= 0 || N <= 0 || K <= 0 || K % 64 != 0) return fail(SCRNA_EINVAL, "need M, N > 0 and K a multiple of 64");
+    if (int r = set_device(ctx)) return r;
+    DevBuf err;
+    CU(err.ensure(sizeof(int)));
+    CU(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    if (int r = tc_gemm(ctx, A, B, C, M, N, K, dtype == 0, err.as<int>())) return r;
+    int h = 0;
+    CU(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (h != 0) return fail(SCRNA_ECUDA, "tensor-core GEMM pipeline wait timed out (stage %d)", h);
+    return SCRNA_OK;
+}

@@ -123,6 +123,19 @@ __global__ void tensor_terms_kernel(const TensorArgs a) {
     reinterpret_cast<T*>(a.act16)[c * a.Kp + a.G + j] = to16<T>(prod);
 }
 
+// Term columns for the fused tcgen05 path (same kernel, its own activation buffer).
+cudaError_t tensor_terms_launch(int dtype, int64_t N, int G, int Kp, int n_terms, int n_src, const NonAdd* na,
+                                const int32_t* na_src, const float* act32, void* act16, cudaStream_t st) {
+    TensorArgs a{};
+    a.N = N; a.G = G; a.Kp = Kp; a.n_terms = n_terms; a.n_src = n_src;
+    a.na = na; a.na_src = na_src; a.act32_cur = act32; a.act16 = act16;
+    const int64_t nt = N * n_terms;
+    if (nt == 0) return cudaSuccess;
+    if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(a);
+    else tensor_terms_kernel<__half><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <int HN>
 __device__ __forceinline__ float tensor_hill(float p, const TensorArgs& a) {
     if (HN == 2) {

@@ -1,4 +1,5 @@
-"""GPU tests of the tensor-core path (dense regulation, 16-bit GEMM inputs, FP32 state).
+"""GPU tests of the tensor-core path (dense regulation, 16-bit GEMM inputs, FP32 state):
+the fused tcgen05 kernel (path "tensor") and the library-GEMM variant ("tensor_library").
 
 Tolerances: the GEMM rounds W = A_eff and the Hill activations to BF16 (8-bit mantissa) or
 FP16 (11-bit), so trajectories are compared against the FP32 register path with
@@ -33,23 +34,25 @@ def _rel(a, b):
     return float(np.max(np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1.0)))
 
 
+@pytest.mark.parametrize("path", ["tensor", "tensor_library"])
 @pytest.mark.parametrize("precision,tol", [("fp32", 5e-2), ("fp32_f16", 1e-2)])
 @pytest.mark.parametrize("bursty", [False, True])
-def test_tensor_matches_register_path(pkg, precision, tol, bursty):
+def test_tensor_matches_register_path(pkg, path, precision, tol, bursty):
     net = _dense(pkg, 64, seed=1, bursty=bursty)
     kin = pkg.WORKLOAD_KINETICS
     ref = _run(pkg, net, kin, "block").read_raw()
-    got = _run(pkg, net, kin, "tensor", precision=precision).read_raw()
+    got = _run(pkg, net, kin, path, precision=precision).read_raw()
     assert np.array_equal(got["prom"], ref["prom"])
     assert _rel(got["M"], ref["M"].astype(np.float64)) < tol
     assert _rel(got["P"], ref["P"].astype(np.float64)) < tol
 
 
-def test_tensor_per_gene_means_vs_oracle(pkg, orc):
+@pytest.mark.parametrize("path", ["tensor", "tensor_library"])
+def test_tensor_per_gene_means_vs_oracle(pkg, orc, path):
     net = _dense(pkg, 200, seed=5, density=0.1)
     kin = pkg.WORKLOAD_KINETICS
     N, steps = 2048, 300
-    got = _run(pkg, net, kin, "tensor", N=N, steps=steps, seed=11).read_raw()
+    got = _run(pkg, net, kin, path, N=N, steps=steps, seed=11).read_raw()
     ref = orc.simulate(net, kin, dt=0.01, cell_num=N, n_steps=steps, seed=11)
     for key in ("M", "P"):
         mg = got[key].astype(np.float64).mean(1)
@@ -78,3 +81,17 @@ def test_auto_picks_tensor_for_large_dense(pkg):
     a = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=128, T=0.2, seed=1)
     b = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=128, T=0.2, seed=1, path="tensor")
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("G,N,bursty", [(300, 333, False), (520, 700, True)])
+def test_fused_matches_library_gemm_path(pkg, G, N, bursty):
+    """Ragged tiles (G not a multiple of 256, N not of 128): the fused tcgen05 kernel and the
+    library-GEMM variant agree on the same increments up to the 16-bit contraction's rounding
+    (different accumulation order); promoter states are exact."""
+    net = _dense(pkg, G, seed=G, density=0.1, bursty=bursty)
+    kin = pkg.WORKLOAD_KINETICS
+    a = _run(pkg, net, kin, "tensor", N=N, steps=60, seed=5).read_raw()
+    b = _run(pkg, net, kin, "tensor_library", N=N, steps=60, seed=5).read_raw()
+    assert np.array_equal(a["prom"], b["prom"])
+    assert _rel(a["M"], b["M"].astype(np.float64)) < 2e-2
+    assert _rel(a["P"], b["P"].astype(np.float64)) < 2e-2
