@@ -400,21 +400,17 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
             tc::tc_fence_after();
             const int64_t c = (int64_t)m * kTcBM + 32 * q + lane;
             const bool cell_ok = c < N;
-            // groups of 8 genes, the next group's state loaded while this one is computed
+            // groups of 8 genes: state loads of the group issued together, then the updates
             const int gs = n * kTcBN + slice * 64;
-            float ms[8], ps[8];
-            if (gs < G) tc_load_group(a, c, cell_ok, gs, ms, ps);
 #pragma unroll 1
             for (int grp = 0; grp < 8; ++grp) {
                 const int g0 = gs + grp * 8;
                 if (g0 >= G) break;  // uniform across the warp
-                float mn[8], pn[8];
-                if (grp + 1 < 8 && g0 + 8 < G) tc_load_group(a, c, cell_ok, g0 + 8, mn, pn);
+                float ms[8], ps[8];
+                tc_load_group(a, c, cell_ok, g0, ms, ps);
                 float v[8];
                 tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTcBN + slice * 64 + grp * 8), v);
                 tc_step_group<T, BURSTY, HN>(a, gtab, v, c, cell_ok, g0, ms, ps);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) { ms[j] = mn[j]; ps[j] = pn[j]; }
             }
             tc::tc_fence_before();
             __syncwarp();
