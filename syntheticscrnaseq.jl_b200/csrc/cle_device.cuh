@@ -288,4 +288,58 @@ __device__ __forceinline__ void em_update(float& m, float& p, float tx, const BM
     p = pn;
 }
 
+// ---- gene pairs in packed FP32 ----------------------------------------------------------
+// sm_100 adds, multiplies and fused multiply-adds two FP32 values per instruction
+// (add/mul/fma .rn.f32x2); each half is rounded exactly as the scalar operation, so the pair
+// forms below give the scalar forms' bits gene by gene and the kernels that use them stay
+// bit-identical to those that do not.  Minimum, maximum and the special functions have no
+// pair form and stay scalar.
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 max0_2(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
+
+// box_muller_parts of the two genes of one Philox block: gene 0 from (w.x, w.y), gene 1 from
+// (w.z, w.w).  2 - a is formed as fma(a, -1, 2): the product is exact, one rounding as the add.
+struct BM2 { float2 L, c, s; };
+__device__ __forceinline__ BM2 box_muller_parts2(uint4 w) {
+    const float2 a = make_float2(__int_as_float(int((w.x >> 9) | 0x3F800000u)),
+                                 __int_as_float(int((w.z >> 9) | 0x3F800000u)));
+    const float2 b = make_float2(__int_as_float(int((w.y >> 9) | 0x3F800000u)),
+                                 __int_as_float(int((w.w >> 9) | 0x3F800000u)));
+    const float2 u1 = fma2(a, f2(-1.0f), f2(2.0f));
+    const float2 th = mul2(f2(6.28318530717958648f), add2(b, f2(-1.5f)));
+    BM2 r;
+    r.L = mul2(f2(-1.38629436111989061f), make_float2(__log2f(u1.x), __log2f(u1.y)));
+    __sincosf(th.x, &r.s.x, &r.c.x);
+    __sincosf(th.y, &r.s.y, &r.c.y);
+    return r;
+}
+
+// em_update for two genes; mu_m_neg = -mu_m, mu_p_neg = -mu_p.
+__device__ __forceinline__ void em_update2(float2& m, float2& p, float2 tx, const BM2& bm, float mu_m,
+                                           float mu_m_neg, float mu_p, float mu_p_neg, float k_t, float dt) {
+    const float2 Ldt = mul2(bm.L, f2(dt));
+    const float2 mo = m, po = p;
+    const float2 var_m = max0_2(fma2(f2(mu_m), mo, tx));
+    const float2 vm = mul2(Ldt, var_m);
+    const float2 mn = max0_2(fma2(bm.c, make_float2(fsqrt_approx(vm.x), fsqrt_approx(vm.y)),
+                                  fma2(fma2(f2(mu_m_neg), mo, tx), f2(dt), mo)));
+    const float2 var_p = fma2(f2(k_t), mn, mul2(f2(mu_p), po));
+    const float2 vp = mul2(Ldt, var_p);
+    const float2 pn = max0_2(fma2(bm.s, make_float2(fsqrt_approx(vp.x), fsqrt_approx(vp.y)),
+                                  fma2(fma2(f2(k_t), mn, mul2(f2(mu_p_neg), po)), f2(dt), po)));
+    m = mn;
+    p = pn;
+}
+
+// hill_act with hill_int == 2 for two genes.
+__device__ __forceinline__ float2 hill2_n2(float2 p, float Kn) {
+    const float2 pn = mul2(p, p);
+    const float2 d = add2(pn, f2(Kn));
+    const float2 r = mul2(pn, make_float2(frcp_approx(d.x), frcp_approx(d.y)));
+    return make_float2(fminf(r.x, 1.0f), fminf(r.y, 1.0f));
+}
+
 }  // namespace scrna

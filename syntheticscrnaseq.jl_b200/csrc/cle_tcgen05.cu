@@ -168,20 +168,19 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
 // step s read ACT[(s-1) & 1] (gene columns from step s-1, term columns written by the terms
 // kernel, zero padding) while the epilogue writes the gene columns of ACT[s & 1].
 struct TcStepArgs {
-    int32_t G, Kp, n_src, step, last, readout, hill_int, pad0;
+    int32_t G, Kp, n_src, step, hill_int, pad0;
     int64_t N, cell_offset;
     float k_t, Kn, hill_n, mu_m, mu_p, dt;
     uint32_t stream;
     uint32_t rk0[10], rk1[10];  // Philox round keys of the seed
     const GeneRec* genes;
     const int32_t* src_of_gene;  // gene -> compact source index of the terms, or -1
-    float* M;                    // [G][N]
+    float* M;                    // [G][N], N < 2^30 (4 N fits in 32 bits)
     float* P;
     uint8_t* prom;
     int2* NS;
     void* act_next;              // [N][Kp], gene columns written
-    float* act32_next;           // [N][n_src]
-    double* out;                 // cells x G (x2) column-major, written by the last step (nullable)
+    float* act32_next;           // [n_src][N]
     int* err;
 };
 
@@ -220,30 +219,47 @@ __device__ __forceinline__ float tc_hill(float p, const TcStepArgs& a) {
     return hill_act(p, a.Kn, a.hill_n, a.hill_int);
 }
 
+// Row `row` of a gene-major FP32 array at this thread's cell: `base_c` points at row 0 of the
+// cell and `nb` = 4 N is the row stride in bytes (N < 2^30), so one 32 x 32 -> 64-bit
+// multiply-add forms the address.
+template <class F>
+__device__ __forceinline__ F* tc_row(F* base_c, int row, uint32_t nb) {
+    using B = typename std::conditional<std::is_const<F>::value, const char, char>::type;
+    return reinterpret_cast<F*>(reinterpret_cast<B*>(base_c) + (uint64_t)(uint32_t)row * nb);
+}
+
 // State of one cell x 8 genes g0 .. g0+7 (16 loads issued together).
-__device__ __forceinline__ void tc_load_group(const TcStepArgs& a, int64_t c, bool cell_ok, int g0, float (&m)[8],
-                                              float (&p)[8]) {
+__device__ __forceinline__ void tc_load_group(const TcStepArgs& a, const float* Mc, const float* Pc, bool cell_ok,
+                                              int g0, float (&m)[8], float (&p)[8]) {
     const int G = a.G;
-    const size_t N = (size_t)a.N;
+    const uint32_t nb = 4u * (uint32_t)a.N;
     const bool full = g0 + 8 <= G;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const size_t idx = (size_t)(g0 + j) * N + (size_t)c;
         const bool ok = cell_ok && (full || g0 + j < G);
-        m[j] = ok ? a.M[idx] : 0.0f;
-        p[j] = ok ? a.P[idx] : 0.0f;
+        m[j] = ok ? *tc_row(Mc, g0 + j, nb) : 0.0f;
+        p[j] = ok ? *tc_row(Pc, g0 + j, nb) : 0.0f;
     }
 }
 
+template <int HN>
+__device__ __forceinline__ float2 tc_hill2(float2 p, const TcStepArgs& a) {
+    if (HN == 2) return hill2_n2(p, a.Kn);
+    return make_float2(hill_act(p.x, a.Kn, a.hill_n, a.hill_int), hill_act(p.y, a.Kn, a.hill_n, a.hill_int));
+}
+
 // One cell (this thread's accumulator row) x 8 genes g0 .. g0+7 of one tile, state already
-// loaded: four Philox blocks, eight updates, the stores and one 16-byte activation store.
+// loaded: four Philox blocks, each driving the pair update of two genes in packed FP32, the
+// stores and one 16-byte activation store.  gc / gsrc: the CTA's gene table (cneg + beta,
+// compact source index), gc padded to an even length.
 template <class T, bool BURSTY, int HN>
-__device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float2* gtab, const float (&v)[8], int64_t c,
-                                              bool cell_ok, int g0, float (&m)[8], float (&p)[8]) {
-    const uint32_t gcell = (uint32_t)(a.cell_offset + (cell_ok ? c : 0));
+__device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float* gc, const int* gsrc,
+                                              const float (&v)[8], int64_t c, bool cell_ok, int g0, float* Mc,
+                                              float* Pc, float (&m)[8], float (&p)[8]) {
+    const uint32_t gcell = (uint32_t)(a.cell_offset + c);  // c < N here or the cell is masked
     const uint32_t c3 = tagword(TAG_NORMAL, a.stream);
     const int G = a.G;
-    const size_t N = (size_t)a.N;
+    const uint32_t n32 = (uint32_t)a.N, nb = 4u * n32;
     const bool full = g0 + 8 <= G;  // uniform across the warp
     uint32_t packed[4];
 #pragma unroll
@@ -252,15 +268,13 @@ __device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float2*
         packed[jp] = 0;
         if (!full && g >= G) continue;  // uniform
         const uint4 w = philox_rk(gcell, (uint32_t)a.step, (uint32_t)(g >> 1), c3, a.rk0, a.rk1);
-        float act2[2] = {0.0f, 0.0f};
+        float2 tx = add2(make_float2(v[2 * jp], v[2 * jp + 1]), *reinterpret_cast<const float2*>(gc + g));
+        if (BURSTY && cell_ok) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int j = 2 * jp + h, gene = g + h;
-            if (!full && gene >= G) continue;
-            const float2 gt = gtab[gene];  // {cneg + beta, compact source index bits}
-            const size_t idx = (size_t)gene * N + (size_t)c;
-            float tx = v[j] + gt.x;
-            if (BURSTY && cell_ok) {
+            for (int h = 0; h < 2; ++h) {
+                const int gene = g + h;
+                if (!full && gene >= G) continue;
+                const uint64_t idx = (uint64_t)(uint32_t)gene * n32 + (uint64_t)c;
                 bool on = a.prom[idx];
                 const int2 sw = a.NS[idx];
                 if ((int)a.step == sw.x) {  // waiting time from the spare bits of the normal words
@@ -270,25 +284,24 @@ __device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float2*
                     a.NS[idx] = switch_at(a.step, sw, us, on, gr.inv_on, gr.inv_off);
                     a.prom[idx] = on;
                 }
-                if (!on) tx = 0.0f;
-            }
-            em_update(m[j], p[j], tx, h == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w), a.mu_m,
-                      a.mu_p, a.k_t, a.dt);
-            const float act = tc_hill<HN>(p[j], a);
-            act2[h] = act;
-            if (cell_ok) {
-                a.M[idx] = m[j];
-                a.P[idx] = p[j];
-                if (a.last && a.out) {
-                    if (a.readout == 0) a.out[idx] = (double)m[j];
-                    else if (a.readout == 1) a.out[idx] = (double)p[j];
-                    else { a.out[idx] = (double)m[j]; a.out[(size_t)(G + gene) * N + (size_t)c] = (double)p[j]; }
-                }
-                const int src = __float_as_int(gt.y);
-                if (src >= 0) a.act32_next[c * a.n_src + src] = act;
+                if (!on) (h == 0 ? tx.x : tx.y) = 0.0f;
             }
         }
-        packed[jp] = TcPack<T>::two(act2[0], act2[1]);
+        float2 m2 = make_float2(m[2 * jp], m[2 * jp + 1]), p2 = make_float2(p[2 * jp], p[2 * jp + 1]);
+        em_update2(m2, p2, tx, box_muller_parts2(w), a.mu_m, -a.mu_m, a.mu_p, -a.mu_p, a.k_t, a.dt);
+        const float2 act = tc_hill2<HN>(p2, a);
+        if (cell_ok) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gene = g + h;
+                if (!full && gene >= G) continue;
+                *tc_row(Mc, gene, nb) = h == 0 ? m2.x : m2.y;
+                *tc_row(Pc, gene, nb) = h == 0 ? p2.x : p2.y;
+                const int src = gsrc[gene];
+                if (src >= 0) *tc_row(a.act32_next + c, src, nb) = h == 0 ? act.x : act.y;
+            }
+        }
+        packed[jp] = TcPack<T>::two(act.x, (full || g + 1 < G) ? act.y : 0.0f);
     }
     if (!cell_ok) return;
     // next activations: gene columns only (the term columns after G belong to the terms kernel)
@@ -315,15 +328,18 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
     unsigned char* a_s = stages;
     unsigned char* b_s = stages + (size_t)kTcStages * kTcABytes;
     TcShared* sh = reinterpret_cast<TcShared*>(b_s + (size_t)kTcStages * kTcBBytes);
-    float2* gtab = reinterpret_cast<float2*>(reinterpret_cast<unsigned char*>(sh) + 256);
+    float* gc = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sh) + 256);
+    int* gsrc = reinterpret_cast<int*>(gc + ((a.G + 1) & ~1));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t N = a.N;
     const int G = a.G;
     for (int i = threadIdx.x; i < G; i += blockDim.x) {  // per-gene constants of the epilogue
         const GeneRec gr = a.genes[i];
-        gtab[i] = make_float2(gr.cneg + gr.beta, __int_as_float(a.src_of_gene[i]));
+        gc[i] = gr.cneg + gr.beta;
+        gsrc[i] = a.src_of_gene[i];
     }
+    if (threadIdx.x == 0 && (G & 1)) gc[G] = 0.0f;  // pad of the last pair
     const int tiles_m = (int)((N + kTcBM - 1) / kTcBM), tiles_n = (G + kTcBN - 1) / kTcBN;
     const int n_tiles = tiles_m * tiles_n;
     const int kb_n = a.Kp / kTcBK;
@@ -398,8 +414,11 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
             const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
             if (!tc::mbar_wait(&sh->tmem_full[acc], acc_phase)) { tc_fail(a.err, 4); break; }
             tc::tc_fence_after();
-            const int64_t c = (int64_t)m * kTcBM + 32 * q + lane;
-            const bool cell_ok = c < N;
+            const int64_t c_raw = (int64_t)m * kTcBM + 32 * q + lane;
+            const bool cell_ok = c_raw < N;
+            const int64_t c = cell_ok ? c_raw : 0;
+            float* Mc = a.M + c;
+            float* Pc = a.P + c;
             // groups of 8 genes: state loads of the group issued together, then the updates
             const int gs = n * kTcBN + slice * 64;
 #pragma unroll 1
@@ -407,10 +426,10 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
                 const int g0 = gs + grp * 8;
                 if (g0 >= G) break;  // uniform across the warp
                 float ms[8], ps[8];
-                tc_load_group(a, c, cell_ok, g0, ms, ps);
+                tc_load_group(a, Mc, Pc, cell_ok, g0, ms, ps);
                 float v[8];
                 tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTcBN + slice * 64 + grp * 8), v);
-                tc_step_group<T, BURSTY, HN>(a, gtab, v, c, cell_ok, g0, ms, ps);
+                tc_step_group<T, BURSTY, HN>(a, gc, gsrc, v, c, cell_ok, g0, Mc, Pc, ms, ps);
             }
             tc::tc_fence_before();
             __syncwarp();
@@ -460,10 +479,10 @@ __global__ void tc_init_kernel(int G, int64_t N, int Kp, int n_src, int64_t cell
     const uint16_t bits = TcPack<T>::one(a0);
     *reinterpret_cast<uint16_t*>(act + (size_t)c * Kp + g) = bits;
     const int src = src_of_gene[g];
-    if (src >= 0) act32[c * n_src + src] = a0;
+    if (src >= 0) act32[(size_t)src * N + c] = a0;
 }
 
-// Readout of a run with no step, and capture (capture.jl:30-44) on the gene-major state.
+// Readout after the last step, and capture (capture.jl:30-44) on the gene-major state.
 __global__ void tc_readout_kernel(int G, int64_t N, const float* M, const float* P, int readout, double* out) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)G * N) return;
@@ -551,7 +570,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     if (int r = tensor_prepare_net(n, dtype)) return r;
     const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, n_terms = (int)n->na.size();
     const int64_t N = st->N;
-    if (N > (int64_t)1 << 30) return fail(SCRNA_ENOTSUP, "too many cells for the tensor-core path");
+    if (N >= (int64_t)1 << 30) return fail(SCRNA_ENOTSUP, "too many cells for the tensor-core path");
     if (G > kTcMaxGenes) return fail(SCRNA_ENOTSUP, "the fused tensor-core kernel takes G <= %d", kTcMaxGenes);
     const bool bf16 = dtype == 0;
     if (int r = state_alloc(st, false, false)) return r;
@@ -593,7 +612,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     if (int r = tc_make_map(&map_b, n->t_w16.p, G, Kp, kTcBN, bf16)) return r;
 
     TcStepArgs a{};
-    a.G = G; a.Kp = Kp; a.n_src = n_src; a.readout = st->readout; a.hill_int = hill_int;
+    a.G = G; a.Kp = Kp; a.n_src = n_src; a.hill_int = hill_int;
     a.N = N; a.cell_offset = o->cell_offset;
     a.k_t = (float)kin->k_t; a.Kn = Kn; a.hill_n = (float)kin->n;
     a.mu_m = (float)(kin->mu_m + kin->dilution);
@@ -606,7 +625,6 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     }
     a.genes = genes; a.src_of_gene = src_of_gene;
     a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int2>();
-    a.out = st->out.as<double>();
     a.err = ctx->tc_err.as<int>();
 
     using StepFn = void (*)(const CUtensorMap, const CUtensorMap, const TcStepArgs);
@@ -616,7 +634,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
                           : (h2 ? tc_cle_step_kernel<__nv_bfloat16, false, 2> : tc_cle_step_kernel<__nv_bfloat16, false, 0>);
     else fn = bursty ? (h2 ? tc_cle_step_kernel<__half, true, 2> : tc_cle_step_kernel<__half, true, 0>)
                      : (h2 ? tc_cle_step_kernel<__half, false, 2> : tc_cle_step_kernel<__half, false, 0>);
-    const size_t smem = kTcSmem + (size_t)G * sizeof(float2);  // + the epilogue's gene table
+    const size_t smem = kTcSmem + (size_t)(((G + 1) & ~1) + G) * 4;  // + the epilogue's gene table
     CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + kTcBN - 1) / kTcBN);
     const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
@@ -629,19 +647,17 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
             ctx->launches++;
         }
         a.step = (int)step;
-        a.last = step == n_steps;
         a.act_next = act[nxt];
         a.act32_next = st->tact32[nxt].as<float>();
         fn<<<grid, kTcStepThreads, smem, s>>>(map_a[cur], map_b, a);
         CU(cudaGetLastError());
         ctx->launches++;
     }
-    if (n_steps == 0) {
-        tc_readout_kernel<<<b_all, 256, 0, s>>>(G, N, st->M.as<float>(), st->P.as<float>(), st->readout,
-                                                st->out.as<double>());
-        CU(cudaGetLastError());
-        ctx->launches++;
-    }
+    // readout after the last step (one pass over the state, instead of a branch in every step)
+    tc_readout_kernel<<<b_all, 256, 0, s>>>(G, N, st->M.as<float>(), st->P.as<float>(), st->readout,
+                                            st->out.as<double>());
+    CU(cudaGetLastError());
+    ctx->launches++;
     if (cap) {
         const double mu_log = std::log(cap->efficiency) -
                               (cap->mean_correction ? cap->efficiency_std * cap->efficiency_std / 2.0 : 0.0);

@@ -53,7 +53,7 @@ struct TensorArgs {
     uint8_t* prom;
     int2* NS;
     void* act16;             // [N][Kp]
-    const float* act32_cur;  // [N][n_src]
+    const float* act32_cur;  // [n_src][N]: source-major, 32 cells of a warp in one 128-byte row piece
     float* act32_next;
 };
 
@@ -88,7 +88,7 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
     const float act = hill_act(p0, a.Kn, a.hill_n, a.hill_int);
     reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
     const int src = a.src_of_gene[g];
-    if (src >= 0) a.act32_next[c * a.n_src + src] = act;
+    if (src >= 0) a.act32_next[(size_t)src * a.N + c] = act;
 }
 
 // One Euler-Maruyama step after the GEMM.  Thread = one gene pair (blockIdx.y, x) for a chunk
@@ -103,24 +103,41 @@ template <class T> struct Pair16;
 template <> struct Pair16<__nv_bfloat16> { using type = __nv_bfloat162; };
 template <> struct Pair16<__half> { using type = __half2; };
 
-// Term columns of the activation matrix: thread = (cell, term), value from the FP32
-// activations of the term's compact source genes written by the previous step.
+// Term columns of the activation matrix: thread = (term blockIdx.y, cell), value from the FP32
+// activations of the term's compact source genes written by the previous step (source-major,
+// so a warp's 32 cells read one 128-byte piece per source; two source loads in flight).
+constexpr int kTermsBlock = 256;
 template <class T>
-__global__ void tensor_terms_kernel(const TensorArgs a) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= a.N * a.n_terms) return;
-    const int64_t c = idx / a.n_terms;
-    const int j = (int)(idx - c * a.n_terms);
-    const float* act = a.act32_cur + c * a.n_src;
+__global__ void __launch_bounds__(kTermsBlock) tensor_terms_kernel(const TensorArgs a) {
+    const int64_t c = (int64_t)blockIdx.x * kTermsBlock + threadIdx.x;
+    if (c >= a.N) return;
+    const int j = blockIdx.y;
     const NonAdd na = a.na[j];
+    const float* act = a.act32_cur + c;
+    const size_t n = (size_t)a.N;
+    const bool red = na.kind != 0;  // redundant: 1 - prod(1 - a)
     float prod = 1.0f;
-    if (na.kind == 0) {
-        for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[a.na_src[t]];
-    } else {
-        for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[a.na_src[t]];
-        prod = 1.0f - prod;
+    int t = na.src_begin;
+    for (; t + 1 < na.src_end; t += 2) {
+        float x0 = act[(size_t)a.na_src[t] * n], x1 = act[(size_t)a.na_src[t + 1] * n];
+        if (red) { x0 = 1.0f - x0; x1 = 1.0f - x1; }
+        prod *= x0;
+        prod *= x1;
     }
-    reinterpret_cast<T*>(a.act16)[c * a.Kp + a.G + j] = to16<T>(prod);
+    if (t < na.src_end) {
+        const float x = act[(size_t)a.na_src[t] * n];
+        prod *= red ? 1.0f - x : x;
+    }
+    if (red) prod = 1.0f - prod;
+    reinterpret_cast<T*>(a.act16)[(size_t)c * a.Kp + a.G + j] = to16<T>(prod);
+}
+
+static cudaError_t terms_launch(int dtype, const TensorArgs& a, cudaStream_t st) {
+    if (a.N == 0 || a.n_terms == 0) return cudaSuccess;
+    const dim3 grid((unsigned)((a.N + kTermsBlock - 1) / kTermsBlock), (unsigned)a.n_terms);
+    if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<grid, kTermsBlock, 0, st>>>(a);
+    else tensor_terms_kernel<__half><<<grid, kTermsBlock, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
 // Term columns for the fused tcgen05 path (same kernel, its own activation buffer).
@@ -129,10 +146,7 @@ cudaError_t tensor_terms_launch(int dtype, int64_t N, int G, int Kp, int n_terms
     TensorArgs a{};
     a.N = N; a.G = G; a.Kp = Kp; a.n_terms = n_terms; a.n_src = n_src;
     a.na = na; a.na_src = na_src; a.act32_cur = act32; a.act16 = act16;
-    const int64_t nt = N * n_terms;
-    if (nt == 0) return cudaSuccess;
-    if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(a);
-    else tensor_terms_kernel<__half><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(a);
+    return terms_launch(dtype, a, st);
     return cudaGetLastError();
 }
 
@@ -211,8 +225,8 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
         act.x = to16<T>(a0);
         act.y = to16<T>(has1 ? a1 : 0.0f);  // the padding column of the activations stays 0
         actp[(size_t)i * (a.Kp >> 1)] = act;
-        if (src0 >= 0) a.act32_next[c * a.n_src + src0] = a0;
-        if (src1 >= 0) a.act32_next[c * a.n_src + src1] = a1;
+        if (src0 >= 0) a.act32_next[(size_t)src0 * a.N + c] = a0;
+        if (src1 >= 0) a.act32_next[(size_t)src1 * a.N + c] = a1;
     }
 }
 
@@ -277,6 +291,7 @@ int tensor_prepare_net(scrna_net* n, int dtype) {
     if (n->t_dtype == dtype) return SCRNA_OK;
     const int G = n->G;
     const int n_terms = (int)n->na.size();
+    if (n_terms > 65535) return fail(SCRNA_ENOTSUP, "the tensor path takes at most 65535 cooperative/redundant terms");
     const int K = G + n_terms;
     const int Kp = (K + 63) / 64 * 64;
     std::vector<float> w((size_t)G * K, 0.0f);
@@ -436,10 +451,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
         a.act32_next = st->tact32[step & 1].as<float>();
         if (a.n_terms > 0) {  // term columns from the previous step's activations
-            const int64_t nt = N * a.n_terms;
-            if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a);
-            else tensor_terms_kernel<__half><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(a);
-            CU(cudaGetLastError());
+            CU(terms_launch(dtype, a, s));
             ctx->launches += 1;
         }
         cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,

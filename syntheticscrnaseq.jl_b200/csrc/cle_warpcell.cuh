@@ -93,6 +93,12 @@ __device__ __forceinline__ float warpcell_hill(float p, const FusedArgs& a) {
     return hill_act(p, a.Kn, a.hill_n, a.hill_int);
 }
 
+template <int HN>
+__device__ __forceinline__ float2 warpcell_hill2(float2 p, const FusedArgs& a) {
+    if (HN == 2) return hill2_n2(p, a.Kn);  // as hill_act with hill_int == 2
+    return make_float2(hill_act(p.x, a.Kn, a.hill_n, a.hill_int), hill_act(p.y, a.Kn, a.hill_n, a.hill_int));
+}
+
 // One block tile (warpcell_cells_per_block cells) of one network through ctl's step range.
 // RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
 // HN: 2 for a Hill exponent of exactly 2, else 0 (any exponent).
@@ -100,6 +106,7 @@ __device__ __forceinline__ float warpcell_hill(float p, const FusedArgs& a) {
 template <int GPL, int EMAX, int TMAX, bool POP, bool RK, int HN, bool MW>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                               unsigned char* smem_raw) {
+    static_assert(GPL % 2 == 0, "genes are updated in pairs");
     constexpr int TM = TMAX > 0 ? TMAX : 1;
     const int G = a.G;
     const int lpc = warpcell_lanes_per_cell(G, GPL);
@@ -266,6 +273,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 
     // ---- fused step loop --------------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
+    const float mu_m_neg = -mu_m, mu_p_neg = -mu_p;
     const bool any_reg = n_reg > 0;
     // Draw the pending waiting times of this lane (the state after the next switch is the
     // opposite of the current one, which holds until that switch).
@@ -279,11 +287,28 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     int32_t ns_min = ns[0];  // earliest switch of the lane's genes
 #pragma unroll
     for (int i = 1; i < GPL; ++i) ns_min = min(ns_min, ns[i]);
+    // Philox blocks of the normals.  AHEAD: drawn one step ahead, step s + 1's rounds issued
+    // beside step s's update (two independent dependency chains per lane), where the
+    // registers allow it without spilling.
+    constexpr bool AHEAD = GPL == 2 && EMAX <= 4 && TMAX <= 1;
+    auto draw = [&](int s, int h) {
+        const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
+        return RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1) : philox(gcell, (uint32_t)s, c2, c3, key);
+    };
+    uint4 wn[GPL / 2];
+    if (AHEAD) {
+#pragma unroll
+        for (int h = 0; h < GPL / 2; ++h) wn[h] = draw(ctl.step_begin, h);
+    }
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
         cell_sync();  // every lane has read the row of the previous step
         if (any_reg) {
 #pragma unroll
-            for (int i = 0; i < GPL; ++i) smem_f32(smem_raw, hill_at[i]) = warpcell_hill<HN>(p[i], a);
+            for (int i = 0; i < GPL; i += 2) {  // gene pairs in packed FP32
+                const float2 h = warpcell_hill2<HN>(make_float2(p[i], p[i + 1]), a);
+                smem_f32(smem_raw, hill_at[i]) = h.x;
+                smem_f32(smem_raw, hill_at[i + 1]) = h.y;
+            }
         }
         // telegraph: a promoter switches when its waiting time runs out, and needs the waiting
         // time drawn at its previous switch.  Those draws wait until some switching gene of the
@@ -296,17 +321,14 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             for (int i = 0; i < GPL; ++i) need |= s == ns[i] && kn[i] < 0;
             if (__any_sync(0xFFFFFFFFu, need)) resolve_pending();
         }
-        BM bm[GPL];
+        BM2 bm[GPL / 2];   // genes 2h, 2h + 1
         uint32_t sb[GPL];  // spare bits of each gene's normal words
 #pragma unroll
         for (int h = 0; h < GPL / 2; ++h) {
-            const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
-            const uint4 w = RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1)
-                               : philox(gcell, (uint32_t)s, c2, c3, key);
+            const uint4 w = AHEAD ? wn[h] : draw(s, h);
             sb[2 * h] = switch_bits(w.x, w.y);
             sb[2 * h + 1] = switch_bits(w.z, w.w);
-            bm[2 * h] = box_muller_parts(w.x, w.y);
-            bm[2 * h + 1] = box_muller_parts(w.z, w.w);
+            bm[h] = box_muller_parts2(w);
         }
         if (warp_due) {  // switch_at for the genes due now, with the next draw left pending
 #pragma unroll
@@ -333,16 +355,26 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             }
             cell_sync();  // the cell's term values are complete
         }
+        if (AHEAD) {
+#pragma unroll
+            for (int h = 0; h < GPL / 2; ++h) wn[h] = draw(s + 1, h);
+        }
         const float Vf = POP ? (float)V : 1.0f;
 #pragma unroll
-        for (int i = 0; i < GPL; ++i) {
-            float reg = cneg[i];
+        for (int i = 0; i < GPL; i += 2) {  // gene pairs in packed FP32 (each half as the scalar form)
+            float2 reg = make_float2(cneg[i], cneg[i + 1]);
 #pragma unroll
-            for (int e = 0; e < EMAX; ++e) reg = fmaf(ew[i][e], smem_f32(smem_raw, ea[i][e]), reg);
-            float tx = reg + beta[i];
-            if (POP) tx *= Vf;
-            if (!(on & (1u << i))) tx = 0.0f;
-            em_update(m[i], p[i], tx, bm[i], mu_m, mu_p, k_t, dt);
+            for (int e = 0; e < EMAX; ++e)
+                reg = fma2(make_float2(ew[i][e], ew[i + 1][e]),
+                           make_float2(smem_f32(smem_raw, ea[i][e]), smem_f32(smem_raw, ea[i + 1][e])), reg);
+            float2 tx = add2(reg, make_float2(beta[i], beta[i + 1]));
+            if (POP) tx = mul2(tx, f2(Vf));
+            if (!(on & (1u << i))) tx.x = 0.0f;
+            if (!(on & (2u << i))) tx.y = 0.0f;
+            float2 m2 = make_float2(m[i], m[i + 1]), p2 = make_float2(p[i], p[i + 1]);
+            em_update2(m2, p2, tx, bm[i / 2], mu_m, mu_m_neg, mu_p, mu_p_neg, k_t, dt);
+            m[i] = m2.x; m[i + 1] = m2.y;
+            p[i] = p2.x; p[i + 1] = p2.y;
         }
         if (POP) V = __dmul_rn(V, a.growth_factor);
     }
