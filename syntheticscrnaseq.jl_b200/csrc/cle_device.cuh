@@ -68,9 +68,11 @@ __device__ __forceinline__ uint32_t tagword(uint32_t tag, uint32_t stream) {
 //   L = -2 ln u1,  (z0, z1) = sqrt(L) (cos 2 pi h, sin 2 pi h).
 // Returned as (L, cos, sin) so callers can fold sqrt(L) into another square root.
 struct BM { float L, c, s; };
+// 1 + (w >> 9) 2^-23 as the bits 0x3F800000 | (w >> 9), one funnel shift of (0x7F : w) by 9.
+__device__ __forceinline__ float one_plus_top23(uint32_t w) { return __uint_as_float(__funnelshift_r(w, 0x7Fu, 9)); }
 __device__ __forceinline__ BM box_muller_parts(uint32_t w0, uint32_t w1) {
-    const float u1 = 2.0f - __int_as_float(int((w0 >> 9) | 0x3F800000u));
-    const float h = __int_as_float(int((w1 >> 9) | 0x3F800000u)) - 1.5f;
+    const float u1 = 2.0f - one_plus_top23(w0);
+    const float h = one_plus_top23(w1) - 1.5f;
     const float th = 6.28318530717958648f * h;
     BM r;
     r.L = -1.38629436111989061f * __log2f(u1);  // -2 ln 2 * log2(u1)
@@ -304,10 +306,8 @@ __device__ __forceinline__ float2 max0_2(float2 a) { return make_float2(fmaxf(a.
 // (w.z, w.w).  2 - a is formed as fma(a, -1, 2): the product is exact, one rounding as the add.
 struct BM2 { float2 L, c, s; };
 __device__ __forceinline__ BM2 box_muller_parts2(uint4 w) {
-    const float2 a = make_float2(__int_as_float(int((w.x >> 9) | 0x3F800000u)),
-                                 __int_as_float(int((w.z >> 9) | 0x3F800000u)));
-    const float2 b = make_float2(__int_as_float(int((w.y >> 9) | 0x3F800000u)),
-                                 __int_as_float(int((w.w >> 9) | 0x3F800000u)));
+    const float2 a = make_float2(one_plus_top23(w.x), one_plus_top23(w.z));
+    const float2 b = make_float2(one_plus_top23(w.y), one_plus_top23(w.w));
     const float2 u1 = fma2(a, f2(-1.0f), f2(2.0f));
     const float2 th = mul2(f2(6.28318530717958648f), add2(b, f2(-1.5f)));
     BM2 r;

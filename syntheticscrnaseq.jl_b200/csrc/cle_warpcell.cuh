@@ -322,13 +322,11 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             if (__any_sync(0xFFFFFFFFu, need)) resolve_pending();
         }
         BM2 bm[GPL / 2];   // genes 2h, 2h + 1
-        uint32_t sb[GPL];  // spare bits of each gene's normal words
+        uint4 wc[GPL / 2];
 #pragma unroll
         for (int h = 0; h < GPL / 2; ++h) {
-            const uint4 w = AHEAD ? wn[h] : draw(s, h);
-            sb[2 * h] = switch_bits(w.x, w.y);
-            sb[2 * h + 1] = switch_bits(w.z, w.w);
-            bm[h] = box_muller_parts2(w);
+            wc[h] = AHEAD ? wn[h] : draw(s, h);
+            bm[h] = box_muller_parts2(wc[h]);
         }
         if (warp_due) {  // switch_at for the genes due now, with the next draw left pending
 #pragma unroll
@@ -337,8 +335,10 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
                 on ^= (uint32_t)sw << i;
                 // s + kn < 2^32 (both < 2^31): the unsigned sum saturates at kNever
                 const int32_t nn = (int32_t)min((uint32_t)s + (uint32_t)kn[i], (uint32_t)kNever);
+                // spare bits of the gene's normal words
+                const uint32_t sb = (i & 1) ? switch_bits(wc[i / 2].z, wc[i / 2].w) : switch_bits(wc[i / 2].x, wc[i / 2].y);
                 ns[i] = sw ? nn : ns[i];
-                kn[i] = sw ? -(int32_t)sb[i] - 1 : kn[i];
+                kn[i] = sw ? -(int32_t)sb - 1 : kn[i];
             }
             ns_min = ns[0];
 #pragma unroll
