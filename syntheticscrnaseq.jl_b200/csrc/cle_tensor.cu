@@ -103,38 +103,83 @@ template <class T> struct Pair16;
 template <> struct Pair16<__nv_bfloat16> { using type = __nv_bfloat162; };
 template <> struct Pair16<__half> { using type = __half2; };
 
-// Term columns of the activation matrix: thread = (term blockIdx.y, cell), value from the FP32
-// activations of the term's compact source genes written by the previous step (source-major,
-// so a warp's 32 cells read one 128-byte piece per source; two source loads in flight).
-constexpr int kTermsBlock = 256;
+// Term columns of the activation matrix: block = (128 cells, 8 consecutive terms), thread =
+// one cell.  The FP32 activations of the terms' compact source genes (written by the previous
+// step) are source-major, so a warp reads one 128-byte piece per source; the first 4 sources
+// of all 8 terms (32 loads) are in flight together, longer terms loop over the rest.  Each
+// cell writes its 8 term columns with one 16-byte store where the row offset allows.
+constexpr int kTermsBlock = 128;
+constexpr int kTermsGroup = 8;
+constexpr int kTermsSrc = 4;
 template <class T>
 __global__ void __launch_bounds__(kTermsBlock) tensor_terms_kernel(const TensorArgs a) {
+    __shared__ int s_src[kTermsGroup][kTermsSrc];  // compact source index or -1
+    __shared__ int s_rest[kTermsGroup][2];         // remaining sources [begin, end) of na_src
+    __shared__ int s_red[kTermsGroup];             // redundant: 1 - prod(1 - a)
+    const int j0 = blockIdx.y * kTermsGroup;
+    const int nj = min(kTermsGroup, a.n_terms - j0);
+    if (threadIdx.x < kTermsGroup * kTermsSrc) {
+        const int k = threadIdx.x / kTermsSrc, q = threadIdx.x % kTermsSrc;
+        int v = -1, rb = 0, re = 0, red = 0;
+        if (k < nj) {
+            const NonAdd na = a.na[j0 + k];
+            const int t = na.src_begin + q;
+            v = t < na.src_end ? a.na_src[t] : -1;
+            rb = na.src_begin + kTermsSrc;
+            re = na.src_end;
+            red = na.kind != 0;
+        }
+        s_src[k][q] = v;
+        if (q == 0) {
+            s_rest[k][0] = rb;
+            s_rest[k][1] = re;
+            s_red[k] = red;
+        }
+    }
+    __syncthreads();
+    const int64_t N = a.N;
     const int64_t c = (int64_t)blockIdx.x * kTermsBlock + threadIdx.x;
-    if (c >= a.N) return;
-    const int j = blockIdx.y;
-    const NonAdd na = a.na[j];
+    if (c >= N) return;
     const float* act = a.act32_cur + c;
-    const size_t n = (size_t)a.N;
-    const bool red = na.kind != 0;  // redundant: 1 - prod(1 - a)
-    float prod = 1.0f;
-    int t = na.src_begin;
-    for (; t + 1 < na.src_end; t += 2) {
-        float x0 = act[(size_t)a.na_src[t] * n], x1 = act[(size_t)a.na_src[t + 1] * n];
-        if (red) { x0 = 1.0f - x0; x1 = 1.0f - x1; }
-        prod *= x0;
-        prod *= x1;
+    float x[kTermsGroup][kTermsSrc];
+#pragma unroll
+    for (int k = 0; k < kTermsGroup; ++k)
+#pragma unroll
+        for (int q = 0; q < kTermsSrc; ++q) {
+            const int si = s_src[k][q];
+            x[k][q] = si >= 0 ? act[(size_t)si * (size_t)N] : 0.0f;
+        }
+    uint16_t v16[kTermsGroup];
+#pragma unroll
+    for (int k = 0; k < kTermsGroup; ++k) {
+        const bool red = s_red[k] != 0;
+        float prod = 1.0f;
+#pragma unroll
+        for (int q = 0; q < kTermsSrc; ++q)
+            if (s_src[k][q] >= 0) prod *= red ? 1.0f - x[k][q] : x[k][q];  // uniform per block
+        for (int t = s_rest[k][0]; t < s_rest[k][1]; ++t) {
+            const float y = act[(size_t)a.na_src[t] * (size_t)N];
+            prod *= red ? 1.0f - y : y;
+        }
+        const T r = to16<T>(red ? 1.0f - prod : prod);
+        v16[k] = *reinterpret_cast<const uint16_t*>(&r);
     }
-    if (t < na.src_end) {
-        const float x = act[(size_t)a.na_src[t] * n];
-        prod *= red ? 1.0f - x : x;
+    uint16_t* row = reinterpret_cast<uint16_t*>(a.act16) + (size_t)c * a.Kp + a.G + j0;
+    const int off = a.G + j0;  // row offset in elements; rows are 16-byte aligned (Kp % 64 == 0)
+    if (nj == kTermsGroup && (off & 7) == 0) {
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = (uint32_t)v16[2 * i] | ((uint32_t)v16[2 * i + 1] << 16);
+        *reinterpret_cast<uint4*>(row) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+        for (int k = 0; k < nj; ++k) row[k] = v16[k];
     }
-    if (red) prod = 1.0f - prod;
-    reinterpret_cast<T*>(a.act16)[(size_t)c * a.Kp + a.G + j] = to16<T>(prod);
 }
 
 static cudaError_t terms_launch(int dtype, const TensorArgs& a, cudaStream_t st) {
     if (a.N == 0 || a.n_terms == 0) return cudaSuccess;
-    const dim3 grid((unsigned)((a.N + kTermsBlock - 1) / kTermsBlock), (unsigned)a.n_terms);
+    const dim3 grid((unsigned)((a.N + kTermsBlock - 1) / kTermsBlock),
+                    (unsigned)((a.n_terms + kTermsGroup - 1) / kTermsGroup));
     if (dtype == 0) tensor_terms_kernel<__nv_bfloat16><<<grid, kTermsBlock, 0, st>>>(a);
     else tensor_terms_kernel<__half><<<grid, kTermsBlock, 0, st>>>(a);
     return cudaGetLastError();
