@@ -264,6 +264,16 @@ int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, const scrna
                                const scrna_cle_opts* opts, double* d_out, int32_t* d_counts,
                                double* d_eff);
 
+/* ---- page-locked host buffers -----------------------------------------------------
+ * Page-locked (pinned) host memory for result arrays: a device-to-host copy into it runs
+ * at the link's DMA rate instead of through the driver's staging of pageable memory.
+ * No counterpart in the reference (Julia returns Arrays in pageable memory); the Python
+ * layer keeps a pool of these blocks for the arrays that simulate() returns.
+ * scrna_host_alloc: *p = bytes of portable pinned memory (SCRNA_ECUDA if refused).
+ * scrna_host_free: releases a block from scrna_host_alloc (NULL is a no-op). */
+int scrna_host_alloc(size_t bytes, void** p);
+int scrna_host_free(void* p);
+
 /* ---- diagnostics ----------------------------------------------------------------
  * Runs Philox4x32-10 on the device for n counters (host arrays ctr[4n], key[2]) and
  * returns the words in out[4n]; used to check the device generator against the

@@ -94,6 +94,8 @@ SIGNATURES = {
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_debug_tc_gemm": (C.c_int, [P, P, P, P, I64, I32, I32, I32]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),
+    "scrna_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
+    "scrna_host_free": (C.c_int, [P]),
 }
 
 

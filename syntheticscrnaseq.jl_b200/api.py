@@ -16,7 +16,7 @@ from typing import List, Optional, Sequence, Union
 
 import numpy as np
 
-from . import _lib
+from . import _lib, _pinned
 from ._lib import Capture, Kinetics, Opts, Population, check
 from .model import CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig
 
@@ -166,9 +166,9 @@ def simulate(net: GeneNetwork, alg: CLE, kin: KineticParams, gpu: bool = True, p
     h = handle or NetHandle(net, ctx)
     N = population.cell_num if population is not None else cell_num
     cols = net.G * (2 if readout == "both" else 1)
-    out = np.empty((N, cols), dtype=np.float64, order="F")
-    counts = np.empty((N, net.G), dtype=np.int32, order="F") if capture is not None else None
-    eff = np.empty(N, dtype=np.float64) if capture is not None else None
+    out = _pinned.empty((N, cols), np.float64, order="F")
+    counts = _pinned.empty((N, net.G), np.int32, order="F") if capture is not None else None
+    eff = _pinned.empty(N, np.float64) if capture is not None else None
     k, p, c = _kin(kin), _pop(population), _cap(capture)
     o = _opts(alg, T=T, cell_num=N, readout=readout, seed=seed, stream=stream, precision=precision,
               path=path, n_steps=n_steps, cell_offset=cell_offset)
@@ -199,9 +199,9 @@ def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg: CLE, kin, *,
     for b, n in enumerate(networks):
         N = pops[b].cell_num if pops[b] is not None else cns[b]
         cols = n.G * (2 if readout == "both" else 1)
-        outs.append(np.empty((N, cols), dtype=np.float64, order="F"))
+        outs.append(_pinned.empty((N, cols), np.float64, order="F"))
         if capture is not None:
-            cnts.append(np.empty((N, n.G), dtype=np.int32, order="F"))
+            cnts.append(_pinned.empty((N, n.G), np.int32, order="F"))
     karr = (Kinetics * len(kins))(*[_kin(k) for k in kins])
     harr = (C.c_void_p * B)(*[h.h.value for h in handles])
     cn_arr = (C.c_int64 * B)(*[int(x) for x in cns])
@@ -262,11 +262,11 @@ class DeviceRun:
 
     def read(self):
         cols = self.G * (2 if self.readout == "both" else 1)
-        out = np.empty((self.N, cols), dtype=np.float64, order="F")
+        out = _pinned.empty((self.N, cols), np.float64, order="F")
         counts = eff = None
         if self.capture is not None:
-            counts = np.empty((self.N, self.G), dtype=np.int32, order="F")
-            eff = np.empty(self.N, dtype=np.float64)
+            counts = _pinned.empty((self.N, self.G), np.int32, order="F")
+            eff = _pinned.empty(self.N, np.float64)
         check(self.ctx.lib.scrna_state_read(self.ctx.h, self.st, out.ctypes.data,
                                             None if counts is None else counts.ctypes.data,
                                             None if eff is None else eff.ctypes.data))
@@ -360,9 +360,9 @@ class Server:
     def wait(self, ticket: int, timeout_ms: int = -1):
         """(readout, counts, efficiencies, latency_s); counts/efficiencies are None without capture."""
         handle, N, cols, cap = self._meta[ticket]
-        out = np.empty((N, cols), dtype=np.float64, order="F")
-        counts = np.empty((N, handle.G), dtype=np.int32, order="F") if cap else None
-        eff = np.empty(N, dtype=np.float64) if cap else None
+        out = _pinned.empty((N, cols), np.float64, order="F")
+        counts = _pinned.empty((N, handle.G), np.int32, order="F") if cap else None
+        eff = _pinned.empty(N, np.float64) if cap else None
         lat = C.c_double()
         check(self.ctx.lib.scrna_wait(self.h, int(ticket), int(timeout_ms), out.ctypes.data,
                                       None if counts is None else counts.ctypes.data,

@@ -844,6 +844,18 @@ extern "C" int scrna_debug_philox(scrna_ctx* ctx, int32_t n, const uint32_t* ctr
     return SCRNA_OK;
 }
 
+extern "C" int scrna_host_alloc(size_t bytes, void** p) {
+    if (!p) return fail(SCRNA_EINVAL, "NULL argument");
+    *p = nullptr;
+    CU(cudaHostAlloc(p, bytes ? bytes : 16, cudaHostAllocPortable));
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_host_free(void* p) {
+    if (p) CU(cudaFreeHost(p));
+    return SCRNA_OK;
+}
+
 extern "C" int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma, double* sfu, double* iops) {
     if (int r = check_ctx(ctx)) return r;
     if (int r = set_device(ctx)) return r;

@@ -320,3 +320,33 @@ def test_batch_mixed_population_equals_single_runs(pkg):
         single = pkg.simulate(nets[b], pkg.CLE(0.01), kin, population=pops[b], cell_num=cells[b], T=1.25,
                               readout="both", seed=9, stream=3 + b)
         assert np.array_equal(outs[b], single), b
+
+
+def test_pinned_result_arrays(pkg):
+    """Results land in pooled page-locked blocks: live arrays are never reused, released ones
+    are, and the values equal a copy into pageable memory (DeviceRun.read of the same run)."""
+    from scrna_b200 import _pinned
+    net = pkg.sample_network(9, seed=12, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    cap = pkg.CaptureModel(efficiency=0.3, efficiency_std=0.1, readout="protein")
+    first = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=300, T=2.0, seed=4, capture=cap)
+    keep = [a.copy() for a in first]
+    second = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=300, T=2.0, seed=5, capture=cap)
+    for a, b in zip(first, keep):  # the live first results were not overwritten
+        assert np.array_equal(a, b)
+    assert not np.array_equal(first[0], second[0])
+    assert not _pinned._pool._disabled  # pinning works on a GPU box
+    ptrs = {a.__array_interface__["data"][0] for a in first + second}
+    assert len(ptrs) == 6
+    del first, keep, second
+    third = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=300, T=2.0, seed=4, capture=cap)
+    assert {a.__array_interface__["data"][0] for a in third} <= ptrs  # released blocks reused
+    run = pkg.DeviceRun(net, pkg.CLE(0.01), kin, cell_num=300, T=2.0, seed=4, capture=cap)
+    run.launch()
+    X, counts, eff = run.read()
+    assert np.array_equal(third[0], X) and np.array_equal(third[1], counts) and np.array_equal(third[2], eff)
+    pageable = np.empty_like(X, order="F")
+    pkg._lib.check(run.ctx.lib.scrna_state_read(run.ctx.h, run.st, pageable.ctypes.data, None, None))
+    assert np.array_equal(pageable, X)
+    assert third[0].flags["F_CONTIGUOUS"] and third[1].flags["F_CONTIGUOUS"]
+    run.close()
