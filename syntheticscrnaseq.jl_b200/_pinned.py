@@ -68,7 +68,7 @@ class PinnedPool:
         self.cap_bytes = int(cap_bytes)
         self._free: dict = {}
         self._idle = 0
-        self._lock = threading.Lock()
+        self._lock = threading.RLock()  # a collected array may return its block from inside a locked section
         self._disabled = False
 
     def _alloc(self, size: int):
