@@ -360,9 +360,10 @@ class Server:
     def wait(self, ticket: int, timeout_ms: int = -1):
         """(readout, counts, efficiencies, latency_s); counts/efficiencies are None without capture."""
         handle, N, cols, cap = self._meta[ticket]
-        out = _pinned.empty((N, cols), np.float64, order="F")
-        counts = _pinned.empty((N, handle.G), np.int32, order="F") if cap else None
-        eff = _pinned.empty(N, np.float64) if cap else None
+        # one-off sizes: pageable (pinning a fresh block costs more than the copy it saves)
+        out = np.empty((N, cols), dtype=np.float64, order="F")
+        counts = np.empty((N, handle.G), dtype=np.int32, order="F") if cap else None
+        eff = np.empty(N, dtype=np.float64) if cap else None
         lat = C.c_double()
         check(self.ctx.lib.scrna_wait(self.h, int(ticket), int(timeout_ms), out.ctypes.data,
                                       None if counts is None else counts.ctypes.data,
