@@ -95,3 +95,20 @@ def test_fused_matches_library_gemm_path(pkg, G, N, bursty):
     assert np.array_equal(a["prom"], b["prom"])
     assert _rel(a["M"], b["M"].astype(np.float64)) < 2e-2
     assert _rel(a["P"], b["P"].astype(np.float64)) < 2e-2
+
+
+@pytest.mark.parametrize("path", ["tensor", "tensor_library"])
+@pytest.mark.parametrize("G,n_terms,n_src", [(67, 13, (5, 7)), (72, 9, (2, 6)), (64, 8, (4, 4))])
+def test_tensor_long_and_ragged_terms(pkg, path, G, n_terms, n_src):
+    """Term columns with more sources than one load round (4) takes, term groups that do
+    not fill 8 columns, and term columns that start off a 16-byte boundary (G odd, or G+8k
+    not a multiple of 8): against the FP32 register path."""
+    net = pkg.dense_network(G, seed=G + n_terms, density=0.2, n_coop=(n_terms + 1) // 2, n_redun=n_terms // 2,
+                            n_sources_range=n_src)
+    assert max(len(e.sources) for e in list(net.cooperative) + list(net.redundant)) >= n_src[0]
+    kin = pkg.WORKLOAD_KINETICS
+    ref = _run(pkg, net, kin, "block", N=257).read_raw()
+    got = _run(pkg, net, kin, path, N=257).read_raw()
+    assert np.array_equal(got["prom"], ref["prom"])
+    assert _rel(got["M"], ref["M"].astype(np.float64)) < 5e-2
+    assert _rel(got["P"], ref["P"].astype(np.float64)) < 5e-2
