@@ -186,7 +186,8 @@ int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinet
                          const scrna_cle_opts* opts, scrna_state* st);
 int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, int32_t* counts,
                      double* efficiencies);
-/* Device pointers of the state's FP32 [G][N] mRNA / protein arrays (for tests). */
+/* Device pointers of the state's FP32 mRNA / protein arrays (for tests): [G][N] after a
+ * run on the block kernel, [N][G] (cell-major) after a run on the lane kernel. */
 int scrna_state_device_ptrs(scrna_state* st, void** d_mrna, void** d_protein);
 /* Copies the raw simulation state of the last run to the host: mRNA and protein as
  * [G][N] float32 (FP32 path) or float64 (FP64 baseline path, then pass doubles),

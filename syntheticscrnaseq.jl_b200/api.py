@@ -288,6 +288,8 @@ class DeviceRun:
         return out
 
     def device_state(self):
+        """Device pointers of the FP32 mRNA / protein state: [G][N] after a block-kernel run,
+        [N][G] after a lane-kernel run."""
         m, p = C.c_void_p(), C.c_void_p()
         check(self.ctx.lib.scrna_state_device_ptrs(self.st, C.byref(m), C.byref(p)))
         return m.value, p.value

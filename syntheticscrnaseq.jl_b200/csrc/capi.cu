@@ -577,6 +577,7 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     auto launch = [&](bool is_pop) -> cudaError_t {
         return use_warp ? warpcell_launch(a, d.lane_gpl, d.lane_emax, d.lane_tmax, is_pop, s) : fused_launch(a, L, is_pop, s);
     };
+    st->last_cell_major = use_warp;  // the lane kernel keeps M, P, prom, NS cell-major
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;
         CU(launch(false));
@@ -697,9 +698,11 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
             return tensor_run(ctx, net, kin, cap, o, st, dtype);
         }
         st->last_tensor = false;  // the fused kernel keeps the register path's gene-major state
+        st->last_cell_major = false;
         return tc_run(ctx, net, kin, cap, o, st, dtype);
     }
     st->last_tensor = false;
+    st->last_cell_major = false;
     if (int r = state_alloc(st, pop != nullptr, plain)) return r;
     st->have_counts = cap != nullptr;
     st->last_plain = plain;
@@ -744,6 +747,27 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
                 if (promoter) promoter[dst] = tpr[src];
             }
         if (volume) return fail(SCRNA_EINVAL, "the last run had no population");
+        return SCRNA_OK;
+    }
+    if (st->last_cell_major) {  // lane-kernel state [N][G]: transpose to [G][N] on the host
+        std::vector<float> tm(gn), tp(gn);
+        std::vector<uint8_t> tpr(gn);
+        if (!st->M.p || !st->P.p) return fail(SCRNA_EINVAL, "the state has not been run");
+        CU(cudaMemcpyAsync(tm.data(), st->M.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tp.data(), st->P.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(tpr.data(), st->prom.p, gn, cudaMemcpyDeviceToHost, ctx->stream));
+        if (volume) {
+            if (!st->last_pop) return fail(SCRNA_EINVAL, "the last run had no population");
+            CU(cudaMemcpyAsync(volume, st->V.p, (size_t)st->N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CU(cudaStreamSynchronize(ctx->stream));
+        for (int64_t c = 0; c < st->N; ++c)
+            for (int g = 0; g < st->G; ++g) {
+                const size_t src = (size_t)c * st->G + g, dst = (size_t)g * st->N + c;
+                if (mrna) static_cast<float*>(mrna)[dst] = tm[src];
+                if (protein) static_cast<float*>(protein)[dst] = tp[src];
+                if (promoter) promoter[dst] = tpr[src];
+            }
         return SCRNA_OK;
     }
     const size_t esz = st->last_plain ? 8 : 4;

@@ -105,6 +105,7 @@ struct scrna_state {
     DevBuf tM, tP, tprom, tNS, tact16, tact32[2], treg;
     int t_ld = 0;  // row stride of the cell-major tensor-path state
     bool last_tensor = false;
+    bool last_cell_major = false;  // the lane kernel ran: M, P, prom, NS are [N][G]
     bool have_counts = false;
     bool last_plain = false;
     bool last_pop = false;

@@ -97,7 +97,8 @@ struct FusedArgs {
     const uint8_t* quad_tel;     // per quad: any gene switches (finite k_on)
     const int2* lane_in;         // [G][kLaneEdges] padded in-edges (warp kernel)
     const LaneTerm* lane_term;   // [n_na] terms with padded sources (warp kernel)
-    // state [G][N]
+    // state: [G][N] for the block kernel, [N][G] (cell-major) for the lane kernel (also the
+    // division scratch below), so a warp's loads and stores of a cell's genes are adjacent
     float* M;
     float* P;
     uint8_t* prom;

@@ -259,14 +259,15 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
         const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
         const int2* Ns = from_daughter ? a.dNS[par] : a.NS;
 #pragma unroll
-        for (int i = 0; i < GPL; ++i) {
+        for (int i = 0; i < GPL; ++i) {  // cell-major state: a warp's lanes read adjacent entries
             const int g = u * GPL + i;
-            m[i] = valid[i] ? Ms[(size_t)g * N + src] : 0.0f;
-            p[i] = valid[i] ? Ps[(size_t)g * N + src] : 0.0f;
-            const int2 sw = valid[i] ? Ns[(size_t)g * N + src] : make_int2(kNever, kNever);
+            const size_t si = (size_t)src * G + g;
+            m[i] = valid[i] ? Ms[si] : 0.0f;
+            p[i] = valid[i] ? Ps[si] : 0.0f;
+            const int2 sw = valid[i] ? Ns[si] : make_int2(kNever, kNever);
             ns[i] = sw.x;
             kn[i] = sw.y;
-            if (valid[i] && !Os[(size_t)g * N + src]) on &= ~(1u << i);
+            if (valid[i] && !Os[si]) on &= ~(1u << i);
         }
         if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
     }
@@ -417,7 +418,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
                 }
                 m[i] = mm;
                 p[i] = pm;
-                const size_t idx = (size_t)g * N + cidx;
+                const size_t idx = (size_t)cidx * G + g;
                 a.dM[par][idx] = dm;
                 a.dP[par][idx] = dp;
                 const uint32_t bon = (on >> i) & 1u;
@@ -437,11 +438,11 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     for (int i = 0; i < GPL; ++i) {
         const int g = u * GPL + i;
         if (!valid[i]) continue;
-        const size_t idx = (size_t)g * N + cell;
-        a.M[idx] = m[i];
-        a.P[idx] = p[i];
-        a.prom[idx] = (on >> i) & 1u;
-        a.NS[idx] = make_int2(ns[i], kn[i]);
+        const size_t si = (size_t)cell * G + g, idx = (size_t)g * N + cell;
+        a.M[si] = m[i];
+        a.P[si] = p[i];
+        a.prom[si] = (on >> i) & 1u;
+        a.NS[si] = make_int2(ns[i], kn[i]);
         if (ctl.last && a.out) {
             if (a.readout == 0) a.out[idx] = (double)m[i];
             else if (a.readout == 1) a.out[idx] = (double)p[i];
