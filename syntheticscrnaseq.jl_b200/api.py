@@ -11,7 +11,10 @@ column-major (Fortran) order, the layout of the reference's Matrix{Float64}.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 import math
+import threading
+from collections import OrderedDict
 from typing import List, Optional, Sequence, Union
 
 import numpy as np
@@ -47,6 +50,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            for nh in self.__dict__.pop("_net_cache", {}).values():  # networks before the context
+                nh.close()
             self.lib.scrna_ctx_destroy(self.h)
             self.h = None
 
@@ -122,6 +127,48 @@ class NetHandle:
             pass
 
 
+# Uploaded networks reused across simulate / simulate_gpu_batch calls on one context, keyed
+# by the network's content (not its identity, so an array changed in place is a new
+# network).  Only networks whose arrays total at most _HANDLE_CACHE_BYTES are hashed and
+# kept; the cache lives on the context and goes with it.
+_HANDLE_CACHE_BYTES = 1 << 20
+_HANDLE_CACHE_SIZE = 64
+_handle_lock = threading.Lock()
+
+
+def _net_digest(net: GeneNetwork) -> Optional[bytes]:
+    arrays = (net.basals, net.interactions, net.k_on, net.k_off)
+    if sum(a.nbytes for a in arrays) > _HANDLE_CACHE_BYTES:
+        return None
+    h = hashlib.blake2b(digest_size=20)
+    h.update(int(net.G).to_bytes(8, "little"))
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    for tag, edges in ((b"c", net.cooperative), (b"r", net.redundant)):
+        h.update(tag)
+        for e in edges:
+            h.update(repr((int(e.target), tuple(int(x) for x in e.sources), float(e.strength))).encode())
+    return h.digest()
+
+
+def _handle_for(net: GeneNetwork, ctx: Context) -> "NetHandle":
+    d = _net_digest(net)
+    if d is None:
+        return NetHandle(net, ctx)
+    with _handle_lock:
+        cache = ctx.__dict__.setdefault("_net_cache", OrderedDict())
+        hit = cache.get(d)
+        if hit is not None and hit.h and getattr(ctx, "h", None):
+            cache.move_to_end(d)
+            return hit
+    h = NetHandle(net, ctx)
+    with _handle_lock:  # an evicted handle is released when its last user drops it
+        cache[d] = h
+        while len(cache) > _HANDLE_CACHE_SIZE:
+            cache.popitem(last=False)
+    return h
+
+
 def _kin(kin: KineticParams) -> Kinetics:
     return Kinetics(kin.k_t, kin.K_d, kin.n, kin.mu_m, kin.mu_p, kin.dilution)
 
@@ -163,7 +210,7 @@ def simulate(net: GeneNetwork, alg: CLE, kin: KineticParams, gpu: bool = True, p
     if not gpu:
         raise NotImplementedError("only the GPU path is provided by this library")
     ctx = ctx or default_context()
-    h = handle or NetHandle(net, ctx)
+    h = handle or _handle_for(net, ctx)
     N = population.cell_num if population is not None else cell_num
     cols = net.G * (2 if readout == "both" else 1)
     out = _pinned.empty((N, cols), np.float64, order="F")
@@ -193,7 +240,7 @@ def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg: CLE, kin, *,
     B = len(networks)
     kins = list(kin) if isinstance(kin, (list, tuple)) else [kin]
     cns = list(cell_num) if isinstance(cell_num, (list, tuple, np.ndarray)) else [int(cell_num)] * B
-    handles = [NetHandle(n, ctx) for n in networks]
+    handles = [_handle_for(n, ctx) for n in networks]
     pops = list(populations) if populations is not None else [None] * B
     outs, cnts = [], []
     for b, n in enumerate(networks):

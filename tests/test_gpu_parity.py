@@ -350,3 +350,20 @@ def test_pinned_result_arrays(pkg):
     assert np.array_equal(pageable, X)
     assert third[0].flags["F_CONTIGUOUS"] and third[1].flags["F_CONTIGUOUS"]
     run.close()
+
+
+def test_network_upload_cache(pkg):
+    """simulate() reuses an uploaded network for the same content on the same context and
+    uploads again after an in-place change: results equal those of an explicit handle."""
+    ctx = pkg.Context(0)
+    net = pkg.sample_network(8, seed=21, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    a = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=64, T=1.0, seed=2, ctx=ctx)
+    b = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=64, T=1.0, seed=2, ctx=ctx)
+    assert len(ctx._net_cache) == 1 and np.array_equal(a, b)
+    net.basals[0] *= 3.0  # same object, new content
+    c = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=64, T=1.0, seed=2, ctx=ctx)
+    ref = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=64, T=1.0, seed=2, ctx=ctx,
+                       handle=pkg.NetHandle(net, ctx))
+    assert len(ctx._net_cache) == 2 and np.array_equal(c, ref) and not np.array_equal(a, c)
+    ctx.close()
