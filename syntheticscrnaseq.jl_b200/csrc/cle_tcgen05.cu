@@ -184,9 +184,18 @@ struct TcStepArgs {
     int* err;
 };
 
-constexpr int kTcEpiWarps = 16;  // 4 per TMEM lane quadrant, 64 accumulator columns each
+// Step kernel tiles: 128 cells x 240 genes, N = 240 = 5 column slices of 48 per TMEM lane
+// quadrant, so 20 epilogue warps (5 per scheduler) hide each other's latencies; the two
+// accumulators sit 256 columns apart in one 512-column allocation.
+constexpr int kTsBN = 240, kTsSlices = 5, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
+constexpr uint32_t kTsBBytes = kTsBN * kTcBK * 2;
+constexpr size_t kTsSmem = 1024 + (size_t)kTcStages * (kTcABytes + kTsBBytes) + 256;
+constexpr int kTcEpiWarps = 4 * kTsSlices;
 constexpr int kTcMaxGenes = 4096; // gene table of the epilogue in shared memory (8 bytes a gene)
 constexpr int kTcStepThreads = 32 * (2 + kTcEpiWarps);
+static_assert(kTsBN % 16 == 0 && kTsBN <= 256 && kTsSliceCols % 8 == 0, "UMMA N and epilogue groups");
+static_assert(kTsBBytes % 1024 == 0, "128-byte-swizzled stages stay 1024-byte aligned");
+static_assert(kTsSmem + 8 * (size_t)kTcMaxGenes + 8 <= 227 * 1024, "shared memory of the step kernel");
 
 template <class T> struct TcPack;
 template <> struct TcPack<__nv_bfloat16> {
@@ -327,7 +336,7 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
     unsigned char* stages = smem_dyn + ((1024 - (base & 1023)) & 1023);
     unsigned char* a_s = stages;
     unsigned char* b_s = stages + (size_t)kTcStages * kTcABytes;
-    TcShared* sh = reinterpret_cast<TcShared*>(b_s + (size_t)kTcStages * kTcBBytes);
+    TcShared* sh = reinterpret_cast<TcShared*>(b_s + (size_t)kTcStages * kTsBBytes);
     float* gc = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sh) + 256);
     int* gsrc = reinterpret_cast<int*>(gc + ((a.G + 1) & ~1));
 
@@ -340,10 +349,10 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
         gsrc[i] = a.src_of_gene[i];
     }
     if (threadIdx.x == 0 && (G & 1)) gc[G] = 0.0f;  // pad of the last pair
-    const int tiles_m = (int)((N + kTcBM - 1) / kTcBM), tiles_n = (G + kTcBN - 1) / kTcBN;
+    const int tiles_m = (int)((N + kTcBM - 1) / kTcBM), tiles_n = (G + kTsBN - 1) / kTsBN;
     const int n_tiles = tiles_m * tiles_n;
     const int kb_n = a.Kp / kTcBK;
-    constexpr uint32_t idesc = tc::umma_idesc_f16(std::is_same<T, __nv_bfloat16>::value, kTcBM, kTcBN);
+    constexpr uint32_t idesc = tc::umma_idesc_f16(std::is_same<T, __nv_bfloat16>::value, kTcBM, kTsBN);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kTcStages; ++s) {
@@ -359,7 +368,7 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
         tc::prefetch_tensormap(&map_b);
     }
     if (warp == 1) {
-        tc::tmem_alloc(&sh->tmem_base, 2 * kTcBN);
+        tc::tmem_alloc(&sh->tmem_base, 2 * kTsAccCols);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -374,9 +383,9 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
             const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
             for (int kb = 0; kb < kb_n; ++kb) {
                 if (!tc::mbar_wait(&sh->empty[stage], phase ^ 1u)) { tc_fail(a.err, 1); goto producer_done; }
-                tc::mbar_arrive_expect_tx(&sh->full[stage], kTcABytes + kTcBBytes);
+                tc::mbar_arrive_expect_tx(&sh->full[stage], kTcABytes + kTsBBytes);
                 tc::tma_load_2d(a_s + (size_t)stage * kTcABytes, &map_a, &sh->full[stage], kb * kTcBK, m * kTcBM);
-                tc::tma_load_2d(b_s + (size_t)stage * kTcBBytes, &map_b, &sh->full[stage], kb * kTcBK, n * kTcBN);
+                tc::tma_load_2d(b_s + (size_t)stage * kTsBBytes, &map_b, &sh->full[stage], kb * kTcBK, n * kTsBN);
                 if (++stage == kTcStages) { stage = 0; phase ^= 1u; }
             }
         }
@@ -387,13 +396,13 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
             if (!tc::mbar_wait(&sh->tmem_empty[acc], acc_phase ^ 1u)) { tc_fail(a.err, 3); break; }
             tc::tc_fence_after();
-            const uint32_t d = tmem + (uint32_t)(acc * kTcBN);
+            const uint32_t d = tmem + (uint32_t)(acc * kTsAccCols);
             bool ok = true;
             for (int kb = 0; kb < kb_n; ++kb) {
                 if (!tc::mbar_wait(&sh->full[stage], phase)) { tc_fail(a.err, 2); ok = false; break; }
                 tc::tc_fence_after();
                 const uint32_t a_addr = tc::smem_u32(a_s + (size_t)stage * kTcABytes);
-                const uint32_t b_addr = tc::smem_u32(b_s + (size_t)stage * kTcBBytes);
+                const uint32_t b_addr = tc::smem_u32(b_s + (size_t)stage * kTsBBytes);
 #pragma unroll
                 for (int k = 0; k < kTcBK / 16; ++k)
                     tc::umma_f16(d, tc::sw128_kmajor_desc(a_addr + 32u * k), tc::sw128_kmajor_desc(b_addr + 32u * k),
@@ -407,7 +416,7 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
         }
     } else if (warp >= 2) {  // ---- epilogue: Euler-Maruyama step of the tile's cells x genes
         const int q = warp & 3;             // TMEM lane quadrant
-        const int slice = (warp - 2) >> 2;  // 64-column slice of the accumulator
+        const int slice = (warp - 2) >> 2;  // 48-column slice of the accumulator
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -420,15 +429,15 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
             float* Mc = a.M + c;
             float* Pc = a.P + c;
             // groups of 8 genes: state loads of the group issued together, then the updates
-            const int gs = n * kTcBN + slice * 64;
+            const int gs = n * kTsBN + slice * kTsSliceCols;
 #pragma unroll 1
-            for (int grp = 0; grp < 8; ++grp) {
+            for (int grp = 0; grp < kTsSliceCols / 8; ++grp) {
                 const int g0 = gs + grp * 8;
                 if (g0 >= G) break;  // uniform across the warp
                 float ms[8], ps[8];
                 tc_load_group(a, Mc, Pc, cell_ok, g0, ms, ps);
                 float v[8];
-                tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTcBN + slice * 64 + grp * 8), v);
+                tc::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * kTsAccCols + slice * kTsSliceCols + grp * 8), v);
                 tc_step_group<T, BURSTY, HN>(a, gc, gsrc, v, c, cell_ok, g0, Mc, Pc, ms, ps);
             }
             tc::tc_fence_before();
@@ -441,7 +450,7 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
     __syncthreads();
     if (warp == 1) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem, 2 * kTcBN);
+        tc::tmem_dealloc(tmem, 2 * kTsAccCols);
     }
 }
 
@@ -609,7 +618,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     CUtensorMap map_a[2], map_b;
     for (int k = 0; k < 2; ++k)
         if (int r = tc_make_map(&map_a[k], act[k], N, Kp, kTcBM, bf16)) return r;
-    if (int r = tc_make_map(&map_b, n->t_w16.p, G, Kp, kTcBN, bf16)) return r;
+    if (int r = tc_make_map(&map_b, n->t_w16.p, G, Kp, kTsBN, bf16)) return r;
 
     TcStepArgs a{};
     a.G = G; a.Kp = Kp; a.n_src = n_src; a.hill_int = hill_int;
@@ -634,9 +643,9 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
                           : (h2 ? tc_cle_step_kernel<__nv_bfloat16, false, 2> : tc_cle_step_kernel<__nv_bfloat16, false, 0>);
     else fn = bursty ? (h2 ? tc_cle_step_kernel<__half, true, 2> : tc_cle_step_kernel<__half, true, 0>)
                      : (h2 ? tc_cle_step_kernel<__half, false, 2> : tc_cle_step_kernel<__half, false, 0>);
-    const size_t smem = kTcSmem + (size_t)(((G + 1) & ~1) + G) * 4;  // + the epilogue's gene table
+    const size_t smem = kTsSmem + (size_t)(((G + 1) & ~1) + G) * 4;  // + the epilogue's gene table
     CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + kTcBN - 1) / kTcBN);
+    const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + kTsBN - 1) / kTsBN);
     const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
     const int64_t n_steps = run_steps(o);
     for (int64_t step = 1; step <= n_steps; ++step) {
