@@ -184,10 +184,12 @@ struct TcStepArgs {
     int* err;
 };
 
-// Step kernel tiles: 128 cells x 240 genes, N = 240 = 5 column slices of 48 per TMEM lane
-// quadrant, so 20 epilogue warps (5 per scheduler) hide each other's latencies; the two
-// accumulators sit 256 columns apart in one 512-column allocation.
-constexpr int kTsBN = 240, kTsSlices = 5, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
+// Step kernel tiles: 128 cells x 192 genes, N = 192 = 6 column slices of 32 per TMEM lane
+// quadrant, so 24 epilogue warps (6 per scheduler) hide each other's latencies (the
+// epilogue is latency-bound: 4 warps per scheduler with 256-gene tiles took 802 us a step,
+// 5 with 240 745 us); the two accumulators sit 256 columns apart in one 512-column
+// allocation.
+constexpr int kTsBN = 192, kTsSlices = 6, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
 constexpr uint32_t kTsBBytes = kTsBN * kTcBK * 2;
 constexpr size_t kTsSmem = 1024 + (size_t)kTcStages * (kTcABytes + kTsBBytes) + 256;
 constexpr int kTcEpiWarps = 4 * kTsSlices;
@@ -416,7 +418,7 @@ tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_const
         }
     } else if (warp >= 2) {  // ---- epilogue: Euler-Maruyama step of the tile's cells x genes
         const int q = warp & 3;             // TMEM lane quadrant
-        const int slice = (warp - 2) >> 2;  // 48-column slice of the accumulator
+        const int slice = (warp - 2) >> 2;  // kTsSliceCols-column slice of the accumulator
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
