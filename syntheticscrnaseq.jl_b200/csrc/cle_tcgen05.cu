@@ -184,12 +184,12 @@ struct TcStepArgs {
     int* err;
 };
 
-// Step kernel tiles: 128 cells x 192 genes, N = 192 = 6 column slices of 32 per TMEM lane
-// quadrant, so 24 epilogue warps (6 per scheduler) hide each other's latencies (the
-// epilogue is latency-bound: 4 warps per scheduler with 256-gene tiles took 802 us a step,
-// 5 with 240 745 us); the two accumulators sit 256 columns apart in one 512-column
-// allocation.
-constexpr int kTsBN = 192, kTsSlices = 6, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
+// Step kernel tiles: 128 cells x 224 genes, N = 224 = 7 column slices of 32 per TMEM lane
+// quadrant, so 28 epilogue warps (7 per scheduler, 960 threads, 64 registers) hide each
+// other's latencies: the epilogue is latency-bound (per dense step 0.925 ms with 4 epilogue
+// warps per scheduler, 0.911 with 5, 0.877 with 6, 0.869 with 7 on one box).  The two
+// accumulators sit 256 columns apart in one 512-column allocation.
+constexpr int kTsBN = 224, kTsSlices = 7, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
 constexpr uint32_t kTsBBytes = kTsBN * kTcBK * 2;
 constexpr size_t kTsSmem = 1024 + (size_t)kTcStages * (kTcABytes + kTsBBytes) + 256;
 constexpr int kTcEpiWarps = 4 * kTsSlices;
