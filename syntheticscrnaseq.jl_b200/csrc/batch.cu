@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -190,11 +191,19 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         CU(cudaMemcpyAsync(g.items.p, items.data(), items.size() * sizeof(TileWork), cudaMemcpyHostToDevice, g.stream));
         const int n_items = (int)items.size();
         const int grid = std::max(1, std::min(n_items, ctx->sm_count * (k.warp ? std::max(1, 24 / k.nwarps) : 8)));
+        // one seed for the whole call: the lane kernel reads the round keys from its parameters
+        KeySchedule ks{};
+        bool same_key = !args.empty();
+        for (const FusedArgs& fa : args) same_key = same_key && fa.key0 == args[0].key0 && fa.key1 == args[0].key1;
+        if (same_key) {
+            std::memcpy(ks.rk0, args[0].rk0, sizeof ks.rk0);
+            std::memcpy(ks.rk1, args[0].rk1, sizeof ks.rk1);
+        }
         auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
             if (k.warp)
                 return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
                                              k.emax, k.tmax, k.pop != 0, smem, grid, k.nwarps, ctl, use_shared,
-                                             g.stream);
+                                             same_key ? &ks : nullptr, g.stream);
             return fused_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
                                       smem, k.pop != 0, grid, ctl, use_shared, g.stream);
         };

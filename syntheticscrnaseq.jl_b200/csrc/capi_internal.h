@@ -134,9 +134,11 @@ int fused_max_quads();
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
                                cudaStream_t st);
+// ks: round keys shared by every network of the launch (NULL: each network's own, computed
+// in the rounds)
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
                                   int emax, int tmax, bool pop, size_t smem, int grid, int nwarps,
-                                  TileCtl shared_ctl, int use_shared, cudaStream_t st);
+                                  TileCtl shared_ctl, int use_shared, const KeySchedule* ks, cudaStream_t st);
 int warpcell_cells_per_block_host(int G, int gpl);
 int warpcell_block_warps_host(int G, int gpl);
 int tensor_prepare_net(scrna_net* n, int dtype);

@@ -54,7 +54,7 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st);
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
-                                    cudaStream_t st);
+                                    const KeySchedule* ks, cudaStream_t st);
 template <int UPT, bool POP>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
@@ -118,10 +118,10 @@ cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, boo
 
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
                                   int emax, int tmax, bool pop, size_t smem, int grid, int nwarps,
-                                  TileCtl shared_ctl, int use_shared, cudaStream_t st) {
+                                  TileCtl shared_ctl, int use_shared, const KeySchedule* ks, cudaStream_t st) {
     return warpcell_dispatch(gpl, emax, tmax, pop, [&](auto g, auto r, auto k, auto p) {
         return warpcell_queue_launch_t<decltype(g)::value, decltype(r)::value, decltype(k)::value, decltype(p)::value>(
-            args, items, n_items, counter, smem, grid, nwarps, shared_ctl, use_shared, st);
+            args, items, n_items, counter, smem, grid, nwarps, shared_ctl, use_shared, ks, st);
     });
 }
 

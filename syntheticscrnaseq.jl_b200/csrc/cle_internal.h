@@ -133,6 +133,12 @@ struct TileWork {
     TileCtl ctl;
 };
 
+// Philox round keys shared by every network of one queued launch (a batch call has one
+// seed): passed as a kernel parameter, so the rounds read them as constant operands.
+struct KeySchedule {
+    uint32_t rk0[10], rk1[10];
+};
+
 // Launch shape of the fused kernel chosen for a network: quads per thread (UPT),
 // warps per block (NW, so 32 cells x NW warps) and dynamic shared memory.
 struct FusedLaunch {

@@ -100,12 +100,12 @@ __device__ __forceinline__ float2 warpcell_hill2(float2 p, const FusedArgs& a) {
 }
 
 // One block tile (warpcell_cells_per_block cells) of one network through ctl's step range.
-// RK: the Euler-step Philox reads its round keys from `a` (kernel parameter space).
+// RK: the Euler-step Philox reads its round keys from rk0 / rk1 (kernel parameter space).
 // HN: 2 for a Hill exponent of exactly 2, else 0 (any exponent).
 // MW: cells span several warps (warpcell_wpc > 1), else several cells share a warp.
 template <int GPL, int EMAX, int TMAX, bool POP, bool RK, int HN, bool MW>
 __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
-                                              unsigned char* smem_raw) {
+                                              unsigned char* smem_raw, const uint32_t* rk0, const uint32_t* rk1) {
     static_assert(GPL % 2 == 0, "genes are updated in pairs");
     constexpr int TM = TMAX > 0 ? TMAX : 1;
     const int G = a.G;
@@ -294,7 +294,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     constexpr bool AHEAD = GPL == 2 && EMAX <= 4 && TMAX <= 1;
     auto draw = [&](int s, int h) {
         const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
-        return RK ? philox_rk(gcell, (uint32_t)s, c2, c3, a.rk0, a.rk1) : philox(gcell, (uint32_t)s, c2, c3, key);
+        return RK ? philox_rk(gcell, (uint32_t)s, c2, c3, rk0, rk1) : philox(gcell, (uint32_t)s, c2, c3, key);
     };
     uint4 wn[GPL / 2];
     if (AHEAD) {
@@ -475,18 +475,18 @@ __global__ void __launch_bounds__(256, 3) cle_warpcell_kernel(const FusedArgs a)
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
     const bool mw = warpcell_wpc(a.G, GPL) > 1;
     if (a.hill_int == 2) {
-        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, true>(a, blockIdx.x, ctl, smem_raw);
-        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, false>(a, blockIdx.x, ctl, smem_raw);
+        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, true>(a, blockIdx.x, ctl, smem_raw, a.rk0, a.rk1);
+        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, false>(a, blockIdx.x, ctl, smem_raw, a.rk0, a.rk1);
     } else {
-        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, true>(a, blockIdx.x, ctl, smem_raw);
-        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, false>(a, blockIdx.x, ctl, smem_raw);
+        if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, true>(a, blockIdx.x, ctl, smem_raw, a.rk0, a.rk1);
+        else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, false>(a, blockIdx.x, ctl, smem_raw, a.rk0, a.rk1);
     }
 }
 
 template <int GPL, int EMAX, int TMAX, bool POP>
 __global__ void __launch_bounds__(256, 3)
 cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
-                       TileCtl shared_ctl, int use_shared) {
+                       TileCtl shared_ctl, int use_shared, const KeySchedule ks, int use_ks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int next;
     while (true) {
@@ -499,12 +499,20 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
         const FusedArgs& a = args[w.arg];
         const TileCtl& ctl = use_shared ? shared_ctl : w.ctl;
         const bool mw = warpcell_wpc(a.G, GPL) > 1;
-        if (a.hill_int == 2) {
-            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, true>(a, w.tile, ctl, smem_raw);
-            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, false>(a, w.tile, ctl, smem_raw);
+        if (use_ks) {  // one key schedule for the whole launch: round keys from the parameters
+            if (a.hill_int == 2) {
+                if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, true>(a, w.tile, ctl, smem_raw, ks.rk0, ks.rk1);
+                else warpcell_tile<GPL, EMAX, TMAX, POP, true, 2, false>(a, w.tile, ctl, smem_raw, ks.rk0, ks.rk1);
+            } else {
+                if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, true>(a, w.tile, ctl, smem_raw, ks.rk0, ks.rk1);
+                else warpcell_tile<GPL, EMAX, TMAX, POP, true, 0, false>(a, w.tile, ctl, smem_raw, ks.rk0, ks.rk1);
+            }
+        } else if (a.hill_int == 2) {
+            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, true>(a, w.tile, ctl, smem_raw, nullptr, nullptr);
+            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 2, false>(a, w.tile, ctl, smem_raw, nullptr, nullptr);
         } else {
-            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, true>(a, w.tile, ctl, smem_raw);
-            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, false>(a, w.tile, ctl, smem_raw);
+            if (mw) warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, true>(a, w.tile, ctl, smem_raw, nullptr, nullptr);
+            else warpcell_tile<GPL, EMAX, TMAX, POP, false, 0, false>(a, w.tile, ctl, smem_raw, nullptr, nullptr);
         }
         __syncthreads();
     }
@@ -526,11 +534,13 @@ cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
-                                    cudaStream_t st) {
+                                    const KeySchedule* ks, cudaStream_t st) {
     auto k = cle_warpcell_queue_kernel<GPL, EMAX, TMAX, POP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, 32 * nwarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
+    const KeySchedule none{};
+    k<<<grid, 32 * nwarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared, ks ? *ks : none,
+                                       ks ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -541,7 +551,8 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
 #define SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, TMAX, POP)                                                        \
     template cudaError_t scrna::warpcell_launch_t<GPL, EMAX, TMAX, POP>(const FusedArgs&, cudaStream_t);         \
     template cudaError_t scrna::warpcell_queue_launch_t<GPL, EMAX, TMAX, POP>(                                   \
-        const FusedArgs*, const TileWork*, int, int*, size_t, int, int, TileCtl, int, cudaStream_t);
+        const FusedArgs*, const TileWork*, int, int*, size_t, int, int, TileCtl, int, const KeySchedule*,        \
+        cudaStream_t);
 #define SCRNA_WARPCELL_INSTANTIATE_ALL(GPL, EMAX)       \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, false)     \
     SCRNA_WARPCELL_INSTANTIATE(GPL, EMAX, 0, true)      \

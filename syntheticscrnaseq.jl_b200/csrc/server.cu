@@ -223,7 +223,7 @@ void scrna_server::run() {
             if (std::get<0>(key))
                 e = warpcell_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<1>(key),
                                           std::get<2>(key), std::get<4>(key), false, sh.second, grid,
-                                          std::get<3>(key), TileCtl{}, 0, stream);
+                                          std::get<3>(key), TileCtl{}, 0, nullptr, stream);
             else
                 e = fused_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<3>(key), sh.first,
                                        sh.second, false, grid, TileCtl{}, 0, stream);
