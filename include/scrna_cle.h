@@ -122,6 +122,10 @@ int scrna_ctx_set_stream(scrna_ctx* ctx, void* cuda_stream);
 int scrna_ctx_synchronize(scrna_ctx* ctx);
 /* Number of kernels this context has launched so far. */
 int64_t scrna_ctx_launch_count(const scrna_ctx* ctx);
+/* Bytes this context's calls have copied host -> device (network tables, per-run gene
+ * tables) and device -> host (results) so far.  No counterpart in the reference: it lets a
+ * caller account for the transfers of an end-to-end call. */
+int scrna_ctx_transfer_bytes(const scrna_ctx* ctx, int64_t* h2d, int64_t* d2h);
 
 /* ---- networks ---------------------------------------------------------------
  * Uploads a GeneNetwork (src/network.jl:55-63): basals, A, cooperative and
@@ -246,20 +250,25 @@ int scrna_server_get_stats(scrna_server* srv, scrna_server_stats* stats);
  * This entry point has no counterpart in the reference.  It is for callers that
  * cannot allocate device memory when they run a simulation (the allocator is owned
  * by another component, a serving loop must not synchronise on cudaMalloc/cudaFree,
- * or device memory is budgeted up front).  It runs the fused FP32 kernel of
- * scrna_cle_run_device, optionally with population and capture, and calls no
+ * or device memory is budgeted up front).  It runs the block-tile FP32 register kernel
+ * of scrna_cle_run_device, optionally with population and capture, and calls no
  * cudaMalloc, cudaFree or other allocating routine: all working memory comes from
- * one array of about 16.0 MB that the library reserves on every GPU it is loaded on,
- * held until the process exits.  Limits per call: 65,536 cells, 512 genes and
- * 262,144 cell-genes; larger runs are rejected with SCRNA_EINVAL.
+ * one file-scope device array of about 16.0 MB, held until the process exits.
+ * Limits per call: 65,536 cells, 512 genes and 262,144 cell-genes; larger runs are
+ * rejected with SCRNA_EINVAL.  opts->path must be AUTO, REGISTER or BLOCK (others:
+ * SCRNA_ENOTSUP).
  *   d_out    device pointer, cells x G (x2 for SCRNA_READOUT_BOTH) float64, column-major
  *   d_counts device pointer, cells x G int32 (required with cap, else ignored)
  *   d_eff    device pointer, cells float64 (required with cap, else ignored)
- * The call only enqueues work on the context stream; synchronise before reading.
- * The first call on a device looks up the array's device address; make that first
- * call before any stream capture.  All calls share the one array: calls whose work
- * overlaps on the GPU (other streams or contexts on the same device) race and
- * corrupt each other's results. */
+ * The call only enqueues work on the context stream; synchronise before reading.  It
+ * leaves the calling thread's current device as it found it.
+ * First call per device: under CUDA's default lazy module loading, the array's memory
+ * is mapped on a device by the first call there (which looks up the array's device
+ * address and may synchronise the device).  Make that first call during set-up, before
+ * the caller can no longer allocate and before any stream capture.
+ * All calls share the one array, which keeps the last call's contents: calls whose work
+ * overlaps on the GPU (other streams or contexts on the same device) race and corrupt
+ * each other's results. */
 int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                const scrna_population* pop, const scrna_capture* cap,
                                const scrna_cle_opts* opts, double* d_out, int32_t* d_counts,
@@ -291,6 +300,9 @@ int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, 
  * unit (MUFU) pipe with two microkernels; results in operations per second. */
 int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma_ops_per_s, double* sfu_ops_per_s,
                              double* int_ops_per_s);
+/* Measures the throughput of the library's Philox4x32-10 generator (round keys from kernel
+ * parameters, as the CLE kernels use it) with a microkernel: generator calls per second. */
+int scrna_measure_philox_rate(scrna_ctx* ctx, double* calls_per_s);
 
 #ifdef __cplusplus
 }

@@ -5,20 +5,28 @@
 // framework's caching allocator or a fixed memory pool that forbids cudaMalloc),
 // code inside a latency-critical serving loop where cudaMalloc/cudaFree would
 // synchronise the device, or host programs embedding the library under a strict
-// device-memory budget decided at start-up.  This entry point runs the same fused
-// FP32 kernel as scrna_cle_run_device but takes all of its working memory from
-// one file-scope device array, reserved when the library is loaded.  The caller
-// passes the network (created earlier) and device pointers for the outputs.
+// device-memory budget decided at start-up.  This entry point runs the block-tile
+// FP32 register kernel of scrna_cle_run_device but takes all of its working memory
+// from one file-scope device array.  The caller passes the network (created
+// earlier) and device pointers for the outputs.
+//
+// The array belongs to this file's device-code module.  Under CUDA's default lazy
+// module loading that module, and the array's memory with it, is loaded onto a
+// device by the first call on that device (the call looks up the array's device
+// address), so the first call per device maps the array and may synchronise the
+// device; later calls allocate nothing.  Callers make that first call during their
+// set-up, before the point from which they cannot allocate.
 //
 // Limits: at most kMaxCells cells, kMaxGenes genes and kMaxCellGenes cell-genes
-// per call.  The array (kScratchBytes, about 16.0 MB) is held on every GPU that
-// loads the library until the process exits.
+// per call.  The array (kScratchBytes, about 16.0 MB) stays on every device it was
+// loaded on until the process exits.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "../../include/scrna_cle.h"
@@ -94,16 +102,36 @@ int scratch_for_device(int dev, unsigned char** out) {
     return SCRNA_OK;
 }
 
-// Host staging for the per-run gene tables (fixed size, no allocation).
-thread_local GeneRec t_genes[kMaxGenes];
-thread_local GeneInit t_ginit[kMaxGenes];
-thread_local uint8_t t_quad[kMaxGenes / 4];
+// Host staging for the per-run gene tables (fixed size, no allocation), laid out as
+// the tables sit in the scratch array from kOffGenes on.
+constexpr size_t kTablesBytes = kScratchBytes - kOffGenes;
+alignas(16) thread_local unsigned char t_tables[kTablesBytes];
+
+// The tables reach the device as the by-value parameter of a small copy kernel, one
+// chunk per launch: the launch copies its parameters, so no host memory is read later
+// and no copy engine call is made.
+constexpr uint32_t kStageChunk = 3968;
+struct StageChunk {
+    uint32_t offset;  // from kOffGenes
+    uint32_t bytes;
+    unsigned char data[kStageChunk];
+};
+
+__global__ void noalloc_stage_kernel(unsigned char* dst, const StageChunk c) {
+    for (uint32_t i = threadIdx.x; i < c.bytes; i += blockDim.x) dst[c.offset + i] = c.data[i];
+}
 
 int cuda_fail(const char* what, cudaError_t e) {
     char msg[256];
     snprintf(msg, sizeof msg, "%s failed: %s", what, cudaGetErrorString(e));
     return set_error(SCRNA_ECUDA, msg);
 }
+
+// Restores the caller's current device when the call returns.
+struct DeviceGuard {
+    int prev = -1;
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
 
 }  // namespace
 
@@ -117,6 +145,8 @@ extern "C" int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, 
     if (cap && (!d_counts || !d_eff)) return set_error(SCRNA_EINVAL, "capture needs d_counts and d_eff");
     if (o->precision != SCRNA_PRECISION_FP32)
         return set_error(SCRNA_ENOTSUP, "the scratch-free entry point runs the FP32 path only");
+    if (o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK)
+        return set_error(SCRNA_ENOTSUP, "the scratch-free entry point runs the block-tile register kernel only");
     const NetDev& d = net_dev(net);
     const int64_t N = pop ? pop->cell_num : o->cell_num;
     if (N <= 0) return set_error(SCRNA_EINVAL, "cell_num must be positive");
@@ -132,20 +162,32 @@ extern "C" int scrna_cle_simulate_noalloc(scrna_ctx* ctx, const scrna_net* net, 
     const int64_t n_steps = run_steps(o);
     if (n_steps >= (1ll << 31)) return set_error(SCRNA_EINVAL, "too many steps");
 
-    cudaError_t e = cudaSetDevice(ctx_device(ctx));
-    if (e != cudaSuccess) return cuda_fail("cudaSetDevice", e);
+    DeviceGuard guard;
+    cudaError_t e = cudaGetDevice(&guard.prev);
+    if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+    if ((e = cudaSetDevice(ctx_device(ctx))) != cudaSuccess) return cuda_fail("cudaSetDevice", e);
     unsigned char* s = nullptr;
     if (int r = scratch_for_device(ctx_device(ctx), &s)) return r;
     cudaStream_t st = ctx_stream(ctx);
 
-    gene_tables_host(net, kin, o->dt, t_genes, t_ginit, t_quad);
+    GeneRec* genes = reinterpret_cast<GeneRec*>(t_tables);
+    GeneInit* ginit = reinterpret_cast<GeneInit*>(t_tables + (kOffGinit - kOffGenes));
+    uint8_t* quad = t_tables + (kOffQuad - kOffGenes);
+    gene_tables_host(net, kin, o->dt, genes, ginit, quad);
     const int nq = (d.G + 3) / 4;
-    if ((e = cudaMemcpyAsync(s + kOffGenes, t_genes, sizeof(GeneRec) * d.G, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return cuda_fail("cudaMemcpyAsync(genes)", e);
-    if ((e = cudaMemcpyAsync(s + kOffGinit, t_ginit, sizeof(GeneInit) * d.G, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return cuda_fail("cudaMemcpyAsync(ginit)", e);
-    if ((e = cudaMemcpyAsync(s + kOffQuad, t_quad, nq, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return cuda_fail("cudaMemcpyAsync(quads)", e);
+    const size_t ranges[3][2] = {{0, sizeof(GeneRec) * d.G},
+                                 {kOffGinit - kOffGenes, sizeof(GeneInit) * d.G},
+                                 {kOffQuad - kOffGenes, (size_t)nq}};
+    for (const auto& r : ranges)
+        for (size_t off = r[0]; off < r[0] + r[1]; off += kStageChunk) {
+            StageChunk c;
+            c.offset = (uint32_t)off;
+            c.bytes = (uint32_t)std::min<size_t>(kStageChunk, r[0] + r[1] - off);
+            std::memcpy(c.data, t_tables + off, c.bytes);
+            noalloc_stage_kernel<<<1, 256, 0, st>>>(s + kOffGenes, c);
+            if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail("table staging launch", e);
+            ctx_add_launches(ctx, 1);
+        }
 
     FusedArgs a{};
     a.G = d.G; a.n_quads = d.n_quads; a.n_reg = d.n_reg; a.n_in = d.n_in; a.n_na = d.n_na; a.n_na_src = d.n_na_src;

@@ -58,6 +58,38 @@ def test_noalloc_matches_regular_entry_point_twice(pkg):
         assert np.array_equal(got_eff, want_eff)
 
 
+def test_noalloc_plain_run_after_population_runs(pkg):
+    """Without population or capture (one launch, readout of both species), twice in a row
+    after the population runs above: leftovers of earlier calls in the shared array do not
+    leak into the result.  The second call maps no device memory (the first may still load
+    the kernel's code module, which CUDA loads lazily at a kernel's first launch)."""
+    import torch
+    from scrna_b200 import api
+    ctx = pkg.default_context()
+    net = pkg.sample_network(9, seed=5, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    N, G = 777, net.G
+    handle = pkg.NetHandle(net, ctx)
+    opts = api._opts(pkg.CLE(0.01), T=2.0, cell_num=N, readout="both", seed=3, stream=2,
+                     precision="fp32", path="auto", n_steps=0, cell_offset=0)
+    want = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=2.0, readout="both", seed=3, stream=2, ctx=ctx)
+    dev = torch.device("cuda", ctx.device)
+    d_out = torch.empty(N * 2 * G, dtype=torch.float64, device=dev)
+    k = api._kin(kin)
+    torch.cuda.synchronize()
+    for i in range(2):
+        free0 = torch.cuda.mem_get_info(dev)[0]
+        rc = ctx.lib.scrna_cle_simulate_noalloc(ctx.h, handle.h, C.byref(k), None, None, C.byref(opts),
+                                                C.c_void_p(d_out.data_ptr()), None, None)
+        pkg._lib.check(rc)
+        ctx.synchronize()
+        if i == 1:
+            assert torch.cuda.mem_get_info(dev)[0] == free0
+        got = d_out.cpu().numpy().reshape(2 * G, N).T
+        err = np.max(np.abs(got - want) / np.maximum(np.abs(want), 1.0))
+        assert err <= RTOL, err
+
+
 def test_noalloc_rejects_oversized_runs(pkg):
     from scrna_b200 import api
     ctx = pkg.default_context()
@@ -72,3 +104,8 @@ def test_noalloc_rejects_oversized_runs(pkg):
                                             C.c_void_p(d_out.data_ptr()), None, None)
     assert rc == -1
     assert b"too large" in ctx.lib.scrna_last_error()
+    opts = api._opts(pkg.CLE(0.01), T=1.0, cell_num=100, readout="protein", seed=0, stream=0,
+                     precision="fp32", path="tensor", n_steps=0, cell_offset=0)
+    rc = ctx.lib.scrna_cle_simulate_noalloc(ctx.h, handle.h, C.byref(k), None, None, C.byref(opts),
+                                            C.c_void_p(d_out.data_ptr()), None, None)
+    assert rc == -6
