@@ -7,19 +7,26 @@ capture to an int32 count matrix.  Work unit: one cell-gene-step; one step is
 
   value      device-resident throughput (network tables already on the GPU), CUDA events
              on the library's stream around each run; L2 flushed between runs.
-  e2e        the same runs through the public host API (scrna_cle_simulate via
-             simulate(...)): network upload from host arrays, run, readout + counts +
-             efficiencies copied back to host, timed on the host clock.
-  roofline   special-function-unit (MUFU) issue bound of the register path: the
-             algorithmic 7 SFU operations per cell-gene-step against the SFU throughput
-             measured live by the library's microkernel.
+  e2e        the same runs through the public host API: every step uploads the network from
+             host arrays, runs, and copies readout + counts + efficiencies back to host
+             (pooled page-locked arrays), timed on the host clock; the bytes are the
+             library's own transfer counters.
+  roofline   the register path's three algorithmic bounds per cell-gene-step (special-function
+             ops, FP32 ops, integer ops of the Philox stream) against peaks measured live by
+             the library's microkernels; the bound is the largest of the three.
+  moment_err the largest per-gene mean / variance / Fano error (src/validate.jl:70-77
+             convention) of the GPU run against the FP64 CPU oracle on the same increments,
+             at the workload's full size.
   fp64_plain the plain FP64 one-kernel-per-step GPU CLE on the same workload.
-  cpu_baseline  the FP64 CPU oracle (a port of the reference's cle.jl) on a bounded
-             sample of the workload, all host threads.
+  cpu_baseline  the FP64 CPU oracle (a port of the reference's cle.jl) on the whole workload,
+             all host threads (the same run gives moment_err).
+  dense / batch / serve  the other workloads at N=1: dense regulation on the tensor-core
+             path, 256 uneven networks in one batch call, and the request server.
 
 --impl reference times that CPU restatement alone (the Julia reference cannot run here).
-Multi-GPU (torchrun): cells are sharded by global index (weak scaling, no collective on
-the data path); the elapsed time is the max over ranks.
+--gpus N without a torchrun environment starts N ranks itself.  Multi-GPU: cells are
+sharded by global index (weak scaling, no collective on the data path); the elapsed time
+is the max over ranks; per-gene moment sums are all-reduced once after the timed region.
 """
 from __future__ import annotations
 
@@ -27,6 +34,7 @@ import argparse
 import json
 import math
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -35,9 +43,13 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SFU_PER_UNIT = 7          # algorithmic special-function ops per cell-gene-step (n = 2)
 CELLS_PER_GPU = 20000
 L2_FLUSH_BYTES = 256 << 20
+# algorithmic work per cell-gene-step of the register path, Hill exponent 2
+SFU_PER_UNIT = 7            # Hill rcp, 2 sqrt, log + sin + cos of Box-Muller counted as 4 for two normals
+FP32_BASE_PER_UNIT = 24     # Hill, M and P updates, Box-Muller, telegraph (+ 2 per in-edge / term source)
+PHILOX_CALLS_PER_UNIT = 0.5  # two normals per cell-gene-step, four per Philox4x32-10 block
+INT_OPS_PER_PHILOX = 80     # 10 rounds x (2 mul.lo + 2 mul.hi + 4 xor)
 
 
 def _args():
@@ -47,18 +59,18 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="telegraph", choices=["telegraph", "dense", "batch", "serve"],
-                    help="telegraph: the headline workload; the others are reported in DESIGN.md")
+                    help="telegraph: the headline line (with the other workloads as extra keys at N=1); "
+                         "dense / batch / serve: that workload alone")
     ap.add_argument("--requests", type=int, default=60, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--batch-networks", type=int, default=256, help="batch: number of networks")
-    ap.add_argument("--dense-steps", type=int, default=0,
-                    help="dense: Euler steps per run (default: the workload's T/dt = 8,000)")
-    ap.add_argument("--cpu-sample-cells", type=int, default=20000)
-    ap.add_argument("--cpu-sample-steps", type=int, default=1000)
+    ap.add_argument("--dense-steps", type=int, default=200, help="dense: Euler steps per timed run")
     ap.add_argument("--ref-sample-steps", type=int, default=250)
+    ap.add_argument("--cpu-sample-cells", type=int, default=20000)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle leg (cpu_baseline, moment_err)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the dense / batch / serve keys")
     return ap.parse_args()
 
 
@@ -69,24 +81,57 @@ def _dist():
     return rank, world, local
 
 
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def spawn_ranks(n: int, script: str = __file__, argv=None) -> int:
+    """Run `script` (this file by default, with this call's arguments) under
+    torch.distributed.run, one rank per GPU; returns the launcher's exit status."""
+    argv = sys.argv[1:] if argv is None else list(argv)
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(script)] + argv
+    return subprocess.call(cmd)
+
+
+def check_world(gpus: int, world: int):
+    """The number of ranks running must be the number of GPUs asked for."""
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but {world} rank(s) are running")
+
+
+def max_over_ranks(x: float, world: int, device="cpu") -> float:
+    """Maximum of x over the process group (x itself for one rank)."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons while the GPU is busy."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=50):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.period_ms)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        return self
 
     def stop(self):
         if self.proc is None:
@@ -112,7 +157,7 @@ class ClockSampler:
 
 
 def _traffic_per_launch():
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary, if any."""
+    """DRAM bytes per launch of the lane kernel from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "cle_warpcell_telegraph_capture_G10_N20000.md")
     if not os.path.exists(path):
         return None
@@ -125,15 +170,52 @@ def _traffic_per_launch():
     return None
 
 
-def cpu_reference(pkg, wl, cells, steps, threads):
-    """FP64 CPU restatement of cle.jl on `cells` x `steps` of the workload; returns units/s."""
+def _measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained", d["bf16_tflops"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+def _fp32_per_unit(net) -> float:
+    """24 + 2 per additive in-edge + 2 per cooperative / redundant source, averaged over genes."""
+    import numpy as np
+    A = np.asarray(net.interactions) * np.asarray(net.basals)[:, None]
+    np.fill_diagonal(A, 0.0)
+    n_add = int(np.count_nonzero(A))
+    n_src = sum(len(e.sources) for e in list(net.cooperative) + list(net.redundant))
+    return FP32_BASE_PER_UNIT + 2.0 * (n_add + n_src) / net.G
+
+
+def roofline_terms(units, kernel_s, fp32_per_unit, peaks):
+    """The three algorithmic bounds of the register path; `peaks` = (fma/s, sfu/s, philox calls/s)."""
+    fma_s, sfu_s, philox_s = peaks
+    int_peak = philox_s * INT_OPS_PER_PHILOX
+    counts = {"sfu": SFU_PER_UNIT, "fp32": fp32_per_unit, "int": PHILOX_CALLS_PER_UNIT * INT_OPS_PER_PHILOX}
+    peak = {"sfu": sfu_s, "fp32": fma_s, "int": int_peak}
+    src = {"sfu": "rsqrt.approx microkernel, 148 SMs", "fp32": "FFMA microkernel, 148 SMs",
+           "int": "Philox4x32-10 microkernel (calls/s x 80 integer ops), round keys from parameters"}
+    terms = {}
+    for k in counts:
+        achieved = counts[k] * units / kernel_s
+        terms[k] = {"ops_per_unit": counts[k], "achieved_gops": achieved / 1e9, "peak_gops": peak[k] / 1e9,
+                    "frac": achieved / peak[k], "ps_per_unit_at_peak": 1e12 * counts[k] / peak[k],
+                    "peak_source": "measured live: " + src[k]}
+    bound = max(terms, key=lambda k: terms[k]["ps_per_unit_at_peak"])
+    return bound, terms
+
+
+def cpu_oracle_run(wl, cells, steps, threads, seed):
+    """FP64 CPU restatement of cle.jl on `cells` x `steps` of the workload: (units/s, s, result)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()
     t0 = time.perf_counter()
-    oracle.simulate(wl.net, wl.kin, dt=wl.dt, cell_num=cells, n_steps=steps, seed=123, nthreads=threads)
+    out = oracle.simulate(wl.net, wl.kin, dt=wl.dt, cell_num=cells, n_steps=steps, seed=seed, nthreads=threads)
     el = time.perf_counter() - t0
-    return cells * wl.net.G * steps / el, el
+    return cells * wl.net.G * steps / el, el, out
 
 
 def run_reference(args):
@@ -146,11 +228,10 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     cells, steps = args.cpu_sample_cells, args.ref_sample_steps
     for _ in range(max(args.warmup, 0)):
-        cpu_reference(pkg, wl, max(cells // 10, 100), max(steps // 10, 10), threads)
-    rates, els = [], []
+        cpu_oracle_run(wl, max(cells // 10, 100), max(steps // 10, 10), threads, 123)
+    els = []
     for _ in range(args.steps):
-        r, el = cpu_reference(pkg, wl, cells, steps, threads)
-        rates.append(r)
+        _, el, _ = cpu_oracle_run(wl, cells, steps, threads, 123)
         els.append(el)
     total_units = cells * wl.net.G * steps * args.steps
     value = total_units / sum(els)
@@ -168,8 +249,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _event_ms(fn, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
 def run_ours(args):
     rank, world, local = _dist()
+    check_world(args.gpus, world)
     import numpy as np
     import torch
     import __graft_entry__
@@ -178,17 +271,19 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     wl = pkg.config1()
     N = CELLS_PER_GPU
     G = wl.net.G
     n_steps = pkg.n_steps(wl.T, wl.dt)
     units = N * G * n_steps
+    seed = 2024
 
     ctx = pkg.Context(local)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout=wl.readout, seed=2024,
+    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout=wl.readout, seed=seed,
                         capture=wl.capture, cell_offset=rank * N, ctx=ctx)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -198,13 +293,11 @@ def run_ours(args):
             torch.distributed.barrier()
             torch.cuda.synchronize()
 
+    clocks = ClockSampler(local).start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             run.launch()
     barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
     launches0 = ctx.launches
     evs = []
     with torch.cuda.stream(stream):
@@ -217,68 +310,91 @@ def run_ours(args):
             e1.record(stream)
             evs.append((e0, e1))
     barrier()
+    clk = clocks.stop()
     launches = ctx.launches - launches0
     per = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(per)
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(per), world, f"cuda:{local}")
     value = units * world * args.steps / (total_ms * 1e-3)
     kernel_ms = statistics.mean(per)  # one fused launch per non-population run
 
-    # roofline: SFU issue bound, peak measured live by the library's microkernel
-    fma_s, sfu_s, int_s = pkg.measure_pipe_peaks(ctx)
-    achieved_sfu = SFU_PER_UNIT * units / (kernel_ms * 1e-3)
-    traffic = _traffic_per_launch()
+    # the per-gene moment sums of all ranks' cells, all-reduced once (FP64) after the timed region
+    from scrna_b200 import sharding
+    allreduce = None
+    if world > 1:
+        tot = sharding.allreduce_moments(sharding.moment_sums(run.read()[0]))
+        allreduce = {"backend": "nccl", "doubles": int(tot.size), "cells": int(round(tot[0, 0]))}
+
+    # roofline: the register path's three bounds, peaks measured live by the library
+    fma_s, sfu_s, _ = pkg.measure_pipe_peaks(ctx)
+    philox_s = pkg.measure_philox_rate(ctx)
+    bound, terms = roofline_terms(units, kernel_ms * 1e-3, _fp32_per_unit(wl.net), (fma_s, sfu_s, philox_s))
+    roof = {"bound": bound, "achieved": terms[bound]["achieved_gops"], "peak": terms[bound]["peak_gops"],
+            "unit": "Gop/s", "frac": terms[bound]["frac"], "traffic": _traffic_per_launch(),
+            "kernel_ms": kernel_ms, "terms": terms,
+            "note": "bound = the term with the longest time per cell-gene-step at its measured peak"}
 
     # FP64 plain one-kernel-per-step baseline on the same workload
     fp64 = None
     if not args.no_fp64:
         run64 = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout=wl.readout,
-                              seed=2024, capture=wl.capture, precision="fp64_plain", cell_offset=rank * N,
+                              seed=seed, capture=wl.capture, precision="fp64_plain", cell_offset=rank * N,
                               ctx=ctx)
         with torch.cuda.stream(stream):
             run64.launch()
             torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
             reps = 2
-            e0.record(stream)
-            for _ in range(reps):
-                run64.launch()
-            e1.record(stream)
-        torch.cuda.synchronize()
-        ms64 = e0.elapsed_time(e1) / reps
+            ms64 = _event_ms(lambda: [run64.launch() for _ in range(reps)], stream) / reps
         fp64 = {"value": units / (ms64 * 1e-3), "ms_per_step": ms64, "unit": "cell·gene·steps/s",
                 "launches_per_step": n_steps + 4}
         run64.close()
 
-    # e2e through the public host API (host arrays in, host arrays out)
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
-    h2d = d2h = 0
-    t0 = time.perf_counter()
-    for i in range(1 + e2e_steps if e2e_steps else 0):
-        if i == 1:
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-        X, counts, eff = pkg.simulate(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout=wl.readout,
-                                      seed=2024, capture=wl.capture, cell_offset=rank * N, ctx=ctx)
-        d2h = X.nbytes + counts.nbytes + eff.nbytes
-    e2e_s = time.perf_counter() - t0
-    net = wl.net
-    h2d = (net.basals.nbytes + net.interactions.nbytes + net.k_on.nbytes + net.k_off.nbytes
-           + 16 * (len(net.cooperative) + len(net.redundant)) + 48 * G)
-    e2e_value = units * world * e2e_steps / e2e_s if e2e_steps else None
+    # e2e through the public host API: network upload, run, results to host, every step
+    e2e = None
+    if not args.no_e2e:
+        e2e_steps = max(3, min(args.steps, 10))
 
-    cpu = None
-    if rank == 0 and not args.no_cpu:
+        def e2e_step():
+            h = pkg.NetHandle(wl.net, ctx)
+            out = pkg.simulate(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout=wl.readout,
+                               seed=seed, capture=wl.capture, cell_offset=rank * N, ctx=ctx, handle=h)
+            h.close()
+            return out
+
+        e2e_step()
+        barrier()
+        b0 = ctx.transfer_bytes()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world, f"cuda:{local}")
+        b1 = ctx.transfer_bytes()
+        e2e = {"value": units * world * e2e_steps / e2e_s, "unit": "cell·gene·steps/s",
+               "h2d_bytes_per_step": (b1[0] - b0[0]) // e2e_steps, "d2h_bytes_per_step": (b1[1] - b0[1]) // e2e_steps,
+               "note": "per step: network upload from host arrays, run, readout + counts + efficiencies to host"}
+        barrier()
+
+    # CPU oracle on the whole workload: the CPU baseline and the moment-error check in one run
+    cpu = moment = None
+    if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cpu_rate, cpu_el = cpu_reference(pkg, wl, args.cpu_sample_cells, args.cpu_sample_steps, threads)
-        cpu = {"value": cpu_rate, "unit": "cell·gene·steps/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_sample_cells} cells x {args.cpu_sample_steps} Euler steps x {G} genes "
-                         f"({cpu_el:.1f} s)"}
+        Xg = pkg.simulate(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=wl.T, readout="both", seed=seed, ctx=ctx)
+        rate, el, ref = cpu_oracle_run(wl, N, n_steps, threads, seed)
+        Xr = np.hstack([ref["M"].T, ref["P"].T])
+        errs = pkg.moment_errors(Xg, Xr)
+        cpu = {"value": rate, "unit": "cell·gene·steps/s", "cores": threads, "kind": "port",
+               "sample": f"the whole workload: {N} cells x {n_steps} Euler steps x {G} genes ({el:.1f} s)"}
+        moment = {"max": max(float(v.max()) for v in errs.values()),
+                  **{k: float(v.max()) for k, v in errs.items()},
+                  "against": "FP64 CPU oracle, same Philox increments, mRNA and protein of every gene",
+                  "convention": "|a-b|/max(|a|,|b|,1e-10) (src/validate.jl:70-77)"}
+
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_extra:
+        for name, fn in (("dense", leg_dense), ("batch", leg_batch), ("serve", leg_serve)):
+            try:
+                extra[name] = fn(pkg, args, local)
+            except Exception as e:  # a failed leg is reported, never silently dropped
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
@@ -290,19 +406,18 @@ def run_ours(args):
                        "dt": wl.dt, "T": wl.T, "telegraph": True, "capture": "lognormal-binomial int32",
                        "units_per_step": units * world, "l2": "flushed (256 MB write) between timed runs",
                        "parallelism": f"cells sharded over {world} GPU(s)"},
-            "roofline": {"bound": "sfu", "achieved": achieved_sfu / 1e9, "peak": sfu_s / 1e9,
-                         "unit": "Gop/s (MUFU)", "frac": achieved_sfu / sfu_s, "traffic": traffic,
-                         "kernel_ms": kernel_ms, "algorithmic_sfu_per_unit": SFU_PER_UNIT,
-                         "peak_source": "measured live (rsqrt.approx microkernel, 148 SMs)",
-                         "fp32_fma_peak_gops": fma_s / 1e9, "int_peak_gops": int_s / 1e9},
+            "moment_err": moment,
+            "roofline": roof,
             "fp64_plain": fp64,
             "speedup_vs_fp64_plain": (value / world) / fp64["value"] if fp64 else None,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "cell·gene·steps/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+            "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if allreduce:
+            line["moment_allreduce"] = allreduce
+        line.update(extra)
         print(json.dumps(line), flush=True)
     run.close()
     if world > 1:
@@ -310,92 +425,81 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
-def _event_time(fn, stream):
+def leg_dense(pkg, args, device):
+    """Dense regulation, G=2000, 65,536 cells, dt=0.005: the fused tcgen05 path, per Euler step."""
     import torch
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) * 1e-3
-
-
-def run_dense(args):
-    """Dense regulation, G=2000, 65,536 cells, dt=0.005, T=40 (8,000 steps): tensor-core path."""
-    import torch
-    import __graft_entry__
-    pkg = __graft_entry__.load_package()
     wl = pkg.config2()
-    ctx = pkg.Context(0)
+    ctx = pkg.Context(device)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    n_steps = args.dense_steps if args.dense_steps > 0 else pkg.n_steps(wl.T, wl.dt)
+    steps = args.dense_steps
     G, N = wl.net.G, wl.cell_num
-    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=0.0, n_steps=n_steps, readout="protein",
+    run = pkg.DeviceRun(wl.net, pkg.CLE(wl.dt), wl.kin, cell_num=N, T=0.0, n_steps=steps, readout="protein",
                         seed=7, ctx=ctx)
     run.launch()
     torch.cuda.synchronize()
-    el = [_event_time(run.launch, stream) for _ in range(max(1, args.steps))]
+    clocks = ClockSampler(device).start()
+    el = [_event_ms(run.launch, stream) * 1e-3 for _ in range(3)]
+    clk = clocks.stop()
     per = sum(el) / len(el)
-    units = G * N * n_steps
+    units = G * N * steps
     K = G + len(wl.net.cooperative) + len(wl.net.redundant)  # gene columns + one column per term
-    flops = 2.0 * G * K * N * n_steps
+    flops = 2.0 * G * K * N * steps
     algo_bytes = 18.0 * units  # M, P read + write (FP32), 16-bit activations written
-    peaks = _measured_peaks()
-    line = {"workload": wl.name, "value": units / per, "unit": "cell·gene·steps/s", "s_per_run": per,
-            "euler_steps": n_steps, "gemm_tflops": flops / per / 1e12, "tensor_frac": flops / per / 1e12 / peaks["bf16_tflops"],
-            "hbm_gbs_algorithmic": algo_bytes / per / 1e9, "hbm_frac": algo_bytes / per / 1e9 / peaks["hbm_gbs"],
-            "peaks": peaks}
-    print(json.dumps(line), flush=True)
+    pk = _measured_peaks()
+    out = {"workload": wl.name, "value": units / per, "unit": "cell·gene·steps/s", "ms_per_euler_step": 1e3 * per / steps,
+           "euler_steps": steps, "gemm_tflops": flops / per / 1e12,
+           "tensor_frac_of_sustained": flops / per / 1e12 / pk["bf16_tflops_sustained"],
+           "hbm_gbs_algorithmic": algo_bytes / per / 1e9, "hbm_frac": algo_bytes / per / 1e9 / pk["hbm_gbs"],
+           "bound_frac": max(flops / per / 1e12 / pk["bf16_tflops_sustained"], algo_bytes / per / 1e9 / pk["hbm_gbs"]),
+           "peaks_source": pk["source"], "dtype": "bf16 contraction inputs, f32 state", "clocks": clk}
+    run.close()
+    ctx.close()
+    return out
 
 
-def _measured_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(path):
-        d = json.load(open(path))
-        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
-    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
-
-
-def run_batch_workload(args):
-    """256 networks, G ~ LogUniform(5, 500), cells ~ LogUniform(1k, 50k), half with a Moran
-    population, dt=0.01, T=50: one simulate_gpu_batch call (persistent launches per group)."""
-    import __graft_entry__
-    pkg = __graft_entry__.load_package()
+def leg_batch(pkg, args, device):
+    """256 networks, G ~ LogUniform(5, 500), cells ~ LogUniform(1k, 50k), half with a Moran population,
+    dt=0.01, T=50: one simulate_gpu_batch call (persistent launches per kernel group)."""
+    import torch
     wls = pkg.config3(n_networks=args.batch_networks)
     nets = [w.net for w in wls]
     cells = [w.cell_num for w in wls]
     pops = [w.population for w in wls]
     units = sum(w.net.G * w.cell_num * pkg.n_steps(w.T, w.dt) for w in wls)
-    kin = wls[0].kin
+    ctx = pkg.Context(device)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    call = lambda: pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), wls[0].kin, cell_num=cells, T=50.0,
+                                          populations=pops, seed=1, ctx=ctx)
     t0 = time.perf_counter()
-    pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=50.0, populations=pops, seed=1)
-    warm = time.perf_counter() - t0
-    els = []
-    for _ in range(max(1, args.steps)):
-        t0 = time.perf_counter()
-        pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=50.0, populations=pops, seed=1)
-        els.append(time.perf_counter() - t0)
-    per = sum(els) / len(els)
-    print(json.dumps({"workload": "batch-%d-uneven" % len(wls), "value": units / per, "unit": "cell·gene·steps/s",
-                      "s_per_run": per, "first_run_s": warm, "units_per_run": units,
-                      "networks_with_population": sum(p is not None for p in pops),
-                      "note": "host wall clock around the whole batch call, results copied to host"}), flush=True)
+    call()
+    first = time.perf_counter() - t0
+    clocks = ClockSampler(device).start()
+    t0 = time.perf_counter()
+    dev_ms = _event_ms(call, stream)
+    host_s = time.perf_counter() - t0
+    clk = clocks.stop()
+    ctx.close()
+    return {"workload": f"batch-{len(wls)}-uneven", "value": units / (dev_ms * 1e-3), "unit": "cell·gene·steps/s",
+            "e2e_value": units / host_s, "s_per_call_device": dev_ms * 1e-3, "s_per_call_host": host_s,
+            "first_call_s": first, "units_per_call": units,
+            "networks_with_population": sum(p is not None for p in pops),
+            "note": "device: CUDA events on the call's stream (results copied to host inside); "
+                    "e2e: host clock around the whole call", "clocks": clk}
 
 
-def run_serve(args):
+def leg_serve(pkg, args, device):
     """Poisson request stream (rate --rate), G ~ LogUniform(5, 500), cells ~ LogUniform(1k, 100k),
     T ~ U(20, 60) h, bursty / constitutive mix, capture on: continuous-batching server."""
     import threading
     import numpy as np
-    import __graft_entry__
-    pkg = __graft_entry__.load_package()
     reqs = pkg.config4_requests(n_requests=args.requests, rate_per_s=args.rate)
-    ctx = pkg.default_context()
+    ctx = pkg.Context(device)
     handles = [pkg.NetHandle(w.net, ctx) for _, w in reqs]
     srv = pkg.Server(ctx, chunk_steps=500)
     tickets = [None] * len(reqs)
+    clocks = ClockSampler(device, period_ms=200).start()
     t_start = time.perf_counter()
 
     def submitter():
@@ -415,28 +519,36 @@ def run_serve(args):
         lats.append(srv.wait(tickets[i], -1)[3])
     th.join()
     makespan = time.perf_counter() - t_start
+    clk = clocks.stop()
     st = srv.stats()
     srv.close()
+    ctx.close()
     units = st["units_done"]
     offered = sum(w.net.G * w.cell_num * pkg.n_steps(w.T, w.dt) for _, w in reqs) / reqs[-1][0]
-    print(json.dumps({"workload": "serve-poisson", "requests": len(reqs), "rate_per_s": args.rate,
-                      "value": units / makespan, "unit": "cell·gene·steps/s", "p50_latency_s": float(np.percentile(lats, 50)),
-                      "p99_latency_s": float(np.percentile(lats, 99)), "makespan_s": makespan,
-                      "busy_s": st["busy_s"], "offered_load": offered,
-                      "max_stable_rate_per_s": (units / st["busy_s"]) / (units / len(reqs)) if st["busy_s"] > 0 else None,
-                      "chunks": st["chunks"]}), flush=True)
+    return {"workload": "serve-poisson", "requests": len(reqs), "rate_per_s": args.rate,
+            "value": units / makespan, "unit": "cell·gene·steps/s",
+            "p50_latency_s": float(np.percentile(lats, 50)), "p99_latency_s": float(np.percentile(lats, 99)),
+            "makespan_s": makespan, "busy_s": st["busy_s"], "offered_load": offered,
+            "sustainable_rate_per_s": (len(reqs) / st["busy_s"]) if st["busy_s"] > 0 else None,
+            "chunks": st["chunks"], "clocks": clk}
+
+
+def run_single_leg(args):
+    import json as _json
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    fn = {"dense": leg_dense, "batch": leg_batch, "serve": leg_serve}[args.workload]
+    print(_json.dumps(fn(pkg, args, 0)), flush=True)
 
 
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "dense":
-        run_dense(args)
-    elif args.workload == "batch":
-        run_batch_workload(args)
-    elif args.workload == "serve":
-        run_serve(args)
+    elif args.workload != "telegraph":
+        run_single_leg(args)
+    elif args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     else:
         run_ours(args)
 

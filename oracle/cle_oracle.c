@@ -219,6 +219,16 @@ typedef struct {
     int G;
     double* Apos;  /* [G*G] row-major, precompute_hill_matrices (network.jl:206-219) */
     double* Aneg;
+    /* Nonzero columns of each row of Apos / Aneg, ascending: row i's are
+     * pos_col[pos_ptr[i] .. pos_ptr[i+1]-1].  The row sums run over these only; the
+     * skipped terms are +0 * finite >= 0 = +0 and s + (+0) = s for the nonnegative partial
+     * sums, so the result is bit-identical to the dense loop of cle.jl:84-86. */
+    int32_t* pos_ptr;
+    int32_t* pos_col;
+    double* pos_val;
+    int32_t* neg_ptr;
+    int32_t* neg_col;
+    double* neg_val;
     float* inv_on;      /* 1 / log2(stay probability OFF) = -ln2 / (k_on dt) */
     float* inv_off;     /* 1 / log2(stay probability ON)  = -ln2 / (k_off dt) */
     uint32_t* thr_init;
@@ -239,6 +249,34 @@ static void prep_build(const orc_net* net, double dt, prep_t* pp) {
             pp->Apos[(size_t)i * G + j] = a > 0.0 ? a : 0.0;
             pp->Aneg[(size_t)i * G + j] = -a > 0.0 ? -a : 0.0;
         }
+    pp->pos_ptr = (int32_t*)calloc((size_t)G + 1, 4);
+    pp->neg_ptr = (int32_t*)calloc((size_t)G + 1, 4);
+    size_t npos = 0, nneg = 0;
+    for (size_t k = 0; k < (size_t)G * G; ++k) {
+        npos += pp->Apos[k] != 0.0;
+        nneg += pp->Aneg[k] != 0.0;
+    }
+    pp->pos_col = (int32_t*)malloc((npos ? npos : 1) * 4);
+    pp->neg_col = (int32_t*)malloc((nneg ? nneg : 1) * 4);
+    pp->pos_val = (double*)malloc((npos ? npos : 1) * sizeof(double));
+    pp->neg_val = (double*)malloc((nneg ? nneg : 1) * sizeof(double));
+    npos = nneg = 0;
+    for (int i = 0; i < G; ++i) {
+        pp->pos_ptr[i] = (int32_t)npos;
+        pp->neg_ptr[i] = (int32_t)nneg;
+        for (int j = 0; j < G; ++j) {
+            if (pp->Apos[(size_t)i * G + j] != 0.0) {
+                pp->pos_col[npos] = j;
+                pp->pos_val[npos++] = pp->Apos[(size_t)i * G + j];
+            }
+            if (pp->Aneg[(size_t)i * G + j] != 0.0) {
+                pp->neg_col[nneg] = j;
+                pp->neg_val[nneg++] = pp->Aneg[(size_t)i * G + j];
+            }
+        }
+    }
+    pp->pos_ptr[G] = (int32_t)npos;
+    pp->neg_ptr[G] = (int32_t)nneg;
     pp->inv_on = (float*)calloc(G, 4);
     pp->inv_off = (float*)calloc(G, 4);
     pp->thr_init = (uint32_t*)calloc(G, 4);
@@ -257,7 +295,8 @@ static void prep_build(const orc_net* net, double dt, prep_t* pp) {
 }
 
 static void prep_free(prep_t* pp) {
-    free(pp->Apos); free(pp->Aneg); free(pp->inv_on); free(pp->inv_off);
+    free(pp->Apos); free(pp->Aneg); free(pp->pos_ptr); free(pp->pos_col); free(pp->pos_val);
+    free(pp->neg_ptr); free(pp->neg_col); free(pp->neg_val); free(pp->inv_on); free(pp->inv_off);
     free(pp->thr_init); free(pp->tel); free(pp->init_rand);
 }
 
@@ -293,13 +332,11 @@ static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, ui
         act[g] = pn / den;
         rep[g] = cf->Kn / den;
     }
-    /* reg = A_pos*act + A_neg*rep (cle.jl:84-86) */
+    /* reg = A_pos*act + A_neg*rep (cle.jl:84-86), over the nonzero columns of each row */
     for (int i = 0; i < G; ++i) {
         double s1 = 0.0, s2 = 0.0;
-        const double* ap = pp->Apos + (size_t)i * G;
-        const double* an = pp->Aneg + (size_t)i * G;
-        for (int j = 0; j < G; ++j) s1 = s1 + ap[j] * act[j];
-        for (int j = 0; j < G; ++j) s2 = s2 + an[j] * rep[j];
+        for (int k = pp->pos_ptr[i]; k < pp->pos_ptr[i + 1]; ++k) s1 = s1 + pp->pos_val[k] * act[pp->pos_col[k]];
+        for (int k = pp->neg_ptr[i]; k < pp->neg_ptr[i + 1]; ++k) s2 = s2 + pp->neg_val[k] * rep[pp->neg_col[k]];
         reg[i] = s1 + s2;
     }
     /* cooperative / redundant corrections (cle.jl:89-106) */

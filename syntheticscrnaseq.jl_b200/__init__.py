@@ -12,14 +12,16 @@ from .model import (CLE, INF, CaptureModel, CoopEdge, GeneNetwork, KineticParams
 from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
                       dense_network, sample_network)
 from .api import (Context, DeviceRun, NetHandle, Server, apply_capture, debug_philox, default_context,
-                  measure_pipe_peaks, simulate, simulate_gpu_batch)
+                  measure_philox_rate, measure_pipe_peaks, simulate, simulate_gpu_batch)
 from ._lib import ScrnaError
+from .validate import column_moments, compare_moments, max_moment_error, moment_errors
 
 __all__ = [
     "CLE", "CaptureModel", "CoopEdge", "GeneNetwork", "KineticParams", "PopulationConfig", "RedunEdge",
     "default_algorithm", "hill_activation", "hill_repression", "is_bursty", "n_steps",
     "precompute_hill_matrices", "steady_state", "sample_network", "dense_network", "config0", "config1",
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
-    "NetHandle", "Server", "apply_capture", "debug_philox", "default_context", "measure_pipe_peaks", "simulate",
-    "simulate_gpu_batch", "ScrnaError", "INF",
+    "NetHandle", "Server", "apply_capture", "debug_philox", "default_context", "measure_philox_rate", "measure_pipe_peaks", "simulate",
+    "simulate_gpu_batch", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
+    "moment_errors",
 ]

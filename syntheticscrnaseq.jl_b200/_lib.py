@@ -70,6 +70,7 @@ SIGNATURES = {
     "scrna_ctx_set_stream": (C.c_int, [P, P]),
     "scrna_ctx_synchronize": (C.c_int, [P]),
     "scrna_ctx_launch_count": (C.c_int64, [P]),
+    "scrna_ctx_transfer_bytes": (C.c_int, [P, C.POINTER(I64), C.POINTER(I64)]),
     "scrna_net_create": (C.c_int, [P, I32, P, P, I32, P, P, P, P, I32, P, P, P, P, P, P, I32,
                                    C.POINTER(P)]),
     "scrna_net_destroy": (C.c_int, [P]),
@@ -94,6 +95,7 @@ SIGNATURES = {
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_debug_tc_gemm": (C.c_int, [P, P, P, P, I64, I32, I32, I32]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),
+    "scrna_measure_philox_rate": (C.c_int, [P, C.POINTER(DBL)]),
     "scrna_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
     "scrna_host_free": (C.c_int, [P]),
 }

@@ -48,6 +48,12 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.scrna_ctx_launch_count(self.h))
 
+    def transfer_bytes(self):
+        """(host->device, device->host) bytes this context's calls have copied so far."""
+        h2d, d2h = C.c_int64(), C.c_int64()
+        check(self.lib.scrna_ctx_transfer_bytes(self.h, C.byref(h2d), C.byref(d2h)))
+        return int(h2d.value), int(d2h.value)
+
     def close(self):
         if getattr(self, "h", None):
             for nh in self.__dict__.pop("_net_cache", {}).values():  # networks before the context
@@ -361,6 +367,14 @@ def debug_philox(ctr: np.ndarray, key, ctx: Optional[Context] = None) -> np.ndar
     out = np.zeros_like(c)
     check(ctx.lib.scrna_debug_philox(ctx.h, c.shape[0], c.ctypes.data, k.ctypes.data, out.ctypes.data))
     return out
+
+
+def measure_philox_rate(ctx: Optional[Context] = None) -> float:
+    """Philox4x32-10 generator calls per second, measured by the library's microkernel."""
+    ctx = ctx or default_context()
+    r = C.c_double()
+    check(ctx.lib.scrna_measure_philox_rate(ctx.h, C.byref(r)))
+    return r.value
 
 
 def measure_pipe_peaks(ctx: Optional[Context] = None):

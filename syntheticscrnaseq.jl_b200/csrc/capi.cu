@@ -37,6 +37,7 @@ cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* 
 cudaError_t philox_check_launch(int n, const uint32_t* d_ctr, uint32_t k0, uint32_t k1,
                                 uint32_t* d_out, cudaStream_t st);
 cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStream_t st);
+cudaError_t peak_philox_launch(int blocks, int iters, float* sink, cudaStream_t st);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype);
 }  // namespace scrna
@@ -130,6 +131,13 @@ extern "C" int scrna_ctx_synchronize(scrna_ctx* ctx) {
 }
 
 extern "C" int64_t scrna_ctx_launch_count(const scrna_ctx* ctx) { return ctx ? ctx->launches.load() : -1; }
+
+extern "C" int scrna_ctx_transfer_bytes(const scrna_ctx* ctx, int64_t* h2d, int64_t* d2h) {
+    if (!ctx) return fail(SCRNA_EINVAL, "context is NULL");
+    if (h2d) *h2d = ctx->h2d_bytes.load();
+    if (d2h) *d2h = ctx->d2h_bytes.load();
+    return SCRNA_OK;
+}
 
 // ---- networks ---------------------------------------------------------------------------------
 static int build_edges(scrna_net* n, int32_t n_e, const int32_t* tgt, const int32_t* ptr,
@@ -255,6 +263,7 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
         cudaError_t e = b.ensure(bytes);
         if (e != cudaSuccess) return e;
+        ctx->h2d_bytes += (int64_t)bytes;
         if (bytes) return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
         return cudaSuccess;
     };
@@ -385,6 +394,7 @@ int scrna::ensure_gene_tables(scrna_net* n, const scrna_kinetics* kin, double dt
     CU(cudaMemcpy(n->b_genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(n->b_ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(n->b_quad_tel.p, qt.data(), nq, cudaMemcpyHostToDevice));
+    n->ctx->h2d_bytes += (int64_t)(G * (sizeof(GeneRec) + sizeof(GeneInit)) + nq);
     n->cache_valid = true;
     n->c_dt = dt;
     n->c_pop = pop;
@@ -722,6 +732,7 @@ extern "C" int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, in
     if (counts) CU(cudaMemcpyAsync(counts, st->counts.p, gn * 4, cudaMemcpyDeviceToHost, ctx->stream));
     if (eff) CU(cudaMemcpyAsync(eff, st->eff.p, (size_t)st->N * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h_bytes += (int64_t)((out ? gn * outcols * 8 : 0) + (counts ? gn * 4 : 0) + (eff ? (size_t)st->N * 8 : 0));
     return SCRNA_OK;
 }
 
@@ -907,6 +918,30 @@ extern "C" int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma, double* sfu
     if (fma) *fma = res[0];
     if (sfu) *sfu = res[1];
     if (iops) *iops = res[2];
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_measure_philox_rate(scrna_ctx* ctx, double* calls_per_s) {
+    if (int r = check_ctx(ctx)) return r;
+    if (!calls_per_s) return fail(SCRNA_EINVAL, "calls_per_s is NULL");
+    if (int r = set_device(ctx)) return r;
+    DevBuf sink;
+    CU(sink.ensure(256 * 4));
+    const int blocks = ctx->sm_count * 8, iters = 2048;
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    CU(peak_philox_launch(blocks, iters / 8, sink.as<float>(), ctx->stream));  // warm-up
+    CU(cudaEventRecord(e0, ctx->stream));
+    CU(peak_philox_launch(blocks, iters, sink.as<float>(), ctx->stream));
+    CU(cudaEventRecord(e1, ctx->stream));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->launches += 2;
+    *calls_per_s = (double)blocks * 256.0 * 4.0 * iters / (ms * 1e-3);
     return SCRNA_OK;
 }
 

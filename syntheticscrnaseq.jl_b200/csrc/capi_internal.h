@@ -52,6 +52,9 @@ struct scrna_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::atomic<int64_t> launches{0};
+    // bytes the library copied host -> device and device -> host for this context's networks,
+    // per-run tables and results (scrna_ctx_transfer_bytes)
+    std::atomic<int64_t> h2d_bytes{0}, d2h_bytes{0};
     int sm_count = 0;
     // states reused by the synchronous simulate calls (most recent last)
     std::vector<scrna_state*> state_cache;

@@ -253,6 +253,33 @@ __global__ void __launch_bounds__(256) peak_int_kernel(int iters, uint32_t seed,
     if (acc == 0x12345u) sink[threadIdx.x] = (float)acc;
 }
 
+// Philox4x32-10 throughput: four independent generator chains per thread (each block's
+// output is the next counter), round keys from the kernel parameters as in the CLE kernels.
+__global__ void __launch_bounds__(256) peak_philox_kernel(int iters, const KeySchedule ks, float* sink) {
+    uint4 c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = make_uint4(blockIdx.x, threadIdx.x, k, 0x01000000u);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[k] = philox_rk(c[k].x, c[k].y, c[k].z, c[k].w, ks.rk0, ks.rk1);
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc ^= c[k].x ^ c[k].y ^ c[k].z ^ c[k].w;
+    if (acc == 0x12345u) sink[threadIdx.x] = (float)acc;
+}
+
+// Philox4x32-10 calls executed per thread: 4 * iters.
+cudaError_t peak_philox_launch(int blocks, int iters, float* sink, cudaStream_t st) {
+    KeySchedule ks{};
+    for (int r = 0; r < 10; ++r) {
+        ks.rk0[r] = 0x243F6A88u + (uint32_t)r * 0x9E3779B9u;
+        ks.rk1[r] = 0x85A308D3u + (uint32_t)r * 0xBB67AE85u;
+    }
+    peak_philox_kernel<<<blocks, 256, 0, st>>>(iters, ks, sink);
+    return cudaGetLastError();
+}
+
 // ops executed per thread per iteration: 16 * 8
 cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStream_t st) {
     if (which == 0) peak_fma_kernel<<<blocks, 256, 0, st>>>(iters, 1.0f, sink);

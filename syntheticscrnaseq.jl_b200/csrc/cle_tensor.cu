@@ -366,6 +366,7 @@ int tensor_prepare_net(scrna_net* n, int dtype) {
     if (!na_src.empty()) CU(cudaMemcpy(n->t_na_src.p, na_src.data(), na_src.size() * 4, cudaMemcpyHostToDevice));
     CU(n->t_src_of_gene.ensure((size_t)G * 4));
     CU(cudaMemcpy(n->t_src_of_gene.p, src_of_gene.data(), (size_t)G * 4, cudaMemcpyHostToDevice));
+    n->ctx->h2d_bytes += (int64_t)(w.size() * 4 + na_src.size() * 4 + (size_t)G * 4);
     n->t_kp = Kp;
     n->t_n_src = (int)src_gene.size();
     n->t_dtype = dtype;
