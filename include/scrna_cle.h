@@ -200,6 +200,39 @@ int scrna_state_device_ptrs(scrna_state* st, void** d_mrna, void** d_protein);
 int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* protein,
                          uint8_t* promoter, double* volume);
 
+/* ---- autotuning ---------------------------------------------------------------------
+ * No counterpart in the reference.  The register path has several kernel variants that
+ * compute the same sums in the same order (block tiles; the lane kernel with 2 or 4 genes
+ * per lane and 2, 4 or 8 warps per block), so they give bit-identical results and differ
+ * only in speed.  With autotuning on (the default; environment SCRNA_AUTOTUNE=0/1/2 sets a
+ * new context's mode), the first run of a network shape (device, G, in-edges per gene,
+ * cooperative/redundant terms, telegraph genes, Hill exponent 2, power-of-two bucket of the
+ * cell count) measures the variants for a few steps and keeps the fastest in memory and in
+ * a JSON cache file (SCRNA_AUTOTUNE_CACHE, else $XDG_CACHE_HOME or ~/.cache
+ * /scrna_b200/autotune.json), which later runs and processes read.  Applies to the AUTO,
+ * REGISTER and WARP paths of scrna_cle_simulate, scrna_cle_run_device (a measurement there
+ * waits for the device), the batch call and the server. */
+typedef struct {
+    int32_t kernel;          /* 0 block tiles, 1 lane kernel */
+    int32_t genes_per_lane;  /* lane kernel: 2 or 4 */
+    int32_t block_warps;     /* lane kernel with cells within one warp: 2, 4 or 8 (0: default) */
+    int32_t found;           /* lookups: 1 if the key was in the cache */
+    double us_per_step;      /* measured time of one Euler step of the whole run */
+} scrna_tune_choice;
+
+/* mode 0: static choice; 1: cached or measured choice; 2: cached choice only, no measurement.
+ * cache_path NULL keeps the current file; "" keeps choices in memory only. */
+int scrna_ctx_set_autotune(scrna_ctx* ctx, int32_t mode, const char* cache_path);
+/* The kernel variant the context's last register-path run used (found = 1 if tuned). */
+int scrna_autotune_last_choice(const scrna_ctx* ctx, scrna_tune_choice* out);
+/* Cache key of a network shape ("<device>|G..|e..|t..|b..|h..|N.."); device as "sm100x148". */
+int scrna_autotune_key(const char* device, int32_t G, int32_t in_edges, int32_t n_terms, int32_t bursty,
+                       int32_t hill2, int64_t cell_num, char* out, int32_t out_len);
+/* Cache file access (host only, no device needed): lookup sets out->found; store adds or
+ * replaces one entry, keeping the entries other processes wrote, by an atomic rename. */
+int scrna_autotune_cache_lookup(const char* path, const char* key, scrna_tune_choice* out);
+int scrna_autotune_cache_store(const char* path, const char* key, const scrna_tune_choice* choice);
+
 /* ---- serving loop ---------------------------------------------------------------------
  * A request server with continuous batching (no counterpart in the reference, which runs
  * one simulate call at a time).  Submitted requests wait in a FIFO queue until their device
@@ -296,6 +329,13 @@ int scrna_debug_philox(scrna_ctx* ctx, int32_t n, const uint32_t* ctr, const uin
  * reference: it checks the tensor-core kernel against another GEMM. */
 int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
                         int32_t K, int32_t dtype);
+/* The same GEMM with its TMA producer stopping before its load number `withhold` (>= 0) in
+ * every CTA, so the MMA issuer's and the epilogue's bounded waits (2 s each) run out: returns
+ * SCRNA_ETIMEOUT after the kernel has left through its normal exit (TMEM released), and the
+ * context stays usable.  No counterpart in the reference: it tests the failure path of the
+ * tensor-core pipeline without faulting or hanging the GPU. */
+int scrna_debug_tc_gemm_withhold(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
+                                 int32_t K, int32_t dtype, int32_t withhold);
 /* Measures the sustained issue rate of the FP32 FMA pipe and of the special-function
  * unit (MUFU) pipe with two microkernels; results in operations per second. */
 int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma_ops_per_s, double* sfu_ops_per_s,

@@ -52,6 +52,11 @@ class Request(C.Structure):
                 ("reserved", C.c_int32), ("capture", Capture)]
 
 
+class TuneChoice(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("genes_per_lane", C.c_int32), ("block_warps", C.c_int32),
+                ("found", C.c_int32), ("us_per_step", C.c_double)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "queued", "running",
                                           "units_done", "bytes_in_use")] + \
@@ -85,6 +90,11 @@ SIGNATURES = {
     "scrna_state_device_ptrs": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "scrna_state_read_raw": (C.c_int, [P, P, P, P, P, P]),
     "scrna_cle_simulate_noalloc": (C.c_int, [P, P, P, P, P, P, P, P, P]),
+    "scrna_ctx_set_autotune": (C.c_int, [P, I32, C.c_char_p]),
+    "scrna_autotune_last_choice": (C.c_int, [P, C.POINTER(TuneChoice)]),
+    "scrna_autotune_key": (C.c_int, [C.c_char_p, I32, I32, I32, I32, I32, I64, C.c_char_p, I32]),
+    "scrna_autotune_cache_lookup": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
+    "scrna_autotune_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
     "scrna_server_create": (C.c_int, [P, I64, I32, C.POINTER(P)]),
     "scrna_server_destroy": (C.c_int, [P]),
     "scrna_submit": (C.c_int, [P, P, C.POINTER(U64)]),
@@ -94,6 +104,7 @@ SIGNATURES = {
     "scrna_server_get_stats": (C.c_int, [P, P]),
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_debug_tc_gemm": (C.c_int, [P, P, P, P, I64, I32, I32, I32]),
+    "scrna_debug_tc_gemm_withhold": (C.c_int, [P, P, P, P, I64, I32, I32, I32, I32]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),
     "scrna_measure_philox_rate": (C.c_int, [P, C.POINTER(DBL)]),
     "scrna_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),

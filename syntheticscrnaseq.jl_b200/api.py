@@ -48,6 +48,17 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.scrna_ctx_launch_count(self.h))
 
+    def set_autotune(self, mode: int, cache_path: Optional[str] = None):
+        """Kernel-variant autotuning: 0 off (static choice), 1 cached or measured, 2 cache only.
+        cache_path None keeps the current cache file, "" keeps choices in memory only."""
+        check(self.lib.scrna_ctx_set_autotune(self.h, int(mode), None if cache_path is None else cache_path.encode()))
+
+    def last_kernel_choice(self) -> dict:
+        """The register-path kernel variant of this context's last run (found: 1 if tuned)."""
+        c = _lib.TuneChoice()
+        check(self.lib.scrna_autotune_last_choice(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in c._fields_}
+
     def transfer_bytes(self):
         """(host->device, device->host) bytes this context's calls have copied so far."""
         h2d, d2h = C.c_int64(), C.c_int64()

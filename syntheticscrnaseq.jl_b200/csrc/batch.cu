@@ -61,7 +61,7 @@ struct Group {
 };
 
 int64_t cells_per_tile(const BatchNet& bn) {
-    if (bn.kc.warp) return warpcell_cells_per_block_host(bn.net->G, bn.kc.gpl);
+    if (bn.kc.warp) return warpcell_cells_per_block_host(bn.net->G, bn.kc.gpl, bn.kc.nw1);
     return 32;
 }
 
@@ -103,9 +103,9 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
         const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
         x.tensor = !x.pop && (d.n_quads > fused_max_quads() || (x.net->G >= 256 && density >= 0.05));
         if (!x.tensor) {
-            x.kc = choose_kernel(x.net, x.o.path);
-            if (x.kc.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
             if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
+            if (int r = choose_kernel_tuned(ctx, x.net, x.kin, &x.o, st, &x.kc)) return r;
+            if (x.kc.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
             x.st->have_counts = cap != nullptr;
         }
     }
@@ -165,6 +165,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         for (size_t i = 0; i < g.nets.size(); ++i) {
             BatchNet* x = g.nets[i];
             fill_fused_args(x->net, x->kin, x->pop, cap, &x->o, x->st, &args[i]);
+            args[i].lane_nw1 = x->kc.nw1;
             nw = std::max(nw, x->kc.block.nw);
             smem = std::max(smem, x->kc.smem);
             const int64_t cpt = cells_per_tile(*x);

@@ -23,7 +23,6 @@ cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cud
 int warpcell_max_genes();
 int warpcell_emax_class(int max_in);
 int warpcell_pick_gpl(int G, bool bursty, int emax);
-size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms);
 cudaError_t warpcell_launch(const FusedArgs& a, int gpl, int emax, int tmax, bool pop, cudaStream_t st);
 cudaError_t plain_step_launch(const PlainArgs& a, cudaStream_t st);
 cudaError_t plain_init_launch(int G, int64_t N, int64_t cell_offset, const GeneInit* gi,
@@ -96,6 +95,7 @@ extern "C" int scrna_ctx_create(int device, scrna_ctx** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(SCRNA_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
     c->own_stream = true;
+    tune_init_ctx(c);
     *out = c;
     return SCRNA_OK;
 }
@@ -559,9 +559,10 @@ scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     k.gpl = d.lane_gpl;
     k.emax = d.lane_emax;
     k.tmax = d.lane_tmax;
-    k.nwarps = warp_ok ? warpcell_block_warps_host(d.G, d.lane_gpl) : 0;
+    k.nw1 = 0;
+    k.nwarps = warp_ok ? warpcell_block_warps_host(d.G, d.lane_gpl, 0) : 0;
     k.block = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
-    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na) : k.block.smem;
+    k.smem = k.warp ? warpcell_smem(d.G, k.gpl, d.n_reg, d.n_na, 0) : k.block.smem;
     return k;
 }
 
@@ -572,22 +573,24 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
     const int64_t n_steps = n_steps_of(o);
     if (n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
-    FusedArgs a{};
-    fill_fused_args(net, kin, pop, cap, o, st, &a);
     const FusedLaunch L = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
     if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
     cudaStream_t s = ctx->stream;
-    // kernel choice: warp-per-cell-group for small networks, block tiles otherwise
+    // kernel choice: the lane kernel for small networks, block tiles otherwise (or as tuned)
     const bool warp_ok = d.lane_in != nullptr;
-    const bool use_warp = o->path == SCRNA_PATH_WARP ? true : o->path == SCRNA_PATH_BLOCK ? false : warp_ok;
-    if (use_warp && !warp_ok)
+    if (o->path == SCRNA_PATH_WARP && !warp_ok)
         return fail(SCRNA_ENOTSUP, "the warp kernel needs G <= %d, <= %d in-edges (additive and cooperative/redundant) "
                     "per gene, terms of <= %d sources and <= %d terms per lane", warpcell_max_genes(), kLaneEdges,
                     kLaneSrc, kLaneTerms);
+    KernelChoice kc{};
+    if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc)) return r;
+    FusedArgs a{};
+    fill_fused_args(net, kin, pop, cap, o, st, &a);
+    a.lane_nw1 = kc.nw1;
     auto launch = [&](bool is_pop) -> cudaError_t {
-        return use_warp ? warpcell_launch(a, d.lane_gpl, d.lane_emax, d.lane_tmax, is_pop, s) : fused_launch(a, L, is_pop, s);
+        return kc.warp ? warpcell_launch(a, kc.gpl, kc.emax, kc.tmax, is_pop, s) : fused_launch(a, kc.block, is_pop, s);
     };
-    st->last_cell_major = use_warp;  // the lane kernel keeps M, P, prom, NS cell-major
+    st->last_cell_major = kc.warp;  // the lane kernel keeps M, P, prom, NS cell-major
     if (!pop) {
         a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;
         CU(launch(false));

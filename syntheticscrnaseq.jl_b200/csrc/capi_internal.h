@@ -5,6 +5,8 @@
 
 #include <atomic>
 #include <cstdint>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "../../include/scrna_cle.h"
@@ -62,6 +64,13 @@ struct scrna_ctx {
     void* lt_handle = nullptr;
     scrna::DevBuf lt_workspace;
     scrna::DevBuf tc_err;        // error flag of the tcgen05 kernels (one int)
+    // autotuning of the register-path kernel (tune.cu): mode 0 off, 1 measure on a miss,
+    // 2 cache only; cache file (empty: memory only); choices made on this context
+    int tune_mode = 1;
+    std::string tune_path;
+    char tune_arch[32] = "sm100";
+    std::map<std::string, scrna_tune_choice> tune_mem;
+    scrna_tune_choice tune_last{};
 };
 
 struct scrna_net {
@@ -121,6 +130,7 @@ namespace scrna {
 struct KernelChoice {
     bool warp;
     int gpl, emax, tmax, nwarps;
+    int nw1;  // lane kernel: warps per block when a cell fits in one warp (0: the default 4)
     FusedLaunch block;
     size_t smem;
 };
@@ -133,6 +143,9 @@ int state_alloc(scrna_state* st, bool pop, bool plain);
 void fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
                      const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, FusedArgs* out);
 KernelChoice choose_kernel(const scrna_net* net, int path);
+void tune_init_ctx(scrna_ctx* ctx);
+int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
+                        scrna_state* st, KernelChoice* out);
 int fused_max_quads();
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
@@ -142,8 +155,10 @@ cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int
 cudaError_t warpcell_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int gpl,
                                   int emax, int tmax, bool pop, size_t smem, int grid, int nwarps,
                                   TileCtl shared_ctl, int use_shared, const KeySchedule* ks, cudaStream_t st);
-int warpcell_cells_per_block_host(int G, int gpl);
-int warpcell_block_warps_host(int G, int gpl);
+int warpcell_cells_per_block_host(int G, int gpl, int nw1);
+int warpcell_block_warps_host(int G, int gpl, int nw1);
+int warpcell_wpc_host(int G, int gpl);
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms, int nw1);
 int tensor_prepare_net(scrna_net* n, int dtype);
 cudaError_t tensor_terms_launch(int dtype, int64_t N, int G, int Kp, int n_terms, int n_src, const NonAdd* na,
                                 const int32_t* na_src, const float* act32, void* act16, cudaStream_t st);

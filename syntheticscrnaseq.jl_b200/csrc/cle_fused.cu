@@ -78,9 +78,12 @@ int warpcell_pick_gpl(int G, bool bursty, int emax) {
     return pick;
 }
 
-size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms) { return warpcell_smem_bytes(G, gpl, n_reg, n_terms); }
-int warpcell_cells_per_block_host(int G, int gpl) { return warpcell_cells_per_block(G, gpl); }
-int warpcell_block_warps_host(int G, int gpl) { return warpcell_block_warps(G, gpl); }
+size_t warpcell_smem(int G, int gpl, int n_reg, int n_terms, int nw1) {
+    return warpcell_smem_bytes(G, gpl, n_reg, n_terms, nw1);
+}
+int warpcell_cells_per_block_host(int G, int gpl, int nw1) { return warpcell_cells_per_block(G, gpl, nw1); }
+int warpcell_block_warps_host(int G, int gpl, int nw1) { return warpcell_block_warps(G, gpl, nw1); }
+int warpcell_wpc_host(int G, int gpl) { return warpcell_wpc(G, gpl); }
 
 template <int V>
 using IntC = std::integral_constant<int, V>;

@@ -118,6 +118,7 @@ struct FusedArgs {
     double* eff;            // cells, nullable
     int32_t capture_species;
     double cap_mu_log, cap_sigma;
+    int32_t lane_nw1;       // lane kernel: warps per block when a cell fits in one warp (0 = 4)
 };
 
 // Step range and division flags of one launch (or one queued work item).

@@ -48,7 +48,7 @@ __device__ __forceinline__ void tc_fail(int* err, int code) { atomicCAS(err, 0, 
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, float* C,
-               int M, int N, int K, uint32_t idesc, int* err) {
+               int M, int N, int K, uint32_t idesc, int* err, int withhold) {
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
     // 1024-byte aligned stage buffers (128-byte swizzle atoms), control block after them
     const uint32_t base = tc::smem_u32(smem_dyn);
@@ -85,11 +85,14 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
     const uint32_t tmem = sh->tmem_base;
 
     if (warp == 0 && lane == 0) {  // ---- TMA producer
-        int stage = 0;
+        int stage = 0, issued = 0;
         uint32_t phase = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
             const int m = t / tiles_n, n = t - (t / tiles_n) * tiles_n;
-            for (int kb = 0; kb < kb_n; ++kb) {
+            for (int kb = 0; kb < kb_n; ++kb, ++issued) {
+                // test hook (withhold >= 0): stop before this CTA's load number `withhold`, so
+                // the consumers' bounded waits run out; nothing stays in flight
+                if (issued == withhold) goto producer_done;
                 if (!tc::mbar_wait(&sh->empty[stage], phase ^ 1u)) { tc_fail(err, 1); goto producer_done; }
                 tc::mbar_arrive_expect_tx(&sh->full[stage], kTcABytes + kTcBBytes);
                 tc::tma_load_2d(a_s + (size_t)stage * kTcABytes, &map_a, &sh->full[stage], kb * kTcBK, m * kTcBM);
@@ -553,7 +556,8 @@ int tc_make_map(CUtensorMap* map, const void* ptr, int64_t rows, int64_t k, int 
     return SCRNA_OK;
 }
 
-int tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int N, int K, bool bf16, int* err_dev) {
+int tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int N, int K, bool bf16, int* err_dev,
+            int withhold) {
     CUtensorMap ma, mb;
     if (int r = tc_make_map(&ma, A, M, K, kTcBM, bf16)) return r;
     if (int r = tc_make_map(&mb, B, N, K, kTcBN, bf16)) return r;
@@ -562,7 +566,7 @@ int tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, i
     const int64_t tiles = ((M + kTcBM - 1) / kTcBM) * ((N + kTcBN - 1) / kTcBN);
     const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
     tc_gemm_kernel<<<grid, kTcThreads, kTcSmem, ctx->stream>>>(ma, mb, C, (int)M, N, K, tc::umma_idesc_f16(bf16, kTcBM, kTcBN),
-                                                                err_dev);
+                                                                err_dev, withhold);
     CU(cudaGetLastError());
     ctx->launches++;
     return SCRNA_OK;
@@ -677,7 +681,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     int h = 0;
     CU(cudaMemcpyAsync(&h, ctx->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    if (h != 0) return fail(SCRNA_ECUDA, "tensor-core step pipeline wait timed out (stage %d)", h);
+    if (h != 0) return fail(SCRNA_ETIMEOUT, "tensor-core step pipeline wait timed out (stage %d)", h);
     return SCRNA_OK;
 }
 
@@ -687,18 +691,29 @@ using namespace scrna;
 
 // Diagnostic entry point (no counterpart in the reference): C = A * B^T on device pointers
 // with the hand-written tcgen05 GEMM, synchronous; fails if a pipeline wait timed out.
-extern "C" int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
-                                   int32_t K, int32_t dtype) {
+static int debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N, int32_t K,
+                         int32_t dtype, int32_t withhold) {
     if (!ctx || !A || !B || !C) return fail(SCRNA_EINVAL, "NULL argument");
     if (M <= 0 || N <= 0 || K <= 0 || K % 64 != 0) return fail(SCRNA_EINVAL, "need M, N > 0 and K a multiple of 64");
     if (int r = set_device(ctx)) return r;
     DevBuf err;
     CU(err.ensure(sizeof(int)));
     CU(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
-    if (int r = tc_gemm(ctx, A, B, C, M, N, K, dtype == 0, err.as<int>())) return r;
+    if (int r = tc_gemm(ctx, A, B, C, M, N, K, dtype == 0, err.as<int>(), withhold)) return r;
     int h = 0;
     CU(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
-    if (h != 0) return fail(SCRNA_ECUDA, "tensor-core GEMM pipeline wait timed out (stage %d)", h);
+    if (h != 0) return fail(SCRNA_ETIMEOUT, "tensor-core GEMM pipeline wait timed out (stage %d)", h);
     return SCRNA_OK;
+}
+
+extern "C" int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
+                                   int32_t K, int32_t dtype) {
+    return debug_tc_gemm(ctx, A, B, C, M, N, K, dtype, -1);
+}
+
+extern "C" int scrna_debug_tc_gemm_withhold(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M,
+                                            int32_t N, int32_t K, int32_t dtype, int32_t withhold) {
+    if (withhold < 0) return fail(SCRNA_EINVAL, "withhold must be >= 0");
+    return debug_tc_gemm(ctx, A, B, C, M, N, K, dtype, withhold);
 }

@@ -34,19 +34,22 @@ __host__ __device__ inline int warpcell_cells_per_warp(int G, int gpl) {
     const int lpc = warpcell_lanes_per_cell(G, gpl);
     return lpc <= 32 ? 32 / lpc : 1;
 }
-// warps per block: 4 independent warps of small cells, or whole multi-warp cells (<= 8 warps)
-__host__ __device__ inline int warpcell_block_warps(int G, int gpl) {
+// warps per block: nw1 (2, 4 or 8; 0 = 4) independent warps of small cells, or whole
+// multi-warp cells (<= 8 warps)
+__host__ __device__ inline int warpcell_block_warps(int G, int gpl, int nw1 = 0) {
     const int w = warpcell_wpc(G, gpl);
-    return w == 1 ? 4 : w * (8 / w);
+    return w == 1 ? (nw1 > 0 ? nw1 : 4) : w * (8 / w);
 }
-__host__ __device__ inline int warpcell_cells_per_block(int G, int gpl) {
+__host__ __device__ inline int warpcell_cells_per_block(int G, int gpl, int nw1 = 0) {
     const int w = warpcell_wpc(G, gpl);
-    return w == 1 ? warpcell_block_warps(G, gpl) * warpcell_cells_per_warp(G, gpl) : warpcell_block_warps(G, gpl) / w;
+    const int bw = warpcell_block_warps(G, gpl, nw1);
+    return w == 1 ? bw * warpcell_cells_per_warp(G, gpl) : bw / w;
 }
 // activation rows of a block: one per cell, plus a row per warp for the spare lanes of small cells
-__host__ __device__ inline int warpcell_rows_per_block(int G, int gpl) {
+__host__ __device__ inline int warpcell_rows_per_block(int G, int gpl, int nw1 = 0) {
     const int w = warpcell_wpc(G, gpl);
-    return w == 1 ? warpcell_block_warps(G, gpl) * (warpcell_cells_per_warp(G, gpl) + 1) : warpcell_block_warps(G, gpl) / w;
+    const int bw = warpcell_block_warps(G, gpl, nw1);
+    return w == 1 ? bw * (warpcell_cells_per_warp(G, gpl) + 1) : bw / w;
 }
 
 // Activation row of one cell: n_reg regulator slots, the constants 0 (slot n_reg) and 1
@@ -54,8 +57,8 @@ __host__ __device__ inline int warpcell_rows_per_block(int G, int gpl) {
 // n_terms term values; odd length so the rows of a warp's cells start in different banks.
 __host__ __device__ inline int warpcell_ld(int n_reg, int n_terms) { return (n_reg + 3 + n_terms) | 1; }
 
-__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg, int n_terms) {
-    const size_t b = (size_t)warpcell_rows_per_block(G, gpl) * warpcell_ld(n_reg, n_terms) * sizeof(float);
+__host__ __device__ inline size_t warpcell_smem_bytes(int G, int gpl, int n_reg, int n_terms, int nw1 = 0) {
+    const size_t b = (size_t)warpcell_rows_per_block(G, gpl, nw1) * warpcell_ld(n_reg, n_terms) * sizeof(float);
     return (b + 15) & ~(size_t)15;
 }
 
@@ -521,12 +524,12 @@ cle_warpcell_queue_kernel(const FusedArgs* args, const TileWork* items, int n_it
 template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     auto k = cle_warpcell_kernel<GPL, EMAX, TMAX, POP>;
-    const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg, a.n_na);
+    const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg, a.n_na, a.lane_nw1);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int64_t cpb = warpcell_cells_per_block(a.G, GPL);
+    const int64_t cpb = warpcell_cells_per_block(a.G, GPL, a.lane_nw1);
     const unsigned blocks = (unsigned)((a.N + cpb - 1) / cpb);
-    k<<<blocks, 32 * warpcell_block_warps(a.G, GPL), smem, st>>>(a);
+    k<<<blocks, 32 * warpcell_block_warps(a.G, GPL, a.lane_nw1), smem, st>>>(a);
     return cudaGetLastError();
 }
 

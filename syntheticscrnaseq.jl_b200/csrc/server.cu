@@ -104,9 +104,11 @@ static int setup_request(scrna_server* s, SrvRequest* r) {
     CU(cudaMemcpy(r->genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(r->ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(r->qtel.p, qt.data(), qt.size(), cudaMemcpyHostToDevice));
-    r->kc = choose_kernel(n, r->req.opts.path);
+    if (int rr = choose_kernel_tuned(s->ctx, const_cast<scrna_net*>(n), &r->req.kin, &r->req.opts, r->st, &r->kc))
+        return rr;
     fill_fused_args(r->net, &r->req.kin, nullptr, r->req.with_capture ? &r->req.capture : nullptr, &r->req.opts,
                     r->st, &r->args);
+    r->args.lane_nw1 = r->kc.nw1;
     r->args.genes = r->genes.as<GeneRec>();
     r->args.ginit = r->ginit.as<GeneInit>();
     r->args.quad_tel = r->qtel.as<uint8_t>();
@@ -186,7 +188,7 @@ void scrna_server::run() {
             auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.emax : 0,
                                        kc.warp ? kc.nwarps : kc.block.upt, kc.warp ? kc.tmax : 0);
             int64_t cpt = 32;
-            if (kc.warp) cpt = warpcell_cells_per_block_host(r->net->G, kc.gpl);
+            if (kc.warp) cpt = warpcell_cells_per_block_host(r->net->G, kc.gpl, kc.nw1);
             const int64_t tiles = (r->N + cpt - 1) / cpt;
             TileCtl ctl{(int32_t)r->s0, (int32_t)r->s1, r->s0 == 1 ? 1 : 0, r->s1 >= r->n_steps ? 1 : 0, 0, 0};
             auto& items = groups[key];

@@ -9,8 +9,9 @@ var / mean, for mRNA and protein.  Bars:
     - telegraph CLE, G=10 bursty genes, 20,000 cells, dt=0.01, T=50 (5,000 steps)
   tensor-core path, dense G=2000 (10 % of A nonzero, 40 + 40 cooperative / redundant edges),
   dt=0.005, on 256 cells x 400 steps (the oracle's dense contraction costs ~1 ms per
-  cell-step): BF16 contraction inputs within TOL_BF16 and FP16 inputs within TOL_F16 for
-  every gene's mean, variance and Fano.
+  cell-step): every gene's mean, variance and Fano within 1 % with BF16 contraction inputs
+  (measured on a B200: largest error 9e-4) and with FP16 inputs (1.4e-4).
+Measured for the register path: 1.8e-7 (plain) and 2.4e-7 (telegraph).
 """
 import os
 
@@ -20,7 +21,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL_FP32 = 0.01
-TOL_BF16 = 0.05
+TOL_BF16 = 0.01
 TOL_F16 = 0.01
 THREADS = os.cpu_count() or 1
 
