@@ -233,6 +233,29 @@ int scrna_autotune_key(const char* device, int32_t G, int32_t in_edges, int32_t 
 int scrna_autotune_cache_lookup(const char* path, const char* key, scrna_tune_choice* out);
 int scrna_autotune_cache_store(const char* path, const char* key, const scrna_tune_choice* choice);
 
+/* ---- validation reductions and count-matrix output ---------------------------------
+ * Computed on the device from a state's last results; only summaries cross to the host.
+ * source 0: the readout (cells x G, or x 2G for BOTH), source 1: the captured counts.
+ * scrna_state_moments: per column mean and unbiased variance (FP64, two passes); the
+ *   host-side comparison is compare_moments (src/validate.jl:70-77).
+ * scrna_state_ks: per column the two-sample Kolmogorov-Smirnov statistic between two
+ *   states' samples, with the tie order of ks_statistic (src/validate.jl:14-41).
+ * scrna_state_histogram: counts of the values of one column rounded to integers and clamped
+ *   to [0, nbins-1] (the empirical distribution compared with telegraph_pmf,
+ *   src/analytical.jl:35-95).
+ * scrna_state_write_mtx: writes dir/matrix.mtx (MatrixMarket coordinate integer general,
+ *   genes x cells, 1-based, entries in cell order: the layout read_10x_mtx of
+ *   experiments/compare_real_scrnaseq.jl:69-93 reads), dir/genes.tsv ("id<TAB>name" per gene,
+ *   names from gene_names or gene<k>) and dir/barcodes.tsv (<prefix><k>, prefix "cell" if
+ *   NULL) from the captured counts, compacting the nonzeros on the device 65,536 cells at a
+ *   time.  The directory must exist. */
+int scrna_state_moments(scrna_ctx* ctx, scrna_state* st, int32_t source, double* mean, double* var);
+int scrna_state_ks(scrna_ctx* ctx, scrna_state* a, scrna_state* b, int32_t source, double* D);
+int scrna_state_histogram(scrna_ctx* ctx, scrna_state* st, int32_t source, int32_t column, int32_t nbins,
+                          int64_t* hist);
+int scrna_state_write_mtx(scrna_ctx* ctx, scrna_state* st, const char* dir, const char* const* gene_names,
+                          const char* barcode_prefix);
+
 /* ---- serving loop ---------------------------------------------------------------------
  * A request server with continuous batching (no counterpart in the reference, which runs
  * one simulate call at a time).  Submitted requests wait in a FIFO queue until their device

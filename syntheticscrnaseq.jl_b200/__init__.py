@@ -12,9 +12,11 @@ from .model import (CLE, INF, CaptureModel, CoopEdge, GeneNetwork, KineticParams
 from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
                       dense_network, sample_network)
 from .api import (Context, DeviceRun, NetHandle, Server, apply_capture, debug_philox, default_context,
-                  measure_philox_rate, measure_pipe_peaks, simulate, simulate_gpu_batch)
+                  ks_statistic_device, measure_philox_rate, measure_pipe_peaks, simulate, simulate_gpu_batch)
 from ._lib import ScrnaError
-from .validate import column_moments, compare_moments, max_moment_error, moment_errors
+from .validate import (column_moments, compare_moments, ks_critical_value, ks_statistic, max_moment_error,
+                       moment_errors, telegraph_fano, telegraph_mean, telegraph_pmf, telegraph_variance)
+from .mtx import read_10x_mtx
 
 __all__ = [
     "CLE", "CaptureModel", "CoopEdge", "GeneNetwork", "KineticParams", "PopulationConfig", "RedunEdge",
@@ -23,5 +25,6 @@ __all__ = [
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
     "NetHandle", "Server", "apply_capture", "debug_philox", "default_context", "measure_philox_rate", "measure_pipe_peaks", "simulate",
     "simulate_gpu_batch", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
-    "moment_errors",
+    "moment_errors", "ks_statistic", "ks_critical_value", "ks_statistic_device", "telegraph_pmf", "telegraph_mean",
+    "telegraph_variance", "telegraph_fano", "read_10x_mtx",
 ]

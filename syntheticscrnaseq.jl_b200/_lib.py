@@ -95,6 +95,10 @@ SIGNATURES = {
     "scrna_autotune_key": (C.c_int, [C.c_char_p, I32, I32, I32, I32, I32, I64, C.c_char_p, I32]),
     "scrna_autotune_cache_lookup": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
     "scrna_autotune_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
+    "scrna_state_moments": (C.c_int, [P, P, I32, P, P]),
+    "scrna_state_ks": (C.c_int, [P, P, P, I32, P]),
+    "scrna_state_histogram": (C.c_int, [P, P, I32, I32, I32, P]),
+    "scrna_state_write_mtx": (C.c_int, [P, P, C.c_char_p, P, C.c_char_p]),
     "scrna_server_create": (C.c_int, [P, I64, I32, C.POINTER(P)]),
     "scrna_server_destroy": (C.c_int, [P]),
     "scrna_submit": (C.c_int, [P, P, C.POINTER(U64)]),

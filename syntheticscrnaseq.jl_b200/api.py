@@ -351,6 +351,35 @@ class DeviceRun:
             out["V"] = V
         return out
 
+    def moments(self, source: str = "readout"):
+        """Per-column (mean, unbiased variance) of the last run's readout or captured counts,
+        reduced on the device (FP64)."""
+        src = _SOURCE[source]
+        cols = self.G * (2 if (src == 0 and self.readout == "both") else 1)
+        mean = np.empty(cols)
+        var = np.empty(cols)
+        check(self.ctx.lib.scrna_state_moments(self.ctx.h, self.st, src, mean.ctypes.data, var.ctypes.data))
+        return mean, var
+
+    def histogram(self, column: int, nbins: int, source: str = "readout") -> np.ndarray:
+        """Counts of one column's values rounded to integers, clamped to [0, nbins - 1]."""
+        h = np.empty(int(nbins), dtype=np.int64)
+        check(self.ctx.lib.scrna_state_histogram(self.ctx.h, self.st, _SOURCE[source], int(column), int(nbins),
+                                                 h.ctypes.data))
+        return h
+
+    def write_mtx(self, directory: str, gene_names: Optional[Sequence[str]] = None, barcode_prefix: str = "cell"):
+        """10x Matrix Market files (matrix.mtx, genes.tsv, barcodes.tsv) of the captured counts."""
+        names = None
+        if gene_names is not None:
+            if len(gene_names) != self.G:
+                raise ValueError(f"need {self.G} gene names")
+            enc = [n.encode() for n in gene_names]
+            names = (C.c_char_p * self.G)(*enc)
+        check(self.ctx.lib.scrna_state_write_mtx(self.ctx.h, self.st, str(directory).encode(),
+                                                 None if names is None else C.cast(names, C.c_void_p),
+                                                 barcode_prefix.encode()))
+
     def device_state(self):
         """Device pointers of the FP32 mRNA / protein state: [G][N] after a block-kernel run,
         [N][G] after a lane-kernel run."""
@@ -369,6 +398,21 @@ class DeviceRun:
             self.close()
         except Exception:
             pass
+
+
+_SOURCE = {"readout": 0, "counts": 1}
+
+
+def ks_statistic_device(a: "DeviceRun", b: "DeviceRun", source: str = "readout") -> np.ndarray:
+    """Per-column two-sample Kolmogorov-Smirnov statistic of two runs' last results, computed on
+    the device (the walk of src/validate.jl:14-41)."""
+    if a.ctx is not b.ctx:
+        raise ValueError("both runs must belong to one context")
+    src = _SOURCE[source]
+    cols = a.G * (2 if (src == 0 and a.readout == "both") else 1)
+    D = np.empty(cols)
+    check(a.ctx.lib.scrna_state_ks(a.ctx.h, a.st, b.st, src, D.ctypes.data))
+    return D
 
 
 def debug_philox(ctr: np.ndarray, key, ctx: Optional[Context] = None) -> np.ndarray:

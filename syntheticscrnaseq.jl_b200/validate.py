@@ -1,10 +1,18 @@
-"""Moment comparisons of simulated count matrices (src/validate.jl:70-77).
+"""Validation helpers on the host (src/validate.jl, src/analytical.jl).
 
 compare_moments(x, y)      the reference's convention for two sample sets: relative error
                            |a - b| / max(|a|, |b|, 1e-10) of the means and of the
-                           (unbiased) variances, and pass = both < rtol.
+                           (unbiased) variances, and pass = both < rtol (validate.jl:70-77).
 moment_errors(X, Y)        the same per column (gene) of two cells x genes matrices, plus
                            the Fano factor var / mean under the same convention.
+ks_statistic(x, y)         two-sample Kolmogorov-Smirnov statistic with the tie order of the
+                           reference's merge walk (validate.jl:14-41); ks_critical_value
+                           its asymptotic critical value (validate.jl:51-61).
+telegraph_pmf / _mean / _variance / _fano
+                           the telegraph model's steady-state mRNA distribution and moments
+                           (analytical.jl:35-119), for comparing histograms of the device
+                           results (DeviceRun.histogram).
+The device-side reductions are DeviceRun.moments / histogram and api.ks_statistic_device.
 """
 from __future__ import annotations
 
@@ -48,3 +56,47 @@ def max_moment_error(X, Y) -> float:
     """Largest per-column mean / variance / Fano error between two matrices."""
     e = moment_errors(X, Y)
     return float(max(e[k].max() for k in e))
+
+
+def ks_statistic(x, y) -> float:
+    """Largest |ecdf_x - ecdf_y| over the steps of the merge walk of validate.jl:14-41, which
+    takes the x sample first on ties: after the i-th x it has taken the y's below x_i, after
+    the j-th y the x's up to y_j."""
+    sx = np.sort(np.asarray(x, dtype=np.float64).reshape(-1))
+    sy = np.sort(np.asarray(y, dtype=np.float64).reshape(-1))
+    nx, ny = len(sx), len(sy)
+    ex = np.arange(1, nx + 1) / nx - np.searchsorted(sy, sx, side="left") / ny
+    ey = np.searchsorted(sx, sy, side="right") / nx - np.arange(1, ny + 1) / ny
+    return float(max(np.abs(ex).max(initial=0.0), np.abs(ey).max(initial=0.0)))
+
+
+def ks_critical_value(n1: int, n2: int, alpha: float = 0.05) -> float:
+    """Asymptotic two-sample critical value c(alpha) sqrt((n1 + n2) / (n1 n2)) (validate.jl:51-61)."""
+    c = 1.63 if alpha <= 0.01 else 1.36 if alpha <= 0.05 else 1.22
+    return c * float(np.sqrt((n1 + n2) / (n1 * n2)))
+
+
+def telegraph_logpmf(n: int, a: float, b: float, c: float) -> float:
+    """log P(n) of the telegraph model with dimensionless rates a (on), b (off), c
+    (transcription), all over the mRNA decay rate (analytical.jl:35-52)."""
+    from scipy.special import gammaln, hyp1f1
+    lp = (-c + n * np.log(c) - gammaln(n + 1) + gammaln(a + n) - gammaln(a) - gammaln(a + b + n)
+          + gammaln(a + b))
+    return float(lp + np.log(hyp1f1(b, a + b + n, c)))
+
+
+def telegraph_pmf(n: int, a: float, b: float, c: float) -> float:
+    return float(np.exp(telegraph_logpmf(n, a, b, c)))
+
+
+def telegraph_mean(a: float, b: float, c: float) -> float:
+    return a * c / (a + b)
+
+
+def telegraph_variance(a: float, b: float, c: float) -> float:
+    mu = telegraph_mean(a, b, c)
+    return mu + a * b * c * c / ((a + b) ** 2 * (a + b + 1))
+
+
+def telegraph_fano(a: float, b: float, c: float) -> float:
+    return 1.0 + b * c / ((a + b) * (a + b + 1))

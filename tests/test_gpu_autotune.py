@@ -1,0 +1,72 @@
+"""The autotuner on the GPU: every kernel variant it chooses between computes the same sums in
+the same order, so tuned runs (measured, then read from the cache) equal untuned runs bit for
+bit, for single runs with and without population and for a batch; the measurement happens
+once per network shape and later contexts read the choice from the cache file."""
+import json
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _nets(pkg):
+    return [(pkg.sample_network(10, seed=1, bursty=True), 3000), (pkg.sample_network(40, seed=2), 777),
+            (pkg.sample_network(150, seed=3, bursty=True), 500), (pkg.sample_network(300, seed=4), 257)]
+
+
+def test_tuned_equals_untuned(pkg, tmp_path):
+    kin = pkg.WORKLOAD_KINETICS
+    cache = tmp_path / "autotune.json"
+    plain = pkg.Context(0)
+    plain.set_autotune(0)
+    tuned = pkg.Context(0)
+    tuned.set_autotune(1, str(cache))
+    for net, N in _nets(pkg):
+        want = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3, ctx=plain)
+        l0 = tuned.launches
+        got = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3, ctx=tuned)
+        assert tuned.launches - l0 > 1  # measured: the candidates ran before the run itself
+        assert tuned.last_kernel_choice()["found"] == 1
+        assert np.array_equal(got, want)
+        l0 = tuned.launches
+        again = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3, ctx=tuned)
+        assert tuned.launches - l0 == 1  # the shape is known: one launch, no measurement
+        assert np.array_equal(again, want)
+    entries = json.load(open(cache))["entries"]
+    assert len(entries) == 4
+    # a new context reads the file: no measurement, same results
+    fresh = pkg.Context(0)
+    fresh.set_autotune(2, str(cache))
+    net, N = _nets(pkg)[0]
+    l0 = fresh.launches
+    got = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3, ctx=fresh)
+    assert fresh.launches - l0 == 1 and fresh.last_kernel_choice()["found"] == 1
+    assert np.array_equal(got, pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3,
+                                            ctx=plain))
+    for c in (plain, tuned, fresh):
+        c.close()
+
+
+def test_tuned_population_and_batch_equal_untuned(pkg, tmp_path):
+    kin = pkg.WORKLOAD_KINETICS
+    plain = pkg.Context(0)
+    plain.set_autotune(0)
+    tuned = pkg.Context(0)
+    tuned.set_autotune(1, str(tmp_path / "autotune.json"))
+    nets = [n for n, _ in _nets(pkg)]
+    pops = [pkg.PopulationConfig(cell_num=400 + 100 * i, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                                 div_check_interval=10) if i % 2 else None for i in range(len(nets))]
+    cells = [600, 500, 300, 700]
+    for net, pop, N in zip(nets, pops, cells):
+        a = pkg.simulate(net, pkg.CLE(0.01), kin, population=pop, cell_num=N, T=0.5, readout="both", seed=8, ctx=plain)
+        b = pkg.simulate(net, pkg.CLE(0.01), kin, population=pop, cell_num=N, T=0.5, readout="both", seed=8, ctx=tuned)
+        assert np.array_equal(a, b)
+    a = pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=0.5, populations=pops, readout="both",
+                               seed=5, ctx=plain)
+    b = pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kin, cell_num=cells, T=0.5, populations=pops, readout="both",
+                               seed=5, ctx=tuned)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    plain.close()
+    tuned.close()
