@@ -170,6 +170,34 @@ int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* 
                              const scrna_capture* cap, const scrna_cle_opts* opts,
                              double* const* outs, int32_t* const* counts);
 
+/* ---- binomial tau-leap --------------------------------------------------------------
+ * Replace the GPU BinomialTauLeap methods of the reference:
+ *   simulate(net, BinomialTauLeap(dt), kin, Val(:gpu); cell_num, T, readout)
+ *     (ext/SyntheticscRNAseqCUDAExt.jl:215-284),
+ *   simulate(net, BinomialTauLeap(dt), kin, Val(:gpu), pop; T, readout) (ext:531-663),
+ *   simulate_gpu_batch(networks, BinomialTauLeap(dt), kin[s]; ...) (ext:290-399, ext:666-837).
+ * Same arguments as the CLE entry points (opts->dt is the tau-leap step).  Per step and gene,
+ * as the reference computes it in FP32: transcription Poisson(max(reg + beta, 0) dt (x V)),
+ * mRNA decay min(Poisson(m (1 - exp(-mu_m dt))), m), translation Poisson(k_t m dt) with the new
+ * m, protein decay likewise; Poisson by inverse CDF over 50 terms (ext:21-39).  Additions as
+ * in the CLE: cooperative / redundant edges and telegraph gating (tauleap_binomial.jl:84-137).
+ * With a population: Hill of the concentration P / V, transcription x V, decay without
+ * dilution, initial counts max(1, round(steady state x V)), and the readout is M / V, P / V
+ * (capture counts are drawn from the molecule counts).  Register path (block tiles), G <= 512,
+ * FP32 precision only. */
+int scrna_tauleap_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                           const scrna_population* pop, const scrna_capture* cap,
+                           const scrna_cle_opts* opts, double* out, int32_t* counts,
+                           double* efficiencies);
+int scrna_tauleap_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets,
+                                 const scrna_kinetics* kins, int32_t n_kins,
+                                 const int64_t* cell_nums, const scrna_population* const* pops,
+                                 const scrna_capture* cap, const scrna_cle_opts* opts,
+                                 double* const* outs, int32_t* const* counts);
+int scrna_tauleap_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                             const scrna_population* pop, const scrna_capture* cap,
+                             const scrna_cle_opts* opts, scrna_state* st);
+
 /* Replaces apply_capture(X, capture; rng) (src/capture.jl:25-47): X is a host
  * cells x G column-major Float64 matrix of molecule values.  Y (host, cells x G
  * int32) gets the captured counts, eff (host, cells, nullable) the efficiencies. */

@@ -304,28 +304,13 @@ typedef struct {
     double k_t, Kn, hill_n, mu_m, mu_p, dt, sqrt_dt;
 } coef_t;
 
-/* One Euler-Maruyama step for one cell (cle.jl:78-121; population form cle.jl:185-234
- * when vol > 0).  m, p, on are this cell's G-vectors; act/rep/reg are scratch. */
-static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, uint64_t seed,
-                      uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
-                      double* p, uint8_t* on, sw_t* sw, double* act, double* rep, double* reg) {
+/* Regulatory input of every gene from the protein levels p: Hill fractions (cle.jl:79-82),
+ * reg = A_pos*act + A_neg*rep over the nonzero columns of each row (cle.jl:84-86), then the
+ * cooperative / redundant corrections (cle.jl:89-106). */
+static void regulation(const orc_net* net, const prep_t* pp, const coef_t* cf, const double* p, double* act,
+                       double* rep, double* reg) {
     int G = net->G;
-    /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
-     * the per-step Bernoulli(1 - exp(-k dt)) switch is sampled as its geometric waiting
-     * time (one switch ahead, see sw_t), from the spare bits of the gene's normal words
-     * of the switch step. */
-    if (pp->bursty) {
-        for (int g = 0; g < G; ++g) {
-            if (!pp->tel[g] || (int64_t)step != sw[g].ns) continue;
-            on[g] ^= 1;
-            uint32_t w[4];
-            draw(seed, cell, step, (uint32_t)(g >> 1), ORC_TAG_NORMAL, stream, w);
-            float u = (g & 1) ? orc_switch_uniform(w[2], w[3]) : orc_switch_uniform(w[0], w[1]);
-            sw[g].ns = clamp_step((int64_t)step + sw[g].kn);
-            sw[g].kn = orc_geom_steps_u(u, on[g] ? pp->inv_on[g] : pp->inv_off[g]);
-        }
-    }
-    /* Hill fractions (cle.jl:79-82) */
+    /* Hill fractions */
     for (int g = 0; g < G; ++g) {
         double pn = pow(p[g], cf->hill_n);
         double den = pn + cf->Kn;
@@ -353,6 +338,30 @@ static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, ui
         int t = net->redun_target[e];
         reg[t] = reg[t] + net->redun_strength[e] * net->basals[t] * (1.0 - prod);
     }
+}
+
+/* One Euler-Maruyama step for one cell (cle.jl:78-121; population form cle.jl:185-234
+ * when vol > 0).  m, p, on are this cell's G-vectors; act/rep/reg are scratch. */
+static void cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, uint64_t seed,
+                      uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
+                      double* p, uint8_t* on, sw_t* sw, double* act, double* rep, double* reg) {
+    int G = net->G;
+    /* telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
+     * the per-step Bernoulli(1 - exp(-k dt)) switch is sampled as its geometric waiting
+     * time (one switch ahead, see sw_t), from the spare bits of the gene's normal words
+     * of the switch step. */
+    if (pp->bursty) {
+        for (int g = 0; g < G; ++g) {
+            if (!pp->tel[g] || (int64_t)step != sw[g].ns) continue;
+            on[g] ^= 1;
+            uint32_t w[4];
+            draw(seed, cell, step, (uint32_t)(g >> 1), ORC_TAG_NORMAL, stream, w);
+            float u = (g & 1) ? orc_switch_uniform(w[2], w[3]) : orc_switch_uniform(w[0], w[1]);
+            sw[g].ns = clamp_step((int64_t)step + sw[g].kn);
+            sw[g].kn = orc_geom_steps_u(u, on[g] ? pp->inv_on[g] : pp->inv_off[g]);
+        }
+    }
+    regulation(net, pp, cf, p, act, rep, reg);
     /* M then P update with the new M (cle.jl:109-120) */
     for (int g = 0; g < G; ++g) {
         uint32_t w[4];
@@ -402,9 +411,109 @@ static void init_promoters(const prep_t* pp, uint64_t seed, uint32_t stream, uin
     }
 }
 
-int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
-                     const orc_opts* opt, double* M, double* P, double* V, uint8_t* prom,
-                     int nthreads) {
+
+/* ---------------------------------------------------------------------------
+ * GPU binomial tau-leap (ext/SyntheticscRNAseqCUDAExt.jl:215-399, population :531-651),
+ * in FP32 like the reference's kernels.  Every FP32 operation below is one IEEE operation
+ * (this file is compiled without FMA contraction; fmaf is the fused one), so the library's
+ * device code, written with the same explicitly rounded operations, returns the same bits.
+ * ------------------------------------------------------------------------- */
+
+/* exp(x) for x <= 0 from its definition: x = k ln2 + r with k = rint(x log2 e) and |r| <=
+ * ln2/2 (two-constant Cody-Waite reduction), e^r by its Taylor series to r^7 (Horner), then
+ * the exact scaling by 2^k (in two steps below 2^-126, so subnormal results round once). */
+float orc_expf(float x) {
+    if (!(x > -104.0f)) return 0.0f;
+    if (x > 0.0f) x = 0.0f;
+    const float k = rintf(x * 1.44269502162933349609375f);
+    float r = fmaf(-k, 0.693145751953125f, x);       /* ln2 high part: 11 significant bits */
+    r = fmaf(-k, 1.428606765330187045e-06f, r);        /* ln2 - high part */
+    float q = fmaf(r, 1.0f / 5040.0f, 1.0f / 720.0f);
+    q = fmaf(r, q, 1.0f / 120.0f);
+    q = fmaf(r, q, 1.0f / 24.0f);
+    q = fmaf(r, q, 1.0f / 6.0f);
+    q = fmaf(r, q, 0.5f);
+    q = fmaf(r, q, 1.0f);
+    q = fmaf(r, q, 1.0f);
+    int ki = (int)k;
+    if (ki < -125) {
+        q = q * f_of_bits(0x1F800000u); /* 2^-64, exact: q >= 2^-1 */
+        ki += 64;
+    }
+    return q * f_of_bits((uint32_t)(ki + 127) << 23);
+}
+
+/* Poisson(lam) by inverse CDF over the first 50 terms (ext:21-31): the number of partial
+ * sums of exp(-lam) lam^j / j! (j < k) that the uniform u exceeds, at most 50. */
+float orc_poisson_icdf(float u, float lam) {
+    float term = orc_expf(-lam);
+    float cdf = term;
+    float events = 0.0f;
+    for (int k = 1; k <= 50; ++k) {
+        if (!(u > cdf)) break; /* the partial sums never decrease: no later term counts */
+        events = (float)k;
+        term = term * (lam / (float)k);
+        cdf = cdf + term;
+    }
+    return events;
+}
+
+/* The four uniforms of a (cell, step, gene) tau-leap block: (w >> 9) 2^-23 in [0, 1). */
+static inline float tau_uniform(uint32_t w) { return (float)(w >> 9) * 1.1920928955078125e-07f; }
+
+typedef struct {
+    float k_t, dt, p_dec_m, p_dec_p;
+} tcoef_t;
+
+/* One tau-leap step for one cell (ext:250-275; population form ext:586-612 when vol > 0:
+ * Hill of the concentration p / V, transcription scaled by V).  m, p hold counts. */
+static void tau_cell_step(const orc_net* net, const prep_t* pp, const coef_t* cf, const tcoef_t* tc,
+                          uint64_t seed, uint32_t stream, uint32_t cell, uint32_t step, double vol, double* m,
+                          double* p, uint8_t* on, sw_t* sw, double* conc, double* act, double* rep, double* reg) {
+    int G = net->G;
+    if (pp->bursty) {
+        for (int g = 0; g < G; ++g) {
+            if (!pp->tel[g] || (int64_t)step != sw[g].ns) continue;
+            on[g] ^= 1;
+            uint32_t w[4];
+            draw(seed, cell, step, (uint32_t)g, ORC_TAG_TAU, stream, w);
+            float u = orc_switch_uniform(w[0], w[1]);
+            sw[g].ns = clamp_step((int64_t)step + sw[g].kn);
+            sw[g].kn = orc_geom_steps_u(u, on[g] ? pp->inv_on[g] : pp->inv_off[g]);
+        }
+    }
+    const float vf = (float)vol;
+    for (int g = 0; g < G; ++g) conc[g] = vol > 0.0 ? (double)((float)p[g] / vf) : p[g];
+    regulation(net, pp, cf, conc, act, rep, reg);
+    for (int g = 0; g < G; ++g) {
+        uint32_t w[4];
+        draw(seed, cell, step, (uint32_t)g, ORC_TAG_TAU, stream, w);
+        float M = (float)m[g], P = (float)p[g];
+        float tx = (float)(reg[g] + net->basals[g]);
+        tx = tx > 0.0f ? tx : 0.0f;
+        if (vol > 0.0) tx = tx * vf;
+        float lam = tx * tc->dt;
+        if (pp->bursty && !on[g]) lam = 0.0f;
+        const float n_tx = orc_poisson_icdf(tau_uniform(w[0]), lam);
+        const float mp = M > 0.0f ? M : 0.0f;
+        float n_md = orc_poisson_icdf(tau_uniform(w[1]), mp * tc->p_dec_m);
+        n_md = n_md < mp ? n_md : mp;
+        M = (M + n_tx) - n_md;
+        M = M > 0.0f ? M : 0.0f;
+        const float n_tl = orc_poisson_icdf(tau_uniform(w[2]), (tc->k_t * M) * tc->dt);
+        const float pp_ = P > 0.0f ? P : 0.0f;
+        float n_pd = orc_poisson_icdf(tau_uniform(w[3]), pp_ * tc->p_dec_p);
+        n_pd = n_pd < pp_ ? n_pd : pp_;
+        P = (P + n_tl) - n_pd;
+        P = P > 0.0f ? P : 0.0f;
+        m[g] = M;
+        p[g] = P;
+    }
+}
+
+static int simulate_impl(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
+                         const orc_opts* opt, double* M, double* P, double* V, uint8_t* prom,
+                         int nthreads, int tau) {
     int G = net->G;
     int64_t N = opt->cell_num;
     if (G <= 0 || N <= 0 || !(opt->dt > 0.0)) return 1;
@@ -423,15 +532,25 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
     cf.mu_p = pop ? kin->mu_p : kin->mu_p + kin->dilution;
     cf.dt = opt->dt;
     cf.sqrt_dt = sqrt(opt->dt);
+    /* tau-leap: FP32 rates; decay probabilities 1 - exp(-mu dt), with dilution unless a
+     * population makes it emergent (ext:240-241, ext:574-575) */
+    tcoef_t tc;
+    tc.k_t = (float)kin->k_t;
+    tc.dt = (float)opt->dt;
+    tc.p_dec_m = (float)(1.0 - exp(-(pop ? kin->mu_m : kin->mu_m + kin->dilution) * opt->dt));
+    tc.p_dec_p = (float)(1.0 - exp(-(pop ? kin->mu_p : kin->mu_p + kin->dilution) * opt->dt));
 
-    /* initial condition: ceil of the steady state (cle.jl:49-53, kinetics.jl:65-70) */
+    /* initial condition: ceil of the steady state (cle.jl:49-53, kinetics.jl:65-70, ext:230-236);
+     * tau-leap populations: max(1, round(steady state x V)) per cell (ext:560-566) */
     double* m0 = (double*)malloc(sizeof(double) * G);
     double* p0 = (double*)malloc(sizeof(double) * G);
+    double* mss = (double*)malloc(sizeof(double) * G);
+    double* pss = (double*)malloc(sizeof(double) * G);
     for (int g = 0; g < G; ++g) {
-        double mss = net->basals[g] / (kin->mu_m + kin->dilution);
-        double pss = kin->k_t * mss / (kin->mu_p + kin->dilution);
-        m0[g] = ceil(mss);
-        p0[g] = ceil(pss);
+        mss[g] = net->basals[g] / (kin->mu_m + kin->dilution);
+        pss[g] = kin->k_t * mss[g] / (kin->mu_p + kin->dilution);
+        m0[g] = ceil(mss[g]);
+        p0[g] = ceil(pss[g]);
     }
     uint64_t seed = opt->seed;
     uint32_t stream = opt->stream;
@@ -450,6 +569,7 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             double* act = (double*)malloc(sizeof(double) * G);
             double* rep = (double*)malloc(sizeof(double) * G);
             double* reg = (double*)malloc(sizeof(double) * G);
+            double* conc = (double*)malloc(sizeof(double) * G);
             uint8_t* on = (uint8_t*)malloc(G);
             sw_t* ns = (sw_t*)malloc(sizeof(sw_t) * G);
 #pragma omp for schedule(static)
@@ -458,16 +578,20 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                 memcpy(p, p0, sizeof(double) * G);
                 const uint32_t gc = (uint32_t)(opt->cell_offset + c);
                 init_promoters(&pp, seed, stream, gc, on, ns);
-                for (int64_t s = 1; s <= n_steps; ++s)
-                    cell_step(net, &pp, &cf, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, ns, act,
-                              rep, reg);
+                for (int64_t s = 1; s <= n_steps; ++s) {
+                    if (tau)
+                        tau_cell_step(net, &pp, &cf, &tc, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, ns, conc,
+                                      act, rep, reg);
+                    else
+                        cell_step(net, &pp, &cf, seed, stream, gc, (uint32_t)s, 0.0, m, p, on, ns, act, rep, reg);
+                }
                 for (int g = 0; g < G; ++g) {
                     M[(size_t)g * N + c] = m[g];
                     P[(size_t)g * N + c] = p[g];
                     if (prom) prom[(size_t)g * N + c] = on[g];
                 }
             }
-            free(m); free(p); free(act); free(rep); free(reg); free(on); free(ns);
+            free(m); free(p); free(act); free(rep); free(reg); free(conc); free(on); free(ns);
         }
     } else {
         /* population: cells in lockstep, state cell-major [c][g] for the step loop */
@@ -484,6 +608,12 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
             uint32_t w[4];
             draw(seed, (uint32_t)c, 0, 0, ORC_TAG_VOLUME, stream, w);
             Vs[c] = pop->V_lo + (pop->V_hi - pop->V_lo) * u53(w[0], w[1]); /* cle.jl:158-159 */
+            if (tau)
+                for (int g = 0; g < G; ++g) {
+                    const double mi = rint(mss[g] * Vs[c]), pi = rint(pss[g] * Vs[c]);
+                    Ms[c * G + g] = mi > 1.0 ? mi : 1.0;
+                    Ps[c * G + g] = pi > 1.0 ? pi : 1.0;
+                }
         }
         int64_t* dividers = (int64_t*)malloc(sizeof(int64_t) * N);
         double* dM = (double*)malloc(sizeof(double) * G * N);
@@ -497,13 +627,18 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                 double* act = (double*)malloc(sizeof(double) * G);
                 double* rep = (double*)malloc(sizeof(double) * G);
                 double* reg = (double*)malloc(sizeof(double) * G);
+                double* conc = (double*)malloc(sizeof(double) * G);
 #pragma omp for schedule(static)
                 for (int64_t c = 0; c < N; ++c) {
-                    cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, Vs[c],
-                              Ms + c * G, Ps + c * G, On + c * G, Ns + c * G, act, rep, reg);
+                    if (tau)
+                        tau_cell_step(net, &pp, &cf, &tc, seed, stream, (uint32_t)c, (uint32_t)s, Vs[c], Ms + c * G,
+                                      Ps + c * G, On + c * G, Ns + c * G, conc, act, rep, reg);
+                    else
+                        cell_step(net, &pp, &cf, seed, stream, (uint32_t)c, (uint32_t)s, Vs[c],
+                                  Ms + c * G, Ps + c * G, On + c * G, Ns + c * G, act, rep, reg);
                     Vs[c] = Vs[c] * growth_factor; /* cle.jl:237 */
                 }
-                free(act); free(rep); free(reg);
+                free(act); free(rep); free(reg); free(conc);
             }
             if (s % pop->div_check_interval != 0) continue;
             /* division (cle.jl:240-273) */
@@ -570,9 +705,19 @@ int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
         free(Ms); free(Ps); free(On); free(Ns); free(dNs); free(Vs); free(dividers); free(dM); free(dP);
         free(dOn); free(dV);
     }
-    free(m0); free(p0);
+    free(m0); free(p0); free(mss); free(pss);
     prep_free(&pp);
     return 0;
+}
+
+int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop, const orc_opts* opt,
+                     double* M, double* P, double* V, uint8_t* prom, int nthreads) {
+    return simulate_impl(net, kin, pop, opt, M, P, V, prom, nthreads, 0);
+}
+
+int orc_tauleap_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop, const orc_opts* opt,
+                         double* M, double* P, double* V, uint8_t* prom, int nthreads) {
+    return simulate_impl(net, kin, pop, opt, M, P, V, prom, nthreads, 1);
 }
 
 /* ---------------------------------------------------------------------------

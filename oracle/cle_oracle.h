@@ -75,7 +75,8 @@ typedef struct {
 /* Random-stream tags (bits 31..24 of Philox counter word 3). */
 enum {
     ORC_TAG_NORMAL = 1, ORC_TAG_SWITCH = 2, ORC_TAG_PROMOTER = 3, ORC_TAG_VOLUME = 4,
-    ORC_TAG_MORAN = 5, ORC_TAG_PARTITION = 6, ORC_TAG_EFFICIENCY = 7, ORC_TAG_CAPTURE = 8
+    ORC_TAG_MORAN = 5, ORC_TAG_PARTITION = 6, ORC_TAG_EFFICIENCY = 7, ORC_TAG_CAPTURE = 8,
+    ORC_TAG_TAU = 9
 };
 
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
@@ -89,6 +90,19 @@ void orc_step_normals(uint64_t seed, uint32_t stream, uint32_t cell, uint32_t st
 int orc_cle_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
                      const orc_opts* opt, double* M, double* P, double* V,
                      uint8_t* prom, int nthreads);
+
+/* GPU binomial tau-leap (ext/SyntheticscRNAseqCUDAExt.jl:215-399, population ext:531-651) in
+ * FP32 as the reference's kernels compute it, with the CPU path's cooperative / redundant
+ * edges and telegraph gating (tauleap_binomial.jl:84-137); same arguments and outputs as
+ * orc_cle_simulate, M and P hold molecule counts. */
+int orc_tauleap_simulate(const orc_net* net, const orc_kin* kin, const orc_pop* pop,
+                         const orc_opts* opt, double* M, double* P, double* V,
+                         uint8_t* prom, int nthreads);
+
+/* exp(x) (x <= 0) and the 50-term Poisson inverse CDF of the tau-leap, bit-exact with the
+ * library's device code. */
+float orc_expf(float x);
+float orc_poisson_icdf(float u, float lam);
 
 /* Per-cell capture efficiency (capture.jl:30-36); mean_correction=1 subtracts sigma^2/2. */
 void orc_capture_efficiency(int64_t N, double efficiency, double efficiency_std,

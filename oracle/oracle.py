@@ -68,6 +68,12 @@ def lib():
                                        C.POINTER(_Opts), C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_int]
         L.orc_cle_simulate.restype = C.c_int
+        L.orc_tauleap_simulate.argtypes = L.orc_cle_simulate.argtypes
+        L.orc_tauleap_simulate.restype = C.c_int
+        L.orc_expf.argtypes = [C.c_float]
+        L.orc_expf.restype = C.c_float
+        L.orc_poisson_icdf.argtypes = [C.c_float, C.c_float]
+        L.orc_poisson_icdf.restype = C.c_float
         L.orc_capture_efficiency.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_int32,
                                              C.c_uint64, C.c_uint32, C.c_void_p]
         L.orc_capture_counts.argtypes = [C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,
@@ -122,12 +128,13 @@ def _edges(keep, edges, G):
 
 
 def simulate(net, kin, *, dt, T=50.0, cell_num=1000, seed=0, stream=0, population=None,
-             n_steps=0, nthreads=0, cell_offset=0):
+             n_steps=0, nthreads=0, cell_offset=0, tauleap=False):
     """FP64 oracle run. `net` is a host GeneNetwork (0-based edge indices).
 
     Returns dict with M, P ([G, N] float64), prom ([G, N] uint8) and V ([N]) when
     population is given. `population` is a PopulationConfig-like object with
-    growth_rate, V_div, V_init, div_check_interval, partition, exclude_mother."""
+    growth_rate, V_div, V_init, div_check_interval, partition, exclude_mother.
+    tauleap=True runs the GPU binomial tau-leap restatement (M, P are counts)."""
     keep = _Keep()
     G = int(net.G)
     cn = _edges(keep, net.cooperative, G)
@@ -147,9 +154,9 @@ def simulate(net, kin, *, dt, T=50.0, cell_num=1000, seed=0, stream=0, populatio
         pp = _Pop(population.growth_rate, population.V_div, lo, hi,
                   population.div_check_interval, population.partition_code,
                   int(population.exclude_mother))
-    rc = lib().orc_cle_simulate(C.byref(n), C.byref(k), C.byref(pp) if pp is not None else None,
-                                C.byref(o), M.ctypes.data, P.ctypes.data,
-                                V.ctypes.data, prom.ctypes.data, int(nthreads))
+    fn = lib().orc_tauleap_simulate if tauleap else lib().orc_cle_simulate
+    rc = fn(C.byref(n), C.byref(k), C.byref(pp) if pp is not None else None, C.byref(o), M.ctypes.data,
+            P.ctypes.data, V.ctypes.data, prom.ctypes.data, int(nthreads))
     if rc != 0:
         raise ValueError("oracle rejected the arguments")
     out = {"M": M, "P": P, "prom": prom}
@@ -211,3 +218,11 @@ def switch_uniform(w0, w1):
     L.orc_switch_uniform.argtypes = [C.c_uint32, C.c_uint32]
     L.orc_switch_uniform.restype = C.c_float
     return L.orc_switch_uniform(int(w0), int(w1))
+
+
+def expf(x):
+    return lib().orc_expf(float(x))
+
+
+def poisson_icdf(u, lam):
+    return lib().orc_poisson_icdf(float(u), float(lam))

@@ -6,7 +6,7 @@ include/scrna_cle.h); this package is the host-side mirror of the reference's
 Julia interface.  The directory name is not a Python identifier, so the package
 is imported under the name ``scrna_b200`` (see __graft_entry__.load_package).
 """
-from .model import (CLE, INF, CaptureModel, CoopEdge, GeneNetwork, KineticParams, PopulationConfig,
+from .model import (CLE, INF, BinomialTauLeap, CaptureModel, CoopEdge, GeneNetwork, KineticParams, PopulationConfig,
                     RedunEdge, default_algorithm, hill_activation, hill_repression, is_bursty, n_steps,
                     precompute_hill_matrices, steady_state)
 from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
@@ -19,7 +19,7 @@ from .validate import (column_moments, compare_moments, ks_critical_value, ks_st
 from .mtx import read_10x_mtx
 
 __all__ = [
-    "CLE", "CaptureModel", "CoopEdge", "GeneNetwork", "KineticParams", "PopulationConfig", "RedunEdge",
+    "CLE", "BinomialTauLeap", "CaptureModel", "CoopEdge", "GeneNetwork", "KineticParams", "PopulationConfig", "RedunEdge",
     "default_algorithm", "hill_activation", "hill_repression", "is_bursty", "n_steps",
     "precompute_hill_matrices", "steady_state", "sample_network", "dense_network", "config0", "config1",
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",

@@ -83,6 +83,9 @@ SIGNATURES = {
     "scrna_cle_simulate": (C.c_int, [P, P, P, P, P, P, P, P, P]),
     "scrna_cle_simulate_batch": (C.c_int, [P, I32, P, P, I32, P, P, P, P, P, P]),
     "scrna_apply_capture": (C.c_int, [P, I64, I32, P, P, U64, U32, P, P]),
+    "scrna_tauleap_simulate": (C.c_int, [P, P, P, P, P, P, P, P, P]),
+    "scrna_tauleap_simulate_batch": (C.c_int, [P, I32, P, P, I32, P, P, P, P, P, P]),
+    "scrna_tauleap_run_device": (C.c_int, [P, P, P, P, P, P, P]),
     "scrna_state_create": (C.c_int, [P, P, I64, I32, I32, C.POINTER(P)]),
     "scrna_state_destroy": (C.c_int, [P]),
     "scrna_cle_run_device": (C.c_int, [P, P, P, P, P, P, P]),

@@ -1,8 +1,10 @@
-"""Reference-facing entry points of the GPU CLE, over the C ABI.
+"""Reference-facing entry points of the GPU CLE and binomial tau-leap, over the C ABI.
 
 simulate(net, CLE(dt), kin, gpu=True; cell_num, T, readout)      ext/SyntheticscRNAseqCUDAExt.jl:48-117
 simulate(net, CLE(dt), kin, gpu=True, population=pop; T, readout) ext:409-529
 simulate_gpu_batch(networks, CLE(dt), kin; cell_num, T, readout)  ext:132-213
+simulate(net, BinomialTauLeap(dt), kin, ...)                       ext:215-284, population ext:531-663
+simulate_gpu_batch(networks, BinomialTauLeap(dt), kin[s], ...)     ext:290-399, ext:666-837
 apply_capture(X, capture)                                          src/capture.jl:25-47
 
 Outputs are cells x G (cells x 2G for readout "both") float64 arrays in
@@ -21,7 +23,7 @@ import numpy as np
 
 from . import _lib, _pinned
 from ._lib import Capture, Kinetics, Opts, Population, check
-from .model import CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig
+from .model import BinomialTauLeap, CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig
 
 READOUT = {"mrna": 0, "protein": 1, "both": 2}
 PRECISION = {"fp32": 0, "fp64_plain": 1, "fp32_f16": 2}
@@ -206,7 +208,15 @@ def _cap(cap: Optional[CaptureModel]):
                    int(bool(cap.mean_correction)))
 
 
-def _opts(alg: CLE, *, T, cell_num, readout, seed, stream, precision, path, n_steps, cell_offset):
+def _is_tau(alg) -> bool:
+    if isinstance(alg, BinomialTauLeap):
+        return True
+    if isinstance(alg, CLE):
+        return False
+    raise TypeError(f"algorithm must be CLE(dt) or BinomialTauLeap(dt), got {alg!r}")
+
+
+def _opts(alg, *, T, cell_num, readout, seed, stream, precision, path, n_steps, cell_offset):
     if readout not in READOUT:
         raise ValueError("readout must be 'mrna', 'protein' or 'both'")
     return Opts(float(alg.dt), float(T), int(cell_num), READOUT[readout], PRECISION[precision], int(seed),
@@ -217,13 +227,14 @@ def _ptr(x):
     return None if x is None else C.byref(x)
 
 
-def simulate(net: GeneNetwork, alg: CLE, kin: KineticParams, gpu: bool = True, population=None, *,
+def simulate(net: GeneNetwork, alg, kin: KineticParams, gpu: bool = True, population=None, *,
              cell_num: int = 1000, T: float = 50.0, readout: str = "protein", seed: int = 0,
              stream: int = 0, capture: Optional[CaptureModel] = None, precision: str = "fp32",
              path: str = "auto", n_steps: int = 0, cell_offset: int = 0,
              ctx: Optional[Context] = None, handle: Optional[NetHandle] = None):
-    """GPU CLE run.  Returns the readout matrix, or (matrix, counts, efficiencies)
-    when `capture` is given.  With `population`, pop.cell_num cells are simulated."""
+    """GPU run of CLE(dt) or BinomialTauLeap(dt).  Returns the readout matrix, or (matrix,
+    counts, efficiencies) when `capture` is given.  With `population`, pop.cell_num cells are
+    simulated (the tau-leap then reads out concentrations M / V, P / V)."""
     if not gpu:
         raise NotImplementedError("only the GPU path is provided by this library")
     ctx = ctx or default_context()
@@ -236,15 +247,15 @@ def simulate(net: GeneNetwork, alg: CLE, kin: KineticParams, gpu: bool = True, p
     k, p, c = _kin(kin), _pop(population), _cap(capture)
     o = _opts(alg, T=T, cell_num=N, readout=readout, seed=seed, stream=stream, precision=precision,
               path=path, n_steps=n_steps, cell_offset=cell_offset)
-    check(ctx.lib.scrna_cle_simulate(ctx.h, h.h, C.byref(k), _ptr(p), _ptr(c), C.byref(o),
-                                     out.ctypes.data, None if counts is None else counts.ctypes.data,
-                                     None if eff is None else eff.ctypes.data))
+    fn = ctx.lib.scrna_tauleap_simulate if _is_tau(alg) else ctx.lib.scrna_cle_simulate
+    check(fn(ctx.h, h.h, C.byref(k), _ptr(p), _ptr(c), C.byref(o), out.ctypes.data,
+             None if counts is None else counts.ctypes.data, None if eff is None else eff.ctypes.data))
     if capture is not None:
         return out, counts, eff
     return out
 
 
-def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg: CLE, kin, *,
+def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg, kin, *,
                        cell_num: Union[int, Sequence[int]] = 1000, T: float = 50.0,
                        readout: str = "protein", seed: int = 0, stream: int = 0,
                        populations: Optional[Sequence[Optional[PopulationConfig]]] = None,
@@ -276,8 +287,8 @@ def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg: CLE, kin, *,
     c = _cap(capture)
     o = _opts(alg, T=T, cell_num=0, readout=readout, seed=seed, stream=stream, precision="fp32",
               path="auto", n_steps=0, cell_offset=0)
-    check(ctx.lib.scrna_cle_simulate_batch(ctx.h, B, harr, karr, len(kins), cn_arr, parr, _ptr(c),
-                                           C.byref(o), oarr, carr))
+    fn = ctx.lib.scrna_tauleap_simulate_batch if _is_tau(alg) else ctx.lib.scrna_cle_simulate_batch
+    check(fn(ctx.h, B, harr, karr, len(kins), cn_arr, parr, _ptr(c), C.byref(o), oarr, carr))
     if capture is not None:
         return outs, cnts
     return outs
@@ -301,7 +312,7 @@ class DeviceRun:
     """Device-resident run of one network (scrna_state): `launch()` enqueues a whole
     simulation on the context stream without host traffic; `read()` fetches results."""
 
-    def __init__(self, net: GeneNetwork, alg: CLE, kin: KineticParams, *, cell_num: int, T: float,
+    def __init__(self, net: GeneNetwork, alg, kin: KineticParams, *, cell_num: int, T: float,
                  readout: str = "protein", seed: int = 0, stream: int = 0,
                  capture: Optional[CaptureModel] = None, population: Optional[PopulationConfig] = None,
                  precision: str = "fp32", n_steps: int = 0, cell_offset: int = 0,
@@ -313,6 +324,7 @@ class DeviceRun:
         self.readout = readout
         self.capture = capture
         self.k, self.p, self.c = _kin(kin), _pop(population), _cap(capture)
+        self.tau = _is_tau(alg)
         self.o = _opts(alg, T=T, cell_num=self.N, readout=readout, seed=seed, stream=stream,
                        precision=precision, path=path, n_steps=n_steps, cell_offset=cell_offset)
         h = C.c_void_p()
@@ -321,8 +333,8 @@ class DeviceRun:
         self.st = h
 
     def launch(self):
-        check(self.ctx.lib.scrna_cle_run_device(self.ctx.h, self.handle.h, C.byref(self.k), _ptr(self.p),
-                                                _ptr(self.c), C.byref(self.o), self.st))
+        fn = self.ctx.lib.scrna_tauleap_run_device if self.tau else self.ctx.lib.scrna_cle_run_device
+        check(fn(self.ctx.h, self.handle.h, C.byref(self.k), _ptr(self.p), _ptr(self.c), C.byref(self.o), self.st))
 
     def read(self):
         cols = self.G * (2 if self.readout == "both" else 1)

@@ -35,14 +35,19 @@ struct BatchNet {
     KernelChoice kc{};
     int64_t n_steps = 0;
     bool tensor = false;
+    bool tau = false;
+    // this entry's gene tables and kernel arguments: one network handle may appear several
+    // times in a batch with other kinetics
+    DevBuf genes, ginit, qtel;
+    FusedArgs args{};
 };
 
 struct GroupKey {
-    int warp, gpl, emax, tmax, nwarps, upt, pop, interval;
+    int tau, warp, gpl, emax, tmax, nwarps, upt, pop, interval;
     int64_t n_steps;
     bool operator<(const GroupKey& r) const {
-        return std::tie(warp, gpl, emax, tmax, nwarps, upt, pop, interval, n_steps) <
-               std::tie(r.warp, r.gpl, r.emax, r.tmax, r.nwarps, r.upt, r.pop, r.interval, r.n_steps);
+        return std::tie(tau, warp, gpl, emax, tmax, nwarps, upt, pop, interval, n_steps) <
+               std::tie(r.tau, r.warp, r.gpl, r.emax, r.tmax, r.nwarps, r.upt, r.pop, r.interval, r.n_steps);
     }
 };
 
@@ -72,12 +77,13 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
 int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,
                    int32_t n_kins, const int64_t* cell_nums, const scrna_population* const* pops,
                    const scrna_capture* cap, const scrna_cle_opts* opts, double* const* outs,
-                   int32_t* const* counts) {
+                   int32_t* const* counts, bool tau) {
     std::vector<BatchNet> bn(B);
     std::vector<std::unique_ptr<scrna_state, int (*)(scrna_state*)>> owned;
     for (int b = 0; b < B; ++b) {
         BatchNet& x = bn[b];
         x.b = b;
+        x.tau = tau;
         x.net = const_cast<scrna_net*>(nets[b]);
         x.kin = &kins[n_kins == 1 ? 0 : b];
         x.pop = pops ? pops[b] : nullptr;
@@ -98,13 +104,36 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
         if (int r = scrna_state_create(ctx, x.net, N, x.o.readout, cap != nullptr, &st)) return r;
         owned.emplace_back(st, scrna_state_destroy);
         x.st = st;
-        if (int r = ensure_gene_tables(x.net, x.kin, x.o.dt, x.pop != nullptr)) return r;
         const NetDev& d = x.net->dev;
         const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
-        x.tensor = !x.pop && (d.n_quads > fused_max_quads() || (x.net->G >= 256 && density >= 0.05));
+        x.tensor = !tau && !x.pop && (d.n_quads > fused_max_quads() || (x.net->G >= 256 && density >= 0.05));
+        if (tau && d.n_quads > fused_max_quads())
+            return fail(SCRNA_ENOTSUP, "network %d: the binomial tau-leap takes G <= %d", b, 4 * fused_max_quads());
         if (!x.tensor) {
             if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
-            if (int r = choose_kernel_tuned(ctx, x.net, x.kin, &x.o, st, &x.kc)) return r;
+            const int G = x.net->G, nq = (G + 3) / 4;
+            std::vector<GeneRec> gr(G);
+            std::vector<GeneInit> gi(G);
+            std::vector<uint8_t> qt(nq);
+            gene_tables_host(x.net, x.kin, x.o.dt, gr.data(), gi.data(), qt.data());
+            CU(x.genes.ensure(G * sizeof(GeneRec)));
+            CU(x.ginit.ensure(G * sizeof(GeneInit)));
+            CU(x.qtel.ensure(nq));
+            CU(cudaMemcpy(x.genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(x.ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(x.qtel.p, qt.data(), nq, cudaMemcpyHostToDevice));
+            ctx->h2d_bytes += (int64_t)(G * (sizeof(GeneRec) + sizeof(GeneInit)) + nq);
+            fill_fused_args(x.net, x.kin, x.pop, cap, &x.o, st, &x.args);
+            x.args.genes = x.genes.as<GeneRec>();
+            x.args.ginit = x.ginit.as<GeneInit>();
+            x.args.quad_tel = x.qtel.as<uint8_t>();
+            if (tau) {
+                fill_tau_args(x.net, x.kin, x.pop, &x.o, &x.args);
+                x.kc = choose_kernel(x.net, SCRNA_PATH_BLOCK);
+            } else if (int r = choose_kernel_tuned(ctx, x.net, x.kin, &x.o, st, &x.kc, &x.args, nullptr)) {
+                return r;
+            }
+            x.args.lane_nw1 = x.kc.nw1;
             if (x.kc.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
             x.st->have_counts = cap != nullptr;
         }
@@ -121,6 +150,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
     // dense networks: tensor-core path, one after another on the context stream
     for (BatchNet* x : all)
         if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
+            if (int r = ensure_gene_tables(x->net, x->kin, x->o.dt, false)) return r;
             const bool fused = x->net->G <= 4096;
             x->st->last_tensor = !fused;
             x->st->last_plain = false;
@@ -135,6 +165,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
     for (BatchNet* x : all) {
         if (x->tensor) continue;
         GroupKey k{};
+        k.tau = x->tau;
         k.warp = x->kc.warp;
         k.gpl = x->kc.warp ? x->kc.gpl : 0;
         k.emax = x->kc.warp ? x->kc.emax : 0;
@@ -164,8 +195,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         size_t smem = 0;
         for (size_t i = 0; i < g.nets.size(); ++i) {
             BatchNet* x = g.nets[i];
-            fill_fused_args(x->net, x->kin, x->pop, cap, &x->o, x->st, &args[i]);
-            args[i].lane_nw1 = x->kc.nw1;
+            args[i] = x->args;
             nw = std::max(nw, x->kc.block.nw);
             smem = std::max(smem, x->kc.smem);
             const int64_t cpt = cells_per_tile(*x);
@@ -201,6 +231,9 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
             std::memcpy(ks.rk1, args[0].rk1, sizeof ks.rk1);
         }
         auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
+            if (k.tau)
+                return tau_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
+                                        smem, k.pop != 0, grid, ctl, use_shared, g.stream);
             if (k.warp)
                 return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
                                              k.emax, k.tmax, k.pop != 0, smem, grid, k.nwarps, ctl, use_shared,

@@ -20,6 +20,7 @@ namespace scrna {
 FusedLaunch fused_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int n_quads);
 int fused_max_quads();
 cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st);
+cudaError_t tau_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st);
 int warpcell_max_genes();
 int warpcell_emax_class(int max_in);
 int warpcell_pick_gpl(int G, bool bursty, int emax);
@@ -549,6 +550,21 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
     *out = a;
 }
 
+// The tau-leap's additions to the kernel arguments: FP32 decay probabilities 1 - exp(-mu dt)
+// (with dilution unless a population makes it emergent, ext:240-241 and ext:574-575), FP64
+// basals and steady-state denominators for a population's initial counts (ext:560-566).
+void scrna::fill_tau_args(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                          const scrna_cle_opts* o, FusedArgs* a) {
+    const double mu_m = pop ? kin->mu_m : kin->mu_m + kin->dilution;
+    const double mu_p = pop ? kin->mu_p : kin->mu_p + kin->dilution;
+    a->p_dec_m = (float)(1.0 - std::exp(-mu_m * o->dt));
+    a->p_dec_p = (float)(1.0 - std::exp(-mu_p * o->dt));
+    a->beta64 = net->dev.beta64;
+    a->ss_mu_m = kin->mu_m + kin->dilution;
+    a->ss_mu_p = kin->mu_p + kin->dilution;
+    a->k_t64 = kin->k_t;
+}
+
 // Register-path kernel of a network: warp-per-cell-group (genes per lane, in-edges and
 // terms per gene) or block tiles.
 scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
@@ -567,7 +583,7 @@ scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
 }
 
 static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
-                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st) {
+                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau) {
     const NetDev& d = net->dev;
     if (d.n_quads > fused_max_quads())
         return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
@@ -583,11 +599,14 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
                     "per gene, terms of <= %d sources and <= %d terms per lane", warpcell_max_genes(), kLaneEdges,
                     kLaneSrc, kLaneTerms);
     KernelChoice kc{};
-    if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc)) return r;
+    if (tau) kc = choose_kernel(net, SCRNA_PATH_BLOCK);  // the tau-leap runs on block tiles
+    else if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc)) return r;
     FusedArgs a{};
     fill_fused_args(net, kin, pop, cap, o, st, &a);
+    if (tau) fill_tau_args(net, kin, pop, o, &a);
     a.lane_nw1 = kc.nw1;
     auto launch = [&](bool is_pop) -> cudaError_t {
+        if (tau) return tau_launch(a, kc.block, is_pop, s);
         return kc.warp ? warpcell_launch(a, kc.gpl, kc.emax, kc.tmax, is_pop, s) : fused_launch(a, kc.block, is_pop, s);
     };
     st->last_cell_major = kc.warp;  // the lane kernel keeps M, P, prom, NS cell-major
@@ -675,9 +694,8 @@ static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     return SCRNA_OK;
 }
 
-extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetics* kin,
-                                    const scrna_population* pop, const scrna_capture* cap,
-                                    const scrna_cle_opts* o, scrna_state* st) {
+static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetics* kin, const scrna_population* pop,
+                      const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau) {
     if (int r = check_ctx(ctx)) return r;
     if (int r = validate_run(cnet, kin, pop, cap, o)) return r;
     if (!st) return fail(SCRNA_EINVAL, "state is NULL");
@@ -689,6 +707,14 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
     if (o->readout != st->readout) return fail(SCRNA_EINVAL, "readout differs from the state's readout");
     if (o->cell_offset < 0 || o->cell_offset + N > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
     const bool plain = o->precision == SCRNA_PRECISION_FP64_PLAIN;
+    if (tau) {
+        if (o->precision != SCRNA_PRECISION_FP32)
+            return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs in FP32 (counts) only");
+        if (o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK)
+            return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs on the block-tile register kernel only");
+        if (net->dev.n_quads > fused_max_quads())
+            return fail(SCRNA_ENOTSUP, "the binomial tau-leap takes G <= %d", 4 * fused_max_quads());
+    }
     if (plain && pop) return fail(SCRNA_ENOTSUP, "the FP64 baseline path has no population dynamics");
     if (o->precision != SCRNA_PRECISION_FP32 && o->precision != SCRNA_PRECISION_FP32_F16 && !plain)
         return fail(SCRNA_EINVAL, "unknown precision");
@@ -697,7 +723,7 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
     // kernel family: tensor cores for large dense networks (or when asked), else the register path
     const NetDev& nd = net->dev;
     const double density = (double)nd.n_in / ((double)net->G * net->G);
-    const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
+    const bool tensor = !plain && !tau && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
                                    (o->path == SCRNA_PATH_AUTO &&
                                     (nd.n_quads > fused_max_quads() || (net->G >= 256 && density >= 0.05))));
     if (tensor) {
@@ -721,7 +747,19 @@ extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* cnet, const
     st->last_plain = plain;
     st->last_pop = pop != nullptr;
     if (plain) return run_plain(ctx, net, kin, cap, o, st);
-    return run_fused(ctx, net, kin, pop, cap, o, st);
+    return run_fused(ctx, net, kin, pop, cap, o, st, tau);
+}
+
+extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                                    const scrna_population* pop, const scrna_capture* cap,
+                                    const scrna_cle_opts* o, scrna_state* st) {
+    return run_device(ctx, net, kin, pop, cap, o, st, false);
+}
+
+extern "C" int scrna_tauleap_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                                        const scrna_population* pop, const scrna_capture* cap,
+                                        const scrna_cle_opts* o, scrna_state* st) {
+    return run_device(ctx, net, kin, pop, cap, o, st, true);
 }
 
 extern "C" int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, int32_t* counts, double* eff) {
@@ -799,9 +837,9 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
     return SCRNA_OK;
 }
 
-extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
-                                  const scrna_population* pop, const scrna_capture* cap,
-                                  const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+static int simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                    const scrna_capture* cap, const scrna_cle_opts* o, double* out, int32_t* counts, double* eff,
+                    bool tau) {
     if (int r = check_ctx(ctx)) return r;
     if (int r = validate_run(net, kin, pop, cap, o)) return r;
     if (!out) return fail(SCRNA_EINVAL, "out is NULL");
@@ -828,8 +866,20 @@ extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const sc
         }
         cache.push_back(st);
     }
-    if (int r = scrna_cle_run_device(ctx, net, kin, pop, cap, o, st)) return r;
+    if (int r = run_device(ctx, net, kin, pop, cap, o, st, tau)) return r;
     return scrna_state_read(ctx, st, out, cap ? counts : nullptr, cap ? eff : nullptr);
+}
+
+extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                                  const scrna_population* pop, const scrna_capture* cap,
+                                  const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+    return simulate(ctx, net, kin, pop, cap, o, out, counts, eff, false);
+}
+
+extern "C" int scrna_tauleap_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                                      const scrna_population* pop, const scrna_capture* cap,
+                                      const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+    return simulate(ctx, net, kin, pop, cap, o, out, counts, eff, true);
 }
 
 extern "C" int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets,
@@ -841,7 +891,19 @@ extern "C" int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_n
     if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
     if (opts->precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "batches run the FP32 path");
     if (int r = set_device(ctx)) return r;
-    return batch_simulate(ctx, B, nets, kins, n_kins, cell_nums, pops, cap, opts, outs, counts);
+    return batch_simulate(ctx, B, nets, kins, n_kins, cell_nums, pops, cap, opts, outs, counts, false);
+}
+
+extern "C" int scrna_tauleap_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets,
+                                            const scrna_kinetics* kins, int32_t n_kins, const int64_t* cell_nums,
+                                            const scrna_population* const* pops, const scrna_capture* cap,
+                                            const scrna_cle_opts* opts, double* const* outs, int32_t* const* counts) {
+    if (int r = check_ctx(ctx)) return r;
+    if (B <= 0 || !nets || !kins || !opts || !outs) return fail(SCRNA_EINVAL, "bad batch arguments");
+    if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
+    if (opts->precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs in FP32 only");
+    if (int r = set_device(ctx)) return r;
+    return batch_simulate(ctx, B, nets, kins, n_kins, cell_nums, pops, cap, opts, outs, counts, true);
 }
 
 extern "C" int scrna_apply_capture(scrna_ctx* ctx, int64_t N, int32_t G, const double* X, const scrna_capture* cap,

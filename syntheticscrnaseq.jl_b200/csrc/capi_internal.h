@@ -145,7 +145,8 @@ void fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_popu
 KernelChoice choose_kernel(const scrna_net* net, int path);
 void tune_init_ctx(scrna_ctx* ctx);
 int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
-                        scrna_state* st, KernelChoice* out);
+                        scrna_state* st, KernelChoice* out, const FusedArgs* base = nullptr,
+                        cudaStream_t stream = nullptr);
 int fused_max_quads();
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
@@ -169,5 +170,11 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
 int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,
                    int32_t n_kins, const int64_t* cell_nums, const scrna_population* const* pops,
                    const scrna_capture* cap, const scrna_cle_opts* opts, double* const* outs,
-                   int32_t* const* counts);
+                   int32_t* const* counts, bool tau);
+void fill_tau_args(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                   const scrna_cle_opts* o, FusedArgs* a);
+void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr, GeneInit* gi,
+                      uint8_t* qt);
+cudaError_t tau_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt, int nw,
+                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 }  // namespace scrna

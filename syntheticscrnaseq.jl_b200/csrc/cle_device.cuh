@@ -18,7 +18,8 @@ enum : uint32_t {
     TAG_MORAN = 5,       // (mother, step, 0)          -> replaced slot
     TAG_PARTITION = 6,   // (cell, step, b<<22|g<<1|s) -> partition bits
     TAG_EFFICIENCY = 7,  // (cell, 0, 0)               -> capture efficiency normal
-    TAG_CAPTURE = 8      // (cell, chunk, gene)        -> capture inverse-CDF uniform
+    TAG_CAPTURE = 8,     // (cell, chunk, gene)        -> capture inverse-CDF uniform
+    TAG_TAU = 9          // (cell, step, gene)         -> the four uniforms of a tau-leap update
 };
 
 constexpr int kCaptureChunk = 512;
@@ -340,6 +341,68 @@ __device__ __forceinline__ float2 hill2_n2(float2 p, float Kn) {
     const float2 d = add2(pn, f2(Kn));
     const float2 r = mul2(pn, make_float2(frcp_approx(d.x), frcp_approx(d.y)));
     return make_float2(fminf(r.x, 1.0f), fminf(r.y, 1.0f));
+}
+
+// ---- binomial tau-leap ------------------------------------------------------------------
+// exp(x) for x <= 0 from its definition, every operation explicitly rounded so that a CPU
+// restatement returns the same bits: x = k ln2 + r, k = rint(x log2 e), |r| <= ln2/2
+// (two-constant Cody-Waite reduction), e^r by its Taylor series to r^7 (Horner), then the
+// exact scaling by 2^k (in two steps below 2^-126 so a subnormal result rounds once).
+__device__ __forceinline__ float own_expf(float x) {
+    if (!(x > -104.0f)) return 0.0f;
+    if (x > 0.0f) x = 0.0f;
+    const float k = rintf(__fmul_rn(x, 1.44269502162933349609375f));
+    float r = __fmaf_rn(-k, 0.693145751953125f, x);
+    r = __fmaf_rn(-k, 1.428606765330187045e-06f, r);
+    float q = __fmaf_rn(r, 1.0f / 5040.0f, 1.0f / 720.0f);
+    q = __fmaf_rn(r, q, 1.0f / 120.0f);
+    q = __fmaf_rn(r, q, 1.0f / 24.0f);
+    q = __fmaf_rn(r, q, 1.0f / 6.0f);
+    q = __fmaf_rn(r, q, 0.5f);
+    q = __fmaf_rn(r, q, 1.0f);
+    q = __fmaf_rn(r, q, 1.0f);
+    int ki = (int)k;
+    if (ki < -125) {
+        q = __fmul_rn(q, __uint_as_float(0x1F800000u));  // 2^-64
+        ki += 64;
+    }
+    return __fmul_rn(q, __uint_as_float((uint32_t)(ki + 127) << 23));
+}
+
+// Poisson(lam) by inverse CDF over the first 50 terms (the reference's GPU sampler): the
+// number of partial sums of exp(-lam) lam^j / j! that u exceeds, at most 50.  The partial
+// sums never decrease, so the loop stops at the first one u does not exceed.
+__device__ __forceinline__ float poisson_icdf50(float u, float lam) {
+    float term = own_expf(-lam);
+    float cdf = term;
+    float events = 0.0f;
+    for (int k = 1; k <= 50; ++k) {
+        if (!(u > cdf)) break;
+        events = (float)k;
+        term = __fmul_rn(term, __fdiv_rn(lam, (float)k));
+        cdf = __fadd_rn(cdf, term);
+    }
+    return events;
+}
+
+// The four uniforms of a tau-leap block: (w >> 9) 2^-23 in [0, 1) (the low 9 bits of words
+// 0 and 1 are the telegraph's spare bits, as for the normal words).
+__device__ __forceinline__ float tau_uniform(uint32_t w) { return __fmul_rn((float)(w >> 9), 1.1920928955078125e-07f); }
+
+// One tau-leap update of (m, p) (ext/SyntheticscRNAseqCUDAExt.jl:258-275): transcription
+// Poisson(lam_tx), mRNA decay min(Poisson(m p_m), m), then translation Poisson(k_t m dt) with
+// the new m and protein decay min(Poisson(p p_p), p); counts never go below 0.
+__device__ __forceinline__ void tau_update(float& m, float& p, float lam_tx, uint4 w, float k_t, float dt,
+                                           float p_dec_m, float p_dec_p) {
+    const float n_tx = poisson_icdf50(tau_uniform(w.x), lam_tx);
+    const float mp = fmaxf(m, 0.0f);
+    const float n_md = fminf(poisson_icdf50(tau_uniform(w.y), __fmul_rn(mp, p_dec_m)), mp);
+    const float mn = fmaxf(__fsub_rn(__fadd_rn(m, n_tx), n_md), 0.0f);
+    const float n_tl = poisson_icdf50(tau_uniform(w.z), __fmul_rn(__fmul_rn(k_t, mn), dt));
+    const float pp = fmaxf(p, 0.0f);
+    const float n_pd = fminf(poisson_icdf50(tau_uniform(w.w), __fmul_rn(pp, p_dec_p)), pp);
+    m = mn;
+    p = fmaxf(__fsub_rn(__fadd_rn(p, n_tl), n_pd), 0.0f);
 }
 
 }  // namespace scrna

@@ -9,7 +9,7 @@
 
 namespace scrna {
 
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st);
 
 size_t fused_smem_bytes_host(int G, int n_reg, int n_in, int n_na, int n_na_src, int n_quads) {
@@ -36,14 +36,14 @@ int fused_max_quads() { return 8 * 16; }
 
 cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
     switch (L.upt * 2 + (pop ? 1 : 0)) {
-        case 2: return fused_launch_t<1, false>(a, L.nw, L.smem, st);
-        case 3: return fused_launch_t<1, true>(a, L.nw, L.smem, st);
-        case 4: return fused_launch_t<2, false>(a, L.nw, L.smem, st);
-        case 5: return fused_launch_t<2, true>(a, L.nw, L.smem, st);
-        case 8: return fused_launch_t<4, false>(a, L.nw, L.smem, st);
-        case 9: return fused_launch_t<4, true>(a, L.nw, L.smem, st);
-        case 16: return fused_launch_t<8, false>(a, L.nw, L.smem, st);
-        case 17: return fused_launch_t<8, true>(a, L.nw, L.smem, st);
+        case 2: return fused_launch_t<1, false, false>(a, L.nw, L.smem, st);
+        case 3: return fused_launch_t<1, true, false>(a, L.nw, L.smem, st);
+        case 4: return fused_launch_t<2, false, false>(a, L.nw, L.smem, st);
+        case 5: return fused_launch_t<2, true, false>(a, L.nw, L.smem, st);
+        case 8: return fused_launch_t<4, false, false>(a, L.nw, L.smem, st);
+        case 9: return fused_launch_t<4, true, false>(a, L.nw, L.smem, st);
+        case 16: return fused_launch_t<8, false, false>(a, L.nw, L.smem, st);
+        case 17: return fused_launch_t<8, true, false>(a, L.nw, L.smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -55,7 +55,7 @@ template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
                                     const KeySchedule* ks, cudaStream_t st);
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 
@@ -132,14 +132,44 @@ cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
                                cudaStream_t st) {
     switch (upt * 2 + (pop ? 1 : 0)) {
-        case 2: return fused_queue_launch_t<1, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 3: return fused_queue_launch_t<1, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 4: return fused_queue_launch_t<2, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 5: return fused_queue_launch_t<2, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 8: return fused_queue_launch_t<4, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 9: return fused_queue_launch_t<4, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 16: return fused_queue_launch_t<8, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 17: return fused_queue_launch_t<8, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 2: return fused_queue_launch_t<1, false, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 3: return fused_queue_launch_t<1, true, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 4: return fused_queue_launch_t<2, false, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 5: return fused_queue_launch_t<2, true, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 8: return fused_queue_launch_t<4, false, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 9: return fused_queue_launch_t<4, true, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 16: return fused_queue_launch_t<8, false, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 17: return fused_queue_launch_t<8, true, false>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Binomial tau-leap variant of the block-tile kernel (cle_fused.cuh, TAU).
+cudaError_t tau_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
+    switch (L.upt * 2 + (pop ? 1 : 0)) {
+        case 2: return fused_launch_t<1, false, true>(a, L.nw, L.smem, st);
+        case 3: return fused_launch_t<1, true, true>(a, L.nw, L.smem, st);
+        case 4: return fused_launch_t<2, false, true>(a, L.nw, L.smem, st);
+        case 5: return fused_launch_t<2, true, true>(a, L.nw, L.smem, st);
+        case 8: return fused_launch_t<4, false, true>(a, L.nw, L.smem, st);
+        case 9: return fused_launch_t<4, true, true>(a, L.nw, L.smem, st);
+        case 16: return fused_launch_t<8, false, true>(a, L.nw, L.smem, st);
+        case 17: return fused_launch_t<8, true, true>(a, L.nw, L.smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t tau_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt, int nw,
+                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
+    switch (upt * 2 + (pop ? 1 : 0)) {
+        case 2: return fused_queue_launch_t<1, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 3: return fused_queue_launch_t<1, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 4: return fused_queue_launch_t<2, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 5: return fused_queue_launch_t<2, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 8: return fused_queue_launch_t<4, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 9: return fused_queue_launch_t<4, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 16: return fused_queue_launch_t<8, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 17: return fused_queue_launch_t<8, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -43,7 +43,11 @@ __host__ __device__ inline size_t fused_smem_bytes(int G, int n_reg, int n_in, i
 }
 
 // One cell tile (32 cells) of one network through the step range of `ctl`.
-template <int UPT, bool POP>
+// TAU: the binomial tau-leap (ext/SyntheticscRNAseqCUDAExt.jl:215-399, population :531-651)
+// instead of the CLE step: one Philox block of four uniforms per (cell, step, gene), integer
+// counts in FP32, Hill activation of the concentration P / V with a population (whose initial
+// counts are max(1, round(steady state x V))) and the concentrations M / V, P / V as readout.
+template <int UPT, bool POP, bool TAU = false>
 __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                            unsigned char* smem_raw) {
     Smem sm;
@@ -128,6 +132,21 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
             const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
             V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
         }
+        if (TAU && POP) {  // counts of a cell of volume V at the steady state (ext:560-566)
+#pragma unroll
+            for (int j = 0; j < UPT; ++j) {
+                const int q = warp + j * NW;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int g = 4 * q + i;
+                    if (!(q < a.n_quads && g < G)) continue;
+                    const double mss = __ddiv_rn(a.beta64[g], a.ss_mu_m);
+                    const double pss = __ddiv_rn(__dmul_rn(a.k_t64, mss), a.ss_mu_p);
+                    m[j][i] = (float)fmax(1.0, rint(__dmul_rn(mss, V)));
+                    p[j][i] = (float)fmax(1.0, rint(__dmul_rn(pss, V)));
+                }
+            }
+        }
     } else {
         // A cell replaced at the previous division takes the daughter of its new owner.
         int64_t src = cidx;
@@ -166,6 +185,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
         // Hill activations of regulator genes -> slot table
         float* act = sm.act + (size_t)buf * a.n_reg * 32;
+        const float Vf = POP ? (float)V : 1.0f;
         if (has_reg) {
 #pragma unroll
             for (int j = 0; j < UPT; ++j) {
@@ -176,14 +196,15 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                         const int g = 4 * q + i;
                         if (g < G) {
                             const int slot = sm.genes[g].slot;
-                            if (slot >= 0) act[slot * 32 + lane] = hill_act(p[j][i], a.Kn, a.hill_n, a.hill_int);
+                            if (slot >= 0)
+                                act[slot * 32 + lane] = hill_act(TAU && POP ? __fdiv_rn(p[j][i], Vf) : p[j][i], a.Kn,
+                                                                 a.hill_n, a.hill_int);
                         }
                     }
                 }
             }
             if (NW > 1) __syncthreads(); else __syncwarp();
         }
-        const float Vf = POP ? (float)V : 1.0f;
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
@@ -192,23 +213,25 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
             for (int h = 0; h < 2; ++h) {  // gene pairs 2q, 2q+1 of this quad
                 const int g0 = 4 * q + 2 * h;
                 if (g0 >= G) continue;
-                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h),
-                                       tagword(TAG_NORMAL, a.stream), key);
+                const uint4 w = TAU ? make_uint4(0u, 0u, 0u, 0u)
+                                    : philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h), tagword(TAG_NORMAL, a.stream), key);
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const int i = 2 * h + k;
                     const int g = g0 + k;
                     if (g >= G) continue;
+                    // the tau-leap's four uniforms of this gene
+                    const uint4 wt = TAU ? philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_TAU, a.stream), key) : w;
                     // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
                     // a gene switches when its waiting time runs out and draws the next one
-                    // from the spare bits of its normal words
+                    // from the spare bits of its normal (or tau-leap) words
                     if (s == ns[j][i].x) {
                         const uint32_t bit = 1u << (4 * j + i);
                         on ^= bit;
-                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                        const float us = TAU ? switch_uniform(wt.x, wt.y)
+                                             : (k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w));
                         ns[j][i] = switch_at(s, ns[j][i], us, on & bit, sm.genes[g].inv_on, sm.genes[g].inv_off);
                     }
-                    const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
                     const GeneRec gr = sm.genes[g];
                     float reg = gr.cneg;
                     for (int e = gr.in_begin; e < gr.in_end; ++e) {
@@ -227,10 +250,19 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                             reg = fmaf(na.coef, 1.0f - prod, reg);
                         }
                     }
-                    float tx = reg + gr.beta;
-                    if (POP) tx *= Vf;
-                    if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
-                    em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
+                    if (TAU) {
+                        float tx = fmaxf(__fadd_rn(reg, gr.beta), 0.0f);
+                        if (POP) tx = __fmul_rn(tx, Vf);
+                        float lam = __fmul_rn(tx, dt);
+                        if (!(on & (1u << (4 * j + i)))) lam = 0.0f;
+                        tau_update(m[j][i], p[j][i], lam, wt, k_t, dt, a.p_dec_m, a.p_dec_p);
+                    } else {
+                        const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+                        float tx = reg + gr.beta;
+                        if (POP) tx *= Vf;
+                        if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
+                        em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
+                    }
                 }
             }
         }
@@ -316,9 +348,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                 a.NS[idx] = ns[j][i];
             }
             if (ctl.last && a.out) {
-                if (a.readout == 0) a.out[idx] = (double)m[j][i];
-                else if (a.readout == 1) a.out[idx] = (double)p[j][i];
-                else { a.out[idx] = (double)m[j][i]; a.out[(size_t)(G + g) * N + cell] = (double)p[j][i]; }
+                // tau-leap populations read out concentrations (ext:654-661)
+                const double om = TAU && POP ? __ddiv_rn((double)m[j][i], V) : (double)m[j][i];
+                const double op = TAU && POP ? __ddiv_rn((double)p[j][i], V) : (double)p[j][i];
+                if (a.readout == 0) a.out[idx] = om;
+                else if (a.readout == 1) a.out[idx] = op;
+                else { a.out[idx] = om; a.out[(size_t)(G + g) * N + cell] = op; }
             }
         }
     }
@@ -347,16 +382,16 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     }
 }
 
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU = false>
 __global__ void __launch_bounds__(UPT <= 2 ? 256 : 512) cle_fused_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    fused_tile<UPT, POP>(a, blockIdx.x, ctl, smem_raw);
+    fused_tile<UPT, POP, TAU>(a, blockIdx.x, ctl, smem_raw);
 }
 
 // Persistent form: blocks pull (network, tile, step range) items from a device work queue
 // until it is empty; items of different networks and sizes share one launch.
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU = false>
 __global__ void __launch_bounds__(UPT <= 2 ? 256 : 512)
 cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
@@ -369,14 +404,14 @@ cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items
         __syncthreads();
         if (it >= n_items) return;
         const TileWork w = items[it];
-        fused_tile<UPT, POP>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        fused_tile<UPT, POP, TAU>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
         __syncthreads();
     }
 }
 
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU = false>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st) {
-    auto k = cle_fused_kernel<UPT, POP>;
+    auto k = cle_fused_kernel<UPT, POP, TAU>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)((a.N + 31) / 32);
@@ -384,10 +419,10 @@ cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t
     return cudaGetLastError();
 }
 
-template <int UPT, bool POP>
+template <int UPT, bool POP, bool TAU = false>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    auto k = cle_fused_queue_kernel<UPT, POP>;
+    auto k = cle_fused_queue_kernel<UPT, POP, TAU>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, nw * 32, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);

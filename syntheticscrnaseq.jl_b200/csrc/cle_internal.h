@@ -119,6 +119,11 @@ struct FusedArgs {
     int32_t capture_species;
     double cap_mu_log, cap_sigma;
     int32_t lane_nw1;       // lane kernel: warps per block when a cell fits in one warp (0 = 4)
+    // binomial tau-leap (block kernel with TAU): FP32 decay probabilities 1 - exp(-mu dt),
+    // FP64 basals and steady-state denominators for a population's initial counts
+    float p_dec_m, p_dec_p;
+    const double* beta64;
+    double ss_mu_m, ss_mu_p, k_t64;
 };
 
 // Step range and division flags of one launch (or one queued work item).

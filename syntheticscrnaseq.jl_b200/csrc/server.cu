@@ -104,14 +104,15 @@ static int setup_request(scrna_server* s, SrvRequest* r) {
     CU(cudaMemcpy(r->genes.p, gr.data(), G * sizeof(GeneRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(r->ginit.p, gi.data(), G * sizeof(GeneInit), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(r->qtel.p, qt.data(), qt.size(), cudaMemcpyHostToDevice));
-    if (int rr = choose_kernel_tuned(s->ctx, const_cast<scrna_net*>(n), &r->req.kin, &r->req.opts, r->st, &r->kc))
-        return rr;
     fill_fused_args(r->net, &r->req.kin, nullptr, r->req.with_capture ? &r->req.capture : nullptr, &r->req.opts,
                     r->st, &r->args);
-    r->args.lane_nw1 = r->kc.nw1;
-    r->args.genes = r->genes.as<GeneRec>();
+    r->args.genes = r->genes.as<GeneRec>();  // this request's tables (the network's own are not uploaded here)
     r->args.ginit = r->ginit.as<GeneInit>();
     r->args.quad_tel = r->qtel.as<uint8_t>();
+    if (int rr = choose_kernel_tuned(s->ctx, const_cast<scrna_net*>(n), &r->req.kin, &r->req.opts, r->st, &r->kc,
+                                     &r->args, s->stream))
+        return rr;
+    r->args.lane_nw1 = r->kc.nw1;
     return SCRNA_OK;
 }
 

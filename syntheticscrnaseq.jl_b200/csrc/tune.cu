@@ -263,15 +263,21 @@ static std::vector<scrna_tune_choice> candidates(const scrna_net* net, int path)
     return out;
 }
 
-// Measures the candidates on the state buffers of `st` (allocated for `N` cells) and returns
-// the fastest; SCRNA_OK with c->found = 0 when there is nothing to choose.
-static int measure(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
-                   scrna_state* st, int path, scrna_tune_choice* best) {
+// Measures the candidates on the state buffers of `st` (allocated for `N` cells) with the
+// kernel arguments `base` (its tables; state, step range and outputs are set here), on
+// `stream`, and returns the fastest; SCRNA_OK with c->found = 0 when there is nothing to
+// choose or the arguments lack a table.
+static int measure(scrna_ctx* ctx, scrna_net* net, const FusedArgs& base, scrna_state* st, int path,
+                   cudaStream_t stream, scrna_tune_choice* best) {
     const auto cands = candidates(net, path);
     *best = scrna_tune_choice{};
     if (cands.size() < 2) return SCRNA_OK;
-    FusedArgs a{};
-    fill_fused_args(net, kin, nullptr, nullptr, o, st, &a);
+    if (!base.genes || !base.ginit || !base.quad_tel || !st->M.p || !st->P.p || !st->prom.p || !st->NS.p)
+        return SCRNA_OK;
+    FusedArgs a = base;
+    a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int2>();
+    a.N = st->N;
+    a.V = nullptr;
     a.out = nullptr;
     a.counts = nullptr;
     a.eff = nullptr;
@@ -289,14 +295,14 @@ static int measure(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, co
         const KernelChoice k = choice_from(net, c);
         a.lane_nw1 = k.nw1;
         auto launch = [&]() {
-            return k.warp ? warpcell_launch(a, k.gpl, k.emax, k.tmax, false, ctx->stream)
-                          : fused_launch(a, k.block, false, ctx->stream);
+            return k.warp ? warpcell_launch(a, k.gpl, k.emax, k.tmax, false, stream)
+                          : fused_launch(a, k.block, false, stream);
         };
         double ms_min = 1e30;
         for (int rep = 0; rep < 4 && err == SCRNA_OK; ++rep) {
-            cudaError_t e = cudaEventRecord(e0, ctx->stream);
+            cudaError_t e = cudaEventRecord(e0, stream);
             if (e == cudaSuccess) e = launch();
-            if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
             if (e == cudaSuccess) e = cudaEventSynchronize(e1);
             float ms = 0;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
@@ -318,10 +324,12 @@ static int measure(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, co
 }
 
 // The register-path kernel of a run: the static choice (choose_kernel), or with autotuning on
-// the cached or measured fastest variant for the network's shape.  `st` must hold state
-// buffers for N cells (state_alloc) when a measurement may be needed.
+// the cached or measured fastest variant for the network's shape.  A measurement runs on
+// `st`'s state buffers (state_alloc for N cells) with the kernel arguments `base` (NULL:
+// those of fill_fused_args, whose gene tables ensure_gene_tables has uploaded) on `stream`
+// (NULL: the context's).
 int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
-                        scrna_state* st, KernelChoice* out) {
+                        scrna_state* st, KernelChoice* out, const FusedArgs* base, cudaStream_t stream) {
     *out = choose_kernel(net, o->path);
     ctx->tune_last = scrna_tune_choice{out->warp ? 1 : 0, out->warp ? out->gpl : 0, out->warp ? out->nw1 : 0, 0, 0.0};
     const int path = o->path;
@@ -340,7 +348,10 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     if (!c.found && !ctx->tune_path.empty())
         if (int r = lookup(ctx->tune_path, key, &c)) return r;
     if (!c.found && ctx->tune_mode == 1) {
-        if (int r = measure(ctx, net, kin, o, st, path, &c)) return r;
+        FusedArgs a{};
+        if (base) a = *base;
+        else fill_fused_args(net, kin, nullptr, nullptr, o, st, &a);
+        if (int r = measure(ctx, net, a, st, path, stream ? stream : ctx->stream, &c)) return r;
         if (c.found && !ctx->tune_path.empty()) store(ctx->tune_path, key, c);  // unwritable: keep it in memory
     }
     if (!c.found) return SCRNA_OK;

@@ -4,6 +4,7 @@ GeneNetwork / CoopEdge / RedunEdge     src/network.jl:16-96
 KineticParams                          src/kinetics.jl:25-50
 PopulationConfig / CaptureModel        src/population.jl:27-74
 CLE                                    src/algorithms/cle.jl:21-23
+BinomialTauLeap                        src/algorithms/tauleap_binomial.jl:19-22
 
 Indices are 0-based in Python (the Julia shim converts from 1-based).
 """
@@ -154,6 +155,13 @@ class CaptureModel:
 @dataclass(frozen=True)
 class CLE:
     """Chemical Langevin Equation with Euler-Maruyama and collapsed noise (cle.jl:21-23)."""
+    dt: float
+
+
+@dataclass(frozen=True)
+class BinomialTauLeap:
+    """Binomial tau-leap with step dt (tauleap_binomial.jl:19-22); on the GPU the reference's
+    FP32 inverse-CDF form (ext/SyntheticscRNAseqCUDAExt.jl:215-399)."""
     dt: float
 
 

@@ -1,0 +1,131 @@
+"""GPU binomial tau-leap (ext/SyntheticscRNAseqCUDAExt.jl:215-399, population :531-663) against
+the oracle's FP32 restatement, through the C ABI.
+
+Unregulated networks (constitutive and telegraph genes, with and without a Moran population):
+the kernel and the oracle run the same explicitly rounded FP32 operations on the same Philox
+uniforms, so counts, promoter states, volumes and the concentration readout are bit-exact.
+Regulated networks: the oracle's regulation is FP64 (cle.jl's contraction) and the kernel's
+FP32, so a count can differ where a uniform falls within rounding of a Poisson CDF step;
+fewer than 1 % of the final counts may differ and per-gene means agree within 1 %.
+Statistical pins of the reference: test/test_analytical_moments.jl:85-96 (means within 3 %,
+variance and Fano within 15 % of the exact two-stage moments) and test/test_gpu_parity.jl:32-42.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _unregulated(pkg, G, bursty, seed):
+    rng = np.random.default_rng(seed)
+    kon = np.exp(rng.uniform(np.log(0.1), np.log(1.0), G)) if bursty else None
+    koff = np.exp(rng.uniform(np.log(1.0), np.log(10.0), G)) if bursty else None
+    return pkg.GeneNetwork(G, np.exp(rng.uniform(0.0, np.log(10.0), G)), np.zeros((G, G)), k_on=kon, k_off=koff)
+
+
+def _tau_run(pkg, net, kin, **kw):
+    run = pkg.DeviceRun(net, pkg.BinomialTauLeap(kw.pop("dt", 0.05)), kin, **kw)
+    run.launch()
+    return run
+
+
+@pytest.mark.parametrize("G,bursty", [(1, False), (4, False), (7, True), (13, True)])
+def test_unregulated_trajectories_bit_exact(pkg, orc, G, bursty):
+    net = _unregulated(pkg, G, bursty, seed=G)
+    kin = pkg.KineticParams(k_t=3.0, K_d=10.0, n=2.0, mu_m=0.7, mu_p=0.3)
+    N, steps = 300, 400
+    got = _tau_run(pkg, net, kin, cell_num=N, T=0.0, n_steps=steps, seed=5, readout="both").read_raw()
+    ref = orc.simulate(net, kin, dt=0.05, cell_num=N, n_steps=steps, seed=5, tauleap=True)
+    assert np.array_equal(got["M"], ref["M"]) and np.array_equal(got["P"], ref["P"])
+    assert np.array_equal(got["prom"], ref["prom"])
+    assert np.all(got["M"] == np.round(got["M"])) and np.all(got["M"] >= 0)
+
+
+@pytest.mark.parametrize("partition,exclude_mother", [("binomial", False), ("halve", True)])
+def test_population_bit_exact(pkg, orc, partition, exclude_mother):
+    net = _unregulated(pkg, 5, True, seed=9)
+    kin = pkg.KineticParams(k_t=2.0, K_d=10.0, n=2.0, mu_m=0.8, mu_p=0.25, dilution=0.1)
+    N, steps = 200, 350
+    pop = pkg.PopulationConfig(cell_num=N, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10,
+                               partition=partition, exclude_mother=exclude_mother)
+    run = _tau_run(pkg, net, kin, cell_num=N, T=0.0, n_steps=steps, seed=8, readout="both", population=pop)
+    got = run.read_raw()
+    ref = orc.simulate(net, kin, dt=0.05, cell_num=N, n_steps=steps, seed=8, population=pop, tauleap=True)
+    assert np.array_equal(got["V"], ref["V"])
+    assert np.array_equal(got["M"], ref["M"]) and np.array_equal(got["P"], ref["P"])
+    # readout: concentrations (ext:654-661)
+    X = run.read()
+    assert np.array_equal(X[:, :5], (ref["M"] / ref["V"]).T) and np.array_equal(X[:, 5:], (ref["P"] / ref["V"]).T)
+
+
+def test_regulated_network_against_oracle(pkg, orc):
+    net = pkg.sample_network(10, seed=1, bursty=True)
+    assert net.cooperative or net.redundant
+    kin = pkg.WORKLOAD_KINETICS
+    N, steps = 2000, 300
+    got = _tau_run(pkg, net, kin, cell_num=N, T=0.0, n_steps=steps, seed=4, readout="both", dt=0.01).read_raw()
+    ref = orc.simulate(net, kin, dt=0.01, cell_num=N, n_steps=steps, seed=4, tauleap=True)
+    assert np.array_equal(got["prom"], ref["prom"])
+    for k in ("M", "P"):
+        assert np.mean(got[k] != ref[k]) < 0.01, k
+        mg, mr = got[k].mean(1), ref[k].mean(1)
+        assert np.max(np.abs(mg - mr) / np.maximum(mr, 1.0)) < 0.01, k
+
+
+def test_two_stage_moments(pkg):
+    """test/test_analytical_moments.jl:85-96 on the GPU tau-leap."""
+    beta, mu_m, mu_p, k_t = 2.0, 0.1, 0.2, 1.0
+    net = pkg.GeneNetwork(1, [beta], np.zeros((1, 1)))
+    kin = pkg.KineticParams(k_t=k_t, K_d=50.0, n=2.0, mu_m=mu_m, mu_p=mu_p)
+    Y = pkg.simulate(net, pkg.BinomialTauLeap(0.1), kin, cell_num=10000, T=500.0, readout="both", seed=42)
+    m, p = Y[:, 0], Y[:, 1]
+    assert abs(m.mean() / (beta / mu_m) - 1) < 0.03
+    assert abs(m.var(ddof=1) / (beta / mu_m) - 1) < 0.15
+    assert abs(p.mean() / (k_t * beta / (mu_m * mu_p)) - 1) < 0.03
+    assert abs((p.var(ddof=1) / p.mean()) / (1 + k_t / (mu_m + mu_p)) - 1) < 0.15
+
+
+def test_gpu_vs_cpu_mean(pkg, orc):
+    """test/test_gpu_parity.jl:32-42: GPU tau-leap mean within 5 % of the CPU run's."""
+    net = pkg.GeneNetwork(1, [5.0], np.zeros((1, 1)))
+    kin = pkg.KineticParams(k_t=2.0, K_d=50.0, n=2.0, mu_m=0.1, mu_p=0.2)
+    Yg = pkg.simulate(net, pkg.BinomialTauLeap(0.1), kin, cell_num=5000, T=200.0, readout="protein", seed=42)
+    Yc = orc.simulate(net, kin, dt=0.1, T=200.0, cell_num=5000, seed=7, tauleap=True)["P"][0]
+    assert abs(Yg.mean() - Yc.mean()) / Yc.mean() < 0.05
+
+
+def test_batch_equals_single_runs_and_oracle(pkg, orc):
+    """simulate_gpu_batch(networks, BinomialTauLeap(dt), kinetics; ...) with uneven G and cells,
+    per-network kinetics and populations (ext:666-837): equal to single runs bit for bit, and
+    for the unregulated networks to the oracle."""
+    nets = [_unregulated(pkg, G, bool(i % 2), seed=50 + i) for i, G in enumerate((2, 5, 9, 3))]
+    nets.append(pkg.sample_network(12, seed=3, bursty=True))
+    kins = [pkg.KineticParams(k_t=2.0 + i, K_d=10.0, n=2.0, mu_m=0.5 + 0.1 * i, mu_p=0.2) for i in range(5)]
+    cells = [100, 257, 64, 300, 150]
+    pops = [None, pkg.PopulationConfig(cell_num=257, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                                       div_check_interval=10, exclude_mother=False), None, None,
+            pkg.PopulationConfig(cell_num=150, growth_rate=0.5, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=5)]
+    T, dt = 2.0, 0.05
+    outs = pkg.simulate_gpu_batch(nets, pkg.BinomialTauLeap(dt), kins, cell_num=cells, T=T, populations=pops,
+                                  readout="both", seed=6, stream=20)
+    for b, net in enumerate(nets):
+        single = pkg.simulate(net, pkg.BinomialTauLeap(dt), kins[b], population=pops[b], cell_num=cells[b], T=T,
+                              readout="both", seed=6, stream=20 + b)
+        assert np.array_equal(outs[b], single), b
+        if b < 4:
+            r = orc.simulate(net, kins[b], dt=dt, T=T, cell_num=cells[b], seed=6, stream=20 + b, population=pops[b],
+                             tauleap=True)
+            M, P = (r["M"] / r["V"], r["P"] / r["V"]) if pops[b] is not None else (r["M"], r["P"])
+            assert np.array_equal(outs[b], np.hstack([M.T, P.T])), b
+
+
+def test_tauleap_capture_and_validation(pkg, orc):
+    net = _unregulated(pkg, 6, True, seed=77)
+    kin = pkg.KineticParams(k_t=4.0, K_d=10.0, n=2.0, mu_m=1.0, mu_p=0.2)
+    cap = pkg.CaptureModel(efficiency=0.3, efficiency_std=0.4, readout="protein")
+    X, counts, eff = pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=400, T=3.0, readout="protein",
+                                  seed=12, capture=cap)
+    want = orc.capture_counts(np.ascontiguousarray(X.T), eff, seed=12)
+    assert np.array_equal(counts.T, want)
+    with pytest.raises(pkg.ScrnaError):
+        pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=10, T=1.0, path="tensor")
