@@ -239,10 +239,12 @@ int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* prot
  * a JSON cache file (SCRNA_AUTOTUNE_CACHE, else $XDG_CACHE_HOME or ~/.cache
  * /scrna_b200/autotune.json), which later runs and processes read.  Applies to the AUTO,
  * REGISTER and WARP paths of scrna_cle_simulate, scrna_cle_run_device (a measurement there
- * waits for the device), the batch call and the server. */
+ * waits for the device), the batch call and the server.  The fused tensor-core step's tile
+ * width (160, 192 or 224 genes; the same contraction order, so identical results) is tuned
+ * the same way per (device, G, operand type, telegraph genes, Hill exponent 2, cell bucket). */
 typedef struct {
-    int32_t kernel;          /* 0 block tiles, 1 lane kernel */
-    int32_t genes_per_lane;  /* lane kernel: 2 or 4 */
+    int32_t kernel;          /* 0 block tiles, 1 lane kernel, 2 the fused tensor-core step */
+    int32_t genes_per_lane;  /* lane kernel: 2 or 4; tensor-core step: genes per tile (160, 192, 224) */
     int32_t block_warps;     /* lane kernel with cells within one warp: 2, 4 or 8 (0: default) */
     int32_t found;           /* lookups: 1 if the key was in the cache */
     double us_per_step;      /* measured time of one Euler step of the whole run */

@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -144,6 +145,11 @@ void fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_popu
                      const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, FusedArgs* out);
 KernelChoice choose_kernel(const scrna_net* net, int path);
 void tune_init_ctx(scrna_ctx* ctx);
+// Tile width of the fused tensor-core step (slices of 32 genes: 5, 6 or 7): 7 with autotuning
+// off, else the cached or measured fastest (measure(S, &us_per_step)); *measured tells
+// whether measurement launches ran.
+int tc_choose_slices(scrna_ctx* ctx, int G, int64_t N, bool bursty, int dtype, bool hill2,
+                     const std::function<int(int, double*)>& measure, int* S, bool* measured);
 int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
                         scrna_state* st, KernelChoice* out, const FusedArgs* base = nullptr,
                         cudaStream_t stream = nullptr);

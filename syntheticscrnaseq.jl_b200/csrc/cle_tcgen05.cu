@@ -187,20 +187,27 @@ struct TcStepArgs {
     int* err;
 };
 
-// Step kernel tiles: 128 cells x 224 genes, N = 224 = 7 column slices of 32 per TMEM lane
-// quadrant, so 28 epilogue warps (7 per scheduler, 960 threads, 64 registers) hide each
-// other's latencies: the epilogue is latency-bound (per dense step 0.925 ms with 4 epilogue
-// warps per scheduler, 0.911 with 5, 0.877 with 6, 0.869 with 7 on one box).  The two
-// accumulators sit 256 columns apart in one 512-column allocation.
-constexpr int kTsBN = 224, kTsSlices = 7, kTsSliceCols = kTsBN / kTsSlices, kTsAccCols = 256;
-constexpr uint32_t kTsBBytes = kTsBN * kTcBK * 2;
-constexpr size_t kTsSmem = 1024 + (size_t)kTcStages * (kTcABytes + kTsBBytes) + 256;
-constexpr int kTcEpiWarps = 4 * kTsSlices;
+// Step kernel tiles: 128 cells x 32 S genes, S column slices of 32 per TMEM lane quadrant and
+// 4 S epilogue warps.  S = 7 (224 genes, 28 epilogue warps: 7 per scheduler, 960 threads, 64
+// registers) is the default: the epilogue is latency-bound and more epilogue warps per
+// scheduler hide each other's latencies (per dense step 0.925 ms with 4 per scheduler, 0.911
+// with 5, 0.877 with 6, 0.869 with 7 on one box).  S = 5 (160) and 6 (192) waste fewer columns
+// when G is just above a multiple of the tile, and the autotuner measures them (tc_run).  The
+// two accumulators sit 256 columns apart in one 512-column allocation.
+constexpr int kTsSliceCols = 32, kTsAccCols = 256;
 constexpr int kTcMaxGenes = 4096; // gene table of the epilogue in shared memory (8 bytes a gene)
-constexpr int kTcStepThreads = 32 * (2 + kTcEpiWarps);
-static_assert(kTsBN % 16 == 0 && kTsBN <= 256 && kTsSliceCols % 8 == 0, "UMMA N and epilogue groups");
-static_assert(kTsBBytes % 1024 == 0, "128-byte-swizzled stages stay 1024-byte aligned");
-static_assert(kTsSmem + 8 * (size_t)kTcMaxGenes + 8 <= 227 * 1024, "shared memory of the step kernel");
+template <int S>
+struct TcTile {
+    static constexpr int BN = 32 * S;
+    static constexpr uint32_t BBytes = BN * kTcBK * 2;
+    static constexpr size_t Smem = 1024 + (size_t)kTcStages * (kTcABytes + BBytes) + 256;
+    static constexpr int EpiWarps = 4 * S;
+    static constexpr int Threads = 32 * (2 + EpiWarps);
+    static_assert(BN % 16 == 0 && BN <= kTsAccCols, "UMMA N and the accumulator spacing");
+    static_assert(BBytes % 1024 == 0, "128-byte-swizzled stages stay 1024-byte aligned");
+    static_assert(Smem + 8 * (size_t)kTcMaxGenes + 8 <= 227 * 1024, "shared memory of the step kernel");
+    static_assert(Threads <= 1024, "threads of the step kernel");
+};
 
 template <class T> struct TcPack;
 template <> struct TcPack<__nv_bfloat16> {
@@ -330,11 +337,13 @@ __device__ __forceinline__ void tc_step_group(const TcStepArgs& a, const float* 
     }
 }
 
-template <class T, bool BURSTY, int HN>
-__global__ void __launch_bounds__(kTcStepThreads, 1)
+template <class T, bool BURSTY, int HN, int S>
+__global__ void __launch_bounds__(TcTile<S>::Threads, 1)
 tc_cle_step_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                    const TcStepArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
+    constexpr int kTsBN = TcTile<S>::BN, kTcEpiWarps = TcTile<S>::EpiWarps;
+    constexpr uint32_t kTsBBytes = TcTile<S>::BBytes;
     const uint32_t base = tc::smem_u32(smem_dyn);
     unsigned char* stages = smem_dyn + ((1024 - (base & 1023)) & 1023);
     unsigned char* a_s = stages;
@@ -574,6 +583,25 @@ int tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, i
 
 int64_t run_steps(const scrna_cle_opts* o);
 
+// The step kernel of a tile width (S slices of 32 genes), operand type, switching and Hill
+// exponent 2, and its static shared memory.
+using TcStepFn = void (*)(const CUtensorMap, const CUtensorMap, const TcStepArgs);
+template <int S>
+static TcStepFn tc_step_fn_s(bool bf16, bool bursty, bool h2) {
+    if (bf16)
+        return bursty ? (h2 ? tc_cle_step_kernel<__nv_bfloat16, true, 2, S> : tc_cle_step_kernel<__nv_bfloat16, true, 0, S>)
+                      : (h2 ? tc_cle_step_kernel<__nv_bfloat16, false, 2, S> : tc_cle_step_kernel<__nv_bfloat16, false, 0, S>);
+    return bursty ? (h2 ? tc_cle_step_kernel<__half, true, 2, S> : tc_cle_step_kernel<__half, true, 0, S>)
+                  : (h2 ? tc_cle_step_kernel<__half, false, 2, S> : tc_cle_step_kernel<__half, false, 0, S>);
+}
+static TcStepFn tc_step_fn(int S, bool bf16, bool bursty, bool h2) {
+    return S == 5 ? tc_step_fn_s<5>(bf16, bursty, h2) : S == 6 ? tc_step_fn_s<6>(bf16, bursty, h2)
+                                                        : tc_step_fn_s<7>(bf16, bursty, h2);
+}
+static size_t tc_step_smem(int S) {
+    return S == 5 ? TcTile<5>::Smem : S == 6 ? TcTile<6>::Smem : TcTile<7>::Smem;
+}
+
 // The dense path with the fused kernel: per Euler step the term columns, then one
 // tc_cle_step_kernel launch.  Synchronous: it reads back the pipeline error flag.
 int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
@@ -602,25 +630,28 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     const unsigned b_all = (unsigned)((gn + 255) / 256);
     const GeneRec* genes = n->b_genes.as<GeneRec>();
     const int32_t* src_of_gene = n->t_src_of_gene.as<int32_t>();
-    if (bf16)
-        tc_init_kernel<__nv_bfloat16><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(),
-                                                            genes, src_of_gene, Kn, (float)kin->n, hill_int, key0, key1,
-                                                            sid, st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(),
-                                                            st->NS.as<int2>(), reinterpret_cast<__nv_bfloat16*>(act[0]),
-                                                            st->tact32[0].as<float>());
-    else
-        tc_init_kernel<__half><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(), genes,
-                                                     src_of_gene, Kn, (float)kin->n, hill_int, key0, key1, sid,
-                                                     st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(),
-                                                     st->NS.as<int2>(), reinterpret_cast<__half*>(act[0]),
-                                                     st->tact32[0].as<float>());
+    auto init = [&]() {
+        if (bf16)
+            tc_init_kernel<__nv_bfloat16><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(),
+                                                                genes, src_of_gene, Kn, (float)kin->n, hill_int, key0, key1,
+                                                                sid, st->M.as<float>(), st->P.as<float>(),
+                                                                st->prom.as<uint8_t>(), st->NS.as<int2>(),
+                                                                reinterpret_cast<__nv_bfloat16*>(act[0]),
+                                                                st->tact32[0].as<float>());
+        else
+            tc_init_kernel<__half><<<b_all, 256, 0, s>>>(G, N, Kp, n_src, o->cell_offset, n->b_ginit.as<GeneInit>(), genes,
+                                                         src_of_gene, Kn, (float)kin->n, hill_int, key0, key1, sid,
+                                                         st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(),
+                                                         st->NS.as<int2>(), reinterpret_cast<__half*>(act[0]),
+                                                         st->tact32[0].as<float>());
+    };
+    init();
     CU(cudaGetLastError());
     ctx->launches++;
 
-    CUtensorMap map_a[2], map_b;
+    CUtensorMap map_a[2];
     for (int k = 0; k < 2; ++k)
         if (int r = tc_make_map(&map_a[k], act[k], N, Kp, kTcBM, bf16)) return r;
-    if (int r = tc_make_map(&map_b, n->t_w16.p, G, Kp, kTsBN, bf16)) return r;
 
     TcStepArgs a{};
     a.G = G; a.Kp = Kp; a.n_src = n_src; a.hill_int = hill_int;
@@ -638,17 +669,63 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
     a.M = st->M.as<float>(); a.P = st->P.as<float>(); a.prom = st->prom.as<uint8_t>(); a.NS = st->NS.as<int2>();
     a.err = ctx->tc_err.as<int>();
 
-    using StepFn = void (*)(const CUtensorMap, const CUtensorMap, const TcStepArgs);
     const bool h2 = hill_int == 2, bursty = n->dev.bursty;
-    StepFn fn;
-    if (bf16) fn = bursty ? (h2 ? tc_cle_step_kernel<__nv_bfloat16, true, 2> : tc_cle_step_kernel<__nv_bfloat16, true, 0>)
-                          : (h2 ? tc_cle_step_kernel<__nv_bfloat16, false, 2> : tc_cle_step_kernel<__nv_bfloat16, false, 0>);
-    else fn = bursty ? (h2 ? tc_cle_step_kernel<__half, true, 2> : tc_cle_step_kernel<__half, true, 0>)
-                     : (h2 ? tc_cle_step_kernel<__half, false, 2> : tc_cle_step_kernel<__half, false, 0>);
-    const size_t smem = kTsSmem + (size_t)(((G + 1) & ~1) + G) * 4;  // + the epilogue's gene table
-    CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + kTsBN - 1) / kTsBN);
-    const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
+    // one launch configuration per tile width (S slices of 32 genes)
+    struct StepCfg {
+        TcStepFn fn;
+        int threads;
+        size_t smem;
+        int grid;
+        CUtensorMap map_b;
+    };
+    auto cfg_of = [&](int S, StepCfg* c) -> int {
+        c->fn = tc_step_fn(S, bf16, bursty, h2);
+        c->threads = 32 * (2 + 4 * S);
+        c->smem = tc_step_smem(S) + (size_t)(((G + 1) & ~1) + G) * 4;  // + the epilogue's gene table
+        const int BN = 32 * S;
+        const int64_t tiles = ((N + kTcBM - 1) / kTcBM) * ((G + BN - 1) / BN);
+        c->grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
+        if (int r = tc_make_map(&c->map_b, n->t_w16.p, G, Kp, BN, bf16)) return r;
+        CU(cudaFuncSetAttribute(c->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem));
+        return SCRNA_OK;
+    };
+    // tile width: 224 genes, or the fastest of 160 / 192 / 224 measured for this shape (the
+    // measurement runs a few steps and the run then starts again from its initial state)
+    int S = 7;
+    bool measured = false;
+    if (int r = tc_choose_slices(ctx, G, N, bursty, dtype, h2, [&](int Sc, double* us) -> int {
+            StepCfg c;
+            if (int r = cfg_of(Sc, &c)) return r;
+            cudaEvent_t e0, e1;
+            CU(cudaEventCreate(&e0));
+            CU(cudaEventCreate(&e1));
+            float best = 1e30f;
+            for (int rep = 0; rep < 4; ++rep) {
+                a.step = 1 + rep;
+                a.act_next = act[1 - (rep & 1)];
+                a.act32_next = st->tact32[1 - (rep & 1)].as<float>();
+                CU(cudaEventRecord(e0, s));
+                c.fn<<<c.grid, c.threads, c.smem, s>>>(map_a[rep & 1], c.map_b, a);
+                CU(cudaGetLastError());
+                CU(cudaEventRecord(e1, s));
+                CU(cudaEventSynchronize(e1));
+                float ms = 0;
+                CU(cudaEventElapsedTime(&ms, e0, e1));
+                ctx->launches++;
+                if (rep > 0) best = std::min(best, ms);
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            *us = 1e3 * best;
+            return SCRNA_OK;
+        }, &S, &measured)) return r;
+    if (measured) {  // the measurement stepped the state: start again from the initial state
+        init();
+        CU(cudaGetLastError());
+        ctx->launches++;
+    }
+    StepCfg cfg;
+    if (int r = cfg_of(S, &cfg)) return r;
     const int64_t n_steps = run_steps(o);
     for (int64_t step = 1; step <= n_steps; ++step) {
         const int cur = (int)((step - 1) & 1), nxt = (int)(step & 1);
@@ -660,7 +737,7 @@ int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_
         a.step = (int)step;
         a.act_next = act[nxt];
         a.act32_next = st->tact32[nxt].as<float>();
-        fn<<<grid, kTcStepThreads, smem, s>>>(map_a[cur], map_b, a);
+        cfg.fn<<<cfg.grid, cfg.threads, cfg.smem, s>>>(map_a[cur], cfg.map_b, a);
         CU(cudaGetLastError());
         ctx->launches++;
     }

@@ -21,6 +21,7 @@
 #pragma once
 #include "cle_device.cuh"
 #include "cle_internal.h"
+#include "philox_hoist.cuh"
 
 namespace scrna {
 
@@ -295,9 +296,17 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
     // beside step s's update (two independent dependency chains per lane), where the
     // registers allow it without spilling.
     constexpr bool AHEAD = GPL == 2 && EMAX <= 4 && TMAX <= 1;
+    // With the round keys given, the part of the first Philox rounds that does not depend on
+    // the step is computed once per lane (philox_hoist.cuh; same bits as philox_rk).
+    PhiloxHoist ph[GPL / 2];
+    if (RK) {
+#pragma unroll
+        for (int h = 0; h < GPL / 2; ++h)
+            ph[h] = philox_hoist(gcell, (uint32_t)(u * (GPL / 2) + h), tagword(TAG_NORMAL, a.stream), rk0, rk1);
+    }
     auto draw = [&](int s, int h) {
         const uint32_t c2 = (uint32_t)(u * (GPL / 2) + h), c3 = tagword(TAG_NORMAL, a.stream);
-        return RK ? philox_rk(gcell, (uint32_t)s, c2, c3, rk0, rk1) : philox(gcell, (uint32_t)s, c2, c3, key);
+        return RK ? philox_hoisted(ph[h], (uint32_t)s, rk0, rk1) : philox(gcell, (uint32_t)s, c2, c3, key);
     };
     uint4 wn[GPL / 2];
     if (AHEAD) {

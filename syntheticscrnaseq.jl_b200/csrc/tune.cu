@@ -369,6 +369,45 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     return SCRNA_OK;
 }
 
+int tc_choose_slices(scrna_ctx* ctx, int G, int64_t N, bool bursty, int dtype, bool hill2,
+                     const std::function<int(int, double*)>& measure, int* S, bool* measured) {
+    *S = 7;
+    *measured = false;
+    ctx->tune_last = scrna_tune_choice{2, 224, 0, 0, 0.0};
+    if (ctx->tune_mode == 0) return SCRNA_OK;
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "%s|tc|G%d|d%d|b%d|h%d|N%d", ctx->tune_arch, G, dtype, bursty ? 1 : 0,
+                  hill2 ? 1 : 0, floor_log2(std::max<int64_t>(N, 1)));
+    const std::string key = buf;
+    scrna_tune_choice c{};
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = ctx->tune_mem.find(key);
+        if (it != ctx->tune_mem.end()) c = it->second;
+    }
+    if (!c.found && !ctx->tune_path.empty())
+        if (int r = lookup(ctx->tune_path, key, &c)) return r;
+    if (!c.found && ctx->tune_mode == 1) {
+        double best = 1e30;
+        for (int s : {5, 6, 7}) {
+            double us = 0;
+            if (int r = measure(s, &us)) return r;
+            *measured = true;
+            if (us < best) { best = us; c = scrna_tune_choice{2, 32 * s, 0, 1, us}; }
+        }
+        if (c.found && !ctx->tune_path.empty()) store(ctx->tune_path, key, c);
+    }
+    if (!c.found || c.kernel != 2 || (c.genes_per_lane != 160 && c.genes_per_lane != 192 && c.genes_per_lane != 224))
+        return SCRNA_OK;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        ctx->tune_mem[key] = c;
+    }
+    *S = c.genes_per_lane / 32;
+    ctx->tune_last = c;
+    return SCRNA_OK;
+}
+
 }  // namespace scrna
 
 using namespace scrna;
@@ -405,6 +444,7 @@ extern "C" int scrna_autotune_cache_lookup(const char* path, const char* key, sc
 
 extern "C" int scrna_autotune_cache_store(const char* path, const char* key, const scrna_tune_choice* c) {
     if (!path || !key || !c) return fail(SCRNA_EINVAL, "NULL argument");
-    if (c->kernel != 0 && c->kernel != 1) return fail(SCRNA_EINVAL, "kernel must be 0 (block tiles) or 1 (lane)");
+    if (c->kernel < 0 || c->kernel > 2)
+        return fail(SCRNA_EINVAL, "kernel must be 0 (block tiles), 1 (lane) or 2 (tensor-core step)");
     return store(path, key, *c);
 }

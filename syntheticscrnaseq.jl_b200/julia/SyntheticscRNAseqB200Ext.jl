@@ -5,6 +5,8 @@
      simulate(net, CLE(dt), kin, Val(:gpu); cell_num, T, readout)       ext/SyntheticscRNAseqCUDAExt.jl:48-52
      simulate(net, CLE(dt), kin, Val(:gpu), pop; T, readout)           ext/SyntheticscRNAseqCUDAExt.jl:409-412
      simulate_gpu_batch(networks, CLE(dt), kin; cell_num, T, readout)  ext/SyntheticscRNAseqCUDAExt.jl:132-136
+     simulate(net, BinomialTauLeap(dt), kin, Val(:gpu)[, pop]; ...)    ext/SyntheticscRNAseqCUDAExt.jl:215-219, 542-546
+     simulate_gpu_batch(networks, BinomialTauLeap(dt), kin[s][, pop])  ext/SyntheticscRNAseqCUDAExt.jl:290-295, 666-671
      apply_capture(X, capture; seed)                                   src/capture.jl:25
 
    The extension owns only ccalls: every number is computed by the library.
@@ -15,7 +17,7 @@
 module SyntheticscRNAseqB200Ext
 
 using SyntheticscRNAseq
-using SyntheticscRNAseq: GeneNetwork, CLE, KineticParams, PopulationConfig, CaptureModel
+using SyntheticscRNAseq: GeneNetwork, CLE, BinomialTauLeap, KineticParams, PopulationConfig, CaptureModel
 
 const LIB = get(ENV, "SCRNA_CLE_LIB", joinpath(@__DIR__, "..", "libscrna_cle.so"))
 
@@ -82,6 +84,27 @@ pop_struct(p::PopulationConfig; partition::Symbol=:binomial, exclude_mother::Boo
 cap_struct(c::CaptureModel; mean_correction::Bool=true) =
     ScrnaCapture(c.efficiency, c.efficiency_std, readout_code(c.readout), Int32(mean_correction))
 
+# The library's entry point of an algorithm (simulate / simulate_batch), same arguments.
+function call_simulate(alg, args...)
+    alg isa BinomialTauLeap ?
+        ccall((:scrna_tauleap_simulate, LIB), Cint,
+              (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ScrnaKinetics}, Ptr{ScrnaPopulation}, Ptr{ScrnaCapture},
+               Ref{ScrnaOpts}, Ptr{Float64}, Ptr{Int32}, Ptr{Float64}), args...) :
+        ccall((:scrna_cle_simulate, LIB), Cint,
+              (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ScrnaKinetics}, Ptr{ScrnaPopulation}, Ptr{ScrnaCapture},
+               Ref{ScrnaOpts}, Ptr{Float64}, Ptr{Int32}, Ptr{Float64}), args...)
+end
+
+function call_batch(alg, args...)
+    alg isa BinomialTauLeap ?
+        ccall((:scrna_tauleap_simulate_batch, LIB), Cint,
+              (Ptr{Cvoid}, Int32, Ptr{Ptr{Cvoid}}, Ptr{ScrnaKinetics}, Int32, Ptr{Int64},
+               Ptr{Ptr{Cvoid}}, Ptr{ScrnaCapture}, Ref{ScrnaOpts}, Ptr{Ptr{Float64}}, Ptr{Ptr{Int32}}), args...) :
+        ccall((:scrna_cle_simulate_batch, LIB), Cint,
+              (Ptr{Cvoid}, Int32, Ptr{Ptr{Cvoid}}, Ptr{ScrnaKinetics}, Int32, Ptr{Int64},
+               Ptr{Ptr{Cvoid}}, Ptr{ScrnaCapture}, Ref{ScrnaOpts}, Ptr{Ptr{Float64}}, Ptr{Ptr{Int32}}), args...)
+end
+
 function run_one(net, alg, kin, pop, N; T, readout, seed, stream, capture)
     h = upload(net)
     try
@@ -92,54 +115,79 @@ function run_one(net, alg, kin, pop, N; T, readout, seed, stream, capture)
         opts = ScrnaOpts(alg.dt, T, N, readout_code(readout), Int32(0), UInt64(seed), UInt32(stream),
                          Int32(0), Int64(0), Int64(0))
         k = kin_struct(kin)
-        check(ccall((:scrna_cle_simulate, LIB), Cint,
-                    (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ScrnaKinetics}, Ptr{ScrnaPopulation}, Ptr{ScrnaCapture},
-                     Ref{ScrnaOpts}, Ptr{Float64}, Ptr{Int32}, Ptr{Float64}),
-                    context(), h, k,
-                    pop === nothing ? C_NULL : Ref(pop),
-                    capture === nothing ? C_NULL : Ref(cap_struct(capture)),
-                    opts, out,
-                    counts === nothing ? C_NULL : counts,
-                    eff === nothing ? C_NULL : eff))
+        check(call_simulate(alg, context(), h, k,
+                            pop === nothing ? C_NULL : Ref(pop),
+                            capture === nothing ? C_NULL : Ref(cap_struct(capture)),
+                            opts, out,
+                            counts === nothing ? C_NULL : counts,
+                            eff === nothing ? C_NULL : eff))
         return capture === nothing ? out : (out, counts, eff)
     finally
         release(h)
     end
 end
 
-function SyntheticscRNAseq.simulate(net::GeneNetwork, alg::CLE, kin::KineticParams, ::Val{:gpu};
+const GpuAlg = Union{CLE, BinomialTauLeap}
+
+function SyntheticscRNAseq.simulate(net::GeneNetwork, alg::GpuAlg, kin::KineticParams, ::Val{:gpu};
                                     cell_num::Int=1000, T::Float64=50.0, readout::Symbol=:protein,
                                     seed::Integer=0, stream::Integer=0, capture=nothing)
     return run_one(net, alg, kin, nothing, cell_num; T, readout, seed, stream, capture)
 end
 
-function SyntheticscRNAseq.simulate(net::GeneNetwork, alg::CLE, kin::KineticParams, ::Val{:gpu},
+# The reference's CLE population path halves at division and excludes the mother from the
+# Moran draw (cle.jl:249-268); its tau-leap path partitions binomially and may replace any
+# cell (ext:643-651).  Both are keywords here.
+function SyntheticscRNAseq.simulate(net::GeneNetwork, alg::GpuAlg, kin::KineticParams, ::Val{:gpu},
                                     pop::PopulationConfig; T::Float64=50.0, readout::Symbol=:protein,
                                     seed::Integer=0, stream::Integer=0, capture=nothing,
-                                    partition::Symbol=:binomial)
-    return run_one(net, alg, kin, pop_struct(pop; partition), pop.cell_num; T, readout, seed, stream, capture)
+                                    partition::Symbol=:binomial, exclude_mother::Bool=!(alg isa BinomialTauLeap))
+    return run_one(net, alg, kin, pop_struct(pop; partition, exclude_mother), pop.cell_num;
+                   T, readout, seed, stream, capture)
 end
 
-function SyntheticscRNAseq.simulate_gpu_batch(networks::Vector{GeneNetwork}, alg::CLE, kin::KineticParams;
-                                              cell_num=1000, T::Float64=50.0,
-                                              readout::Symbol=:protein, seed::Integer=0, stream::Integer=0)
+function run_batch(networks, alg, kins::Vector{ScrnaKinetics}, pops, cells; T, readout, seed, stream)
     B = length(networks)
-    cells = cell_num isa Integer ? fill(Int64(cell_num), B) : Int64.(cell_num)
     hs = [upload(n) for n in networks]
     try
         outs = [Matrix{Float64}(undef, cells[b], readout === :both ? 2 * networks[b].G : networks[b].G) for b in 1:B]
         opts = ScrnaOpts(alg.dt, T, 0, readout_code(readout), Int32(0), UInt64(seed), UInt32(stream),
                          Int32(0), Int64(0), Int64(0))
-        k = [kin_struct(kin)]
-        check(ccall((:scrna_cle_simulate_batch, LIB), Cint,
-                    (Ptr{Cvoid}, Int32, Ptr{Ptr{Cvoid}}, Ptr{ScrnaKinetics}, Int32, Ptr{Int64},
-                     Ptr{Ptr{Cvoid}}, Ptr{ScrnaCapture}, Ref{ScrnaOpts}, Ptr{Ptr{Float64}}, Ptr{Ptr{Int32}}),
-                    context(), Int32(B), hs, k, Int32(1), cells, C_NULL, C_NULL, opts,
-                    [pointer(o) for o in outs], C_NULL))
+        popref = pops === nothing ? nothing : [Ref(p) for p in pops]
+        GC.@preserve popref begin
+            pptrs = pops === nothing ? C_NULL :
+                    [Base.unsafe_convert(Ptr{ScrnaPopulation}, r) for r in popref]
+            check(call_batch(alg, context(), Int32(B), hs, kins, Int32(length(kins)), cells,
+                             pptrs, C_NULL, opts, [pointer(o) for o in outs], C_NULL))
+        end
         return outs
     finally
         foreach(release, hs)
     end
+end
+
+# One KineticParams for all networks, or one per network (ext:689-720).
+function SyntheticscRNAseq.simulate_gpu_batch(networks::Vector{GeneNetwork}, alg::GpuAlg,
+                                              kin::Union{KineticParams, Vector{<:KineticParams}};
+                                              cell_num=1000, T::Float64=50.0,
+                                              readout::Symbol=:protein, seed::Integer=0, stream::Integer=0)
+    B = length(networks)
+    cells = cell_num isa Integer ? fill(Int64(cell_num), B) : Int64.(cell_num)
+    kins = kin isa KineticParams ? [kin_struct(kin)] : [kin_struct(k) for k in kin]
+    return run_batch(networks, alg, kins, nothing, cells; T, readout, seed, stream)
+end
+
+# With one population config for every network (ext:666-671).
+function SyntheticscRNAseq.simulate_gpu_batch(networks::Vector{GeneNetwork}, alg::GpuAlg,
+                                              kin::Union{KineticParams, Vector{<:KineticParams}},
+                                              pop::PopulationConfig; T::Float64=50.0,
+                                              readout::Symbol=:protein, seed::Integer=0, stream::Integer=0,
+                                              partition::Symbol=:binomial,
+                                              exclude_mother::Bool=!(alg isa BinomialTauLeap))
+    B = length(networks)
+    kins = kin isa KineticParams ? [kin_struct(kin)] : [kin_struct(k) for k in kin]
+    ps = [pop_struct(pop; partition, exclude_mother) for _ in 1:B]
+    return run_batch(networks, alg, kins, ps, fill(Int64(pop.cell_num), B); T, readout, seed, stream)
 end
 
 function SyntheticscRNAseq.apply_capture(X::Matrix{<:Real}, capture::CaptureModel, ::Val{:gpu};

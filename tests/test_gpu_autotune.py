@@ -70,3 +70,22 @@ def test_tuned_population_and_batch_equal_untuned(pkg, tmp_path):
         assert np.array_equal(x, y)
     plain.close()
     tuned.close()
+
+
+def test_tuned_tensor_tile_equals_default(pkg, tmp_path):
+    """The fused tensor-core step's tile width (160, 192 or 224 genes) changes which genes share a
+    tile, not the order of the contraction over K, so a tuned run equals the default width's."""
+    kin = pkg.WORKLOAD_KINETICS
+    plain = pkg.Context(0)
+    plain.set_autotune(0)
+    tuned = pkg.Context(0)
+    tuned.set_autotune(1, str(tmp_path / "autotune.json"))
+    for G, N in ((300, 700), (520, 333)):
+        net = pkg.dense_network(G, seed=G, density=0.1, n_coop=4, n_redun=4)
+        a = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=0.3, readout="both", seed=2, path="tensor", ctx=plain)
+        b = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=0.3, readout="both", seed=2, path="tensor", ctx=tuned)
+        choice = tuned.last_kernel_choice()
+        assert choice["kernel"] == 2 and choice["found"] == 1 and choice["genes_per_lane"] in (160, 192, 224)
+        assert np.array_equal(a, b), (G, choice)
+    plain.close()
+    tuned.close()
