@@ -286,6 +286,31 @@ int scrna_state_histogram(scrna_ctx* ctx, scrna_state* st, int32_t source, int32
 int scrna_state_write_mtx(scrna_ctx* ctx, scrna_state* st, const char* dir, const char* const* gene_names,
                           const char* barcode_prefix);
 
+/* ---- continuation and checkpoints ---------------------------------------------------
+ * A run of the register path (CLE or tau-leap) is a pure function of its inputs and of
+ * increments keyed by (seed, stream, cell, step, gene), and its state is exact between
+ * launches, so a run continued from step T1 to T2 equals one run of T2 steps bit for bit.
+ * The reference's nearest counterpart returns the final population state for inspection
+ * (simulate_with_state, src/algorithms/tauleap_binomial.jl:270-324).
+ * scrna_cle_resume / scrna_tauleap_resume: continue the run `st` holds (from a run on this
+ * state or scrna_state_restore) to the total step count of opts (T or n_steps, counted from
+ * step 1); same network, kinetics, population mode, seed, stream, cells and readout as the
+ * run being continued; the readout and capture are written at the end as for a full run.
+ * scrna_state_steps_done: steps the held run has done (0 if none).
+ * scrna_state_checkpoint: with buf NULL sets *bytes to the size needed; else writes the held
+ * run's state (header "SCRNACK1", G, flags, N, steps, divisions; M, P float32, promoter
+ * uint8, switching int32 pairs, all [G][N]; volumes float64 with a population) into buf.
+ * scrna_state_restore: loads a checkpoint into a state created for the same G and N. */
+int scrna_cle_resume(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                     const scrna_population* pop, const scrna_capture* cap, const scrna_cle_opts* opts,
+                     scrna_state* st);
+int scrna_tauleap_resume(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
+                         const scrna_population* pop, const scrna_capture* cap, const scrna_cle_opts* opts,
+                         scrna_state* st);
+int scrna_state_steps_done(const scrna_state* st, int64_t* steps);
+int scrna_state_checkpoint(scrna_ctx* ctx, scrna_state* st, void* buf, size_t capacity, size_t* bytes);
+int scrna_state_restore(scrna_ctx* ctx, scrna_state* st, const void* buf, size_t bytes);
+
 /* ---- serving loop ---------------------------------------------------------------------
  * A request server with continuous batching (no counterpart in the reference, which runs
  * one simulate call at a time).  Submitted requests wait in a FIFO queue until their device

@@ -102,6 +102,11 @@ SIGNATURES = {
     "scrna_state_ks": (C.c_int, [P, P, P, I32, P]),
     "scrna_state_histogram": (C.c_int, [P, P, I32, I32, I32, P]),
     "scrna_state_write_mtx": (C.c_int, [P, P, C.c_char_p, P, C.c_char_p]),
+    "scrna_cle_resume": (C.c_int, [P, P, P, P, P, P, P]),
+    "scrna_tauleap_resume": (C.c_int, [P, P, P, P, P, P, P]),
+    "scrna_state_steps_done": (C.c_int, [P, C.POINTER(I64)]),
+    "scrna_state_checkpoint": (C.c_int, [P, P, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "scrna_state_restore": (C.c_int, [P, P, P, C.c_size_t]),
     "scrna_server_create": (C.c_int, [P, I64, I32, C.POINTER(P)]),
     "scrna_server_destroy": (C.c_int, [P]),
     "scrna_submit": (C.c_int, [P, P, C.POINTER(U64)]),

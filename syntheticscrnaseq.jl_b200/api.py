@@ -336,6 +336,35 @@ class DeviceRun:
         fn = self.ctx.lib.scrna_tauleap_run_device if self.tau else self.ctx.lib.scrna_cle_run_device
         check(fn(self.ctx.h, self.handle.h, C.byref(self.k), _ptr(self.p), _ptr(self.c), C.byref(self.o), self.st))
 
+    def resume(self, *, T: Optional[float] = None, n_steps: int = 0):
+        """Continue the held run to T (or n_steps) steps in total from its current step; the
+        results equal one run of that length."""
+        o = _opts(BinomialTauLeap(self.o.dt) if self.tau else CLE(self.o.dt), T=self.o.T if T is None else T,
+                  cell_num=self.N, readout=self.readout, seed=self.o.seed, stream=self.o.stream,
+                  precision="fp32", path=[k for k, v in PATH.items() if v == self.o.path][0], n_steps=n_steps,
+                  cell_offset=self.o.cell_offset)
+        fn = self.ctx.lib.scrna_tauleap_resume if self.tau else self.ctx.lib.scrna_cle_resume
+        check(fn(self.ctx.h, self.handle.h, C.byref(self.k), _ptr(self.p), _ptr(self.c), C.byref(o), self.st))
+
+    @property
+    def steps_done(self) -> int:
+        v = C.c_int64()
+        check(self.ctx.lib.scrna_state_steps_done(self.st, C.byref(v)))
+        return int(v.value)
+
+    def checkpoint(self) -> bytes:
+        """The held run's state as bytes (scrna_state_checkpoint)."""
+        n = C.c_size_t()
+        check(self.ctx.lib.scrna_state_checkpoint(self.ctx.h, self.st, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(self.ctx.lib.scrna_state_checkpoint(self.ctx.h, self.st, buf, n.value, C.byref(n)))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Load a checkpoint (of the same G and cell count) to continue with resume()."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        check(self.ctx.lib.scrna_state_restore(self.ctx.h, self.st, buf, len(data)))
+
     def read(self):
         cols = self.G * (2 if self.readout == "both" else 1)
         out = _pinned.empty((self.N, cols), np.float64, order="F")

@@ -582,8 +582,14 @@ scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
     return k;
 }
 
+// A register-path run of `st` from step start + 1 to the run's total step count.  start = 0:
+// a new run from the initial state; start > 0: the continuation of the state's previous run
+// (its state and `start_epoch` divisions), bit for bit the same as one run of the total
+// length.  A continuation measures no kernel variants (that would overwrite the state) and
+// converts the state to the layout of the kernel it runs.
 static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
-                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau) {
+                     const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau,
+                     int64_t start = 0, int start_epoch = 0) {
     const NetDev& d = net->dev;
     if (d.n_quads > fused_max_quads())
         return fail(SCRNA_ENOTSUP, "G=%d exceeds the register path limit of %d genes", d.G, 4 * fused_max_quads());
@@ -600,7 +606,9 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
                     kLaneSrc, kLaneTerms);
     KernelChoice kc{};
     if (tau) kc = choose_kernel(net, SCRNA_PATH_BLOCK);  // the tau-leap runs on block tiles
-    else if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc)) return r;
+    else if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc, nullptr, nullptr, start == 0)) return r;
+    if (start > 0 && st->last_cell_major != kc.warp)
+        if (int r = state_relayout(ctx, st, kc.warp)) return r;
     FusedArgs a{};
     fill_fused_args(net, kin, pop, cap, o, st, &a);
     if (tau) fill_tau_args(net, kin, pop, o, &a);
@@ -610,17 +618,29 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         return kc.warp ? warpcell_launch(a, kc.gpl, kc.emax, kc.tmax, is_pop, s) : fused_launch(a, kc.block, is_pop, s);
     };
     st->last_cell_major = kc.warp;  // the lane kernel keeps M, P, prom, NS cell-major
+    st->steps_done = std::max(n_steps, start);
+    st->last_tau = tau;
     if (!pop) {
-        a.step_begin = 1; a.step_end = (int)n_steps; a.first = 1; a.last = 1; a.check = 0; a.epoch = 0;
+        a.step_begin = (int)start + 1; a.step_end = (int)n_steps; a.first = start == 0 ? 1 : 0; a.last = 1;
+        a.check = 0; a.epoch = 0;
         CU(launch(false));
         ctx->launches++;
+        st->epoch = 0;
         return SCRNA_OK;
     }
+    // Moran slot owners start empty; a continuation's previous placements are already in its state
     for (int k = 0; k < 2; ++k) CU(cudaMemsetAsync(st->owner[k].p, 0, (size_t)st->N * 8, s));
     const int64_t I = pop->div_check_interval;
-    int64_t s0 = 1;
-    int epoch = 0;
-    bool first = true;
+    int64_t s0 = start + 1;
+    int epoch = start_epoch;
+    bool first = start == 0;
+    if (s0 > n_steps && start > 0) {  // nothing left to run: read out the state as it is
+        a.step_begin = (int)s0; a.step_end = (int)s0 - 1; a.first = 0; a.epoch = epoch; a.check = 0; a.last = 1;
+        CU(launch(true));
+        ctx->launches++;
+        st->epoch = epoch;
+        return SCRNA_OK;
+    }
     while (true) {
         int64_t s1 = std::min(n_steps, ((s0 - 1) / I + 1) * I);
         if (n_steps == 0) s1 = 0;
@@ -646,7 +666,35 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         }
         s0 = s1 + 1;
     }
+    st->epoch = epoch;
     return SCRNA_OK;
+}
+
+// Continuation of a register-path run (scrna_cle_resume / scrna_tauleap_resume).
+int scrna::resume_register_run(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                               const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau) {
+    if (int r = validate_run(net, kin, pop, cap, o)) return r;
+    if (!st->has_register_state) return fail(SCRNA_EINVAL, "the state holds no register-path run to continue");
+    if (st->last_tau != tau) return fail(SCRNA_EINVAL, "the state was run by the other algorithm");
+    if (st->G != net->G) return fail(SCRNA_EINVAL, "state was created for G=%d, network has G=%d", st->G, net->G);
+    const int64_t N = pop ? pop->cell_num : o->cell_num;
+    if (N != st->N) return fail(SCRNA_EINVAL, "state holds %lld cells, run asks for %lld", (long long)st->N, (long long)N);
+    if ((pop != nullptr) != st->last_pop) return fail(SCRNA_EINVAL, "population mode differs from the state's run");
+    if (cap && !st->capture) return fail(SCRNA_EINVAL, "state was created without capture buffers");
+    if (o->readout != st->readout) return fail(SCRNA_EINVAL, "readout differs from the state's readout");
+    if (o->precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "continuations run the FP32 register path");
+    if (o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK &&
+        o->path != SCRNA_PATH_WARP)
+        return fail(SCRNA_ENOTSUP, "continuations run the register path");
+    const int64_t total = n_steps_of(o);
+    if (total < st->steps_done)
+        return fail(SCRNA_EINVAL, "the run asks for %lld steps in total, the state has done %lld",
+                    (long long)total, (long long)st->steps_done);
+    if (int r = set_device(ctx)) return r;
+    if (int r = ensure_gene_tables(net, kin, o->dt, pop != nullptr)) return r;
+    if (int r = state_alloc(st, pop != nullptr, false)) return r;
+    st->have_counts = cap != nullptr;
+    return run_fused(ctx, net, kin, pop, cap, o, st, tau, st->steps_done, st->epoch);
 }
 
 static int run_plain(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_capture* cap,
@@ -728,6 +776,7 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
                                     (nd.n_quads > fused_max_quads() || (net->G >= 256 && density >= 0.05))));
     if (tensor) {
         if (pop) return fail(SCRNA_ENOTSUP, "the tensor-core path has no population dynamics");
+        st->has_register_state = false;
         st->have_counts = cap != nullptr;
         st->last_plain = false;
         st->last_pop = false;
@@ -746,8 +795,11 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
     st->have_counts = cap != nullptr;
     st->last_plain = plain;
     st->last_pop = pop != nullptr;
+    st->has_register_state = false;
     if (plain) return run_plain(ctx, net, kin, cap, o, st);
-    return run_fused(ctx, net, kin, pop, cap, o, st, tau);
+    const int r = run_fused(ctx, net, kin, pop, cap, o, st, tau);
+    st->has_register_state = r == SCRNA_OK;
+    return r;
 }
 
 extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,

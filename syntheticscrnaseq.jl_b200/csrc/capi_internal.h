@@ -123,6 +123,12 @@ struct scrna_state {
     bool last_plain = false;
     bool last_pop = false;
     const double* p64_final = nullptr;
+    // continuation of register-path runs (scrna_cle_resume, checkpoints): the state holds the
+    // end of a run of `steps_done` steps with `epoch` divisions, by the CLE or the tau-leap
+    bool has_register_state = false;
+    bool last_tau = false;
+    int64_t steps_done = 0;
+    int32_t epoch = 0;
 };
 
 
@@ -152,7 +158,12 @@ int tc_choose_slices(scrna_ctx* ctx, int G, int64_t N, bool bursty, int dtype, b
                      const std::function<int(int, double*)>& measure, int* S, bool* measured);
 int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
                         scrna_state* st, KernelChoice* out, const FusedArgs* base = nullptr,
-                        cudaStream_t stream = nullptr);
+                        cudaStream_t stream = nullptr, bool may_measure = true);
+// Converts a state's M, P, promoter and switching arrays between gene-major [G][N] and
+// cell-major [N][G] (the lane kernel's layout).
+int state_relayout(scrna_ctx* ctx, scrna_state* st, bool to_cell_major);
+int resume_register_run(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
+                        const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau);
 int fused_max_quads();
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,

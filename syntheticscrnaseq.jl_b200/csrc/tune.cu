@@ -329,7 +329,8 @@ static int measure(scrna_ctx* ctx, scrna_net* net, const FusedArgs& base, scrna_
 // those of fill_fused_args, whose gene tables ensure_gene_tables has uploaded) on `stream`
 // (NULL: the context's).
 int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_cle_opts* o,
-                        scrna_state* st, KernelChoice* out, const FusedArgs* base, cudaStream_t stream) {
+                        scrna_state* st, KernelChoice* out, const FusedArgs* base, cudaStream_t stream,
+                        bool may_measure) {
     *out = choose_kernel(net, o->path);
     ctx->tune_last = scrna_tune_choice{out->warp ? 1 : 0, out->warp ? out->gpl : 0, out->warp ? out->nw1 : 0, 0, 0.0};
     const int path = o->path;
@@ -347,7 +348,7 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     }
     if (!c.found && !ctx->tune_path.empty())
         if (int r = lookup(ctx->tune_path, key, &c)) return r;
-    if (!c.found && ctx->tune_mode == 1) {
+    if (!c.found && ctx->tune_mode == 1 && may_measure) {
         FusedArgs a{};
         if (base) a = *base;
         else fill_fused_args(net, kin, nullptr, nullptr, o, st, &a);
