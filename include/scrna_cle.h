@@ -239,7 +239,8 @@ int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna, void* prot
  * a JSON cache file (SCRNA_AUTOTUNE_CACHE, else $XDG_CACHE_HOME or ~/.cache
  * /scrna_b200/autotune.json), which later runs and processes read.  Applies to the AUTO,
  * REGISTER and WARP paths of scrna_cle_simulate, scrna_cle_run_device (a measurement there
- * waits for the device), the batch call and the server.  The fused tensor-core step's tile
+ * waits for the device) and the batch call; the server uses cached choices only (a request
+ * stream's shapes mostly occur once, and measuring would stall the running requests).  The fused tensor-core step's tile
  * width (160, 192 or 224 genes; the same contraction order, so identical results) is tuned
  * the same way per (device, G, operand type, telegraph genes, Hill exponent 2, cell bucket). */
 typedef struct {

@@ -38,6 +38,7 @@ cudaError_t philox_check_launch(int n, const uint32_t* d_ctr, uint32_t k0, uint3
                                 uint32_t* d_out, cudaStream_t st);
 cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStream_t st);
 cudaError_t peak_philox_launch(int blocks, int iters, float* sink, cudaStream_t st);
+cudaError_t switch_log2_init_launch(float* tab, uint32_t n, cudaStream_t st);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype);
 }  // namespace scrna
@@ -543,6 +544,7 @@ void scrna::fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scr
     }
     a.lane_in = d.lane_in;
     a.lane_term = d.lane_term;
+    a.log2_tab = d.bursty ? switch_log2_table(net->ctx) : nullptr;
     for (int r = 0; r < 10; ++r) {
         a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
         a.rk1[r] = a.key1 + (uint32_t)r * 0xBB67AE85u;
@@ -563,6 +565,19 @@ void scrna::fill_tau_args(const scrna_net* net, const scrna_kinetics* kin, const
     a->ss_mu_m = kin->mu_m + kin->dilution;
     a->ss_mu_p = kin->mu_p + kin->dilution;
     a->k_t64 = kin->k_t;
+}
+
+const float* scrna::switch_log2_table(scrna_ctx* ctx) {
+    if (ctx->log2_tab_ready) return ctx->log2_tab.as<float>();
+    const uint32_t n = 1u << 18;
+    if (ctx->log2_tab.ensure((size_t)n * 4) != cudaSuccess) return nullptr;
+    if (switch_log2_init_launch(ctx->log2_tab.as<float>(), n, ctx->stream) != cudaSuccess) return nullptr;
+    ctx->launches++;
+    // once per context: wait for the table, so kernels on any stream (batch groups, the
+    // server's) read it filled
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return nullptr;
+    ctx->log2_tab_ready = true;
+    return ctx->log2_tab.as<float>();
 }
 
 // Register-path kernel of a network: warp-per-cell-group (genes per lane, in-edges and

@@ -65,6 +65,8 @@ struct scrna_ctx {
     void* lt_handle = nullptr;
     scrna::DevBuf lt_workspace;
     scrna::DevBuf tc_err;        // error flag of the tcgen05 kernels (one int)
+    scrna::DevBuf log2_tab;      // own_log2f of the 2^18 switch uniforms (switch_table.cuh)
+    bool log2_tab_ready = false;
     // autotuning of the register-path kernel (tune.cu): mode 0 off, 1 measure on a miss,
     // 2 cache only; cache file (empty: memory only); choices made on this context
     int tune_mode = 1;
@@ -151,6 +153,9 @@ void fill_fused_args(scrna_net* net, const scrna_kinetics* kin, const scrna_popu
                      const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, FusedArgs* out);
 KernelChoice choose_kernel(const scrna_net* net, int path);
 void tune_init_ctx(scrna_ctx* ctx);
+// The context's table of switch-uniform log2 values, filled on first use; null if it cannot
+// be allocated (the kernels then evaluate the series).
+const float* switch_log2_table(scrna_ctx* ctx);
 // Tile width of the fused tensor-core step (slices of 32 genes: 5, 6 or 7): 7 with autotuning
 // off, else the cached or measured fastest (measure(S, &us_per_step)); *measured tells
 // whether measurement launches ran.

@@ -124,6 +124,8 @@ struct FusedArgs {
     float p_dec_m, p_dec_p;
     const double* beta64;
     double ss_mu_m, ss_mu_p, k_t64;
+    // own_log2f of every 18-bit switch uniform (switch_table.cuh), or null
+    const float* log2_tab;
 };
 
 // Step range and division flags of one launch (or one queued work item).

@@ -183,6 +183,17 @@ cudaError_t capture_launch(int G, int64_t N, int64_t cell_offset, const double* 
     return cudaGetLastError();
 }
 
+// ---- table of switch-uniform log2 values (switch_table.cuh) ------------------------------------
+__global__ void switch_log2_init_kernel(float* tab, uint32_t n) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < n) tab[b] = own_log2f(switch_uniform_bits(b));
+}
+
+cudaError_t switch_log2_init_launch(float* tab, uint32_t n, cudaStream_t st) {
+    switch_log2_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(tab, n);
+    return cudaGetLastError();
+}
+
 // ---- device Philox check ------------------------------------------------------------------
 __global__ void philox_check_kernel(int n, const uint32_t* ctr, uint32_t k0, uint32_t k1,
                                     uint32_t* out) {

@@ -22,6 +22,7 @@
 #include "cle_device.cuh"
 #include "cle_internal.h"
 #include "philox_hoist.cuh"
+#include "switch_table.cuh"
 
 namespace scrna {
 
@@ -286,8 +287,7 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
 #pragma unroll
         for (int i = 0; i < GPL; ++i)
             if (kn[i] < 0)
-                kn[i] = geom_steps_u(switch_uniform_bits((uint32_t)(-kn[i] - 1)),
-                                     (on >> i) & 1u ? inv_on[i] : inv_off[i]);
+                kn[i] = switch_steps(a.log2_tab, (uint32_t)(-kn[i] - 1), (on >> i) & 1u ? inv_on[i] : inv_off[i]);
     };
     int32_t ns_min = ns[0];  // earliest switch of the lane's genes
 #pragma unroll

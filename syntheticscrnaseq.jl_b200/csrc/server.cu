@@ -109,8 +109,10 @@ static int setup_request(scrna_server* s, SrvRequest* r) {
     r->args.genes = r->genes.as<GeneRec>();  // this request's tables (the network's own are not uploaded here)
     r->args.ginit = r->ginit.as<GeneInit>();
     r->args.quad_tel = r->qtel.as<uint8_t>();
+    // cached kernel choices only: a measurement here would stall every running request for
+    // shapes that, in a request stream, mostly occur once
     if (int rr = choose_kernel_tuned(s->ctx, const_cast<scrna_net*>(n), &r->req.kin, &r->req.opts, r->st, &r->kc,
-                                     &r->args, s->stream))
+                                     &r->args, s->stream, false))
         return rr;
     r->args.lane_nw1 = r->kc.nw1;
     return SCRNA_OK;
