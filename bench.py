@@ -294,6 +294,7 @@ def run_ours(args):
             torch.cuda.synchronize()
 
     clocks = ClockSampler(local).start()
+    time.sleep(0.5)  # nvidia-smi's first sample comes a few hundred ms after it starts
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             run.launch()

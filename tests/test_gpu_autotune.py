@@ -41,7 +41,8 @@ def test_tuned_equals_untuned(pkg, tmp_path):
     net, N = _nets(pkg)[0]
     l0 = fresh.launches
     got = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3, ctx=fresh)
-    assert fresh.launches - l0 == 1 and fresh.last_kernel_choice()["found"] == 1
+    # the run plus, on a new context, the one-time fill of its switch-time table; no measurement
+    assert fresh.launches - l0 <= 2 and fresh.last_kernel_choice()["found"] == 1
     assert np.array_equal(got, pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=1.0, readout="both", seed=3,
                                             ctx=plain))
     for c in (plain, tuned, fresh):
