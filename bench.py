@@ -20,8 +20,10 @@ capture to an int32 count matrix.  Work unit: one cell-gene-step; one step is
   fp64_plain the plain FP64 one-kernel-per-step GPU CLE on the same workload.
   cpu_baseline  the FP64 CPU oracle (a port of the reference's cle.jl) on the whole workload,
              all host threads (the same run gives moment_err).
-  dense / batch / serve  the other workloads at N=1: dense regulation on the tensor-core
-             path, 256 uneven networks in one batch call, and the request server.
+  readme / dense / batch / serve  the other workloads at N=1: the reference's published
+             timing workload (CLE and binomial tau-leap, host wall clock per call), dense
+             regulation on the tensor-core path, 256 uneven networks in one batch call, and the
+             request server.
 
 --impl reference times that CPU restatement alone (the Julia reference cannot run here).
 --gpus N without a torchrun environment starts N ranks itself.  Multi-GPU: cells are
@@ -58,7 +60,7 @@ def _args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="telegraph", choices=["telegraph", "dense", "batch", "serve"],
+    ap.add_argument("--workload", default="telegraph", choices=["telegraph", "readme", "dense", "batch", "serve"],
                     help="telegraph: the headline line (with the other workloads as extra keys at N=1); "
                          "dense / batch / serve: that workload alone")
     ap.add_argument("--requests", type=int, default=60, help="serve: number of requests")
@@ -391,7 +393,7 @@ def run_ours(args):
 
     extra = {}
     if rank == 0 and world == 1 and not args.no_extra:
-        for name, fn in (("dense", leg_dense), ("batch", leg_batch), ("serve", leg_serve)):
+        for name, fn in (("readme", leg_readme), ("dense", leg_dense), ("batch", leg_batch), ("serve", leg_serve)):
             try:
                 extra[name] = fn(pkg, args, local)
             except Exception as e:  # a failed leg is reported, never silently dropped
@@ -534,11 +536,40 @@ def leg_serve(pkg, args, device):
             "chunks": st["chunks"], "clocks": clk}
 
 
+def leg_readme(pkg, args, device):
+    """The workload of the reference's published timing table (README.md:68-80, the 5-gene case
+    of experiments/validate_analytical.jl:184-232): 5 unregulated genes with basals 1..5, k_t=1,
+    mu_m=0.1, mu_p=0.2, 5,000 cells, dt=0.1, T=300 (3,000 steps), protein readout.  Each call is
+    timed on the host clock around simulate (upload, run, copy back), after one warm-up call,
+    as the reference times it; errors are against the exact two-stage moments."""
+    import numpy as np
+    ctx = pkg.Context(device)
+    net = pkg.GeneNetwork(5, [1.0, 2.0, 3.0, 4.0, 5.0], np.zeros((5, 5)))
+    k_t, mu_m, mu_p = 1.0, 0.1, 0.2
+    kin = pkg.KineticParams(k_t=k_t, K_d=50.0, n=2.0, mu_m=mu_m, mu_p=mu_p)
+    beta = np.arange(1.0, 6.0)
+    p_mean = k_t * beta / (mu_m * mu_p)
+    p_var = p_mean * (1.0 + k_t / (mu_m + mu_p))
+    units = 5 * 5000 * 3000
+    out = {"workload": "readme-G5-N5000-T300-dt0.1", "units_per_call": units,
+           "reference_rtx5060_s": {"CLE": 0.22, "BinomialTauLeap": 0.45}}
+    for name, alg in (("CLE", pkg.CLE(0.1)), ("BinomialTauLeap", pkg.BinomialTauLeap(0.1))):
+        pkg.simulate(net, alg, kin, cell_num=100, T=10.0, readout="protein", seed=1, ctx=ctx)
+        t0 = time.perf_counter()
+        Y = pkg.simulate(net, alg, kin, cell_num=5000, T=300.0, readout="protein", seed=42, ctx=ctx)
+        el = time.perf_counter() - t0
+        out[name] = {"s_per_call": el, "value": units / el, "unit": "cell·gene·steps/s",
+                     "max_mean_err": float(np.max(np.abs(Y.mean(0) - p_mean) / p_mean)),
+                     "max_var_err": float(np.max(np.abs(Y.var(0, ddof=1) - p_var) / p_var))}
+    ctx.close()
+    return out
+
+
 def run_single_leg(args):
     import json as _json
     import __graft_entry__
     pkg = __graft_entry__.load_package()
-    fn = {"dense": leg_dense, "batch": leg_batch, "serve": leg_serve}[args.workload]
+    fn = {"readme": leg_readme, "dense": leg_dense, "batch": leg_batch, "serve": leg_serve}[args.workload]
     print(_json.dumps(fn(pkg, args, 0)), flush=True)
 
 
