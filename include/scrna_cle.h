@@ -415,6 +415,13 @@ int scrna_debug_tc_gemm(scrna_ctx* ctx, const void* A, const void* B, float* C, 
  * tensor-core pipeline without faulting or hanging the GPU. */
 int scrna_debug_tc_gemm_withhold(scrna_ctx* ctx, const void* A, const void* B, float* C, int64_t M, int32_t N,
                                  int32_t K, int32_t dtype, int32_t withhold);
+/* Compares the tau-leap's branch-free quotient lam / k (the Poisson inverse CDF's terms,
+ * ext/SyntheticscRNAseqCUDAExt.jl:21-39) with IEEE division for every float lam whose bit
+ * pattern lies in [lo, hi) and is in the quotient's range (0 or 2^-100..2^100), for every
+ * k = 1..50; returns the number of differing quotients and the first (lam bits, k) that
+ * differs.  No counterpart in the reference: it checks the library's own arithmetic. */
+int scrna_debug_small_div_check(scrna_ctx* ctx, uint32_t lo, uint32_t hi, int64_t* mismatches,
+                                uint32_t* first_bad_lam, int32_t* first_bad_k);
 /* Measures the sustained issue rate of the FP32 FMA pipe and of the special-function
  * unit (MUFU) pipe with two microkernels; results in operations per second. */
 int scrna_measure_pipe_peaks(scrna_ctx* ctx, double* fma_ops_per_s, double* sfu_ops_per_s,

@@ -115,6 +115,7 @@ SIGNATURES = {
     "scrna_cancel": (C.c_int, [P, U64]),
     "scrna_server_get_stats": (C.c_int, [P, P]),
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
+    "scrna_debug_small_div_check": (C.c_int, [P, U32, U32, P, P, P]),
     "scrna_debug_tc_gemm": (C.c_int, [P, P, P, P, I64, I32, I32, I32]),
     "scrna_debug_tc_gemm_withhold": (C.c_int, [P, P, P, P, I64, I32, I32, I32, I32]),
     "scrna_measure_pipe_peaks": (C.c_int, [P, C.POINTER(DBL), C.POINTER(DBL), C.POINTER(DBL)]),

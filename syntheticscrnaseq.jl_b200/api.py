@@ -465,6 +465,15 @@ def debug_philox(ctr: np.ndarray, key, ctx: Optional[Context] = None) -> np.ndar
     return out
 
 
+def debug_small_div_check(lo_bits: int, hi_bits: int, ctx: Optional[Context] = None):
+    """(mismatches, first differing lam bits, its k) of the tau-leap's branch-free quotient
+    lam / k against IEEE division over the floats with bit patterns in [lo_bits, hi_bits)."""
+    ctx = ctx or default_context()
+    n, lam, k = C.c_int64(), C.c_uint32(), C.c_int32()
+    check(ctx.lib.scrna_debug_small_div_check(ctx.h, lo_bits, hi_bits, C.byref(n), C.byref(lam), C.byref(k)))
+    return n.value, lam.value, k.value
+
+
 def measure_philox_rate(ctx: Optional[Context] = None) -> float:
     """Philox4x32-10 generator calls per second, measured by the library's microkernel."""
     ctx = ctx or default_context()

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -565,6 +566,15 @@ void scrna::fill_tau_args(const scrna_net* net, const scrna_kinetics* kin, const
     a->ss_mu_m = kin->mu_m + kin->dilution;
     a->ss_mu_p = kin->mu_p + kin->dilution;
     a->k_t64 = kin->k_t;
+    a->tau_lockstep = tau_lockstep_default();
+}
+
+// The tau-leap's draw schedule: in lock step (measured faster on every workload tried: the
+// 5-gene constitutive case, 10 telegraph genes, 100 regulated genes at 2,000 and 20,000
+// cells), unless SCRNA_TAU_LOCKSTEP=0 asks for one draw after another; both give the same counts.
+int scrna::tau_lockstep_default() {
+    if (const char* e = std::getenv("SCRNA_TAU_LOCKSTEP")) return std::atoi(e) != 0 ? 1 : 0;
+    return 1;
 }
 
 const float* scrna::switch_log2_table(scrna_ctx* ctx) {

@@ -195,6 +195,7 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
                    int32_t* const* counts, bool tau);
 void fill_tau_args(const scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
                    const scrna_cle_opts* o, FusedArgs* a);
+int tau_lockstep_default();
 void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr, GeneInit* gi,
                       uint8_t* qt);
 cudaError_t tau_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt, int nw,

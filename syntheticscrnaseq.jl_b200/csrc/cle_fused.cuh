@@ -16,6 +16,7 @@
 //     the final readout / capture.
 #pragma once
 #include "cle_device.cuh"
+#include "tau_lockstep.cuh"
 #include "cle_internal.h"
 
 namespace scrna {
@@ -181,6 +182,28 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
 
     // ---- fused step loop ---------------------------------------------------------
     const float k_t = a.k_t, mu_m = a.mu_m, mu_p = a.mu_p, dt = a.dt;
+    // regulation sum of a gene from the step's activation slots: additive in-edges, then the
+    // cooperative (product of activations) and redundant (1 - product of 1 - activations) terms
+    auto regulation = [&](const GeneRec& gr, const float* act) {
+        float reg = gr.cneg;
+        for (int e = gr.in_begin; e < gr.in_end; ++e) {
+            const float2 ed = sm.in_edge[e];
+            reg = fmaf(ed.x, act[__float_as_int(ed.y) * 32 + lane], reg);
+        }
+        const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
+        for (int e = nab; e < nab + nac; ++e) {
+            const NonAdd na = sm.na[e];
+            float prod = 1.0f;
+            if (na.kind == 0) {
+                for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[sm.na_src[t] * 32 + lane];
+                reg = fmaf(na.coef, prod, reg);
+            } else {
+                for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[sm.na_src[t] * 32 + lane];
+                reg = fmaf(na.coef, 1.0f - prod, reg);
+            }
+        }
+        return reg;
+    };
     int buf = 0;
     for (int s = ctl.step_begin; s <= ctl.step_end; ++s) {
         // Hill activations of regulator genes -> slot table
@@ -209,60 +232,60 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
             if (q >= a.n_quads) continue;
+            if (TAU) {
+                // the quad's four genes: telegraph switching (tauleap_binomial.jl:111-121) from the
+                // spare bits of each gene's tau-leap words, transcription propensity, then the
+                // draws of the quad (tau_lockstep.cuh)
+                float lam[4];
+                uint4 wt[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int g = 4 * q + i;
+                    lam[i] = 0.0f;
+                    wt[i] = make_uint4(0u, 0u, 0u, 0u);
+                    if (g >= G) continue;
+                    wt[i] = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_TAU, a.stream), key);
+                    const uint32_t bit = 1u << (4 * j + i);
+                    if (s == ns[j][i].x) {
+                        on ^= bit;
+                        ns[j][i] = switch_at(s, ns[j][i], switch_uniform(wt[i].x, wt[i].y), on & bit,
+                                             sm.genes[g].inv_on, sm.genes[g].inv_off);
+                    }
+                    const GeneRec gr = sm.genes[g];
+                    float tx = fmaxf(__fadd_rn(regulation(gr, act), gr.beta), 0.0f);
+                    if (POP) tx = __fmul_rn(tx, Vf);
+                    lam[i] = (on & bit) ? __fmul_rn(tx, dt) : 0.0f;
+                }
+                tau_update_quad(m[j], p[j], lam, wt, min(4, G - 4 * q), a.tau_lockstep != 0, k_t, dt, a.p_dec_m,
+                                a.p_dec_p);
+                continue;
+            }
 #pragma unroll
             for (int h = 0; h < 2; ++h) {  // gene pairs 2q, 2q+1 of this quad
                 const int g0 = 4 * q + 2 * h;
                 if (g0 >= G) continue;
-                const uint4 w = TAU ? make_uint4(0u, 0u, 0u, 0u)
-                                    : philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h), tagword(TAG_NORMAL, a.stream), key);
+                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h), tagword(TAG_NORMAL, a.stream), key);
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
                     const int i = 2 * h + k;
                     const int g = g0 + k;
                     if (g >= G) continue;
-                    // the tau-leap's four uniforms of this gene
-                    const uint4 wt = TAU ? philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_TAU, a.stream), key) : w;
                     // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
                     // a gene switches when its waiting time runs out and draws the next one
-                    // from the spare bits of its normal (or tau-leap) words
+                    // from the spare bits of its normal words
                     if (s == ns[j][i].x) {
                         const uint32_t bit = 1u << (4 * j + i);
                         on ^= bit;
-                        const float us = TAU ? switch_uniform(wt.x, wt.y)
-                                             : (k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w));
+                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
                         ns[j][i] = switch_at(s, ns[j][i], us, on & bit, sm.genes[g].inv_on, sm.genes[g].inv_off);
                     }
                     const GeneRec gr = sm.genes[g];
-                    float reg = gr.cneg;
-                    for (int e = gr.in_begin; e < gr.in_end; ++e) {
-                        const float2 ed = sm.in_edge[e];
-                        reg = fmaf(ed.x, act[__float_as_int(ed.y) * 32 + lane], reg);
-                    }
-                    const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
-                    for (int e = nab; e < nab + nac; ++e) {
-                        const NonAdd na = sm.na[e];
-                        float prod = 1.0f;
-                        if (na.kind == 0) {
-                            for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[sm.na_src[t] * 32 + lane];
-                            reg = fmaf(na.coef, prod, reg);
-                        } else {
-                            for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[sm.na_src[t] * 32 + lane];
-                            reg = fmaf(na.coef, 1.0f - prod, reg);
-                        }
-                    }
-                    if (TAU) {
-                        float tx = fmaxf(__fadd_rn(reg, gr.beta), 0.0f);
-                        if (POP) tx = __fmul_rn(tx, Vf);
-                        float lam = __fmul_rn(tx, dt);
-                        if (!(on & (1u << (4 * j + i)))) lam = 0.0f;
-                        tau_update(m[j][i], p[j][i], lam, wt, k_t, dt, a.p_dec_m, a.p_dec_p);
-                    } else {
-                        const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
-                        float tx = reg + gr.beta;
-                        if (POP) tx *= Vf;
-                        if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
-                        em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
-                    }
+                    const float reg = regulation(gr, act);
+                    const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+                    float tx = reg + gr.beta;
+                    if (POP) tx *= Vf;
+                    if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
+                    em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
                 }
             }
         }

@@ -124,6 +124,9 @@ struct FusedArgs {
     float p_dec_m, p_dec_p;
     const double* beta64;
     double ss_mu_m, ss_mu_p, k_t64;
+    // tau-leap draw schedule (same counts either way): 1 = the Poisson draws of a gene quad in
+    // lock step, 0 = one draw after another
+    int32_t tau_lockstep;
     // own_log2f of every 18-bit switch uniform (switch_table.cuh), or null
     const float* log2_tab;
 };

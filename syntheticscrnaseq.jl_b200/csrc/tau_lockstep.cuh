@@ -1,0 +1,133 @@
+// Binomial tau-leap update of the genes of one quad, with the Poisson draws either in lock
+// step or one after another.  Each draw is the 50-term inverse CDF of poisson_icdf50 (the
+// reference's GPU sampler, ext/SyntheticscRNAseqCUDAExt.jl:21-39) with the same operations
+// in the same order, and its quotients lam / k are the correctly rounded ones (small_div.cuh,
+// or IEEE division outside its range), so every count is bit-identical to poisson_icdf50's;
+// only the schedule changes.
+//
+// Lock step: of a gene's four draws, transcription, mRNA decay and protein decay depend on
+// the state at the start of the step alone, and translation on the new mRNA count; so the
+// quad's 12 independent draws share one loop, then its 4 translations share a second.  Each
+// chain's count is the last k whose preceding partial sum u exceeds, and the loop ends
+// (checked every second term) when u exceeds no chain's partial sum or after 50 terms.  That
+// issues 12 x the longest chain's terms instead of the sum of the chains' terms, in exchange
+// for 12 independent chains in flight.
+#pragma once
+
+#include "cle_device.cuh"
+#include "small_div.cuh"
+
+namespace scrna {
+
+// poisson_icdf50 with the branch-free quotient (same result).
+__device__ __forceinline__ float poisson_icdf50_fast(float u, float lam) {
+    if (!small_div_ok(lam)) return poisson_icdf50(u, lam);
+    float term = own_expf(-lam);
+    float cdf = term;
+    float events = 0.0f;
+    for (int k = 1; k <= 50; ++k) {
+        if (!(u > cdf)) break;
+        const float kf = (float)k;
+        events = kf;
+        term = __fmul_rn(term, small_div(lam, kf, kRecipSmall[k]));
+        cdf = __fadd_rn(cdf, term);
+    }
+    return events;
+}
+
+template <int C>
+__device__ __forceinline__ void poisson_icdf50_lockstep(const float (&u)[C], const float (&lam)[C],
+                                                        float (&events)[C]) {
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < C; ++c) ok &= small_div_ok(lam[c]);
+    if (!ok) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) events[c] = poisson_icdf50(u[c], lam[c]);
+        return;
+    }
+    float term[C], cdf[C];
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        term[c] = own_expf(-lam[c]);
+        cdf[c] = term[c];
+        events[c] = 0.0f;
+        any |= u[c] > cdf[c];
+    }
+    // A stopped chain keeps adding terms: they are >= 0 and rounding is monotone, so its
+    // partial sum never falls back below u and its count stays where it stopped.
+    for (int k = 1; k <= 50 && any; k += 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float kf = (float)(k + h);
+            const float y = kRecipSmall[k + h];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                events[c] = u[c] > cdf[c] ? kf : events[c];
+                term[c] = __fmul_rn(term[c], small_div(lam[c], kf, y));
+                cdf[c] = __fadd_rn(cdf[c], term[c]);
+            }
+        }
+        any = false;
+#pragma unroll
+        for (int c = 0; c < C; ++c) any |= u[c] > cdf[c];
+    }
+}
+
+// One tau-leap step of the first `ng` genes of a quad (tau_update per gene: transcription
+// Poisson(lam_tx), mRNA decay min(Poisson(m p_m), m), translation Poisson(k_t m' dt) with the
+// new m', protein decay min(Poisson(p p_p), p); counts never below 0).  w[i] holds gene i's
+// four words; in lock step a slot without a gene passes u = 0 (no events) and keeps
+// m = p = 0.
+__device__ __forceinline__ void tau_update_quad(float (&m)[4], float (&p)[4], const float (&lam_tx)[4],
+                                                const uint4 (&w)[4], int ng, bool lockstep, float k_t, float dt,
+                                                float p_dec_m, float p_dec_p) {
+    if (!lockstep) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (i >= ng) break;
+            const float n_tx = poisson_icdf50_fast(tau_uniform(w[i].x), lam_tx[i]);
+            const float mp = fmaxf(m[i], 0.0f);
+            const float n_md = fminf(poisson_icdf50_fast(tau_uniform(w[i].y), __fmul_rn(mp, p_dec_m)), mp);
+            const float mn = fmaxf(__fsub_rn(__fadd_rn(m[i], n_tx), n_md), 0.0f);
+            const float n_tl = poisson_icdf50_fast(tau_uniform(w[i].z), __fmul_rn(__fmul_rn(k_t, mn), dt));
+            const float pp = fmaxf(p[i], 0.0f);
+            const float n_pd = fminf(poisson_icdf50_fast(tau_uniform(w[i].w), __fmul_rn(pp, p_dec_p)), pp);
+            m[i] = mn;
+            p[i] = fmaxf(__fsub_rn(__fadd_rn(p[i], n_tl), n_pd), 0.0f);
+        }
+        return;
+    }
+    float u1[12], l1[12], n1[12];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float mp = fmaxf(m[i], 0.0f);
+        const float pp = fmaxf(p[i], 0.0f);
+        u1[3 * i + 0] = tau_uniform(w[i].x);
+        l1[3 * i + 0] = lam_tx[i];
+        u1[3 * i + 1] = tau_uniform(w[i].y);
+        l1[3 * i + 1] = __fmul_rn(mp, p_dec_m);
+        u1[3 * i + 2] = tau_uniform(w[i].w);
+        l1[3 * i + 2] = __fmul_rn(pp, p_dec_p);
+    }
+    poisson_icdf50_lockstep<12>(u1, l1, n1);
+    float u2[4], l2[4], n2[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float mp = fmaxf(m[i], 0.0f);
+        const float n_md = fminf(n1[3 * i + 1], mp);
+        m[i] = fmaxf(__fsub_rn(__fadd_rn(m[i], n1[3 * i + 0]), n_md), 0.0f);
+        u2[i] = tau_uniform(w[i].z);
+        l2[i] = __fmul_rn(__fmul_rn(k_t, m[i]), dt);
+    }
+    poisson_icdf50_lockstep<4>(u2, l2, n2);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float pp = fmaxf(p[i], 0.0f);
+        const float n_pd = fminf(n1[3 * i + 2], pp);
+        p[i] = fmaxf(__fsub_rn(__fadd_rn(p[i], n2[i]), n_pd), 0.0f);
+    }
+}
+
+}  // namespace scrna

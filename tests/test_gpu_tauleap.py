@@ -7,6 +7,9 @@ uniforms, so counts, promoter states, volumes and the concentration readout are 
 Regulated networks: the oracle's regulation is FP64 (cle.jl's contraction) and the kernel's
 FP32, so a count can differ where a uniform falls within rounding of a Poisson CDF step;
 fewer than 1 % of the final counts may differ and per-gene means agree within 1 %.
+The kernel draws a gene quad's Poisson counts either in lock step or one after another
+(SCRNA_TAU_LOCKSTEP=1 / 0 forces one; lock step by default): both schedules give
+the same bits, so the bit-exact cases run under each.
 Statistical pins of the reference: test/test_analytical_moments.jl:85-96 (means within 3 %,
 variance and Fano within 15 % of the exact two-stage moments) and test/test_gpu_parity.jl:32-42.
 """
@@ -29,8 +32,14 @@ def _tau_run(pkg, net, kin, **kw):
     return run
 
 
+@pytest.fixture(params=["0", "1"], ids=["serial", "lockstep"])
+def schedule(request, monkeypatch):
+    monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("G,bursty", [(1, False), (4, False), (7, True), (13, True)])
-def test_unregulated_trajectories_bit_exact(pkg, orc, G, bursty):
+def test_unregulated_trajectories_bit_exact(pkg, orc, G, bursty, schedule):
     net = _unregulated(pkg, G, bursty, seed=G)
     kin = pkg.KineticParams(k_t=3.0, K_d=10.0, n=2.0, mu_m=0.7, mu_p=0.3)
     N, steps = 300, 400
@@ -42,7 +51,7 @@ def test_unregulated_trajectories_bit_exact(pkg, orc, G, bursty):
 
 
 @pytest.mark.parametrize("partition,exclude_mother", [("binomial", False), ("halve", True)])
-def test_population_bit_exact(pkg, orc, partition, exclude_mother):
+def test_population_bit_exact(pkg, orc, partition, exclude_mother, schedule):
     net = _unregulated(pkg, 5, True, seed=9)
     kin = pkg.KineticParams(k_t=2.0, K_d=10.0, n=2.0, mu_m=0.8, mu_p=0.25, dilution=0.1)
     N, steps = 200, 350
@@ -70,6 +79,31 @@ def test_regulated_network_against_oracle(pkg, orc):
         assert np.mean(got[k] != ref[k]) < 0.01, k
         mg, mr = got[k].mean(1), ref[k].mean(1)
         assert np.max(np.abs(mg - mr) / np.maximum(mr, 1.0)) < 0.01, k
+
+
+def test_schedules_equal_on_regulated_network(pkg, monkeypatch):
+    """Lock-step and one-after-another draws: same counts, promoters and volumes, with
+    regulation, telegraph genes and a population (cells beyond several tiles)."""
+    net = pkg.sample_network(23, seed=5, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    pop = pkg.PopulationConfig(cell_num=700, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
+    outs = []
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", mode)
+        outs.append(_tau_run(pkg, net, kin, cell_num=700, T=0.0, n_steps=250, seed=3, readout="both", dt=0.01,
+                             population=pop).read_raw())
+    for k in ("M", "P", "prom", "V"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_small_div_matches_ieee_division(pkg):
+    """The tau-leap's branch-free quotient lam / k (Markstein's correction of lam * RN(1/k))
+    equals IEEE division for every float lam in [2^-100, 2^100] and every k = 1..50."""
+    lo = 27 << 23          # 2^-100
+    hi = (227 << 23) + 1   # 2^100, included
+    n, lam, k = pkg.debug_small_div_check(lo, hi)
+    assert n == 0, (hex(lam), k)
+    assert pkg.debug_small_div_check(0, 1)[0] == 0  # lam = 0
 
 
 def test_two_stage_moments(pkg):
