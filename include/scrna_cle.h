@@ -357,6 +357,16 @@ int scrna_wait(scrna_server* srv, uint64_t ticket, int32_t timeout_ms, double* o
                double* efficiencies, double* latency_s);
 int scrna_cancel(scrna_server* srv, uint64_t ticket);
 int scrna_server_get_stats(scrna_server* srv, scrna_server_stats* stats);
+/* Trace of the server's most recent chunks (up to 4,096, oldest first): per chunk the
+ * worker's clock (seconds since the server was created) when its launches were issued and
+ * when they had finished, the requests and kernel groups it ran, and its cell·gene·steps.
+ * With recs NULL sets *n to the number held; else copies min(capacity, held) records. */
+typedef struct {
+    double t_start, t_end;
+    int32_t requests, groups;
+    int64_t units;
+} scrna_chunk_record;
+int scrna_server_trace(scrna_server* srv, scrna_chunk_record* recs, int32_t capacity, int32_t* n);
 
 /* ---- scratch-free run ---------------------------------------------------------------
  * This entry point has no counterpart in the reference.  It is for callers that

@@ -11,9 +11,9 @@ from .model import (CLE, INF, BinomialTauLeap, CaptureModel, CoopEdge, GeneNetwo
                     precompute_hill_matrices, steady_state)
 from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, config3, config4_requests,
                       dense_network, sample_network)
-from .api import (Context, DeviceRun, NetHandle, Server, apply_capture, debug_philox, debug_small_div_check,
-                  default_context, ks_statistic_device, measure_philox_rate, measure_pipe_peaks, simulate,
-                  simulate_gpu_batch)
+from .api import (Context, DeviceRun, NetHandle, Server, ServerPool, apply_capture, debug_philox,
+                  debug_small_div_check, default_context, ks_statistic_device, least_loaded, measure_philox_rate,
+                  measure_pipe_peaks, simulate, simulate_gpu_batch)
 from ._lib import ScrnaError
 from .validate import (column_moments, compare_moments, ks_critical_value, ks_statistic, max_moment_error,
                        moment_errors, telegraph_fano, telegraph_mean, telegraph_pmf, telegraph_variance)
@@ -24,7 +24,7 @@ __all__ = [
     "default_algorithm", "hill_activation", "hill_repression", "is_bursty", "n_steps",
     "precompute_hill_matrices", "steady_state", "sample_network", "dense_network", "config0", "config1",
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
-    "NetHandle", "Server", "apply_capture", "debug_philox", "debug_small_div_check", "default_context",
+    "NetHandle", "Server", "ServerPool", "least_loaded", "apply_capture", "debug_philox", "debug_small_div_check", "default_context",
     "measure_philox_rate", "measure_pipe_peaks", "simulate",
     "simulate_gpu_batch", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
     "moment_errors", "ks_statistic", "ks_critical_value", "ks_statistic_device", "telegraph_pmf", "telegraph_mean",

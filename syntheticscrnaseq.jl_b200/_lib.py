@@ -63,6 +63,11 @@ class ServerStats(C.Structure):
                [("busy_s", C.c_double), ("chunks", C.c_int64)]
 
 
+class ChunkRecord(C.Structure):
+    _fields_ = [("t_start", C.c_double), ("t_end", C.c_double), ("requests", C.c_int32), ("groups", C.c_int32),
+                ("units", C.c_int64)]
+
+
 P = C.c_void_p
 I32, I64, U32, U64, DBL = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
 
@@ -114,6 +119,7 @@ SIGNATURES = {
     "scrna_wait": (C.c_int, [P, U64, I32, P, P, P, C.POINTER(DBL)]),
     "scrna_cancel": (C.c_int, [P, U64]),
     "scrna_server_get_stats": (C.c_int, [P, P]),
+    "scrna_server_trace": (C.c_int, [P, P, I32, P]),
     "scrna_debug_philox": (C.c_int, [P, I32, P, P, P]),
     "scrna_debug_small_div_check": (C.c_int, [P, U32, U32, P, P, P]),
     "scrna_debug_tc_gemm": (C.c_int, [P, P, P, P, I64, I32, I32, I32]),

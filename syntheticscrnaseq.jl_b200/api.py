@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _lib, _pinned
 from ._lib import Capture, Kinetics, Opts, Population, check
-from .model import BinomialTauLeap, CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig
+from .model import BinomialTauLeap, CLE, CaptureModel, GeneNetwork, KineticParams, PopulationConfig, n_steps as n_steps_of
 
 READOUT = {"mrna": 0, "protein": 1, "both": 2}
 PRECISION = {"fp32": 0, "fp64_plain": 1, "fp32_f16": 2}
@@ -547,6 +547,15 @@ class Server:
         check(self.ctx.lib.scrna_server_get_stats(self.h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in s._fields_}
 
+    def trace(self) -> List[dict]:
+        """The most recent chunks (oldest first): t_start / t_end on the server's clock
+        (seconds since creation), requests, kernel groups and cell·gene·steps of each."""
+        n = C.c_int32()
+        check(self.ctx.lib.scrna_server_trace(self.h, None, 0, C.byref(n)))
+        recs = (_lib.ChunkRecord * max(n.value, 1))()
+        check(self.ctx.lib.scrna_server_trace(self.h, recs, n.value, C.byref(n)))
+        return [{f: getattr(recs[i], f) for f, _ in _lib.ChunkRecord._fields_} for i in range(n.value)]
+
     def close(self):
         if getattr(self, "h", None):
             if getattr(self.ctx, "h", None):
@@ -558,3 +567,71 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def least_loaded(loads: Sequence[float]) -> int:
+    """Index of the smallest outstanding load (the first of equal ones)."""
+    best = 0
+    for i, x in enumerate(loads):
+        if x < loads[best]:
+            best = i
+    return best
+
+
+class ServerPool:
+    """One Server per context (normally one context per GPU): each request goes to the server
+    with the fewest outstanding cell·gene·steps (submitted, not yet done), so a request stream
+    larger than one GPU's compute spreads over the devices.  Requests are independent and each
+    runs wholly on one device, so results equal `simulate`'s whichever server takes them."""
+
+    def __init__(self, contexts: Sequence[Context], *, hbm_budget_bytes: int = 0, chunk_steps: int = 250):
+        if not contexts:
+            raise ValueError("ServerPool needs at least one context")
+        self.servers = [Server(c, hbm_budget_bytes=hbm_budget_bytes, chunk_steps=chunk_steps) for c in contexts]
+        self._submitted = [0] * len(self.servers)
+        self._where = {}
+        self._next = 1
+
+    def loads(self) -> list:
+        """Outstanding cell·gene·steps of each server."""
+        return [self._submitted[i] - s.stats()["units_done"] for i, s in enumerate(self.servers)]
+
+    def submit(self, net: GeneNetwork, alg: CLE, kin: KineticParams, *, cell_num: int, T: float = 50.0,
+               n_steps: int = 0, **kw) -> int:
+        i = least_loaded(self.loads())
+        srv = self.servers[i]
+        t = srv.submit(_handle_for(net, srv.ctx), alg, kin, cell_num=cell_num, T=T, n_steps=n_steps, **kw)
+        steps = n_steps if n_steps > 0 else n_steps_of(T, alg.dt)
+        self._submitted[i] += net.G * int(cell_num) * steps
+        ticket = self._next
+        self._next += 1
+        self._where[ticket] = (i, t)
+        return ticket
+
+    def server_of(self, ticket: int) -> int:
+        return self._where[ticket][0]
+
+    def poll(self, ticket: int) -> str:
+        i, t = self._where[ticket]
+        return self.servers[i].poll(t)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        i, t = self._where[ticket]
+        out = self.servers[i].wait(t, timeout_ms)
+        del self._where[ticket]
+        return out
+
+    def cancel(self, ticket: int):
+        i, t = self._where[ticket]
+        self.servers[i].cancel(t)
+
+    def stats(self) -> dict:
+        per = [s.stats() for s in self.servers]
+        tot = {k: sum(p[k] for p in per) for k in per[0]}
+        tot["busy_s_max"] = max(p["busy_s"] for p in per)
+        tot["per_server"] = per
+        return tot
+
+    def close(self):
+        for s in self.servers:
+            s.close()

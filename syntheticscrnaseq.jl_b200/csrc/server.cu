@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -79,6 +80,14 @@ struct scrna_server {
     uint64_t next_ticket = 1;
     scrna_server_stats stats{};
     DevBuf args_dev, items_dev, counters_dev;
+    // the kernel groups of a chunk run side by side, one stream each, between two events
+    static constexpr int kGroupStreams = 8;
+    cudaStream_t gstream[kGroupStreams] = {};
+    cudaEvent_t ev_inputs = nullptr, ev_group[kGroupStreams] = {};
+    int n_group_streams = kGroupStreams;  // SCRNA_SERVER_GROUP_STREAMS=1: the groups one after another
+    double t0 = 0.0;                      // creation time, origin of the trace clock
+    static constexpr size_t kTrace = 4096;
+    std::deque<scrna_chunk_record> trace;
     void run();
 };
 
@@ -215,9 +224,14 @@ void scrna_server::run() {
             (e = cudaMemcpyAsync(items_dev.p, h_items.data(), h_items.size() * sizeof(TileWork), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
             (e = cudaMemsetAsync(counters_dev.p, 0, groups.size() * sizeof(int), stream)) != cudaSuccess)
             rc = SCRNA_ECUDA;
+        // every group stream waits for this chunk's argument and work-item copies
+        if (rc == SCRNA_OK && (e = cudaEventRecord(ev_inputs, stream)) != cudaSuccess) rc = SCRNA_ECUDA;
+        for (int k = 0; rc == SCRNA_OK && k < n_group_streams && k < (int)groups.size(); ++k)
+            if ((e = cudaStreamWaitEvent(gstream[k], ev_inputs, 0)) != cudaSuccess) rc = SCRNA_ECUDA;
         size_t gi = 0;
         for (auto& kv : groups) {
             if (rc != SCRNA_OK) break;
+            cudaStream_t gs = gstream[gi % n_group_streams];
             const auto& key = kv.first;
             const int n_items = (int)kv.second.size();
             const TileWork* items = items_dev.as<TileWork>() + offsets[gi];
@@ -228,16 +242,32 @@ void scrna_server::run() {
             if (std::get<0>(key))
                 e = warpcell_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<1>(key),
                                           std::get<2>(key), std::get<4>(key), false, sh.second, grid,
-                                          std::get<3>(key), TileCtl{}, 0, nullptr, stream);
+                                          std::get<3>(key), TileCtl{}, 0, nullptr, gs);
             else
                 e = fused_queue_launch(args_dev.as<FusedArgs>(), items, n_items, counter, std::get<3>(key), sh.first,
-                                       sh.second, false, grid, TileCtl{}, 0, stream);
+                                       sh.second, false, grid, TileCtl{}, 0, gs);
             if (e != cudaSuccess) rc = SCRNA_ECUDA;
             ++gi;
         }
-        if (rc == SCRNA_OK && (e = cudaStreamSynchronize(stream)) != cudaSuccess) rc = SCRNA_ECUDA;
+        // the chunk ends when every group stream has finished
+        for (int k = 0; k < n_group_streams && k < (int)groups.size(); ++k) {
+            cudaError_t e2 = cudaEventRecord(ev_group[k], gstream[k]);
+            if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(stream, ev_group[k], 0);
+            if (e2 != cudaSuccess && rc == SCRNA_OK) { rc = SCRNA_ECUDA; e = e2; }
+        }
+        {
+            cudaError_t e2 = cudaStreamSynchronize(stream);
+            if (e2 != cudaSuccess && rc == SCRNA_OK) { rc = SCRNA_ECUDA; e = e2; }
+        }
         const double t_end = now_s();
         std::lock_guard<std::mutex> lk(mu);
+        {
+            scrna_chunk_record rec{t_chunk - t0, t_end - t0, (int32_t)run_set.size(), (int32_t)groups.size(), 0};
+            for (SrvRequest* r : run_set)
+                if (r->s1 >= r->s0) rec.units += (int64_t)r->net->G * r->N * (r->s1 - r->s0 + 1);
+            if (trace.size() == kTrace) trace.pop_front();
+            trace.push_back(rec);
+        }
         stats.busy_s += t_end - t_chunk;
         stats.chunks += (int64_t)groups.size();
         ctx->launches += (int64_t)groups.size();
@@ -265,6 +295,15 @@ void scrna_server::run() {
     }
 }
 
+static void destroy_streams(scrna_server* s) {
+    for (int k = 0; k < scrna_server::kGroupStreams; ++k) {
+        if (s->ev_group[k]) cudaEventDestroy(s->ev_group[k]);
+        if (s->gstream[k]) cudaStreamDestroy(s->gstream[k]);
+    }
+    if (s->ev_inputs) cudaEventDestroy(s->ev_inputs);
+    if (s->stream) cudaStreamDestroy(s->stream);
+}
+
 extern "C" int scrna_server_create(scrna_ctx* ctx, int64_t budget, int32_t chunk_steps, scrna_server** out) {
     if (!ctx || !out) return fail(SCRNA_EINVAL, "ctx/out is NULL");
     if (chunk_steps <= 0) return fail(SCRNA_EINVAL, "chunk_steps must be positive");
@@ -278,8 +317,20 @@ extern "C" int scrna_server_create(scrna_ctx* ctx, int64_t budget, int32_t chunk
         budget = (int64_t)(0.8 * (double)fr);
     }
     s->budget = budget;
+    s->t0 = now_s();
+    if (const char* g = std::getenv("SCRNA_SERVER_GROUP_STREAMS"))
+        s->n_group_streams = std::min(std::max(std::atoi(g), 1), (int)scrna_server::kGroupStreams);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) { delete s; return fail(SCRNA_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_inputs, cudaEventDisableTiming);
+    for (int k = 0; k < scrna_server::kGroupStreams && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&s->gstream[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_group[k], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        destroy_streams(s);
+        delete s;
+        return fail(SCRNA_ECUDA, "stream/event creation: %s", cudaGetErrorString(e));
+    }
     s->worker = std::thread([s] { s->run(); });
     *out = s;
     return SCRNA_OK;
@@ -295,8 +346,10 @@ extern "C" int scrna_server_destroy(scrna_server* s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->stream);
+    for (int k = 0; k < scrna_server::kGroupStreams; ++k)
+        if (s->gstream[k]) cudaStreamSynchronize(s->gstream[k]);
     for (auto& kv : s->reqs) release(kv.second);
-    cudaStreamDestroy(s->stream);
+    destroy_streams(s);
     delete s;
     return SCRNA_OK;
 }
@@ -386,6 +439,19 @@ extern "C" int scrna_cancel(scrna_server* s, uint64_t ticket) {
     else if (r->state == SCRNA_REQ_RUNNING) r->cancel = true;         // dropped at the next chunk boundary
     s->cv_done.notify_all();
     s->cv_work.notify_all();
+    return SCRNA_OK;
+}
+
+extern "C" int scrna_server_trace(scrna_server* s, scrna_chunk_record* recs, int32_t capacity, int32_t* n) {
+    if (!s || !n) return fail(SCRNA_EINVAL, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!recs) {
+        *n = (int32_t)s->trace.size();
+        return SCRNA_OK;
+    }
+    const int32_t k = std::min<int32_t>(std::max(capacity, 0), (int32_t)s->trace.size());
+    for (int32_t i = 0; i < k; ++i) recs[i] = s->trace[i];
+    *n = k;
     return SCRNA_OK;
 }
 

@@ -39,6 +39,11 @@ def test_server_alone_equals_mixed_equals_simulate(pkg):
         assert np.all(np.isfinite(out)) and lat >= 0.0
     st = srv.stats()
     assert st["completed"] == 2 + len(tickets) and st["failed"] == 0 and st["bytes_in_use"] == 0
+    # the chunk trace accounts for every cell·gene·step and every group launch
+    tr = srv.trace()
+    assert sum(r["units"] for r in tr) == st["units_done"] and sum(r["groups"] for r in tr) == st["chunks"]
+    assert all(r["t_end"] >= r["t_start"] >= 0.0 and r["requests"] >= 1 for r in tr)
+    assert all(a["t_end"] <= b["t_start"] for a, b in zip(tr, tr[1:]))
     srv.close()
 
 
@@ -84,3 +89,24 @@ def test_server_cancel(pkg):
     t2 = srv.submit(pkg.NetHandle(net), pkg.CLE(0.01), kin, cell_num=100, T=0.2)
     assert np.all(np.isfinite(srv.wait(t2, WAIT_MS)[0]))
     srv.close()
+
+
+def test_server_pool_spreads_requests_and_matches_simulate(pkg):
+    """Two servers (here on one GPU, normally one per device): requests go to the less
+    loaded one, and every result equals simulate's."""
+    kin = pkg.WORKLOAD_KINETICS
+    nets = _nets(pkg)
+    ctxs = [pkg.Context(0), pkg.Context(0)]
+    pool = pkg.ServerPool(ctxs, chunk_steps=45)
+    jobs = [(nets[i % len(nets)], dict(cell_num=150 + 60 * i, T=0.6 + 0.1 * i, readout="mrna", seed=70 + i, stream=i))
+            for i in range(8)]
+    tickets = [pool.submit(n, pkg.CLE(0.01), kin, **kw) for n, kw in jobs]
+    assert {pool.server_of(t) for t in tickets} == {0, 1}
+    for (n, kw), t in zip(jobs, tickets):
+        got = pool.wait(t, WAIT_MS)[0]
+        assert np.array_equal(got, pkg.simulate(n, pkg.CLE(0.01), kin, **kw))
+    st = pool.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0 and pool.loads() == [0, 0]
+    pool.close()
+    for c in ctxs:
+        c.close()

@@ -106,3 +106,38 @@ def test_network_digest_skips_large_networks(pkg):
     from scrna_b200 import api
     big = pkg.dense_network(400, seed=1, density=0.1, n_coop=2, n_redun=2)  # 400 x 400 doubles = 1.28 MB
     assert api._net_digest(big) is None
+
+
+class _FakeServer:
+    """A server stand-in that records submissions and never finishes them."""
+
+    def __init__(self):
+        self.ctx = object()
+        self.jobs = []
+
+    def submit(self, handle, alg, kin, **kw):
+        self.jobs.append(kw)
+        return len(self.jobs)
+
+    def stats(self):
+        return {"units_done": 0, "completed": 0, "failed": 0, "busy_s": 0.0}
+
+
+def test_least_loaded_and_pool_placement(pkg, monkeypatch):
+    assert pkg.least_loaded([3, 1, 1, 5]) == 1 and pkg.least_loaded([0]) == 0
+    from importlib import import_module
+    api = import_module(pkg.__name__ + ".api")
+    monkeypatch.setattr(api, "_handle_for", lambda net, ctx: None)
+    pool = object.__new__(pkg.ServerPool)
+    pool.servers = [_FakeServer(), _FakeServer()]
+    pool._submitted = [0, 0]
+    pool._where = {}
+    pool._next = 1
+    kin = pkg.WORKLOAD_KINETICS
+    big = pkg.GeneNetwork(100, np.ones(100), np.zeros((100, 100)))
+    small = pkg.GeneNetwork(2, np.ones(2), np.zeros((2, 2)))
+    t1 = pool.submit(big, pkg.CLE(0.01), kin, cell_num=1000, T=1.0)      # 1e7 units -> server 0
+    t2 = pool.submit(small, pkg.CLE(0.01), kin, cell_num=1000, T=1.0)    # server 1 (empty)
+    t3 = pool.submit(small, pkg.CLE(0.01), kin, cell_num=1000, T=1.0)    # server 1 (2e5 < 1e7)
+    assert [pool.server_of(t) for t in (t1, t2, t3)] == [0, 1, 1]
+    assert pool.loads() == [100 * 1000 * 100, 2 * 2 * 1000 * 100]
