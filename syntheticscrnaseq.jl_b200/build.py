@@ -88,7 +88,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             print("\n".join(logs))
     if jobs or force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
-        _run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcublasLt"], verbose)
+        _run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcublasLt", "-ldl"], verbose)
         os.replace(tmp, LIB)
     return LIB
 

@@ -15,6 +15,7 @@
 
 #include "../../include/scrna_cle.h"
 #include "capi_internal.h"
+#include "nvtx_range.h"
 #include "cle_internal.h"
 
 namespace scrna {
@@ -830,16 +831,19 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
 extern "C" int scrna_cle_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                     const scrna_population* pop, const scrna_capture* cap,
                                     const scrna_cle_opts* o, scrna_state* st) {
+    NvtxRange nvtx_range_("scrna_cle_run_device");
     return run_device(ctx, net, kin, pop, cap, o, st, false);
 }
 
 extern "C" int scrna_tauleap_run_device(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                         const scrna_population* pop, const scrna_capture* cap,
                                         const scrna_cle_opts* o, scrna_state* st) {
+    NvtxRange nvtx_range_("scrna_tauleap_run_device");
     return run_device(ctx, net, kin, pop, cap, o, st, true);
 }
 
 extern "C" int scrna_state_read(scrna_ctx* ctx, scrna_state* st, double* out, int32_t* counts, double* eff) {
+    NvtxRange nvtx_range_("scrna_state_read");
     if (int r = check_ctx(ctx)) return r;
     if (!st) return fail(SCRNA_EINVAL, "state is NULL");
     if (int r = set_device(ctx)) return r;
@@ -950,12 +954,14 @@ static int simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* 
 extern "C" int scrna_cle_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                   const scrna_population* pop, const scrna_capture* cap,
                                   const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+    NvtxRange nvtx_range_("scrna_cle_simulate");
     return simulate(ctx, net, kin, pop, cap, o, out, counts, eff, false);
 }
 
 extern "C" int scrna_tauleap_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                       const scrna_population* pop, const scrna_capture* cap,
                                       const scrna_cle_opts* o, double* out, int32_t* counts, double* eff) {
+    NvtxRange nvtx_range_("scrna_tauleap_simulate");
     return simulate(ctx, net, kin, pop, cap, o, out, counts, eff, true);
 }
 
@@ -963,6 +969,7 @@ extern "C" int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_n
                                         const scrna_kinetics* kins, int32_t n_kins, const int64_t* cell_nums,
                                         const scrna_population* const* pops, const scrna_capture* cap,
                                         const scrna_cle_opts* opts, double* const* outs, int32_t* const* counts) {
+    NvtxRange nvtx_range_("scrna_cle_simulate_batch");
     if (int r = check_ctx(ctx)) return r;
     if (B <= 0 || !nets || !kins || !opts || !outs) return fail(SCRNA_EINVAL, "bad batch arguments");
     if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
@@ -975,6 +982,7 @@ extern "C" int scrna_tauleap_simulate_batch(scrna_ctx* ctx, int32_t B, const scr
                                             const scrna_kinetics* kins, int32_t n_kins, const int64_t* cell_nums,
                                             const scrna_population* const* pops, const scrna_capture* cap,
                                             const scrna_cle_opts* opts, double* const* outs, int32_t* const* counts) {
+    NvtxRange nvtx_range_("scrna_tauleap_simulate_batch");
     if (int r = check_ctx(ctx)) return r;
     if (B <= 0 || !nets || !kins || !opts || !outs) return fail(SCRNA_EINVAL, "bad batch arguments");
     if (n_kins != 1 && n_kins != B) return fail(SCRNA_EINVAL, "n_kins must be 1 or B");
@@ -985,6 +993,7 @@ extern "C" int scrna_tauleap_simulate_batch(scrna_ctx* ctx, int32_t B, const scr
 
 extern "C" int scrna_apply_capture(scrna_ctx* ctx, int64_t N, int32_t G, const double* X, const scrna_capture* cap,
                                    uint64_t seed, uint32_t stream, int32_t* Y, double* eff) {
+    NvtxRange nvtx_range_("scrna_apply_capture");
     if (int r = check_ctx(ctx)) return r;
     if (N <= 0 || G <= 0 || !X || !cap || !Y) return fail(SCRNA_EINVAL, "bad capture arguments");
     if (!(cap->efficiency > 0.0) || !(cap->efficiency_std >= 0.0)) return fail(SCRNA_EINVAL, "capture efficiency must be > 0 and std >= 0");

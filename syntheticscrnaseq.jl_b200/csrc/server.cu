@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "capi_internal.h"
+#include "nvtx_range.h"
 
 namespace scrna {
 void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr, GeneInit* gi,
@@ -186,6 +187,7 @@ void scrna_server::run() {
         }
         if (run_set.empty()) continue;
         const double t_chunk = now_s();
+        NvtxRange nvtx_chunk_("scrna_server_chunk");
         // one persistent launch per kernel group over the running requests' tiles
         h_args.clear();
         std::map<std::tuple<int, int, int, int, int>, std::vector<TileWork>> groups;
@@ -394,6 +396,7 @@ extern "C" int scrna_poll(scrna_server* s, uint64_t ticket, int32_t* state) {
 
 extern "C" int scrna_wait(scrna_server* s, uint64_t ticket, int32_t timeout_ms, double* out, int32_t* counts,
                           double* eff, double* latency_s) {
+    NvtxRange nvtx_range_("scrna_wait");
     if (!s) return fail(SCRNA_EINVAL, "server is NULL");
     SrvRequest* r = nullptr;
     {

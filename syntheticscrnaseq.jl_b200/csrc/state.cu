@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "capi_internal.h"
+#include "nvtx_range.h"
 
 namespace scrna {
 namespace {
@@ -83,6 +84,7 @@ using namespace scrna;
 extern "C" int scrna_cle_resume(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                 const scrna_population* pop, const scrna_capture* cap, const scrna_cle_opts* opts,
                                 scrna_state* st) {
+    NvtxRange nvtx_range_("scrna_cle_resume");
     if (!ctx || !net || !st) return fail(SCRNA_EINVAL, "NULL argument");
     return resume_register_run(ctx, const_cast<scrna_net*>(net), kin, pop, cap, opts, st, false);
 }
@@ -90,6 +92,7 @@ extern "C" int scrna_cle_resume(scrna_ctx* ctx, const scrna_net* net, const scrn
 extern "C" int scrna_tauleap_resume(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                                     const scrna_population* pop, const scrna_capture* cap, const scrna_cle_opts* opts,
                                     scrna_state* st) {
+    NvtxRange nvtx_range_("scrna_tauleap_resume");
     if (!ctx || !net || !st) return fail(SCRNA_EINVAL, "NULL argument");
     return resume_register_run(ctx, const_cast<scrna_net*>(net), kin, pop, cap, opts, st, true);
 }
@@ -101,6 +104,7 @@ extern "C" int scrna_state_steps_done(const scrna_state* st, int64_t* steps) {
 }
 
 extern "C" int scrna_state_checkpoint(scrna_ctx* ctx, scrna_state* st, void* buf, size_t capacity, size_t* bytes) {
+    NvtxRange nvtx_range_("scrna_state_checkpoint");
     if (!ctx || !st || !bytes) return fail(SCRNA_EINVAL, "NULL argument");
     if (!st->has_register_state) return fail(SCRNA_EINVAL, "the state holds no register-path run");
     const size_t need = checkpoint_bytes(st->G, st->N, st->last_pop);
@@ -131,6 +135,7 @@ extern "C" int scrna_state_checkpoint(scrna_ctx* ctx, scrna_state* st, void* buf
 }
 
 extern "C" int scrna_state_restore(scrna_ctx* ctx, scrna_state* st, const void* buf, size_t bytes) {
+    NvtxRange nvtx_range_("scrna_state_restore");
     if (!ctx || !st || !buf) return fail(SCRNA_EINVAL, "NULL argument");
     if (bytes < sizeof(CheckpointHeader)) return fail(SCRNA_EINVAL, "not a checkpoint (too short)");
     CheckpointHeader h;

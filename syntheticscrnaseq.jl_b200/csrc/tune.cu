@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "capi_internal.h"
+#include "nvtx_range.h"
 
 namespace scrna {
 
@@ -349,6 +350,7 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     if (!c.found && !ctx->tune_path.empty())
         if (int r = lookup(ctx->tune_path, key, &c)) return r;
     if (!c.found && ctx->tune_mode == 1 && may_measure) {
+        NvtxRange nvtx_range_("scrna_autotune_measure");
         FusedArgs a{};
         if (base) a = *base;
         else fill_fused_args(net, kin, nullptr, nullptr, o, st, &a);

@@ -22,6 +22,7 @@
 #include <cub/device/device_segmented_sort.cuh>
 
 #include "capi_internal.h"
+#include "nvtx_range.h"
 
 namespace scrna {
 namespace {
@@ -189,6 +190,7 @@ int sorted_columns(scrna_ctx* ctx, const scrna_state* st, int source, DevBuf& ou
 using namespace scrna;
 
 extern "C" int scrna_state_moments(scrna_ctx* ctx, scrna_state* st, int32_t source, double* mean, double* var) {
+    NvtxRange nvtx_range_("scrna_state_moments");
     if (!ctx || !st) return fail(SCRNA_EINVAL, "NULL argument");
     if (int r = set_device(ctx)) return r;
     const void* data;
@@ -213,6 +215,7 @@ extern "C" int scrna_state_moments(scrna_ctx* ctx, scrna_state* st, int32_t sour
 }
 
 extern "C" int scrna_state_ks(scrna_ctx* ctx, scrna_state* a, scrna_state* b, int32_t source, double* D) {
+    NvtxRange nvtx_range_("scrna_state_ks");
     if (!ctx || !a || !b || !D) return fail(SCRNA_EINVAL, "NULL argument");
     if (int r = set_device(ctx)) return r;
     DevBuf sa, sb;
@@ -237,6 +240,7 @@ extern "C" int scrna_state_ks(scrna_ctx* ctx, scrna_state* a, scrna_state* b, in
 
 extern "C" int scrna_state_histogram(scrna_ctx* ctx, scrna_state* st, int32_t source, int32_t column, int32_t nbins,
                                      int64_t* hist) {
+    NvtxRange nvtx_range_("scrna_state_histogram");
     if (!ctx || !st || !hist) return fail(SCRNA_EINVAL, "NULL argument");
     if (nbins <= 0) return fail(SCRNA_EINVAL, "nbins must be positive");
     if (int r = set_device(ctx)) return r;
@@ -264,6 +268,7 @@ extern "C" int scrna_state_histogram(scrna_ctx* ctx, scrna_state* st, int32_t so
 
 extern "C" int scrna_state_write_mtx(scrna_ctx* ctx, scrna_state* st, const char* dir, const char* const* gene_names,
                                      const char* barcode_prefix) {
+    NvtxRange nvtx_range_("scrna_state_write_mtx");
     if (!ctx || !st || !dir) return fail(SCRNA_EINVAL, "NULL argument");
     if (int r = set_device(ctx)) return r;
     const void* data;
