@@ -1,0 +1,88 @@
+"""The paths at their size limits, through the C ABI: the register path's largest network
+(512 genes = 128 gene quads; the lane kernel's limit too), the binomial tau-leap's, and the
+fused tensor-core kernel's (4,096 genes, its epilogue gene table in shared memory), plus the
+sizes just beyond them: rejected on the register path, routed to the library-GEMM variant
+on the tensor path.  Tolerances as in the parity tests (2e-3 relative against the FP64
+oracle on the same increments; bit-exact for the unregulated tau-leap; the 16-bit
+contraction's rounding between the two tensor variants)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 2e-3
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1.0)))
+
+
+def _raw(pkg, net, alg, kin, *, N, steps, seed, path="auto", precision="fp32"):
+    run = pkg.DeviceRun(net, alg, kin, cell_num=N, T=0.0, n_steps=steps, readout="both", seed=seed, path=path,
+                        precision=precision)
+    run.launch()
+    out = run.read_raw()
+    run.close()
+    return out
+
+
+def test_register_path_at_512_genes(pkg, orc):
+    net = pkg.sample_network(512, seed=31, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    N, steps = 40, 60
+    lane = _raw(pkg, net, pkg.CLE(0.01), kin, N=N, steps=steps, seed=2, path="warp")
+    block = _raw(pkg, net, pkg.CLE(0.01), kin, N=N, steps=steps, seed=2, path="block")
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(lane[k], block[k]), k
+    ref = orc.simulate(net, kin, dt=0.01, cell_num=N, n_steps=steps, seed=2)
+    assert np.array_equal(lane["prom"], ref["prom"])
+    assert _rel(lane["M"], ref["M"]) < RTOL and _rel(lane["P"], ref["P"]) < RTOL
+
+
+def test_register_path_rejects_513_genes(pkg):
+    net = pkg.sample_network(513, seed=32, bursty=False)
+    for path in ("register", "warp", "block"):
+        with pytest.raises(pkg.ScrnaError):
+            pkg.simulate(net, pkg.CLE(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1, path=path)
+    with pytest.raises(pkg.ScrnaError):
+        pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1)
+
+
+def test_tauleap_at_512_genes_bit_exact(pkg, orc):
+    rng = np.random.default_rng(512)
+    G = 512
+    net = pkg.GeneNetwork(G, np.exp(rng.uniform(0.0, np.log(10.0), G)), np.zeros((G, G)),
+                          k_on=np.exp(rng.uniform(np.log(0.1), np.log(1.0), G)),
+                          k_off=np.exp(rng.uniform(np.log(1.0), np.log(10.0), G)))
+    kin = pkg.KineticParams(k_t=3.0, K_d=10.0, n=2.0, mu_m=0.7, mu_p=0.3)
+    N, steps = 40, 80
+    got = _raw(pkg, net, pkg.BinomialTauLeap(0.05), kin, N=N, steps=steps, seed=6)
+    ref = orc.simulate(net, kin, dt=0.05, cell_num=N, n_steps=steps, seed=6, tauleap=True)
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(got[k], ref[k]), k
+
+
+def _dense(pkg, G, seed):
+    return pkg.dense_network(G, seed=seed, density=0.02, n_coop=4, n_redun=4)
+
+
+def test_fused_tensor_kernel_at_4096_genes(pkg):
+    """G = 4096: the fused kernel's largest network, against the library-GEMM variant."""
+    net = _dense(pkg, 4096, seed=41)
+    kin = pkg.WORKLOAD_KINETICS
+    a = _raw(pkg, net, pkg.CLE(0.01), kin, N=256, steps=20, seed=3, path="tensor")
+    b = _raw(pkg, net, pkg.CLE(0.01), kin, N=256, steps=20, seed=3, path="tensor_library")
+    assert np.array_equal(a["prom"], b["prom"])
+    assert _rel(a["M"], b["M"]) < 2e-2 and _rel(a["P"], b["P"]) < 2e-2
+    assert np.all(np.isfinite(a["M"])) and np.all(a["M"] >= 0)
+
+
+def test_tensor_path_beyond_4096_genes_uses_library_variant(pkg):
+    """G = 4100 on path "tensor": the library-GEMM variant runs (the same result as asking
+    for it), since the fused kernel's gene table holds 4,096 genes."""
+    net = _dense(pkg, 4100, seed=42)
+    kin = pkg.WORKLOAD_KINETICS
+    a = _raw(pkg, net, pkg.CLE(0.01), kin, N=200, steps=10, seed=4, path="tensor")
+    b = _raw(pkg, net, pkg.CLE(0.01), kin, N=200, steps=10, seed=4, path="tensor_library")
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(a[k], b[k]), k
