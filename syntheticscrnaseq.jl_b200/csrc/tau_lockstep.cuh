@@ -5,13 +5,15 @@
 // or IEEE division outside its range), so every count is bit-identical to poisson_icdf50's;
 // only the schedule changes.
 //
-// Lock step: of a gene's four draws, transcription, mRNA decay and protein decay depend on
-// the state at the start of the step alone, and translation on the new mRNA count; so the
-// quad's 12 independent draws share one loop, then its 4 translations share a second.  Each
-// chain's count is the last k whose preceding partial sum u exceeds, and the loop ends
-// (checked every second term) when u exceeds no chain's partial sum or after 50 terms.  That
-// issues 12 x the longest chain's terms instead of the sum of the chains' terms, in exchange
-// for 12 independent chains in flight.
+// Lock step: of a gene's four draws, translation needs the new mRNA count and the other three
+// only the state at the start of the step.  The quad's transcription and mRNA-decay draws
+// share one loop, then its translation and protein-decay draws a second: near the steady
+// state the two draws of a loop have about the same Poisson mean (transcription balances
+// mRNA decay, translation protein decay), so few terms are spent on chains that have stopped.
+// Each chain's count is the last k whose preceding partial sum u exceeds, and a loop ends
+// (checked every second term) when u exceeds no chain's partial sum or after 50 terms.  A
+// loop issues 8 x its longest chain's terms instead of the sum of its chains' terms, in
+// exchange for 8 independent chains in flight.
 #pragma once
 
 #include "cle_device.cuh"
@@ -99,34 +101,32 @@ __device__ __forceinline__ void tau_update_quad(float (&m)[4], float (&p)[4], co
         }
         return;
     }
-    float u1[12], l1[12], n1[12];
+    // transcription and mRNA decay of the four genes
+    float ua[8], la[8], na[8];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float mp = fmaxf(m[i], 0.0f);
-        const float pp = fmaxf(p[i], 0.0f);
-        u1[3 * i + 0] = tau_uniform(w[i].x);
-        l1[3 * i + 0] = lam_tx[i];
-        u1[3 * i + 1] = tau_uniform(w[i].y);
-        l1[3 * i + 1] = __fmul_rn(mp, p_dec_m);
-        u1[3 * i + 2] = tau_uniform(w[i].w);
-        l1[3 * i + 2] = __fmul_rn(pp, p_dec_p);
+        ua[2 * i] = tau_uniform(w[i].x);
+        la[2 * i] = lam_tx[i];
+        ua[2 * i + 1] = tau_uniform(w[i].y);
+        la[2 * i + 1] = __fmul_rn(fmaxf(m[i], 0.0f), p_dec_m);
     }
-    poisson_icdf50_lockstep<12>(u1, l1, n1);
-    float u2[4], l2[4], n2[4];
+    poisson_icdf50_lockstep<8>(ua, la, na);
+    // translation with the new mRNA counts, and protein decay
+    float ub[8], lb[8], nb[8];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float mp = fmaxf(m[i], 0.0f);
-        const float n_md = fminf(n1[3 * i + 1], mp);
-        m[i] = fmaxf(__fsub_rn(__fadd_rn(m[i], n1[3 * i + 0]), n_md), 0.0f);
-        u2[i] = tau_uniform(w[i].z);
-        l2[i] = __fmul_rn(__fmul_rn(k_t, m[i]), dt);
+        const float n_md = fminf(na[2 * i + 1], fmaxf(m[i], 0.0f));
+        m[i] = fmaxf(__fsub_rn(__fadd_rn(m[i], na[2 * i]), n_md), 0.0f);
+        ub[2 * i] = tau_uniform(w[i].z);
+        lb[2 * i] = __fmul_rn(__fmul_rn(k_t, m[i]), dt);
+        ub[2 * i + 1] = tau_uniform(w[i].w);
+        lb[2 * i + 1] = __fmul_rn(fmaxf(p[i], 0.0f), p_dec_p);
     }
-    poisson_icdf50_lockstep<4>(u2, l2, n2);
+    poisson_icdf50_lockstep<8>(ub, lb, nb);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float pp = fmaxf(p[i], 0.0f);
-        const float n_pd = fminf(n1[3 * i + 2], pp);
-        p[i] = fmaxf(__fsub_rn(__fadd_rn(p[i], n2[i]), n_pd), 0.0f);
+        const float n_pd = fminf(nb[2 * i + 1], fmaxf(p[i], 0.0f));
+        p[i] = fmaxf(__fsub_rn(__fadd_rn(p[i], nb[2 * i]), n_pd), 0.0f);
     }
 }
 
