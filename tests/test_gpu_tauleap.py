@@ -96,6 +96,18 @@ def test_schedules_equal_on_regulated_network(pkg, monkeypatch):
         assert np.array_equal(outs[0][k], outs[1][k]), k
 
 
+def test_means_outside_the_quotient_range_bit_exact(pkg, orc, schedule):
+    """Basals so small that the transcription means fall below 2^-100 (a quad then takes IEEE
+    division instead of the branch-free quotient), beside ordinary genes in the same quads."""
+    G = 7
+    basals = np.array([1e-33, 3.0, 2e-32, 5.0, 1e-34, 0.5, 4.0])
+    net = pkg.GeneNetwork(G, basals, np.zeros((G, G)))
+    kin = pkg.KineticParams(k_t=2.0, K_d=10.0, n=2.0, mu_m=0.6, mu_p=0.3)
+    got = _tau_run(pkg, net, kin, cell_num=100, T=0.0, n_steps=150, seed=9, readout="both").read_raw()
+    ref = orc.simulate(net, kin, dt=0.05, cell_num=100, n_steps=150, seed=9, tauleap=True)
+    assert np.array_equal(got["M"], ref["M"]) and np.array_equal(got["P"], ref["P"])
+
+
 def test_small_div_matches_ieee_division(pkg):
     """The tau-leap's branch-free quotient lam / k (Markstein's correction of lam * RN(1/k))
     equals IEEE division for every float lam in [2^-100, 2^100] and every k = 1..50."""
