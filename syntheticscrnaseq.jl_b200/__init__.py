@@ -15,8 +15,9 @@ from .api import (Context, DeviceRun, NetHandle, Server, ServerPool, apply_captu
                   debug_small_div_check, default_context, ks_statistic_device, least_loaded, measure_philox_rate,
                   measure_pipe_peaks, simulate, simulate_gpu_batch)
 from ._lib import ScrnaError
-from .validate import (column_moments, compare_moments, ks_critical_value, ks_statistic, max_moment_error,
-                       moment_errors, telegraph_fano, telegraph_mean, telegraph_pmf, telegraph_variance)
+from .validate import (column_moments, compare_moments, empirical_pmf, ks_critical_value, ks_statistic, ks_vs_exact,
+                       l1_distance, max_moment_error, moment_errors, pmf_comparison_from_histogram,
+                       telegraph_distribution, telegraph_fano, telegraph_mean, telegraph_pmf, telegraph_variance)
 from .mtx import read_10x_mtx
 
 __all__ = [
@@ -28,5 +29,6 @@ __all__ = [
     "measure_philox_rate", "measure_pipe_peaks", "simulate",
     "simulate_gpu_batch", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
     "moment_errors", "ks_statistic", "ks_critical_value", "ks_statistic_device", "telegraph_pmf", "telegraph_mean",
-    "telegraph_variance", "telegraph_fano", "read_10x_mtx",
+    "telegraph_variance", "telegraph_fano", "read_10x_mtx", "telegraph_distribution", "empirical_pmf",
+    "l1_distance", "ks_vs_exact", "pmf_comparison_from_histogram",
 ]

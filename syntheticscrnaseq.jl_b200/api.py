@@ -409,6 +409,13 @@ class DeviceRun:
                                                  h.ctypes.data))
         return h
 
+    def compare_pmf(self, column: int, p_exact, source: str = "readout") -> dict:
+        """L1 distance and KS statistic of one column's rounded values against an exact
+        distribution P(0..L-1) (experiments/validate_telegraph.jl:80-125), from a histogram
+        computed on the device: {"l1", "ks", "n"}."""
+        from .validate import pmf_comparison_from_histogram
+        return pmf_comparison_from_histogram(self.histogram(column, len(p_exact) + 1, source), p_exact)
+
     def write_mtx(self, directory: str, gene_names: Optional[Sequence[str]] = None, barcode_prefix: str = "cell"):
         """10x Matrix Market files (matrix.mtx, genes.tsv, barcodes.tsv) of the captured counts."""
         names = None

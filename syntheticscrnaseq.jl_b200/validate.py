@@ -16,7 +16,7 @@ The device-side reductions are DeviceRun.moments / histogram and api.ks_statisti
 """
 from __future__ import annotations
 
-from typing import Dict
+from typing import Dict, Optional
 
 import numpy as np
 
@@ -100,3 +100,71 @@ def telegraph_variance(a: float, b: float, c: float) -> float:
 
 def telegraph_fano(a: float, b: float, c: float) -> float:
     return 1.0 + b * c / ((a + b) * (a + b + 1))
+
+
+def telegraph_distribution(a: float, b: float, c: float, nmax: Optional[int] = None,
+                           tol: float = 1e-12) -> np.ndarray:
+    """P(0), ..., P(nmax) of the telegraph model (analytical.jl:71-95): nmax defaults to
+    max(ceil(mean + 10 sd), 100); the vector is cut after the last n with P(n) > tol x max P
+    and normalised."""
+    if nmax is None:
+        mu = telegraph_mean(a, b, c)
+        sd = float(np.sqrt(telegraph_variance(a, b, c)))
+        nmax = max(int(np.ceil(mu + 10.0 * sd)), 100)
+    logp = np.array([telegraph_logpmf(n, a, b, c) for n in range(nmax + 1)])
+    top = logp.max()
+    keep = np.nonzero(logp > np.log(tol) + top)[0]
+    if len(keep):
+        logp = logp[: keep[-1] + 1]
+    p = np.exp(logp - top)
+    return p / p.sum()
+
+
+def empirical_pmf(samples, nmax: int) -> np.ndarray:
+    """Fraction of the samples at each n = 0..nmax after rounding max(x, 0) half to even;
+    samples above nmax count in the total only (experiments/validate_telegraph.jl:80-89)."""
+    s = np.rint(np.maximum(np.asarray(samples, dtype=np.float64).reshape(-1), 0.0)).astype(np.int64)
+    counts = np.bincount(s[s <= nmax], minlength=nmax + 1)[: nmax + 1]
+    return counts / len(s)
+
+
+def l1_distance(p_empirical, p_exact) -> float:
+    """Sum of |p_empirical - p_exact| over the common support plus the tail mass of the longer
+    vector (experiments/validate_telegraph.jl:91-106)."""
+    pe, px = np.asarray(p_empirical, np.float64), np.asarray(p_exact, np.float64)
+    n = min(len(pe), len(px))
+    return float(np.abs(pe[:n] - px[:n]).sum() + np.abs(pe[n:]).sum() + np.abs(px[n:]).sum())
+
+
+def ks_vs_exact(samples, p_exact) -> float:
+    """Largest |ecdf - F| at each sorted sample (rounded as in empirical_pmf), taken after
+    and just before the sample's step, F the exact CDF at min(sample, len - 1)
+    (experiments/validate_telegraph.jl:108-125).  On integer samples the term before a step
+    compares F(n) with the ECDF below n, so the statistic is at least about max_n P(n)
+    whatever the samples (the first sample alone gives P(0) when it is 0): l1_distance is
+    the measure that shrinks with agreement."""
+    cdf = np.cumsum(np.asarray(p_exact, np.float64))
+    s = np.sort(np.rint(np.maximum(np.asarray(samples, dtype=np.float64).reshape(-1), 0.0)).astype(np.int64))
+    n = len(s)
+    F = cdf[np.minimum(s, len(cdf) - 1)]
+    i = np.arange(1, n + 1)
+    return float(max(np.abs(i / n - F).max(initial=0.0), np.abs((i - 1) / n - F).max(initial=0.0)))
+
+
+def pmf_comparison_from_histogram(hist, p_exact) -> dict:
+    """l1_distance(empirical_pmf) and ks_vs_exact from counts of the rounded samples at
+    0..L-1 and of all samples >= L in hist[L] (L = len(p_exact); nbins = L + 1), the same
+    values as from the samples themselves: samples at or above L - 1 all meet F[L - 1], so
+    the walk over sorted samples needs only the cumulative counts."""
+    h = np.asarray(hist, dtype=np.float64)
+    L = len(p_exact)
+    if len(h) != L + 1:
+        raise ValueError("the histogram needs len(p_exact) + 1 bins")
+    n = h.sum()
+    cdf = np.cumsum(np.asarray(p_exact, np.float64))
+    C = np.cumsum(h)
+    prev = np.concatenate([[0.0], C[:-1]])
+    F = cdf[np.minimum(np.arange(L + 1), L - 1)]
+    occ = h > 0
+    ks = float(max(np.abs(C[occ] / n - F[occ]).max(initial=0.0), np.abs(prev[occ] / n - F[occ]).max(initial=0.0)))
+    return {"l1": l1_distance(h[:L] / n, p_exact), "ks": ks, "n": int(n)}
