@@ -13,7 +13,7 @@ from .sampler import (WORKLOAD_KINETICS, Workload, config0, config1, config2, co
                       dense_network, sample_network)
 from .api import (Context, DeviceRun, NetHandle, Server, ServerPool, apply_capture, debug_philox,
                   debug_small_div_check, default_context, ks_statistic_device, least_loaded, measure_philox_rate,
-                  measure_pipe_peaks, simulate, simulate_gpu_batch)
+                  measure_pipe_peaks, simulate, simulate_gpu_batch, simulate_gpu_batch_sharded)
 from ._lib import ScrnaError
 from .validate import (column_moments, compare_moments, empirical_pmf, ks_critical_value, ks_statistic, ks_vs_exact,
                        l1_distance, max_moment_error, moment_errors, pmf_comparison_from_histogram,
@@ -27,7 +27,7 @@ __all__ = [
     "config2", "config3", "config4_requests", "Workload", "WORKLOAD_KINETICS", "Context", "DeviceRun",
     "NetHandle", "Server", "ServerPool", "least_loaded", "apply_capture", "debug_philox", "debug_small_div_check", "default_context",
     "measure_philox_rate", "measure_pipe_peaks", "simulate",
-    "simulate_gpu_batch", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
+    "simulate_gpu_batch", "simulate_gpu_batch_sharded", "ScrnaError", "INF", "column_moments", "compare_moments", "max_moment_error",
     "moment_errors", "ks_statistic", "ks_critical_value", "ks_statistic_device", "telegraph_pmf", "telegraph_mean",
     "telegraph_variance", "telegraph_fano", "read_10x_mtx", "telegraph_distribution", "empirical_pmf",
     "l1_distance", "ks_vs_exact", "pmf_comparison_from_histogram",

@@ -294,6 +294,40 @@ def simulate_gpu_batch(networks: Sequence[GeneNetwork], alg, kin, *,
     return outs
 
 
+def simulate_gpu_batch_sharded(networks: Sequence[GeneNetwork], alg, kin, *, contexts: Sequence[Context],
+                               cell_num: Union[int, Sequence[int]] = 1000, T: float = 50.0,
+                               readout: str = "protein", seed: int = 0, stream: int = 0,
+                               populations: Optional[Sequence[Optional[PopulationConfig]]] = None,
+                               capture: Optional[CaptureModel] = None):
+    """simulate_gpu_batch over several contexts, normally one per GPU: whole networks (a
+    Moran population couples a network's cells) in contiguous ranges of balanced cost
+    (genes x cells), one batch call per context in its own thread.  A range starting at
+    network lo runs with base stream `stream + lo`, so network b keeps stream `stream + b`
+    and the results equal one simulate_gpu_batch call's."""
+    from concurrent.futures import ThreadPoolExecutor
+    from .sharding import shard_network_ranges
+    B = len(networks)
+    kins = list(kin) if isinstance(kin, (list, tuple)) else None
+    cns = list(cell_num) if isinstance(cell_num, (list, tuple, np.ndarray)) else [int(cell_num)] * B
+    pops = list(populations) if populations is not None else [None] * B
+    sizes = [pops[b].cell_num if pops[b] is not None else cns[b] for b in range(B)]
+    ranges = shard_network_ranges([networks[b].G * sizes[b] for b in range(B)], len(contexts))
+
+    def run(k):
+        lo, hi = ranges[k]
+        if hi <= lo:
+            return ([], []) if capture is not None else []
+        return simulate_gpu_batch(networks[lo:hi], alg, kins[lo:hi] if kins is not None else kin,
+                                  cell_num=cns[lo:hi], T=T, readout=readout, seed=seed, stream=stream + lo,
+                                  populations=pops[lo:hi], capture=capture, ctx=contexts[k])
+
+    with ThreadPoolExecutor(max_workers=len(contexts)) as ex:
+        parts = list(ex.map(run, range(len(contexts))))
+    if capture is not None:
+        return [x for p in parts for x in p[0]], [x for p in parts for x in p[1]]
+    return [x for p in parts for x in p]
+
+
 def apply_capture(X: np.ndarray, capture: CaptureModel, *, seed: int = 0, stream: int = 0,
                   ctx: Optional[Context] = None, return_efficiencies: bool = False):
     """GPU LogNormal-Binomial capture of a cells x G molecule matrix (capture.jl:25-47)."""

@@ -39,6 +39,49 @@ def shard_networks(costs: Sequence[float], world: int) -> List[List[int]]:
     return out
 
 
+def shard_network_ranges(costs: Sequence[float], world: int) -> List[Tuple[int, int]]:
+    """Contiguous ranges [lo, hi) of networks, one per rank (empty ones at the end), whose
+    largest total cost is the smallest a contiguous split allows (bisection on that bound,
+    each range filled greedily).  Contiguous ranges keep each network's batch index offset
+    by the range start, so a batch call per range with base stream `stream + lo` gives every
+    network the Philox stream it has in one call over all of them."""
+    if world <= 0:
+        raise ValueError("bad world size")
+    c = [float(x) for x in costs]
+    if any(x < 0 for x in c):
+        raise ValueError("costs must be non-negative")
+    n = len(c)
+
+    def n_ranges(bound):
+        k, s = 1, 0.0
+        for x in c:
+            if s + x > bound:
+                k, s = k + 1, x
+            else:
+                s += x
+        return k
+
+    lo, hi = max(c, default=0.0), sum(c)
+    for _ in range(200):
+        if hi - lo <= 1e-12 * max(hi, 1.0):
+            break
+        mid = 0.5 * (lo + hi)
+        if n_ranges(mid) <= world:
+            hi = mid
+        else:
+            lo = mid
+    ranges, start, s = [], 0, 0.0
+    for i, x in enumerate(c):
+        if s + x > hi and i > start:
+            ranges.append((start, i))
+            start, s = i, 0.0
+        s += x
+    ranges.append((start, n))
+    while len(ranges) < world:
+        ranges.append((n, n))
+    return ranges
+
+
 def moment_sums(X: np.ndarray) -> np.ndarray:
     """Per-column [count, sum, sum of squares] in FP64 for a cells x genes matrix."""
     Xd = np.asarray(X, dtype=np.float64)

@@ -71,3 +71,31 @@ def test_batch_per_network_kinetics(pkg, orc):
     shared = pkg.simulate_gpu_batch(nets, pkg.CLE(dt), kins[0], cell_num=cells, T=T, readout="both", seed=seed,
                                     stream=stream)
     assert np.array_equal(shared[0], outs[0]) and not np.array_equal(shared[1], outs[1])
+
+
+def test_sharded_batch_equals_one_batch(pkg):
+    """simulate_gpu_batch_sharded over two contexts (here both on one GPU; normally one per
+    GPU): whole networks in contiguous ranges, each keeping its Philox stream, so readouts
+    and captured counts equal one simulate_gpu_batch call's bit for bit (populations,
+    per-network kinetics and capture included)."""
+    rng = np.random.default_rng(11)
+    nets, cells, pops, kins = [], [], [], []
+    for b in range(7):
+        G = int(rng.choice([3, 8, 20, 45, 90]))
+        nets.append(pkg.sample_network(G, seed=500 + b, bursty=bool(b % 2)))
+        N = int(rng.integers(40, 300))
+        cells.append(N)
+        pops.append(pkg.PopulationConfig(cell_num=N, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                                         div_check_interval=10) if b % 3 == 0 else None)
+        kins.append(pkg.KineticParams(k_t=3.0 + b, K_d=10.0, n=2.0, mu_m=0.8, mu_p=0.2))
+    cap = pkg.CaptureModel(efficiency=0.3, efficiency_std=0.4, readout="protein")
+    kw = dict(cell_num=cells, T=1.2, readout="both", seed=17, stream=30, populations=pops, capture=cap)
+    want_x, want_c = pkg.simulate_gpu_batch(nets, pkg.CLE(0.01), kins, **kw)
+    ctxs = [pkg.Context(0), pkg.Context(0)]
+    got_x, got_c = pkg.simulate_gpu_batch_sharded(nets, pkg.CLE(0.01), kins, contexts=ctxs, **kw)
+    for c in ctxs:
+        c.close()
+    assert len(got_x) == len(nets)
+    for b in range(len(nets)):
+        assert np.array_equal(got_x[b], want_x[b]), b
+        assert np.array_equal(got_c[b], want_c[b]), b

@@ -78,3 +78,34 @@ def test_shard_helpers(pkg):
     assert sorted(sum(placement, [])) == [0, 1, 2, 3, 4]
     loads = [sum([5, 1, 1, 1, 4][i] for i in pl) for pl in placement]
     assert max(loads) - min(loads) <= 1
+
+
+def _best_contiguous(costs, world):
+    """Smallest largest-range cost over all contiguous splits (exhaustive, small inputs)."""
+    import itertools
+    n = len(costs)
+    if n == 0:
+        return 0.0
+    best = float("inf")
+    for cuts in itertools.combinations(range(1, n), min(world - 1, n - 1)):
+        b = (0,) + cuts + (n,)
+        best = min(best, max(sum(costs[b[i]:b[i + 1]]) for i in range(len(b) - 1)))
+    return best
+
+
+def test_shard_network_ranges(pkg):
+    from scrna_b200 import sharding
+    rng = np.random.default_rng(3)
+    for trial in range(40):
+        n = int(rng.integers(0, 9))
+        world = int(rng.integers(1, 5))
+        costs = [float(x) for x in rng.integers(1, 50, n)]
+        r = sharding.shard_network_ranges(costs, world)
+        assert len(r) == world
+        # contiguous, in order, covering every network once
+        assert r[0][0] == 0 and r[-1][1] == n and all(a[1] == b[0] for a, b in zip(r, r[1:]))
+        assert all(lo <= hi for lo, hi in r)
+        worst = max((sum(costs[lo:hi]) for lo, hi in r), default=0.0)
+        assert worst <= _best_contiguous(costs, world) * (1 + 1e-9) + 1e-9, (costs, world, r)
+    with pytest.raises(ValueError):
+        sharding.shard_network_ranges([1.0], 0)
