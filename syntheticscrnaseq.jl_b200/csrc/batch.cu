@@ -43,11 +43,11 @@ struct BatchNet {
 };
 
 struct GroupKey {
-    int tau, warp, gpl, emax, tmax, nwarps, upt, pop, interval;
+    int tau, warp, gpl, emax, tmax, nwarps, upt, qg, pop, interval;
     int64_t n_steps;
     bool operator<(const GroupKey& r) const {
-        return std::tie(tau, warp, gpl, emax, tmax, nwarps, upt, pop, interval, n_steps) <
-               std::tie(r.tau, r.warp, r.gpl, r.emax, r.tmax, r.nwarps, r.upt, r.pop, r.interval, r.n_steps);
+        return std::tie(tau, warp, gpl, emax, tmax, nwarps, upt, qg, pop, interval, n_steps) <
+               std::tie(r.tau, r.warp, r.gpl, r.emax, r.tmax, r.nwarps, r.upt, r.qg, r.pop, r.interval, r.n_steps);
     }
 };
 
@@ -130,6 +130,9 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
             if (tau) {
                 fill_tau_args(x.net, x.kin, x.pop, &x.o, &x.args);
                 x.kc = choose_kernel(x.net, SCRNA_PATH_BLOCK);
+                x.kc.block = tau_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src,
+                                      tau_genes_per_unit(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, st->N));
+                x.kc.smem = x.kc.block.smem;
             } else if (int r = choose_kernel_tuned(ctx, x.net, x.kin, &x.o, st, &x.kc, &x.args, nullptr)) {
                 return r;
             }
@@ -172,6 +175,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         k.tmax = x->kc.warp ? x->kc.tmax : 0;
         k.nwarps = x->kc.warp ? x->kc.nwarps : 0;
         k.upt = x->kc.warp ? 0 : x->kc.block.upt;
+        k.qg = x->kc.warp ? 0 : x->kc.block.qg;
         k.pop = x->pop != nullptr;
         k.interval = x->pop ? x->pop->div_check_interval : 0;
         k.n_steps = x->pop ? x->n_steps : 0;
@@ -233,7 +237,7 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
         auto launch = [&](int* counter, TileCtl ctl, int use_shared) -> cudaError_t {
             if (k.tau)
                 return tau_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.upt, nw,
-                                        smem, k.pop != 0, grid, ctl, use_shared, g.stream);
+                                        smem, k.pop != 0, grid, ctl, use_shared, k.qg, g.stream);
             if (k.warp)
                 return warpcell_queue_launch(g.args.as<FusedArgs>(), g.items.as<TileWork>(), n_items, counter, k.gpl,
                                              k.emax, k.tmax, k.pop != 0, smem, grid, k.nwarps, ctl, use_shared,

@@ -631,7 +631,14 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
                     "per gene, terms of <= %d sources and <= %d terms per lane", warpcell_max_genes(), kLaneEdges,
                     kLaneSrc, kLaneTerms);
     KernelChoice kc{};
-    if (tau) kc = choose_kernel(net, SCRNA_PATH_BLOCK);  // the tau-leap runs on block tiles
+    if (tau) {  // the tau-leap runs on block tiles, in gene pairs or quads per thread unit
+        kc = choose_kernel(net, SCRNA_PATH_BLOCK);
+        kc.block = tau_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src,
+                            tau_genes_per_unit(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, st->N));
+        kc.smem = kc.block.smem;
+        if (kc.block.smem > 227 * 1024)
+            return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", kc.block.smem);
+    }
     else if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc, nullptr, nullptr, start == 0)) return r;
     if (start > 0 && st->last_cell_major != kc.warp)
         if (int r = state_relayout(ctx, st, kc.warp)) return r;

@@ -199,5 +199,8 @@ int tau_lockstep_default();
 void gene_tables_host(const scrna_net* n, const scrna_kinetics* kin, double dt, GeneRec* gr, GeneInit* gi,
                       uint8_t* qt);
 cudaError_t tau_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt, int nw,
-                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
+                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, int qg,
+                             cudaStream_t st);
+FusedLaunch tau_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int qg);
+int tau_genes_per_unit(int G, int n_reg, int n_in, int n_na, int n_na_src, int64_t N);
 }  // namespace scrna

@@ -1,6 +1,7 @@
 // Launch planning and dispatch of the fused register-path kernel (the kernel
 // template is in cle_fused.cuh; each quads-per-thread variant is compiled in its
 // own translation unit).
+#include <cstdlib>
 #include <type_traits>
 
 #include "cle_internal.h"
@@ -9,7 +10,7 @@
 
 namespace scrna {
 
-template <int UPT, bool POP, bool TAU>
+template <int UPT, bool POP, bool TAU, int QG = 4>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st);
 
 size_t fused_smem_bytes_host(int G, int n_reg, int n_in, int n_na, int n_na_src, int n_quads) {
@@ -55,7 +56,7 @@ template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                     size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
                                     const KeySchedule* ks, cudaStream_t st);
-template <int UPT, bool POP, bool TAU>
+template <int UPT, bool POP, bool TAU, int QG = 4>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st);
 
@@ -144,34 +145,84 @@ cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int
     }
 }
 
-// Binomial tau-leap variant of the block-tile kernel (cle_fused.cuh, TAU).
-cudaError_t tau_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
+// Binomial tau-leap variant of the block-tile kernel (cle_fused.cuh, TAU), in gene quads or
+// gene pairs per thread unit (same counts).  The plan is fused_plan's over units of qg genes.
+FusedLaunch tau_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int qg) {
+    while (qg < 4 && (G + qg - 1) / qg > fused_max_quads()) qg *= 2;  // at most 8 units a thread, 16 warps a block
+    FusedLaunch L = fused_plan(G, n_reg, n_in, n_na, n_na_src, (G + qg - 1) / qg);
+    L.qg = qg;
+    return L;
+}
+
+// Genes per thread unit of the tau-leap for a network of G genes over N cells (every choice gives
+// the same counts; SCRNA_TAU_GENES_PER_THREAD=1, 2 or 4 forces one).  Single genes when they give
+// a tile more warps than pairs do, or the same warps in a launch of at least 4 warps per SM
+// sub-partition; pairs otherwise, where the 4 chains of a pair's lock-step loops hide latency
+// that a launch of few warps cannot.  Measured on a B200 (ms; quads / pairs / single genes):
+// 5 genes x 5,000 cells 8.8 / 5.5 / 3.7; 10 telegraph genes x 20,000 cells 26.1 / 18.1 / 17.7;
+// 100 regulated genes x 20,000 cells 78 / 41 / 39, x 2,000 cells 25 / 8.3 / 9.5.
+int tau_genes_per_unit(int G, int n_reg, int n_in, int n_na, int n_na_src, int64_t N) {
+    if (const char* e = std::getenv("SCRNA_TAU_GENES_PER_THREAD")) {
+        const int q = std::atoi(e);
+        return q == 1 || q == 4 ? q : 2;
+    }
+    const FusedLaunch one = tau_plan(G, n_reg, n_in, n_na, n_na_src, 1);
+    const FusedLaunch two = tau_plan(G, n_reg, n_in, n_na, n_na_src, 2);
+    if (one.qg != 1) return two.qg;  // too many genes for single-gene units
+    if (one.nw > two.nw) return 1;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    const int64_t warps = (N + 31) / 32 * one.nw;
+    return warps >= (int64_t)sms * 4 * 4 ? 1 : 2;
+}
+
+template <int QG>
+static cudaError_t tau_launch_q(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
     switch (L.upt * 2 + (pop ? 1 : 0)) {
-        case 2: return fused_launch_t<1, false, true>(a, L.nw, L.smem, st);
-        case 3: return fused_launch_t<1, true, true>(a, L.nw, L.smem, st);
-        case 4: return fused_launch_t<2, false, true>(a, L.nw, L.smem, st);
-        case 5: return fused_launch_t<2, true, true>(a, L.nw, L.smem, st);
-        case 8: return fused_launch_t<4, false, true>(a, L.nw, L.smem, st);
-        case 9: return fused_launch_t<4, true, true>(a, L.nw, L.smem, st);
-        case 16: return fused_launch_t<8, false, true>(a, L.nw, L.smem, st);
-        case 17: return fused_launch_t<8, true, true>(a, L.nw, L.smem, st);
+        case 2: return fused_launch_t<1, false, true, QG>(a, L.nw, L.smem, st);
+        case 3: return fused_launch_t<1, true, true, QG>(a, L.nw, L.smem, st);
+        case 4: return fused_launch_t<2, false, true, QG>(a, L.nw, L.smem, st);
+        case 5: return fused_launch_t<2, true, true, QG>(a, L.nw, L.smem, st);
+        case 8: return fused_launch_t<4, false, true, QG>(a, L.nw, L.smem, st);
+        case 9: return fused_launch_t<4, true, true, QG>(a, L.nw, L.smem, st);
+        case 16: return fused_launch_t<8, false, true, QG>(a, L.nw, L.smem, st);
+        case 17: return fused_launch_t<8, true, true, QG>(a, L.nw, L.smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t tau_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
+    return L.qg == 1 ? tau_launch_q<1>(a, L, pop, st)
+         : L.qg == 2 ? tau_launch_q<2>(a, L, pop, st)
+                     : tau_launch_q<4>(a, L, pop, st);
+}
+
+template <int QG>
+static cudaError_t tau_queue_launch_q(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
+                                      int upt, int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl,
+                                      int use_shared, cudaStream_t st) {
+    switch (upt * 2 + (pop ? 1 : 0)) {
+        case 2: return fused_queue_launch_t<1, false, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 3: return fused_queue_launch_t<1, true, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 4: return fused_queue_launch_t<2, false, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 5: return fused_queue_launch_t<2, true, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 8: return fused_queue_launch_t<4, false, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 9: return fused_queue_launch_t<4, true, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 16: return fused_queue_launch_t<8, false, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
+        case 17: return fused_queue_launch_t<8, true, true, QG>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t tau_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt, int nw,
-                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    switch (upt * 2 + (pop ? 1 : 0)) {
-        case 2: return fused_queue_launch_t<1, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 3: return fused_queue_launch_t<1, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 4: return fused_queue_launch_t<2, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 5: return fused_queue_launch_t<2, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 8: return fused_queue_launch_t<4, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 9: return fused_queue_launch_t<4, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 16: return fused_queue_launch_t<8, false, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        case 17: return fused_queue_launch_t<8, true, true>(args, items, n_items, counter, nw, smem, grid, shared_ctl, use_shared, st);
-        default: return cudaErrorInvalidValue;
-    }
+                             size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared, int qg,
+                             cudaStream_t st) {
+    if (qg == 1)
+        return tau_queue_launch_q<1>(args, items, n_items, counter, upt, nw, smem, pop, grid, shared_ctl, use_shared, st);
+    if (qg == 2)
+        return tau_queue_launch_q<2>(args, items, n_items, counter, upt, nw, smem, pop, grid, shared_ctl, use_shared, st);
+    return tau_queue_launch_q<4>(args, items, n_items, counter, upt, nw, smem, pop, grid, shared_ctl, use_shared, st);
 }
 
 }  // namespace scrna

@@ -48,9 +48,14 @@ __host__ __device__ inline size_t fused_smem_bytes(int G, int n_reg, int n_in, i
 // instead of the CLE step: one Philox block of four uniforms per (cell, step, gene), integer
 // counts in FP32, Hill activation of the concentration P / V with a population (whose initial
 // counts are max(1, round(steady state x V))) and the concentrations M / V, P / V as readout.
-template <int UPT, bool POP, bool TAU = false>
+// QG: genes per thread unit, 4 (a quad; the CLE), or 4, 2 or 1 for the tau-leap (any grouping:
+// the Philox counters of its draws name genes, and the initial promoter word of gene g is
+// word g mod 4 of its quad's block whatever the grouping).
+template <int UPT, bool POP, bool TAU = false, int QG = 4>
 __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, const TileCtl& ctl,
                                            unsigned char* smem_raw) {
+    static_assert(QG == 4 || (TAU && (QG == 2 || QG == 1)), "the CLE runs gene quads; the tau-leap quads, pairs or single genes");
+    static_assert(UPT * QG <= 32, "one promoter bit per gene of the thread");
     Smem sm;
     {
         unsigned char* p = smem_raw;
@@ -80,10 +85,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     const uint32_t gcell = (uint32_t)(a.cell_offset + cidx);
     const Key key{a.key0, a.key1};
     const int G = a.G;
+    const int n_units = (G + QG - 1) / QG;  // thread units of QG genes (the last one may be partial)
     const bool has_reg = a.n_reg > 0;
 
-    float m[UPT][4], p[UPT][4];
-    int2 ns[UPT][4];            // switching state of each gene (fresh_switch in cle_device.cuh)
+    float m[UPT][QG], p[UPT][QG];
+    int2 ns[UPT][QG];            // switching state of each gene (fresh_switch in cle_device.cuh)
     uint32_t on = 0xFFFFFFFFu;  // bit 4j+i: promoter of gene 4q_j+i is ON
     double V = 0.0;
 
@@ -93,38 +99,38 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int g = 4 * q + i;
-                m[j][i] = (q < a.n_quads && g < G) ? a.ginit[g].m0 : 0.0f;
-                p[j][i] = (q < a.n_quads && g < G) ? a.ginit[g].p0 : 0.0f;
+            for (int i = 0; i < QG; ++i) {
+                const int g = QG * q + i;
+                m[j][i] = (q < n_units && g < G) ? a.ginit[g].m0 : 0.0f;
+                p[j][i] = (q < n_units && g < G) ? a.ginit[g].p0 : 0.0f;
             }
-            if (q < a.n_quads) {
+            if (q < n_units) {
                 bool any = false;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int g = 4 * q + i;
+                for (int i = 0; i < QG; ++i) {
+                    const int g = QG * q + i;
                     any |= (g < G) && a.ginit[g].init_rand;
                 }
                 if (any) {
-                    const uint4 w = philox(gcell, 0u, (uint32_t)q, tagword(TAG_PROMOTER, a.stream), key);
+                    const uint4 w = philox(gcell, 0u, (uint32_t)((QG * q) >> 2), tagword(TAG_PROMOTER, a.stream), key);
                     const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int g = 4 * q + i;
-                        if (g < G && a.ginit[g].init_rand && !(ws[i] < a.ginit[g].thr_init))
-                            on &= ~(1u << (4 * j + i));
+                    for (int i = 0; i < QG; ++i) {
+                        const int g = QG * q + i;
+                        if (g < G && a.ginit[g].init_rand && !(ws[g & 3] < a.ginit[g].thr_init))
+                            on &= ~(1u << (QG * j + i));
                     }
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {  // first waiting times (NaN parameter: gene never switches)
-                const int g = 4 * q + i;
+            for (int i = 0; i < QG; ++i) {  // first waiting times (NaN parameter: gene never switches)
+                const int g = QG * q + i;
                 ns[j][i] = make_int2(kNever, kNever);
-                if (q < a.n_quads && g < G) {
+                if (q < n_units && g < G) {
                     const GeneRec gr = sm.genes[g];
                     if (gr.inv_off == gr.inv_off) {
                         const uint4 w = philox(gcell, 0u, (uint32_t)g, tagword(TAG_SWITCH, a.stream), key);
-                        ns[j][i] = fresh_switch(0, w.x, w.y, (on >> (4 * j + i)) & 1u, gr.inv_on, gr.inv_off);
+                        ns[j][i] = fresh_switch(0, w.x, w.y, (on >> (QG * j + i)) & 1u, gr.inv_on, gr.inv_off);
                     }
                 }
             }
@@ -138,9 +144,9 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
             for (int j = 0; j < UPT; ++j) {
                 const int q = warp + j * NW;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int g = 4 * q + i;
-                    if (!(q < a.n_quads && g < G)) continue;
+                for (int i = 0; i < QG; ++i) {
+                    const int g = QG * q + i;
+                    if (!(q < n_units && g < G)) continue;
                     const double mss = __ddiv_rn(a.beta64[g], a.ss_mu_m);
                     const double pss = __ddiv_rn(__dmul_rn(a.k_t64, mss), a.ss_mu_p);
                     m[j][i] = (float)fmax(1.0, rint(__dmul_rn(mss, V)));
@@ -168,13 +174,13 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int g = 4 * q + i;
-                const bool ok = q < a.n_quads && g < G;
+            for (int i = 0; i < QG; ++i) {
+                const int g = QG * q + i;
+                const bool ok = q < n_units && g < G;
                 m[j][i] = ok ? Ms[(size_t)g * N + src] : 0.0f;
                 p[j][i] = ok ? Ps[(size_t)g * N + src] : 0.0f;
                 ns[j][i] = ok ? Ns[(size_t)g * N + src] : make_int2(kNever, kNever);
-                if (ok && !Os[(size_t)g * N + src]) on &= ~(1u << (4 * j + i));
+                if (ok && !Os[(size_t)g * N + src]) on &= ~(1u << (QG * j + i));
             }
         }
         if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
@@ -213,10 +219,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
 #pragma unroll
             for (int j = 0; j < UPT; ++j) {
                 const int q = warp + j * NW;
-                if (q < a.n_quads) {
+                if (q < n_units) {
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int g = 4 * q + i;
+                    for (int i = 0; i < QG; ++i) {
+                        const int g = QG * q + i;
                         if (g < G) {
                             const int slot = sm.genes[g].slot;
                             if (slot >= 0)
@@ -231,21 +237,21 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
 #pragma unroll
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
-            if (q >= a.n_quads) continue;
-            if (TAU) {
-                // the quad's four genes: telegraph switching (tauleap_binomial.jl:111-121) from the
+            if (q >= n_units) continue;
+            if constexpr (TAU) {
+                // the unit's genes: telegraph switching (tauleap_binomial.jl:111-121) from the
                 // spare bits of each gene's tau-leap words, transcription propensity, then the
-                // draws of the quad (tau_lockstep.cuh)
-                float lam[4];
-                uint4 wt[4];
+                // draws of the unit (tau_lockstep.cuh)
+                float lam[QG];
+                uint4 wt[QG];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int g = 4 * q + i;
+                for (int i = 0; i < QG; ++i) {
+                    const int g = QG * q + i;
                     lam[i] = 0.0f;
                     wt[i] = make_uint4(0u, 0u, 0u, 0u);
                     if (g >= G) continue;
                     wt[i] = philox(gcell, (uint32_t)s, (uint32_t)g, tagword(TAG_TAU, a.stream), key);
-                    const uint32_t bit = 1u << (4 * j + i);
+                    const uint32_t bit = 1u << (QG * j + i);
                     if (s == ns[j][i].x) {
                         on ^= bit;
                         ns[j][i] = switch_at(s, ns[j][i], switch_uniform(wt[i].x, wt[i].y), on & bit,
@@ -256,36 +262,36 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                     if (POP) tx = __fmul_rn(tx, Vf);
                     lam[i] = (on & bit) ? __fmul_rn(tx, dt) : 0.0f;
                 }
-                tau_update_quad(m[j], p[j], lam, wt, min(4, G - 4 * q), a.tau_lockstep != 0, k_t, dt, a.p_dec_m,
-                                a.p_dec_p);
-                continue;
-            }
+                tau_update_unit<QG>(m[j], p[j], lam, wt, min(QG, G - QG * q), a.tau_lockstep != 0, k_t, dt,
+                                    a.p_dec_m, a.p_dec_p);
+            } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {  // gene pairs 2q, 2q+1 of this quad
-                const int g0 = 4 * q + 2 * h;
-                if (g0 >= G) continue;
-                const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h), tagword(TAG_NORMAL, a.stream), key);
+                for (int h = 0; h < 2; ++h) {  // gene pairs 2q, 2q+1 of this quad
+                    const int g0 = 4 * q + 2 * h;
+                    if (g0 >= G) continue;
+                    const uint4 w = philox(gcell, (uint32_t)s, (uint32_t)(2 * q + h), tagword(TAG_NORMAL, a.stream), key);
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int i = 2 * h + k;
-                    const int g = g0 + k;
-                    if (g >= G) continue;
-                    // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
-                    // a gene switches when its waiting time runs out and draws the next one
-                    // from the spare bits of its normal words
-                    if (s == ns[j][i].x) {
-                        const uint32_t bit = 1u << (4 * j + i);
-                        on ^= bit;
-                        const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
-                        ns[j][i] = switch_at(s, ns[j][i], us, on & bit, sm.genes[g].inv_on, sm.genes[g].inv_off);
+                    for (int k = 0; k < 2; ++k) {
+                        const int i = 2 * h + k;
+                        const int g = g0 + k;
+                        if (g >= G) continue;
+                        // telegraph switching before the transcription update (tauleap_binomial.jl:111-121):
+                        // a gene switches when its waiting time runs out and draws the next one
+                        // from the spare bits of its normal words
+                        if (s == ns[j][i].x) {
+                            const uint32_t bit = 1u << (QG * j + i);
+                            on ^= bit;
+                            const float us = k == 0 ? switch_uniform(w.x, w.y) : switch_uniform(w.z, w.w);
+                            ns[j][i] = switch_at(s, ns[j][i], us, on & bit, sm.genes[g].inv_on, sm.genes[g].inv_off);
+                        }
+                        const GeneRec gr = sm.genes[g];
+                        const float reg = regulation(gr, act);
+                        const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
+                        float tx = reg + gr.beta;
+                        if (POP) tx *= Vf;
+                        if (!(on & (1u << (QG * j + i)))) tx = 0.0f;
+                        em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
                     }
-                    const GeneRec gr = sm.genes[g];
-                    const float reg = regulation(gr, act);
-                    const BM bm = k == 0 ? box_muller_parts(w.x, w.y) : box_muller_parts(w.z, w.w);
-                    float tx = reg + gr.beta;
-                    if (POP) tx *= Vf;
-                    if (!(on & (1u << (4 * j + i)))) tx = 0.0f;
-                    em_update(m[j][i], p[j][i], tx, bm, mu_m, mu_p, k_t, dt);
                 }
             }
         }
@@ -319,9 +325,9 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
             for (int j = 0; j < UPT; ++j) {
                 const int q = warp + j * NW;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int g = 4 * q + i;
-                    if (!(live && q < a.n_quads && g < G)) continue;
+                for (int i = 0; i < QG; ++i) {
+                    const int g = QG * q + i;
+                    if (!(live && q < n_units && g < G)) continue;
                     float mm, dm, pm, dp;
                     if (a.partition == 1) {  // halve
                         mm = dm = m[j][i] * 0.5f;
@@ -339,7 +345,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
                     const size_t idx = (size_t)g * N + cidx;
                     a.dM[par][idx] = dm;
                     a.dP[par][idx] = dp;
-                    const uint32_t bon = (on >> (4 * j + i)) & 1u;
+                    const uint32_t bon = (on >> (QG * j + i)) & 1u;
                     a.dprom[par][idx] = bon;
                     // the daughter's promoter switches independently of the mother's
                     int2 dns = make_int2(kNever, kNever);
@@ -360,14 +366,14 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     for (int j = 0; j < UPT; ++j) {
         const int q = warp + j * NW;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int g = 4 * q + i;
-            if (!(q < a.n_quads && g < G)) continue;
+        for (int i = 0; i < QG; ++i) {
+            const int g = QG * q + i;
+            if (!(q < n_units && g < G)) continue;
             const size_t idx = (size_t)g * N + cell;
             if (write_state || ctl.last) {
                 a.M[idx] = m[j][i];
                 a.P[idx] = p[j][i];
-                a.prom[idx] = (on >> (4 * j + i)) & 1u;
+                a.prom[idx] = (on >> (QG * j + i)) & 1u;
                 a.NS[idx] = ns[j][i];
             }
             if (ctl.last && a.out) {
@@ -392,9 +398,9 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
         for (int j = 0; j < UPT; ++j) {
             const int q = warp + j * NW;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int g = 4 * q + i;
-                if (!(q < a.n_quads && g < G)) continue;
+            for (int i = 0; i < QG; ++i) {
+                const int g = QG * q + i;
+                if (!(q < n_units && g < G)) continue;
                 const double x = rint((double)(a.capture_species == 0 ? m[j][i] : p[j][i]));
                 const int64_t n = x > 0.0 ? (int64_t)x : 0;
                 int64_t y = 0;
@@ -405,16 +411,16 @@ __device__ __forceinline__ void fused_tile(const FusedArgs& a, int64_t tile, con
     }
 }
 
-template <int UPT, bool POP, bool TAU = false>
+template <int UPT, bool POP, bool TAU = false, int QG = 4>
 __global__ void __launch_bounds__(UPT <= 2 ? 256 : 512) cle_fused_kernel(const FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const TileCtl ctl{a.step_begin, a.step_end, a.first, a.last, a.check, a.epoch};
-    fused_tile<UPT, POP, TAU>(a, blockIdx.x, ctl, smem_raw);
+    fused_tile<UPT, POP, TAU, QG>(a, blockIdx.x, ctl, smem_raw);
 }
 
 // Persistent form: blocks pull (network, tile, step range) items from a device work queue
 // until it is empty; items of different networks and sizes share one launch.
-template <int UPT, bool POP, bool TAU = false>
+template <int UPT, bool POP, bool TAU = false, int QG = 4>
 __global__ void __launch_bounds__(UPT <= 2 ? 256 : 512)
 cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                        TileCtl shared_ctl, int use_shared) {
@@ -427,14 +433,14 @@ cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items
         __syncthreads();
         if (it >= n_items) return;
         const TileWork w = items[it];
-        fused_tile<UPT, POP, TAU>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
+        fused_tile<UPT, POP, TAU, QG>(args[w.arg], w.tile, use_shared ? shared_ctl : w.ctl, smem_raw);
         __syncthreads();
     }
 }
 
-template <int UPT, bool POP, bool TAU = false>
+template <int UPT, bool POP, bool TAU = false, int QG = 4>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st) {
-    auto k = cle_fused_kernel<UPT, POP, TAU>;
+    auto k = cle_fused_kernel<UPT, POP, TAU, QG>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)((a.N + 31) / 32);
@@ -442,10 +448,10 @@ cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t
     return cudaGetLastError();
 }
 
-template <int UPT, bool POP, bool TAU = false>
+template <int UPT, bool POP, bool TAU = false, int QG = 4>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
-    auto k = cle_fused_queue_kernel<UPT, POP, TAU>;
+    auto k = cle_fused_queue_kernel<UPT, POP, TAU, QG>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, nw * 32, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);

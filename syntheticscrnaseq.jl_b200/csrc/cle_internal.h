@@ -153,9 +153,10 @@ struct KeySchedule {
 // Launch shape of the fused kernel chosen for a network: quads per thread (UPT),
 // warps per block (NW, so 32 cells x NW warps) and dynamic shared memory.
 struct FusedLaunch {
-    int upt;
-    int nw;
+    int upt;     // gene units per thread
+    int nw;      // warps per block
     size_t smem;
+    int qg = 4;  // genes per unit: 4 (the CLE), 4 or 2 (the tau-leap)
 };
 
 // Arguments of the plain FP64 one-kernel-per-step baseline.

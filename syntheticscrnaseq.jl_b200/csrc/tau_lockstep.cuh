@@ -1,19 +1,19 @@
-// Binomial tau-leap update of the genes of one quad, with the Poisson draws either in lock
-// step or one after another.  Each draw is the 50-term inverse CDF of poisson_icdf50 (the
+// Binomial tau-leap update of the genes of one thread unit (a quad or a pair), with the
+// Poisson draws either in lock step or one after another.  Each draw is the 50-term inverse CDF of poisson_icdf50 (the
 // reference's GPU sampler, ext/SyntheticscRNAseqCUDAExt.jl:21-39) with the same operations
 // in the same order, and its quotients lam / k are the correctly rounded ones (small_div.cuh,
 // or IEEE division outside its range), so every count is bit-identical to poisson_icdf50's;
 // only the schedule changes.
 //
 // Lock step: of a gene's four draws, translation needs the new mRNA count and the other three
-// only the state at the start of the step.  The quad's transcription and mRNA-decay draws
+// only the state at the start of the step.  The unit's transcription and mRNA-decay draws
 // share one loop, then its translation and protein-decay draws a second: near the steady
 // state the two draws of a loop have about the same Poisson mean (transcription balances
 // mRNA decay, translation protein decay), so few terms are spent on chains that have stopped.
 // Each chain's count is the last k whose preceding partial sum u exceeds, and a loop ends
 // (checked every second term) when u exceeds no chain's partial sum or after 50 terms.  A
-// loop issues 8 x its longest chain's terms instead of the sum of its chains' terms, in
-// exchange for 8 independent chains in flight.
+// loop issues 2 QG x its longest chain's terms instead of the sum of its chains' terms, in
+// exchange for 2 QG independent chains in flight.
 #pragma once
 
 #include "cle_device.cuh"
@@ -77,17 +77,18 @@ __device__ __forceinline__ void poisson_icdf50_lockstep(const float (&u)[C], con
     }
 }
 
-// One tau-leap step of the first `ng` genes of a quad (tau_update per gene: transcription
-// Poisson(lam_tx), mRNA decay min(Poisson(m p_m), m), translation Poisson(k_t m' dt) with the
-// new m', protein decay min(Poisson(p p_p), p); counts never below 0).  w[i] holds gene i's
-// four words; in lock step a slot without a gene passes u = 0 (no events) and keeps
-// m = p = 0.
-__device__ __forceinline__ void tau_update_quad(float (&m)[4], float (&p)[4], const float (&lam_tx)[4],
-                                                const uint4 (&w)[4], int ng, bool lockstep, float k_t, float dt,
+// One tau-leap step of the first `ng` genes of a unit of QG (4 or 2) genes (tau_update per
+// gene: transcription Poisson(lam_tx), mRNA decay min(Poisson(m p_m), m), translation
+// Poisson(k_t m' dt) with the new m', protein decay min(Poisson(p p_p), p); counts never
+// below 0).  w[i] holds gene i's four words; in lock step a slot without a gene passes u = 0
+// (no events) and keeps m = p = 0.
+template <int QG>
+__device__ __forceinline__ void tau_update_unit(float (&m)[QG], float (&p)[QG], const float (&lam_tx)[QG],
+                                                const uint4 (&w)[QG], int ng, bool lockstep, float k_t, float dt,
                                                 float p_dec_m, float p_dec_p) {
     if (!lockstep) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < QG; ++i) {
             if (i >= ng) break;
             const float n_tx = poisson_icdf50_fast(tau_uniform(w[i].x), lam_tx[i]);
             const float mp = fmaxf(m[i], 0.0f);
@@ -101,20 +102,20 @@ __device__ __forceinline__ void tau_update_quad(float (&m)[4], float (&p)[4], co
         }
         return;
     }
-    // transcription and mRNA decay of the four genes
-    float ua[8], la[8], na[8];
+    // transcription and mRNA decay of the unit's genes
+    float ua[2 * QG], la[2 * QG], na[2 * QG];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < QG; ++i) {
         ua[2 * i] = tau_uniform(w[i].x);
         la[2 * i] = lam_tx[i];
         ua[2 * i + 1] = tau_uniform(w[i].y);
         la[2 * i + 1] = __fmul_rn(fmaxf(m[i], 0.0f), p_dec_m);
     }
-    poisson_icdf50_lockstep<8>(ua, la, na);
+    poisson_icdf50_lockstep<2 * QG>(ua, la, na);
     // translation with the new mRNA counts, and protein decay
-    float ub[8], lb[8], nb[8];
+    float ub[2 * QG], lb[2 * QG], nb[2 * QG];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < QG; ++i) {
         const float n_md = fminf(na[2 * i + 1], fmaxf(m[i], 0.0f));
         m[i] = fmaxf(__fsub_rn(__fadd_rn(m[i], na[2 * i]), n_md), 0.0f);
         ub[2 * i] = tau_uniform(w[i].z);
@@ -122,9 +123,9 @@ __device__ __forceinline__ void tau_update_quad(float (&m)[4], float (&p)[4], co
         ub[2 * i + 1] = tau_uniform(w[i].w);
         lb[2 * i + 1] = __fmul_rn(fmaxf(p[i], 0.0f), p_dec_p);
     }
-    poisson_icdf50_lockstep<8>(ub, lb, nb);
+    poisson_icdf50_lockstep<2 * QG>(ub, lb, nb);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < QG; ++i) {
         const float n_pd = fminf(nb[2 * i + 1], fmaxf(p[i], 0.0f));
         p[i] = fmaxf(__fsub_rn(__fadd_rn(p[i], nb[2 * i]), n_pd), 0.0f);
     }

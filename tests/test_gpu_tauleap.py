@@ -7,9 +7,10 @@ uniforms, so counts, promoter states, volumes and the concentration readout are 
 Regulated networks: the oracle's regulation is FP64 (cle.jl's contraction) and the kernel's
 FP32, so a count can differ where a uniform falls within rounding of a Poisson CDF step;
 fewer than 1 % of the final counts may differ and per-gene means agree within 1 %.
-The kernel draws a gene quad's Poisson counts either in lock step or one after another
-(SCRNA_TAU_LOCKSTEP=1 / 0 forces one; lock step by default): both schedules give
-the same bits, so the bit-exact cases run under each.
+The kernel draws a thread unit's Poisson counts either in lock step or one after another
+(SCRNA_TAU_LOCKSTEP=1 / 0 forces one; lock step by default), for units of gene pairs or
+quads or single genes (SCRNA_TAU_GENES_PER_THREAD=2 / 4 / 1; pairs by default): every combination gives the same
+bits, so the bit-exact cases run under several.
 Statistical pins of the reference: test/test_analytical_moments.jl:85-96 (means within 3 %,
 variance and Fano within 15 % of the exact two-stage moments) and test/test_gpu_parity.jl:32-42.
 """
@@ -32,9 +33,11 @@ def _tau_run(pkg, net, kin, **kw):
     return run
 
 
-@pytest.fixture(params=["0", "1"], ids=["serial", "lockstep"])
+@pytest.fixture(params=[("0", "4"), ("1", "4"), ("1", "2"), ("1", "1")],
+                ids=["serial-quads", "lockstep-quads", "lockstep-pairs", "lockstep-singles"])
 def schedule(request, monkeypatch):
-    monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", request.param)
+    monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", request.param[0])
+    monkeypatch.setenv("SCRNA_TAU_GENES_PER_THREAD", request.param[1])
     return request.param
 
 
@@ -81,19 +84,23 @@ def test_regulated_network_against_oracle(pkg, orc):
         assert np.max(np.abs(mg - mr) / np.maximum(mr, 1.0)) < 0.01, k
 
 
-def test_schedules_equal_on_regulated_network(pkg, monkeypatch):
-    """Lock-step and one-after-another draws: same counts, promoters and volumes, with
-    regulation, telegraph genes and a population (cells beyond several tiles)."""
-    net = pkg.sample_network(23, seed=5, bursty=True)
+@pytest.mark.parametrize("G", [23, 130])
+def test_schedules_equal_on_regulated_network(pkg, monkeypatch, G):
+    """Lock-step and one-after-another draws, gene quads and gene pairs per thread: same
+    counts, promoters and volumes, with regulation, telegraph genes and a population (cells
+    beyond several tiles; 130 genes: several units per thread)."""
+    net = pkg.sample_network(G, seed=5, bursty=True)
     kin = pkg.WORKLOAD_KINETICS
     pop = pkg.PopulationConfig(cell_num=700, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
     outs = []
-    for mode in ("0", "1"):
+    for mode, unit in (("0", "4"), ("1", "4"), ("1", "2"), ("0", "2"), ("1", "1")):
         monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", mode)
+        monkeypatch.setenv("SCRNA_TAU_GENES_PER_THREAD", unit)
         outs.append(_tau_run(pkg, net, kin, cell_num=700, T=0.0, n_steps=250, seed=3, readout="both", dt=0.01,
                              population=pop).read_raw())
-    for k in ("M", "P", "prom", "V"):
-        assert np.array_equal(outs[0][k], outs[1][k]), k
+    for o in outs[1:]:
+        for k in ("M", "P", "prom", "V"):
+            assert np.array_equal(outs[0][k], o[k]), k
 
 
 def test_means_outside_the_quotient_range_bit_exact(pkg, orc, schedule):
