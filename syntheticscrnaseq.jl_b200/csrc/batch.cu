@@ -106,9 +106,11 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
         x.st = st;
         const NetDev& d = x.net->dev;
         const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
-        x.tensor = !tau && !x.pop && (d.n_quads > fused_max_quads() || (x.net->G >= 256 && density >= 0.05));
-        if (tau && d.n_quads > fused_max_quads())
-            return fail(SCRNA_ENOTSUP, "network %d: the binomial tau-leap takes G <= %d", b, 4 * fused_max_quads());
+        // the tau-leap leaves the register path only for networks it cannot hold
+        x.tensor = !x.pop && (d.n_quads > fused_max_quads() || (!tau && x.net->G >= 256 && density >= 0.05));
+        if (tau && x.pop && d.n_quads > fused_max_quads())
+            return fail(SCRNA_ENOTSUP, "network %d: the binomial tau-leap with a population takes G <= %d", b,
+                        4 * fused_max_quads());
         if (!x.tensor) {
             if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
             const int G = x.net->G, nq = (G + 3) / 4;
@@ -154,13 +156,14 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
     for (BatchNet* x : all)
         if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
             if (int r = ensure_gene_tables(x->net, x->kin, x->o.dt, false)) return r;
-            const bool fused = x->net->G <= 4096;
+            const bool fused = !x->tau && x->net->G <= 4096;  // the tau-leap: library-GEMM variant only
             x->st->last_tensor = !fused;
             x->st->last_plain = false;
             x->st->last_pop = false;
+            x->st->last_tau = x->tau;
             x->st->have_counts = cap != nullptr;
             if (int r = fused ? tc_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)
-                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0))
+                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0, x->tau))
                 return r;
         }
     // register-path networks: one persistent launch (or one captured chunk sequence) per group

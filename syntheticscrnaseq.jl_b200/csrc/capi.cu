@@ -42,7 +42,7 @@ cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStrea
 cudaError_t peak_philox_launch(int blocks, int iters, float* sink, cudaStream_t st);
 cudaError_t switch_log2_init_launch(float* tab, uint32_t n, cudaStream_t st);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
-               const scrna_cle_opts* o, scrna_state* st, int dtype);
+               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau);
 }  // namespace scrna
 
 using namespace scrna;
@@ -789,12 +789,12 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
     if (o->cell_offset < 0 || o->cell_offset + N > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
     const bool plain = o->precision == SCRNA_PRECISION_FP64_PLAIN;
     if (tau) {
-        if (o->precision != SCRNA_PRECISION_FP32)
+        if (o->precision != SCRNA_PRECISION_FP32 && o->precision != SCRNA_PRECISION_FP32_F16)
             return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs in FP32 (counts) only");
-        if (o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK)
-            return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs on the block-tile register kernel only");
-        if (net->dev.n_quads > fused_max_quads())
-            return fail(SCRNA_ENOTSUP, "the binomial tau-leap takes G <= %d", 4 * fused_max_quads());
+        if (o->path == SCRNA_PATH_WARP)
+            return fail(SCRNA_ENOTSUP, "the binomial tau-leap runs on the block-tile kernel or the tensor path");
+        if ((o->path == SCRNA_PATH_REGISTER || o->path == SCRNA_PATH_BLOCK) && net->dev.n_quads > fused_max_quads())
+            return fail(SCRNA_ENOTSUP, "the register-path tau-leap takes G <= %d", 4 * fused_max_quads());
     }
     if (plain && pop) return fail(SCRNA_ENOTSUP, "the FP64 baseline path has no population dynamics");
     if (o->precision != SCRNA_PRECISION_FP32 && o->precision != SCRNA_PRECISION_FP32_F16 && !plain)
@@ -804,9 +804,10 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
     // kernel family: tensor cores for large dense networks (or when asked), else the register path
     const NetDev& nd = net->dev;
     const double density = (double)nd.n_in / ((double)net->G * net->G);
-    const bool tensor = !plain && !tau && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
+    // (the tau-leap takes the tensor path only when asked or when the register path cannot hold it)
+    const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
                                    (o->path == SCRNA_PATH_AUTO &&
-                                    (nd.n_quads > fused_max_quads() || (net->G >= 256 && density >= 0.05))));
+                                    (nd.n_quads > fused_max_quads() || (!tau && net->G >= 256 && density >= 0.05))));
     if (tensor) {
         if (pop) return fail(SCRNA_ENOTSUP, "the tensor-core path has no population dynamics");
         st->has_register_state = false;
@@ -814,9 +815,11 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
         st->last_plain = false;
         st->last_pop = false;
         const int dtype = o->precision == SCRNA_PRECISION_FP32_F16 ? 1 : 0;
-        if (o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {  // library-GEMM variant, cell-major state
+        // library-GEMM variant, cell-major state (the tau-leap's only tensor form)
+        if (tau || o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {
             st->last_tensor = true;
-            return tensor_run(ctx, net, kin, cap, o, st, dtype);
+            st->last_tau = tau;
+            return tensor_run(ctx, net, kin, cap, o, st, dtype, tau);
         }
         st->last_tensor = false;  // the fused kernel keeps the register path's gene-major state
         st->last_cell_major = false;

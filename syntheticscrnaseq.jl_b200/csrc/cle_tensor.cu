@@ -23,6 +23,7 @@
 
 #include "capi_internal.h"
 #include "cle_device.cuh"
+#include "tau_lockstep.cuh"
 
 namespace scrna {
 
@@ -55,6 +56,7 @@ struct TensorArgs {
     void* act16;             // [N][Kp]
     const float* act32_cur;  // [n_src][N]: source-major, 32 cells of a warp in one 128-byte row piece
     float* act32_next;
+    float p_dec_m, p_dec_p;  // binomial tau-leap: decay probabilities 1 - exp(-mu dt)
 };
 
 // Initial state (cle.jl:49-53), promoter draws and first activations; thread per (cell, gene).
@@ -275,6 +277,86 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
     }
 }
 
+// One binomial tau-leap step after the GEMM (ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks
+// of any size): the layout of tensor_step_kernel (thread = gene pair for a chunk of cells), the
+// tau-leap's per-gene Philox blocks (tag 9), switching from their spare bits, and the pair's
+// draws in lock step (tau_update_unit, the register path's arithmetic).  With no regulation the
+// GEMM gives exactly 0, so the counts equal the register path's and the oracle's bit for bit.
+template <class T, bool BURSTY, int HN>
+__global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(const TensorArgs a) {
+    using T2 = typename Pair16<T>::type;
+    const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
+    if (k >= (a.ld >> 1)) return;
+    const int g0 = 2 * k;
+    const bool has1 = g0 + 1 < a.G;  // the second gene of the pair exists (else: row padding)
+    const GeneRec r0 = a.genes[g0];
+    const GeneRec r1 = a.genes[has1 ? g0 + 1 : g0];
+    const int src0 = a.src_of_gene[g0];
+    const int src1 = has1 ? a.src_of_gene[g0 + 1] : -1;
+    const uint32_t c3 = tagword(TAG_TAU, a.stream);
+    const int s = a.step;
+    const int64_t c_begin = (int64_t)blockIdx.x * kTensorCellsPerThread;
+    const int64_t c_end = c_begin + kTensorCellsPerThread < a.N ? c_begin + kTensorCellsPerThread : a.N;
+    const size_t rs = (size_t)(a.ld >> 1);  // row stride in pairs
+    const float2* regp = reinterpret_cast<const float2*>(a.reg) + (size_t)c_begin * rs + k;
+    float2* Mp = reinterpret_cast<float2*>(a.M) + (size_t)c_begin * rs + k;
+    float2* Pp = reinterpret_cast<float2*>(a.P) + (size_t)c_begin * rs + k;
+    T2* actp = reinterpret_cast<T2*>(a.act16) + (size_t)c_begin * (a.Kp >> 1) + k;
+    constexpr int CPT = kTensorCellsPerThread;
+    const int nc = (int)(c_end - c_begin);
+    float2 rg[CPT], mm[CPT], pp[CPT];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+        if (i < nc) {
+            rg[i] = regp[i * rs];
+            mm[i] = Mp[i * rs];
+            pp[i] = Pp[i * rs];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+        if (i >= nc) break;
+        const int64_t c = c_begin + i;
+        const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+        uint4 w[2];
+        w[0] = philox_rk(gcell, (uint32_t)s, (uint32_t)g0, c3, a.rk0, a.rk1);
+        w[1] = has1 ? philox_rk(gcell, (uint32_t)s, (uint32_t)(g0 + 1), c3, a.rk0, a.rk1) : make_uint4(0u, 0u, 0u, 0u);
+        const float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg[i].x, r0.cneg), r0.beta), 0.0f);
+        const float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg[i].y, r1.cneg), r1.beta), 0.0f);
+        bool on0 = true, on1 = true;
+        if (BURSTY) {  // switching before the transcription update (tauleap_binomial.jl:111-121)
+            const size_t e = (size_t)c * a.ld + g0;
+            const uchar2 on = *reinterpret_cast<const uchar2*>(a.prom + e);
+            const int4 sw = *reinterpret_cast<const int4*>(a.NS + e);
+            on0 = on.x;
+            on1 = on.y;
+            if (s == sw.x) {
+                on0 = !on0;
+                a.NS[e] = switch_at(s, make_int2(sw.x, sw.y), switch_uniform(w[0].x, w[0].y), on0, r0.inv_on, r0.inv_off);
+                a.prom[e] = on0;
+            }
+            if (has1 && s == sw.z) {
+                on1 = !on1;
+                a.NS[e + 1] = switch_at(s, make_int2(sw.z, sw.w), switch_uniform(w[1].x, w[1].y), on1, r1.inv_on, r1.inv_off);
+                a.prom[e + 1] = on1;
+            }
+        }
+        const float lam[2] = {on0 ? __fmul_rn(tx0, a.dt) : 0.0f, (has1 && on1) ? __fmul_rn(tx1, a.dt) : 0.0f};
+        // the padding slot of an odd G holds no state (never initialised): counts 0
+        float m2[2] = {mm[i].x, has1 ? mm[i].y : 0.0f}, p2[2] = {pp[i].x, has1 ? pp[i].y : 0.0f};
+        tau_update_unit<2>(m2, p2, lam, w, has1 ? 2 : 1, true, a.k_t, a.dt, a.p_dec_m, a.p_dec_p);
+        Mp[i * rs] = make_float2(m2[0], m2[1]);
+        Pp[i * rs] = make_float2(p2[0], p2[1]);
+        const float a0 = tensor_hill<HN>(p2[0], a), a1 = tensor_hill<HN>(p2[1], a);
+        T2 act;
+        act.x = to16<T>(a0);
+        act.y = to16<T>(has1 ? a1 : 0.0f);  // the padding column of the activations stays 0
+        actp[(size_t)i * (a.Kp >> 1)] = act;
+        if (src0 >= 0) a.act32_next[(size_t)src0 * a.N + c] = a0;
+        if (src1 >= 0) a.act32_next[(size_t)src1 * a.N + c] = a1;
+    }
+}
+
 // Readout: cell-major FP32 state -> cells x G (x2) column-major Float64, through a
 // shared-memory tile so both the reads and the writes are coalesced.
 __global__ void tensor_readout_kernel(int G, int ld, int64_t N, const float* M, const float* P, int readout,
@@ -425,7 +507,7 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
 int64_t run_steps(const scrna_cle_opts* o);
 
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
-               const scrna_cle_opts* o, scrna_state* st, int dtype) {
+               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau) {
     if (int r = tensor_prepare_net(n, dtype)) return r;
     const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, ld = tensor_ld(G);
     const int64_t N = st->N;
@@ -454,6 +536,8 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.mu_m = (float)(kin->mu_m + kin->dilution);
     a.mu_p = (float)(kin->mu_p + kin->dilution);
     a.dt = (float)o->dt;
+    a.p_dec_m = (float)(1.0 - std::exp(-(kin->mu_m + kin->dilution) * o->dt));  // as fill_tau_args without population
+    a.p_dec_p = (float)(1.0 - std::exp(-(kin->mu_p + kin->dilution) * o->dt));
     a.key0 = (uint32_t)o->seed; a.key1 = (uint32_t)(o->seed >> 32); a.stream = o->stream & 0xFFFFFFu;
     for (int r = 0; r < 10; ++r) {
         a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
@@ -489,6 +573,14 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
                                      : (h2 ? tensor_step_kernel<__nv_bfloat16, false, 2> : tensor_step_kernel<__nv_bfloat16, false, 0>);
     else step_fn = bursty ? (h2 ? tensor_step_kernel<__half, true, 2> : tensor_step_kernel<__half, true, 0>)
                           : (h2 ? tensor_step_kernel<__half, false, 2> : tensor_step_kernel<__half, false, 0>);
+    if (tau) {
+        if (dtype == 0)
+            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__nv_bfloat16, true, 2> : tensor_tau_step_kernel<__nv_bfloat16, true, 0>)
+                             : (h2 ? tensor_tau_step_kernel<__nv_bfloat16, false, 2> : tensor_tau_step_kernel<__nv_bfloat16, false, 0>);
+        else
+            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2> : tensor_tau_step_kernel<__half, true, 0>)
+                             : (h2 ? tensor_tau_step_kernel<__half, false, 2> : tensor_tau_step_kernel<__half, false, 0>);
+    }
     const dim3 g_step((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
                       (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
     if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");

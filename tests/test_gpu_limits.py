@@ -2,7 +2,7 @@
 (512 genes = 128 gene quads; the lane kernel's limit too), the binomial tau-leap's, and the
 fused tensor-core kernel's (4,096 genes, its epilogue gene table in shared memory), plus the
 sizes just beyond them: rejected on the register path, routed to the library-GEMM variant
-on the tensor path.  Tolerances as in the parity tests (2e-3 relative against the FP64
+on the tensor path (the tau-leap included).  Tolerances as in the parity tests (2e-3 relative against the FP64
 oracle on the same increments; bit-exact for the unregulated tau-leap; the 16-bit
 contraction's rounding between the two tensor variants)."""
 import numpy as np
@@ -44,8 +44,63 @@ def test_register_path_rejects_513_genes(pkg):
     for path in ("register", "warp", "block"):
         with pytest.raises(pkg.ScrnaError):
             pkg.simulate(net, pkg.CLE(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1, path=path)
+    for path in ("register", "block", "warp"):
+        with pytest.raises(pkg.ScrnaError):
+            pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1, path=path)
+    # a population at that size has no tensor form
+    pop = pkg.PopulationConfig(cell_num=8, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
     with pytest.raises(pkg.ScrnaError):
-        pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1)
+        pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, population=pop, T=0.1)
+
+
+def _unregulated(pkg, G, seed):
+    rng = np.random.default_rng(seed)
+    return pkg.GeneNetwork(G, np.exp(rng.uniform(0.0, np.log(10.0), G)), np.zeros((G, G)),
+                           k_on=np.exp(rng.uniform(np.log(0.1), np.log(1.0), G)),
+                           k_off=np.exp(rng.uniform(np.log(1.0), np.log(10.0), G)))
+
+
+@pytest.mark.parametrize("G", [601, 1200])
+def test_tauleap_beyond_the_register_path_bit_exact(pkg, orc, G):
+    """G > 512: the tau-leap runs on the tensor path's library-GEMM variant (ext:215-399 takes any
+    G).  Without regulation the GEMM gives exactly 0, so counts and promoters equal the oracle's."""
+    net = _unregulated(pkg, G, seed=G)
+    kin = pkg.KineticParams(k_t=3.0, K_d=10.0, n=2.0, mu_m=0.7, mu_p=0.3)
+    N, steps = 48, 60
+    got = _raw(pkg, net, pkg.BinomialTauLeap(0.05), kin, N=N, steps=steps, seed=8)
+    ref = orc.simulate(net, kin, dt=0.05, cell_num=N, n_steps=steps, seed=8, tauleap=True)
+    for k in ("M", "P", "prom"):
+        assert np.array_equal(got[k], ref[k]), k
+
+
+def test_tauleap_tensor_path_matches_register_path(pkg):
+    """A regulated 300-gene network on both tau-leap forms: the same uniforms, regulation in FP32
+    (register) or from a BF16 contraction (tensor), so a count can move where a uniform falls
+    within rounding of a Poisson CDF step; promoters are exact, counts agree almost everywhere
+    and per-gene means within 1 %."""
+    net = pkg.sample_network(300, seed=9, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    a = _raw(pkg, net, pkg.BinomialTauLeap(0.01), kin, N=500, steps=200, seed=4, path="register")
+    b = _raw(pkg, net, pkg.BinomialTauLeap(0.01), kin, N=500, steps=200, seed=4, path="tensor")
+    assert np.array_equal(a["prom"], b["prom"])
+    for k in ("M", "P"):
+        assert np.mean(a[k] != b[k]) < 0.05, k
+        ma, mb = a[k].mean(1), b[k].mean(1)
+        assert np.max(np.abs(ma - mb) / np.maximum(ma, 1.0)) < 0.01, k
+
+
+def test_tauleap_batch_with_a_network_beyond_the_register_path(pkg, orc):
+    nets = [_unregulated(pkg, 7, 1), _unregulated(pkg, 700, 2), _unregulated(pkg, 30, 3)]
+    kin = pkg.KineticParams(k_t=2.0, K_d=10.0, n=2.0, mu_m=0.6, mu_p=0.2)
+    cells = [100, 40, 70]
+    outs = pkg.simulate_gpu_batch(nets, pkg.BinomialTauLeap(0.05), kin, cell_num=cells, T=2.0, readout="both",
+                                  seed=3, stream=11)
+    for b, net in enumerate(nets):
+        single = pkg.simulate(net, pkg.BinomialTauLeap(0.05), kin, cell_num=cells[b], T=2.0, readout="both", seed=3,
+                              stream=11 + b)
+        assert np.array_equal(outs[b], single), b
+        r = orc.simulate(net, kin, dt=0.05, T=2.0, cell_num=cells[b], seed=3, stream=11 + b, tauleap=True)
+        assert np.array_equal(outs[b], np.hstack([r["M"].T, r["P"].T])), b
 
 
 def test_tauleap_at_512_genes_bit_exact(pkg, orc):

@@ -180,5 +180,11 @@ def test_tauleap_capture_and_validation(pkg, orc):
                                   seed=12, capture=cap)
     want = orc.capture_counts(np.ascontiguousarray(X.T), eff, seed=12)
     assert np.array_equal(counts.T, want)
-    with pytest.raises(pkg.ScrnaError):
-        pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=10, T=1.0, path="tensor")
+    with pytest.raises(pkg.ScrnaError):  # the lane kernel has no tau-leap form
+        pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=10, T=1.0, path="warp")
+    # the tensor path's tau-leap (the library-GEMM variant under either name): with no regulation
+    # its counts, capture included, equal the register path's
+    for path in ("tensor", "tensor_library"):
+        Xt, ct, et = pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=400, T=3.0, readout="protein",
+                                  seed=12, capture=cap, path=path)
+        assert np.array_equal(Xt, X) and np.array_equal(ct, counts) and np.array_equal(et, eff), path
