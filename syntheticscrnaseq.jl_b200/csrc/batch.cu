@@ -106,11 +106,8 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
         x.st = st;
         const NetDev& d = x.net->dev;
         const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
-        // the tau-leap leaves the register path only for networks it cannot hold
-        x.tensor = !x.pop && (d.n_quads > fused_max_quads() || (!tau && x.net->G >= 256 && density >= 0.05));
-        if (tau && x.pop && d.n_quads > fused_max_quads())
-            return fail(SCRNA_ENOTSUP, "network %d: the binomial tau-leap with a population takes G <= %d", b,
-                        4 * fused_max_quads());
+        // the tau-leap and populations leave the register path only for networks it cannot hold
+        x.tensor = d.n_quads > fused_max_quads() || (!tau && !x.pop && x.net->G >= 256 && density >= 0.05);
         if (!x.tensor) {
             if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
             const int G = x.net->G, nq = (G + 3) / 4;
@@ -155,15 +152,16 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
     // dense networks: tensor-core path, one after another on the context stream
     for (BatchNet* x : all)
         if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
-            if (int r = ensure_gene_tables(x->net, x->kin, x->o.dt, false)) return r;
-            const bool fused = !x->tau && x->net->G <= 4096;  // the tau-leap: library-GEMM variant only
+            if (int r = ensure_gene_tables(x->net, x->kin, x->o.dt, x->pop != nullptr)) return r;
+            // the tau-leap and populations: library-GEMM variant only
+            const bool fused = !x->tau && !x->pop && x->net->G <= 4096;
             x->st->last_tensor = !fused;
             x->st->last_plain = false;
-            x->st->last_pop = false;
+            x->st->last_pop = x->pop != nullptr;
             x->st->last_tau = x->tau;
             x->st->have_counts = cap != nullptr;
             if (int r = fused ? tc_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)
-                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0, x->tau))
+                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0, x->tau, x->pop))
                 return r;
         }
     // register-path networks: one persistent launch (or one captured chunk sequence) per group

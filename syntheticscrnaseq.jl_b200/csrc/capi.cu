@@ -42,7 +42,8 @@ cudaError_t peak_launch(int which, int blocks, int iters, float* sink, cudaStrea
 cudaError_t peak_philox_launch(int blocks, int iters, float* sink, cudaStream_t st);
 cudaError_t switch_log2_init_launch(float* tab, uint32_t n, cudaStream_t st);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
-               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau);
+               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau,
+               const scrna_population* pop);
 }  // namespace scrna
 
 using namespace scrna;
@@ -807,19 +808,19 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
     // (the tau-leap takes the tensor path only when asked or when the register path cannot hold it)
     const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
                                    (o->path == SCRNA_PATH_AUTO &&
-                                    (nd.n_quads > fused_max_quads() || (!tau && net->G >= 256 && density >= 0.05))));
+                                    (nd.n_quads > fused_max_quads() ||
+                                     (!tau && !pop && net->G >= 256 && density >= 0.05))));
     if (tensor) {
-        if (pop) return fail(SCRNA_ENOTSUP, "the tensor-core path has no population dynamics");
         st->has_register_state = false;
         st->have_counts = cap != nullptr;
         st->last_plain = false;
-        st->last_pop = false;
+        st->last_pop = pop != nullptr;
         const int dtype = o->precision == SCRNA_PRECISION_FP32_F16 ? 1 : 0;
-        // library-GEMM variant, cell-major state (the tau-leap's only tensor form)
-        if (tau || o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {
+        // library-GEMM variant, cell-major state (the only tensor form of the tau-leap and of populations)
+        if (tau || pop || o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {
             st->last_tensor = true;
             st->last_tau = tau;
-            return tensor_run(ctx, net, kin, cap, o, st, dtype, tau);
+            return tensor_run(ctx, net, kin, cap, o, st, dtype, tau, pop);
         }
         st->last_tensor = false;  // the fused kernel keeps the register path's gene-major state
         st->last_cell_major = false;
@@ -881,6 +882,10 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
         CU(cudaMemcpyAsync(tm.data(), st->tM.p, ln * 4, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(tp.data(), st->tP.p, ln * 4, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(tpr.data(), st->tprom.p, ln, cudaMemcpyDeviceToHost, ctx->stream));
+        if (volume) {
+            if (!st->last_pop) return fail(SCRNA_EINVAL, "the last run had no population");
+            CU(cudaMemcpyAsync(volume, st->V.p, (size_t)st->N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
         CU(cudaStreamSynchronize(ctx->stream));
         for (int64_t c = 0; c < st->N; ++c)
             for (int g = 0; g < st->G; ++g) {
@@ -889,7 +894,6 @@ extern "C" int scrna_state_read_raw(scrna_ctx* ctx, scrna_state* st, void* mrna,
                 if (protein) static_cast<float*>(protein)[dst] = tp[src];
                 if (promoter) promoter[dst] = tpr[src];
             }
-        if (volume) return fail(SCRNA_EINVAL, "the last run had no population");
         return SCRNA_OK;
     }
     if (st->last_cell_major) {  // lane-kernel state [N][G]: transpose to [G][N] on the host

@@ -188,7 +188,8 @@ cudaError_t tensor_terms_launch(int dtype, int64_t N, int G, int Kp, int n_terms
 int tc_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
            const scrna_cle_opts* o, scrna_state* st, int dtype);
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
-               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau = false);
+               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau = false,
+               const scrna_population* pop = nullptr);
 int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, const scrna_kinetics* kins,
                    int32_t n_kins, const int64_t* cell_nums, const scrna_population* const* pops,
                    const scrna_capture* cap, const scrna_cle_opts* opts, double* const* outs,

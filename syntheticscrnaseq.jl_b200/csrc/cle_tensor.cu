@@ -57,6 +57,20 @@ struct TensorArgs {
     const float* act32_cur;  // [n_src][N]: source-major, 32 cells of a warp in one 128-byte row piece
     float* act32_next;
     float p_dec_m, p_dec_p;  // binomial tau-leap: decay probabilities 1 - exp(-mu dt)
+    // population (cle.jl:143-284, ext:409-529, tau-leap ext:531-663); V == nullptr without one.
+    // The daughter buffers are cell-major [N][ld] like the state.
+    double* V;               // [N] volume at the start of the step
+    double growth_factor, V_div, V_lo, V_hi;
+    int32_t partition, exclude_mother, tau, epoch;  // tau: Hill of P / V, counts from steady state x V
+    unsigned long long* owner;  // [N] epoch << 32 | donor cell of the last claim
+    uint8_t* divided;        // [N] the cell divided at this check
+    float* dM;
+    float* dP;
+    uint8_t* dprom;
+    int2* dNS;
+    double* dV;              // [N] the daughter's volume
+    const double* beta64;    // tau-leap initial counts max(1, round(steady state x V)) (ext:560-566)
+    double ss_mu_m, ss_mu_p, k_t64;
 };
 
 // Initial state (cle.jl:49-53), promoter draws and first activations; thread per (cell, gene).
@@ -71,8 +85,20 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
     const GeneInit gi = a.ginit[g];
     const int64_t sidx = c * a.ld + g;  // state index
     const GeneRec gr = a.genes[g];
-    const float p0 = gi.p0;
-    a.M[sidx] = gi.m0;
+    float m0 = gi.m0, p0 = gi.p0;
+    double V = 1.0;
+    if (a.V) {  // the cell's birth volume (TAG_VOLUME), as the register path draws it
+        const uint4 w = philox(gcell, 0u, 0u, tagword(TAG_VOLUME, a.stream), key);
+        V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
+        if (g == 0) a.V[c] = V;
+        if (a.tau) {
+            const double mss = __ddiv_rn(a.beta64[g], a.ss_mu_m);
+            const double pss = __ddiv_rn(__dmul_rn(a.k_t64, mss), a.ss_mu_p);
+            m0 = (float)fmax(1.0, rint(__dmul_rn(mss, V)));
+            p0 = (float)fmax(1.0, rint(__dmul_rn(pss, V)));
+        }
+    }
+    a.M[sidx] = m0;
     a.P[sidx] = p0;
     bool on = true;
     if (gi.init_rand) {
@@ -87,7 +113,7 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
         ns = fresh_switch(0, w.x, w.y, on, gr.inv_on, gr.inv_off);
     }
     a.NS[sidx] = ns;
-    const float act = hill_act(p0, a.Kn, a.hill_n, a.hill_int);
+    const float act = hill_act(a.V && a.tau ? __fdiv_rn(p0, (float)V) : p0, a.Kn, a.hill_n, a.hill_int);
     reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
     const int src = a.src_of_gene[g];
     if (src >= 0) a.act32_next[(size_t)src * a.N + c] = act;
@@ -244,6 +270,11 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
         const uint32_t gcell = (uint32_t)(a.cell_offset + c);
         const uint4 w = philox_rk(gcell, (uint32_t)s, (uint32_t)k, c3, a.rk0, a.rk1);
         float tx0 = (rg[i].x + r0.cneg) + r0.beta, tx1 = (rg[i].y + r1.cneg) + r1.beta;
+        if (a.V) {  // population: transcription x V (cle.jl:200-214)
+            const float Vf = (float)a.V[c];
+            tx0 *= Vf;
+            tx1 *= Vf;
+        }
         if (BURSTY) {
             const size_t e = (size_t)c * a.ld + g0;
             const uchar2 on = *reinterpret_cast<const uchar2*>(a.prom + e);
@@ -321,8 +352,15 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(c
         uint4 w[2];
         w[0] = philox_rk(gcell, (uint32_t)s, (uint32_t)g0, c3, a.rk0, a.rk1);
         w[1] = has1 ? philox_rk(gcell, (uint32_t)s, (uint32_t)(g0 + 1), c3, a.rk0, a.rk1) : make_uint4(0u, 0u, 0u, 0u);
-        const float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg[i].x, r0.cneg), r0.beta), 0.0f);
-        const float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg[i].y, r1.cneg), r1.beta), 0.0f);
+        float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg[i].x, r0.cneg), r0.beta), 0.0f);
+        float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg[i].y, r1.cneg), r1.beta), 0.0f);
+        float Vn = 1.0f;  // the volume at the start of the next step (Hill of P / V)
+        if (a.V) {
+            const double V = a.V[c];
+            tx0 = __fmul_rn(tx0, (float)V);
+            tx1 = __fmul_rn(tx1, (float)V);
+            Vn = (float)__dmul_rn(V, a.growth_factor);
+        }
         bool on0 = true, on1 = true;
         if (BURSTY) {  // switching before the transcription update (tauleap_binomial.jl:111-121)
             const size_t e = (size_t)c * a.ld + g0;
@@ -347,7 +385,8 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(c
         tau_update_unit<2>(m2, p2, lam, w, has1 ? 2 : 1, true, a.k_t, a.dt, a.p_dec_m, a.p_dec_p);
         Mp[i * rs] = make_float2(m2[0], m2[1]);
         Pp[i * rs] = make_float2(p2[0], p2[1]);
-        const float a0 = tensor_hill<HN>(p2[0], a), a1 = tensor_hill<HN>(p2[1], a);
+        const float a0 = tensor_hill<HN>(a.V ? __fdiv_rn(p2[0], Vn) : p2[0], a);
+        const float a1 = tensor_hill<HN>(a.V ? __fdiv_rn(p2[1], Vn) : p2[1], a);
         T2 act;
         act.x = to16<T>(a0);
         act.y = to16<T>(has1 ? a1 : 0.0f);  // the padding column of the activations stays 0
@@ -357,10 +396,118 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(c
     }
 }
 
+// ---- population on the tensor path: growth, division checks, Moran replacement ---------------
+// The register path's semantics (cle_fused.cuh epilogue, cle.jl:240-273): after each step
+// V <- V growth_factor; at a check step a cell with V > V_div halves V, partitions each gene's
+// counts (halved, or a binomial split of the rounded counts) into itself and a daughter, and the
+// daughter replaces a Moran slot drawn from (cell, step); of several claims on one slot the
+// largest donor index wins.  The daughter keeps the mother's promoters and draws fresh waiting
+// times.  Three kernels per check: decide and claim (per cell), partition (per cell x gene),
+// place daughters and refresh the next step's activations of every changed cell.
+
+__global__ void tensor_growth_kernel(double* V, int64_t N, double growth_factor) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < N) V[c] = __dmul_rn(V[c], growth_factor);
+}
+
+__global__ void tensor_divide_kernel(const TensorArgs a) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    double V = a.V[c];
+    if (!(V > a.V_div)) {
+        a.divided[c] = 0;
+        return;
+    }
+    V = V * 0.5;
+    a.V[c] = V;
+    a.dV[c] = V;
+    a.divided[c] = 1;
+    const Key key{a.key0, a.key1};
+    const uint4 w = philox((uint32_t)(a.cell_offset + c), (uint32_t)a.step, 0u, tagword(TAG_MORAN, a.stream), key);
+    int64_t r;
+    if (a.exclude_mother) {
+        r = (int64_t)(((uint64_t)w.x * (uint64_t)(a.N - 1)) >> 32);
+        if (r >= c) r += 1;
+    } else {
+        r = (int64_t)(((uint64_t)w.x * (uint64_t)a.N) >> 32);
+    }
+    atomicMax(&a.owner[r], ((unsigned long long)(uint32_t)(a.epoch + 1) << 32) | (unsigned long long)c);
+}
+
+__global__ void tensor_partition_kernel(const TensorArgs a) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.N * a.G) return;
+    const int64_t c = idx / a.G;
+    const int g = (int)(idx - c * a.G);
+    if (!a.divided[c]) return;
+    const size_t e = (size_t)c * a.ld + g;
+    const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+    const Key key{a.key0, a.key1};
+    const float m = a.M[e], p = a.P[e];
+    float mm, dm, pm, dp;
+    if (a.partition == 1) {  // halve
+        mm = dm = m * 0.5f;
+        pm = dp = p * 0.5f;
+    } else {  // binomial split of rounded counts
+        const int64_t mi = (int64_t)rintf(m);
+        const int64_t pi = (int64_t)rintf(p);
+        const int64_t mk = binomial_half(mi, key, a.stream, gcell, (uint32_t)a.step, (uint32_t)g, 0u);
+        const int64_t pk = binomial_half(pi, key, a.stream, gcell, (uint32_t)a.step, (uint32_t)g, 1u);
+        mm = (float)mk; dm = (float)(mi - mk);
+        pm = (float)pk; dp = (float)(pi - pk);
+    }
+    a.M[e] = mm;
+    a.P[e] = pm;
+    a.dM[e] = dm;
+    a.dP[e] = dp;
+    const uint8_t bon = a.prom[e];
+    a.dprom[e] = bon;
+    int2 dns = make_int2(kNever, kNever);
+    const GeneRec gr = a.genes[g];
+    if (gr.inv_off == gr.inv_off) {  // the daughter's promoter switches independently of the mother's
+        const uint4 w = philox(gcell, (uint32_t)a.step, (uint32_t)g | kDaughterSwitch, tagword(TAG_SWITCH, a.stream), key);
+        dns = fresh_switch(a.step, w.x, w.y, bon, gr.inv_on, gr.inv_off);
+    }
+    a.dNS[e] = dns;
+}
+
+template <class T, int HN>
+__global__ void tensor_replace_kernel(const TensorArgs a) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.N * a.G) return;
+    const int64_t c = idx / a.G;
+    const int g = (int)(idx - c * a.G);
+    const unsigned long long o = a.owner[c];
+    const bool replaced = (uint32_t)(o >> 32) == (uint32_t)(a.epoch + 1);
+    if (!replaced && !a.divided[c]) return;
+    const size_t e = (size_t)c * a.ld + g;
+    float p;
+    double V;
+    if (replaced) {  // the donor's daughter takes this slot
+        const int64_t src = (int64_t)(o & 0xFFFFFFFFull);
+        const size_t es = (size_t)src * a.ld + g;
+        a.M[e] = a.dM[es];
+        p = a.dP[es];
+        a.P[e] = p;
+        a.prom[e] = a.dprom[es];
+        a.NS[e] = a.dNS[es];
+        V = a.dV[src];
+        if (g == 0) a.V[c] = V;
+    } else {  // a mother that kept its slot: its halved counts
+        p = a.P[e];
+        V = a.V[c];
+    }
+    const float act = tensor_hill<HN>(a.tau ? __fdiv_rn(p, (float)V) : p, a);
+    reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
+    const int src_idx = a.src_of_gene[g];
+    if (src_idx >= 0) a.act32_next[(size_t)src_idx * a.N + c] = act;
+}
+
 // Readout: cell-major FP32 state -> cells x G (x2) column-major Float64, through a
 // shared-memory tile so both the reads and the writes are coalesced.
+// With V (a tau-leap population) the readout is the concentrations M / V, P / V (ext:654-661).
 __global__ void tensor_readout_kernel(int G, int ld, int64_t N, const float* M, const float* P, int readout,
-                                      double* out) {
+                                      double* out, const double* V) {
     __shared__ float tile[2][32][33];
     const int64_t c0 = (int64_t)blockIdx.x * 32;
     const int g0 = blockIdx.y * 32;
@@ -376,7 +523,11 @@ __global__ void tensor_readout_kernel(int G, int ld, int64_t N, const float* M, 
         const int g = g0 + r;
         const int64_t c = c0 + threadIdx.x;
         if (g >= G || c >= N) continue;
-        const float mv = tile[0][threadIdx.x][r], pv = tile[1][threadIdx.x][r];
+        double mv = tile[0][threadIdx.x][r], pv = tile[1][threadIdx.x][r];
+        if (V) {
+            mv = __ddiv_rn(mv, V[c]);
+            pv = __ddiv_rn(pv, V[c]);
+        }
         if (readout == 0) out[(size_t)g * N + c] = mv;
         else if (readout == 1) out[(size_t)g * N + c] = pv;
         else { out[(size_t)g * N + c] = mv; out[(size_t)(G + g) * N + c] = pv; }
@@ -507,7 +658,7 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
 int64_t run_steps(const scrna_cle_opts* o);
 
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
-               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau) {
+               const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau, const scrna_population* pop) {
     if (int r = tensor_prepare_net(n, dtype)) return r;
     const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, ld = tensor_ld(G);
     const int64_t N = st->N;
@@ -533,11 +684,14 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.Kn = (float)std::pow(kin->K_d, kin->n);
     a.hill_n = (float)kin->n;
     a.hill_int = (kin->n == std::floor(kin->n) && kin->n >= 1.0 && kin->n <= 16.0) ? (int)kin->n : 0;
-    a.mu_m = (float)(kin->mu_m + kin->dilution);
-    a.mu_p = (float)(kin->mu_p + kin->dilution);
+    // decay: intrinsic rates with a population (dilution is then the growth), else with dilution
+    const double mu_m = pop ? kin->mu_m : kin->mu_m + kin->dilution;
+    const double mu_p = pop ? kin->mu_p : kin->mu_p + kin->dilution;
+    a.mu_m = (float)mu_m;
+    a.mu_p = (float)mu_p;
     a.dt = (float)o->dt;
-    a.p_dec_m = (float)(1.0 - std::exp(-(kin->mu_m + kin->dilution) * o->dt));  // as fill_tau_args without population
-    a.p_dec_p = (float)(1.0 - std::exp(-(kin->mu_p + kin->dilution) * o->dt));
+    a.p_dec_m = (float)(1.0 - std::exp(-mu_m * o->dt));  // as fill_tau_args
+    a.p_dec_p = (float)(1.0 - std::exp(-mu_p * o->dt));
     a.key0 = (uint32_t)o->seed; a.key1 = (uint32_t)(o->seed >> 32); a.stream = o->stream & 0xFFFFFFu;
     for (int r = 0; r < 10; ++r) {
         a.rk0[r] = a.key0 + (uint32_t)r * 0x9E3779B9u;
@@ -555,6 +709,32 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.act16 = st->tact16.p;
     a.act32_cur = st->tact32[1].as<float>();
     a.act32_next = st->tact32[0].as<float>();
+    if (pop) {  // population buffers (the register path's, as cell-major arrays)
+        CU(st->V.ensure((size_t)N * 8));
+        CU(st->dV[0].ensure((size_t)N * 8));
+        CU(st->owner[0].ensure((size_t)N * 8));
+        CU(st->dprom[1].ensure((size_t)N));  // division flags
+        CU(st->dM[0].ensure(ln * 4));
+        CU(st->dP[0].ensure(ln * 4));
+        CU(st->dprom[0].ensure(ln));
+        CU(st->dNS[0].ensure(ln * sizeof(int2)));
+        CU(cudaMemsetAsync(st->owner[0].p, 0, (size_t)N * 8, s));
+        a.V = st->V.as<double>();
+        a.growth_factor = std::exp(pop->growth_rate * o->dt);
+        a.V_div = pop->V_div; a.V_lo = pop->V_init_lo; a.V_hi = pop->V_init_hi;
+        a.partition = pop->partition;
+        a.exclude_mother = pop->exclude_mother ? 1 : 0;
+        a.tau = tau ? 1 : 0;
+        a.epoch = 0;
+        a.owner = st->owner[0].as<unsigned long long>();
+        a.divided = st->dprom[1].as<uint8_t>();
+        a.dM = st->dM[0].as<float>(); a.dP = st->dP[0].as<float>();
+        a.dprom = st->dprom[0].as<uint8_t>(); a.dNS = st->dNS[0].as<int2>(); a.dV = st->dV[0].as<double>();
+        a.beta64 = n->dev.beta64;
+        a.ss_mu_m = kin->mu_m + kin->dilution;
+        a.ss_mu_p = kin->mu_p + kin->dilution;
+        a.k_t64 = kin->k_t;
+    }
     const unsigned b_init = (unsigned)((gn + 255) / 256);
     if (dtype == 0) tensor_init_kernel<__nv_bfloat16><<<b_init, 256, 0, s>>>(a);
     else tensor_init_kernel<__half><<<b_init, 256, 0, s>>>(a);
@@ -581,6 +761,8 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
             step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2> : tensor_tau_step_kernel<__half, true, 0>)
                              : (h2 ? tensor_tau_step_kernel<__half, false, 2> : tensor_tau_step_kernel<__half, false, 0>);
     }
+    StepFn replace_fn = dtype == 0 ? (h2 ? tensor_replace_kernel<__nv_bfloat16, 2> : tensor_replace_kernel<__nv_bfloat16, 0>)
+                                   : (h2 ? tensor_replace_kernel<__half, 2> : tensor_replace_kernel<__half, 0>);
     const dim3 g_step((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
                       (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
     if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");
@@ -599,10 +781,24 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         step_fn<<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
         CU(cudaGetLastError());
         ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
+        if (pop) {
+            const unsigned b_cells = (unsigned)((N + 255) / 256);
+            tensor_growth_kernel<<<b_cells, 256, 0, s>>>(a.V, N, a.growth_factor);
+            CU(cudaGetLastError());
+            ctx->launches += 1;
+            if (step % pop->div_check_interval == 0) {
+                tensor_divide_kernel<<<b_cells, 256, 0, s>>>(a);
+                tensor_partition_kernel<<<b_init, 256, 0, s>>>(a);
+                replace_fn<<<b_init, 256, 0, s>>>(a);
+                CU(cudaGetLastError());
+                ctx->launches += 3;
+                a.epoch += 1;
+            }
+        }
     }
     dim3 rgrid((unsigned)((N + 31) / 32), (unsigned)((G + 31) / 32));
     tensor_readout_kernel<<<rgrid, dim3(32, 8), 0, s>>>(G, ld, N, st->tM.as<float>(), st->tP.as<float>(), st->readout,
-                                                        st->out.as<double>());
+                                                        st->out.as<double>(), pop && tau ? a.V : nullptr);
     CU(cudaGetLastError());
     ctx->launches++;
     if (cap) {

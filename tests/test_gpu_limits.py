@@ -47,10 +47,11 @@ def test_register_path_rejects_513_genes(pkg):
     for path in ("register", "block", "warp"):
         with pytest.raises(pkg.ScrnaError):
             pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, cell_num=8, T=0.1, path=path)
-    # a population at that size has no tensor form
+    # the automatic path takes them to the tensor path, populations included
     pop = pkg.PopulationConfig(cell_num=8, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
-    with pytest.raises(pkg.ScrnaError):
-        pkg.simulate(net, pkg.BinomialTauLeap(0.01), pkg.WORKLOAD_KINETICS, population=pop, T=0.1)
+    for alg in (pkg.CLE(0.01), pkg.BinomialTauLeap(0.01)):
+        X = pkg.simulate(net, alg, pkg.WORKLOAD_KINETICS, population=pop, T=0.2, readout="both")
+        assert X.shape == (8, 2 * 513) and np.all(np.isfinite(X))
 
 
 def _unregulated(pkg, G, seed):
