@@ -15,6 +15,7 @@
 //   * HBM is touched only at chunk boundaries (state, division buffers) and for
 //     the final readout / capture.
 #pragma once
+#include "launch_attr.h"
 #include "cle_device.cuh"
 #include "tau_lockstep.cuh"
 #include "cle_internal.h"
@@ -441,7 +442,7 @@ cle_fused_queue_kernel(const FusedArgs* args, const TileWork* items, int n_items
 template <int UPT, bool POP, bool TAU = false, int QG = 4>
 cudaError_t fused_launch_t(const FusedArgs& a, int nw, size_t smem, cudaStream_t st) {
     auto k = cle_fused_kernel<UPT, POP, TAU, QG>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)((a.N + 31) / 32);
     k<<<blocks, nw * 32, smem, st>>>(a);
@@ -452,7 +453,7 @@ template <int UPT, bool POP, bool TAU = false, int QG = 4>
 cudaError_t fused_queue_launch_t(const FusedArgs* args, const TileWork* items, int n_items, int* counter,
                                  int nw, size_t smem, int grid, TileCtl shared_ctl, int use_shared, cudaStream_t st) {
     auto k = cle_fused_queue_kernel<UPT, POP, TAU, QG>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     k<<<grid, nw * 32, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared);
     return cudaGetLastError();

@@ -19,6 +19,7 @@
 // padded term source reads the constant 1 (cooperative) or 0 (redundant), which leave
 // the product unchanged), so both kernels give identical results.
 #pragma once
+#include "launch_attr.h"
 #include "cle_device.cuh"
 #include "cle_internal.h"
 #include "philox_hoist.cuh"
@@ -534,7 +535,7 @@ template <int GPL, int EMAX, int TMAX, bool POP>
 cudaError_t warpcell_launch_t(const FusedArgs& a, cudaStream_t st) {
     auto k = cle_warpcell_kernel<GPL, EMAX, TMAX, POP>;
     const size_t smem = warpcell_smem_bytes(a.G, GPL, a.n_reg, a.n_na, a.lane_nw1);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     const int64_t cpb = warpcell_cells_per_block(a.G, GPL, a.lane_nw1);
     const unsigned blocks = (unsigned)((a.N + cpb - 1) / cpb);
@@ -548,7 +549,7 @@ cudaError_t warpcell_queue_launch_t(const FusedArgs* args, const TileWork* items
                                     size_t smem, int grid, int nwarps, TileCtl shared_ctl, int use_shared,
                                     const KeySchedule* ks, cudaStream_t st) {
     auto k = cle_warpcell_queue_kernel<GPL, EMAX, TMAX, POP>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k), smem);
     if (e != cudaSuccess) return e;
     const KeySchedule none{};
     k<<<grid, 32 * nwarps, smem, st>>>(args, items, n_items, counter, shared_ctl, use_shared, ks ? *ks : none,

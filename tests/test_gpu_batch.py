@@ -99,3 +99,37 @@ def test_sharded_batch_equals_one_batch(pkg):
     for b in range(len(nets)):
         assert np.array_equal(got_x[b], want_x[b]), b
         assert np.array_equal(got_c[b], want_c[b]), b
+
+
+def test_concurrent_calls_on_two_contexts_of_one_gpu(pkg):
+    """Two threads, each with its own context on the same GPU, run networks whose kernels need
+    different amounts of dynamic shared memory, many times over.  The kernels' shared-memory
+    limit is one attribute of the device's context, which both contexts share; the library only
+    ever raises it, so no launch finds it set below its own size by the other thread.  Every
+    result equals the same call made alone."""
+    import threading
+    kin = pkg.WORKLOAD_KINETICS
+    jobs = [(pkg.sample_network(G, seed=900 + G, bursty=bool(G % 2)), G) for G in (12, 45, 90, 150)]
+    want = {G: pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=200, T=0.3, readout="both", seed=G)
+            for net, G in jobs}
+    errors = []
+
+    def worker(k):
+        ctx = pkg.Context(0)
+        try:
+            for rep in range(12):
+                net, G = jobs[(k + rep) % len(jobs)]
+                got = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=200, T=0.3, readout="both", seed=G, ctx=ctx)
+                if not np.array_equal(got, want[G]):
+                    errors.append((k, G, "differs"))
+        except Exception as e:  # noqa: BLE001 (reported below)
+            errors.append((k, repr(e)))
+        finally:
+            ctx.close()
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
