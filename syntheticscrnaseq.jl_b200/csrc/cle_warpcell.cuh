@@ -250,32 +250,32 @@ __device__ __forceinline__ void warpcell_tile(const FusedArgs& a, int64_t tile, 
             V = __dadd_rn(a.V_lo, __dmul_rn(__dadd_rn(a.V_hi, -a.V_lo), u53(w.x, w.y)));
         }
     } else {
-        int64_t src = cidx;
-        bool from_daughter = false;
+        // The cell's own state and, with a population, its slot's owner word are read together;
+        // a cell replaced at the previous division then reads its donor's daughter instead (one
+        // memory round trip for the cells that kept their slot instead of two).
         const int par = ctl.epoch & 1;
-        if (POP && ctl.epoch > 0) {
-            const unsigned long long o = a.owner[par][cidx];
-            if ((uint32_t)(o >> 32) == (uint32_t)ctl.epoch) {
-                src = (int64_t)(o & 0xFFFFFFFFull);
-                from_daughter = true;
-            }
-        }
-        const float* Ms = from_daughter ? a.dM[par] : a.M;
-        const float* Ps = from_daughter ? a.dP[par] : a.P;
-        const uint8_t* Os = from_daughter ? a.dprom[par] : a.prom;
-        const int2* Ns = from_daughter ? a.dNS[par] : a.NS;
+        const unsigned long long o = POP && ctl.epoch > 0 ? a.owner[par][cidx] : 0ull;
+        auto load = [&](const float* Ms, const float* Ps, const uint8_t* Os, const int2* Ns, int64_t src) {
+            on = 0xFFFFFFFFu;
 #pragma unroll
-        for (int i = 0; i < GPL; ++i) {  // cell-major state: a warp's lanes read adjacent entries
-            const int g = u * GPL + i;
-            const size_t si = (size_t)src * G + g;
-            m[i] = valid[i] ? Ms[si] : 0.0f;
-            p[i] = valid[i] ? Ps[si] : 0.0f;
-            const int2 sw = valid[i] ? Ns[si] : make_int2(kNever, kNever);
-            ns[i] = sw.x;
-            kn[i] = sw.y;
-            if (valid[i] && !Os[si]) on &= ~(1u << i);
+            for (int i = 0; i < GPL; ++i) {  // cell-major state: a warp's lanes read adjacent entries
+                const int g = u * GPL + i;
+                const size_t si = (size_t)src * G + g;
+                m[i] = valid[i] ? Ms[si] : 0.0f;
+                p[i] = valid[i] ? Ps[si] : 0.0f;
+                const int2 sw = valid[i] ? Ns[si] : make_int2(kNever, kNever);
+                ns[i] = sw.x;
+                kn[i] = sw.y;
+                if (valid[i] && !Os[si]) on &= ~(1u << i);
+            }
+        };
+        load(a.M, a.P, a.prom, a.NS, cidx);
+        if (POP) V = a.V[cidx];
+        if (POP && ctl.epoch > 0 && (uint32_t)(o >> 32) == (uint32_t)ctl.epoch) {
+            const int64_t src = (int64_t)(o & 0xFFFFFFFFull);
+            load(a.dM[par], a.dP[par], a.dprom[par], a.dNS[par], src);
+            V = a.dV[par][src];
         }
-        if (POP) V = from_daughter ? a.dV[par][src] : a.V[cidx];
     }
 
     // ---- fused step loop --------------------------------------------------------------
