@@ -18,6 +18,7 @@
 #include <cuda_fp16.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -313,7 +314,9 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
 // tau-leap's per-gene Philox blocks (tag 9), switching from their spare bits, and the pair's
 // draws in lock step (tau_update_unit, the register path's arithmetic).  With no regulation the
 // GEMM gives exactly 0, so the counts equal the register path's and the oracle's bit for bit.
-template <class T, bool BURSTY, int HN>
+// CPT cells per thread: the tau-leap's step is bound by the latency of its draws, not by HBM,
+// so it runs fewer cells a thread than the CLE's step (more threads in flight).
+template <class T, bool BURSTY, int HN, int CPT>
 __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(const TensorArgs a) {
     using T2 = typename Pair16<T>::type;
     const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
@@ -326,14 +329,13 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(c
     const int src1 = has1 ? a.src_of_gene[g0 + 1] : -1;
     const uint32_t c3 = tagword(TAG_TAU, a.stream);
     const int s = a.step;
-    const int64_t c_begin = (int64_t)blockIdx.x * kTensorCellsPerThread;
-    const int64_t c_end = c_begin + kTensorCellsPerThread < a.N ? c_begin + kTensorCellsPerThread : a.N;
+    const int64_t c_begin = (int64_t)blockIdx.x * CPT;
+    const int64_t c_end = c_begin + CPT < a.N ? c_begin + CPT : a.N;
     const size_t rs = (size_t)(a.ld >> 1);  // row stride in pairs
     const float2* regp = reinterpret_cast<const float2*>(a.reg) + (size_t)c_begin * rs + k;
     float2* Mp = reinterpret_cast<float2*>(a.M) + (size_t)c_begin * rs + k;
     float2* Pp = reinterpret_cast<float2*>(a.P) + (size_t)c_begin * rs + k;
     T2* actp = reinterpret_cast<T2*>(a.act16) + (size_t)c_begin * (a.Kp >> 1) + k;
-    constexpr int CPT = kTensorCellsPerThread;
     const int nc = (int)(c_end - c_begin);
     float2 rg[CPT], mm[CPT], pp[CPT];
 #pragma unroll
@@ -655,6 +657,33 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
     return SCRNA_OK;
 }
 
+// Cells per thread of the tau-leap's tensor step: SCRNA_TENSOR_TAU_CELLS_PER_THREAD=1, 2, 4 or 8.
+static int tensor_tau_cells_per_thread() {
+    if (const char* e = std::getenv("SCRNA_TENSOR_TAU_CELLS_PER_THREAD")) {
+        const int c = std::atoi(e);
+        if (c == 1 || c == 2 || c == 4 || c == 8) return c;
+    }
+    return 2;
+}
+
+template <int CPT>
+static void (*tau_step_fn_c(int dtype, bool bursty, bool h2))(TensorArgs) {
+    if (dtype == 0)
+        return bursty ? (h2 ? tensor_tau_step_kernel<__nv_bfloat16, true, 2, CPT> : tensor_tau_step_kernel<__nv_bfloat16, true, 0, CPT>)
+                      : (h2 ? tensor_tau_step_kernel<__nv_bfloat16, false, 2, CPT> : tensor_tau_step_kernel<__nv_bfloat16, false, 0, CPT>);
+    return bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2, CPT> : tensor_tau_step_kernel<__half, true, 0, CPT>)
+                  : (h2 ? tensor_tau_step_kernel<__half, false, 2, CPT> : tensor_tau_step_kernel<__half, false, 0, CPT>);
+}
+
+static void (*tau_step_fn(int dtype, bool bursty, bool h2, int cpt))(TensorArgs) {
+    switch (cpt) {
+        case 1: return tau_step_fn_c<1>(dtype, bursty, h2);
+        case 4: return tau_step_fn_c<4>(dtype, bursty, h2);
+        case 8: return tau_step_fn_c<8>(dtype, bursty, h2);
+        default: return tau_step_fn_c<2>(dtype, bursty, h2);
+    }
+}
+
 int64_t run_steps(const scrna_cle_opts* o);
 
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
@@ -753,17 +782,14 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
                                      : (h2 ? tensor_step_kernel<__nv_bfloat16, false, 2> : tensor_step_kernel<__nv_bfloat16, false, 0>);
     else step_fn = bursty ? (h2 ? tensor_step_kernel<__half, true, 2> : tensor_step_kernel<__half, true, 0>)
                           : (h2 ? tensor_step_kernel<__half, false, 2> : tensor_step_kernel<__half, false, 0>);
+    int cpt = kTensorCellsPerThread;
     if (tau) {
-        if (dtype == 0)
-            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__nv_bfloat16, true, 2> : tensor_tau_step_kernel<__nv_bfloat16, true, 0>)
-                             : (h2 ? tensor_tau_step_kernel<__nv_bfloat16, false, 2> : tensor_tau_step_kernel<__nv_bfloat16, false, 0>);
-        else
-            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2> : tensor_tau_step_kernel<__half, true, 0>)
-                             : (h2 ? tensor_tau_step_kernel<__half, false, 2> : tensor_tau_step_kernel<__half, false, 0>);
+        cpt = tensor_tau_cells_per_thread();
+        step_fn = tau_step_fn(dtype, bursty, h2, cpt);
     }
     StepFn replace_fn = dtype == 0 ? (h2 ? tensor_replace_kernel<__nv_bfloat16, 2> : tensor_replace_kernel<__nv_bfloat16, 0>)
                                    : (h2 ? tensor_replace_kernel<__half, 2> : tensor_replace_kernel<__half, 0>);
-    const dim3 g_step((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
+    const dim3 g_step((unsigned)((N + cpt - 1) / cpt),
                       (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
     if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");
     for (int64_t step = 1; step <= n_steps; ++step) {
