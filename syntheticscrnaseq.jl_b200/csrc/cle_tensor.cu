@@ -310,91 +310,138 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
 }
 
 // One binomial tau-leap step after the GEMM (ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks
-// of any size): the layout of tensor_step_kernel (thread = gene pair for a chunk of cells), the
-// tau-leap's per-gene Philox blocks (tag 9), switching from their spare bits, and the pair's
-// draws in lock step (tau_update_unit, the register path's arithmetic).  With no regulation the
-// GEMM gives exactly 0, so the counts equal the register path's and the oracle's bit for bit.
-// CPT cells per thread: the tau-leap's step is bound by the latency of its draws, not by HBM,
-// so it runs fewer cells a thread than the CLE's step (more threads in flight).
-template <class T, bool BURSTY, int HN, int CPT>
-__global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_tau_step_kernel(const TensorArgs a) {
+// of any size), on tiles of 32 cells x 16 gene pairs.  The draws are bound by latency and warp
+// divergence, not by HBM: a warp's lanes are the 32 cells of one gene pair, whose Poisson means
+// are alike (lanes over different genes would wait for the gene with the longest chains).  The
+// tile moves between the cell-major state and shared memory along gene pairs (coalesced), and
+// the compute reads it along cells.  Per (cell, gene): the tau-leap's Philox block (tag 9),
+// switching from its spare bits, and the pair's draws in lock step (tau_update_unit, the
+// register path's arithmetic); without regulation the GEMM gives exactly 0, so the counts equal
+// the register path's and the oracle's bit for bit.
+constexpr int kTauTileCells = 32, kTauTilePairs = 16, kTauTileThreads = 256;
+
+template <class T, bool BURSTY, int HN>
+__global__ void __launch_bounds__(kTauTileThreads) tensor_tau_step_kernel(const TensorArgs a) {
     using T2 = typename Pair16<T>::type;
-    const int k = blockIdx.y * kTensorPairsPerBlock + threadIdx.x;
-    if (k >= (a.ld >> 1)) return;
-    const int g0 = 2 * k;
-    const bool has1 = g0 + 1 < a.G;  // the second gene of the pair exists (else: row padding)
-    const GeneRec r0 = a.genes[g0];
-    const GeneRec r1 = a.genes[has1 ? g0 + 1 : g0];
-    const int src0 = a.src_of_gene[g0];
-    const int src1 = has1 ? a.src_of_gene[g0 + 1] : -1;
-    const uint32_t c3 = tagword(TAG_TAU, a.stream);
-    const int s = a.step;
-    const int64_t c_begin = (int64_t)blockIdx.x * CPT;
-    const int64_t c_end = c_begin + CPT < a.N ? c_begin + CPT : a.N;
-    const size_t rs = (size_t)(a.ld >> 1);  // row stride in pairs
-    const float2* regp = reinterpret_cast<const float2*>(a.reg) + (size_t)c_begin * rs + k;
-    float2* Mp = reinterpret_cast<float2*>(a.M) + (size_t)c_begin * rs + k;
-    float2* Pp = reinterpret_cast<float2*>(a.P) + (size_t)c_begin * rs + k;
-    T2* actp = reinterpret_cast<T2*>(a.act16) + (size_t)c_begin * (a.Kp >> 1) + k;
-    const int nc = (int)(c_end - c_begin);
-    float2 rg[CPT], mm[CPT], pp[CPT];
-#pragma unroll
-    for (int i = 0; i < CPT; ++i) {
-        if (i < nc) {
-            rg[i] = regp[i * rs];
-            mm[i] = Mp[i * rs];
-            pp[i] = Pp[i * rs];
+    constexpr int TP = kTauTilePairs + 1;  // padded row: lanes (cells) fall in different banks
+    __shared__ float2 s_reg[kTauTileCells][TP], s_m[kTauTileCells][TP], s_p[kTauTileCells][TP];
+    __shared__ T2 s_act[kTauTileCells][TP];
+    __shared__ int4 s_ns[BURSTY ? kTauTileCells : 1][TP];
+    __shared__ uchar2 s_on[BURSTY ? kTauTileCells : 1][TP];
+    __shared__ uint8_t s_sw[BURSTY ? kTauTileCells : 1][TP];  // a promoter of the pair switched
+    const int t = threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.x * kTauTileCells;
+    const int k0 = blockIdx.y * kTauTilePairs;
+    const int pairs = a.ld >> 1;
+    const size_t rs = (size_t)pairs;  // state row stride in pairs
+    // load along gene pairs
+    for (int i = t; i < kTauTileCells * kTauTilePairs; i += kTauTileThreads) {
+        const int r = i / kTauTilePairs, q = i - r * kTauTilePairs;
+        const int64_t c = c0 + r;
+        const int k = k0 + q;
+        if (c >= a.N || k >= pairs) continue;
+        const size_t e = (size_t)c * rs + k;
+        s_reg[r][q] = reinterpret_cast<const float2*>(a.reg)[e];
+        s_m[r][q] = reinterpret_cast<const float2*>(a.M)[e];
+        s_p[r][q] = reinterpret_cast<const float2*>(a.P)[e];
+        if (BURSTY) {
+            s_on[r][q] = reinterpret_cast<const uchar2*>(a.prom)[e];
+            s_ns[r][q] = reinterpret_cast<const int4*>(a.NS)[e];
+            s_sw[r][q] = 0;
         }
     }
-#pragma unroll
-    for (int i = 0; i < CPT; ++i) {
-        if (i >= nc) break;
-        const int64_t c = c_begin + i;
-        const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+    __syncthreads();
+    // compute along cells: lane = cell, warp = gene pair (and the pair 8 further)
+    const int r = t & 31;
+    const int64_t c = c0 + r;
+    const uint32_t gcell = (uint32_t)(a.cell_offset + c);
+    const uint32_t c3 = tagword(TAG_TAU, a.stream);
+    const int s = a.step;
+    float Vf = 1.0f, Vn = 1.0f;  // the volume now and at the start of the next step (Hill of P / V)
+    if (a.V && c < a.N) {
+        const double V = a.V[c];
+        Vf = (float)V;
+        Vn = (float)__dmul_rn(V, a.growth_factor);
+    }
+    for (int q = t >> 5; q < kTauTilePairs; q += kTauTileThreads / 32) {
+        const int k = k0 + q;
+        if (c >= a.N || k >= pairs) continue;
+        const int g0 = 2 * k;
+        const bool has1 = g0 + 1 < a.G;  // the second gene of the pair exists (else: row padding)
+        const GeneRec r0 = a.genes[g0];
+        const GeneRec r1 = a.genes[has1 ? g0 + 1 : g0];
         uint4 w[2];
         w[0] = philox_rk(gcell, (uint32_t)s, (uint32_t)g0, c3, a.rk0, a.rk1);
         w[1] = has1 ? philox_rk(gcell, (uint32_t)s, (uint32_t)(g0 + 1), c3, a.rk0, a.rk1) : make_uint4(0u, 0u, 0u, 0u);
-        float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg[i].x, r0.cneg), r0.beta), 0.0f);
-        float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg[i].y, r1.cneg), r1.beta), 0.0f);
-        float Vn = 1.0f;  // the volume at the start of the next step (Hill of P / V)
+        const float2 rg = s_reg[r][q];
+        float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg.x, r0.cneg), r0.beta), 0.0f);
+        float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg.y, r1.cneg), r1.beta), 0.0f);
         if (a.V) {
-            const double V = a.V[c];
-            tx0 = __fmul_rn(tx0, (float)V);
-            tx1 = __fmul_rn(tx1, (float)V);
-            Vn = (float)__dmul_rn(V, a.growth_factor);
+            tx0 = __fmul_rn(tx0, Vf);
+            tx1 = __fmul_rn(tx1, Vf);
         }
         bool on0 = true, on1 = true;
         if (BURSTY) {  // switching before the transcription update (tauleap_binomial.jl:111-121)
-            const size_t e = (size_t)c * a.ld + g0;
-            const uchar2 on = *reinterpret_cast<const uchar2*>(a.prom + e);
-            const int4 sw = *reinterpret_cast<const int4*>(a.NS + e);
+            const uchar2 on = s_on[r][q];
+            int4 sw = s_ns[r][q];
             on0 = on.x;
             on1 = on.y;
+            bool changed = false;
             if (s == sw.x) {
                 on0 = !on0;
-                a.NS[e] = switch_at(s, make_int2(sw.x, sw.y), switch_uniform(w[0].x, w[0].y), on0, r0.inv_on, r0.inv_off);
-                a.prom[e] = on0;
+                const int2 n0 = switch_at(s, make_int2(sw.x, sw.y), switch_uniform(w[0].x, w[0].y), on0, r0.inv_on,
+                                          r0.inv_off);
+                sw.x = n0.x;
+                sw.y = n0.y;
+                changed = true;
             }
             if (has1 && s == sw.z) {
                 on1 = !on1;
-                a.NS[e + 1] = switch_at(s, make_int2(sw.z, sw.w), switch_uniform(w[1].x, w[1].y), on1, r1.inv_on, r1.inv_off);
-                a.prom[e + 1] = on1;
+                const int2 n1 = switch_at(s, make_int2(sw.z, sw.w), switch_uniform(w[1].x, w[1].y), on1, r1.inv_on,
+                                          r1.inv_off);
+                sw.z = n1.x;
+                sw.w = n1.y;
+                changed = true;
+            }
+            if (changed) {
+                s_ns[r][q] = sw;
+                s_on[r][q] = make_uchar2(on0, on1);
+                s_sw[r][q] = 1;
             }
         }
         const float lam[2] = {on0 ? __fmul_rn(tx0, a.dt) : 0.0f, (has1 && on1) ? __fmul_rn(tx1, a.dt) : 0.0f};
         // the padding slot of an odd G holds no state (never initialised): counts 0
-        float m2[2] = {mm[i].x, has1 ? mm[i].y : 0.0f}, p2[2] = {pp[i].x, has1 ? pp[i].y : 0.0f};
+        const float2 mm = s_m[r][q], pp = s_p[r][q];
+        float m2[2] = {mm.x, has1 ? mm.y : 0.0f}, p2[2] = {pp.x, has1 ? pp.y : 0.0f};
         tau_update_unit<2>(m2, p2, lam, w, has1 ? 2 : 1, true, a.k_t, a.dt, a.p_dec_m, a.p_dec_p);
-        Mp[i * rs] = make_float2(m2[0], m2[1]);
-        Pp[i * rs] = make_float2(p2[0], p2[1]);
+        s_m[r][q] = make_float2(m2[0], m2[1]);
+        s_p[r][q] = make_float2(p2[0], p2[1]);
         const float a0 = tensor_hill<HN>(a.V ? __fdiv_rn(p2[0], Vn) : p2[0], a);
         const float a1 = tensor_hill<HN>(a.V ? __fdiv_rn(p2[1], Vn) : p2[1], a);
         T2 act;
         act.x = to16<T>(a0);
         act.y = to16<T>(has1 ? a1 : 0.0f);  // the padding column of the activations stays 0
-        actp[(size_t)i * (a.Kp >> 1)] = act;
-        if (src0 >= 0) a.act32_next[(size_t)src0 * a.N + c] = a0;
+        s_act[r][q] = act;
+        const int src0 = a.src_of_gene[g0];
+        const int src1 = has1 ? a.src_of_gene[g0 + 1] : -1;
+        if (src0 >= 0) a.act32_next[(size_t)src0 * a.N + c] = a0;  // lanes: consecutive cells
         if (src1 >= 0) a.act32_next[(size_t)src1 * a.N + c] = a1;
+    }
+    __syncthreads();
+    // store along gene pairs
+    for (int i = t; i < kTauTileCells * kTauTilePairs; i += kTauTileThreads) {
+        const int rr = i / kTauTilePairs, q = i - rr * kTauTilePairs;
+        const int64_t cc = c0 + rr;
+        const int k = k0 + q;
+        if (cc >= a.N || k >= pairs) continue;
+        const size_t e = (size_t)cc * rs + k;
+        reinterpret_cast<float2*>(a.M)[e] = s_m[rr][q];
+        reinterpret_cast<float2*>(a.P)[e] = s_p[rr][q];
+        reinterpret_cast<T2*>(a.act16)[(size_t)cc * (a.Kp >> 1) + k] = s_act[rr][q];
+        if (BURSTY && s_sw[rr][q]) {
+            reinterpret_cast<uchar2*>(a.prom)[e] = s_on[rr][q];
+            reinterpret_cast<int4*>(a.NS)[e] = s_ns[rr][q];
+        }
     }
 }
 
@@ -657,33 +704,6 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
     return SCRNA_OK;
 }
 
-// Cells per thread of the tau-leap's tensor step: SCRNA_TENSOR_TAU_CELLS_PER_THREAD=1, 2, 4 or 8.
-static int tensor_tau_cells_per_thread() {
-    if (const char* e = std::getenv("SCRNA_TENSOR_TAU_CELLS_PER_THREAD")) {
-        const int c = std::atoi(e);
-        if (c == 1 || c == 2 || c == 4 || c == 8) return c;
-    }
-    return 2;
-}
-
-template <int CPT>
-static void (*tau_step_fn_c(int dtype, bool bursty, bool h2))(TensorArgs) {
-    if (dtype == 0)
-        return bursty ? (h2 ? tensor_tau_step_kernel<__nv_bfloat16, true, 2, CPT> : tensor_tau_step_kernel<__nv_bfloat16, true, 0, CPT>)
-                      : (h2 ? tensor_tau_step_kernel<__nv_bfloat16, false, 2, CPT> : tensor_tau_step_kernel<__nv_bfloat16, false, 0, CPT>);
-    return bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2, CPT> : tensor_tau_step_kernel<__half, true, 0, CPT>)
-                  : (h2 ? tensor_tau_step_kernel<__half, false, 2, CPT> : tensor_tau_step_kernel<__half, false, 0, CPT>);
-}
-
-static void (*tau_step_fn(int dtype, bool bursty, bool h2, int cpt))(TensorArgs) {
-    switch (cpt) {
-        case 1: return tau_step_fn_c<1>(dtype, bursty, h2);
-        case 4: return tau_step_fn_c<4>(dtype, bursty, h2);
-        case 8: return tau_step_fn_c<8>(dtype, bursty, h2);
-        default: return tau_step_fn_c<2>(dtype, bursty, h2);
-    }
-}
-
 int64_t run_steps(const scrna_cle_opts* o);
 
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
@@ -782,15 +802,21 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
                                      : (h2 ? tensor_step_kernel<__nv_bfloat16, false, 2> : tensor_step_kernel<__nv_bfloat16, false, 0>);
     else step_fn = bursty ? (h2 ? tensor_step_kernel<__half, true, 2> : tensor_step_kernel<__half, true, 0>)
                           : (h2 ? tensor_step_kernel<__half, false, 2> : tensor_step_kernel<__half, false, 0>);
-    int cpt = kTensorCellsPerThread;
     if (tau) {
-        cpt = tensor_tau_cells_per_thread();
-        step_fn = tau_step_fn(dtype, bursty, h2, cpt);
+        if (dtype == 0)
+            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__nv_bfloat16, true, 2> : tensor_tau_step_kernel<__nv_bfloat16, true, 0>)
+                             : (h2 ? tensor_tau_step_kernel<__nv_bfloat16, false, 2> : tensor_tau_step_kernel<__nv_bfloat16, false, 0>);
+        else
+            step_fn = bursty ? (h2 ? tensor_tau_step_kernel<__half, true, 2> : tensor_tau_step_kernel<__half, true, 0>)
+                             : (h2 ? tensor_tau_step_kernel<__half, false, 2> : tensor_tau_step_kernel<__half, false, 0>);
     }
     StepFn replace_fn = dtype == 0 ? (h2 ? tensor_replace_kernel<__nv_bfloat16, 2> : tensor_replace_kernel<__nv_bfloat16, 0>)
                                    : (h2 ? tensor_replace_kernel<__half, 2> : tensor_replace_kernel<__half, 0>);
-    const dim3 g_step((unsigned)((N + cpt - 1) / cpt),
-                      (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
+    const dim3 g_step = tau ? dim3((unsigned)((N + kTauTileCells - 1) / kTauTileCells),
+                                   (unsigned)((pairs + kTauTilePairs - 1) / kTauTilePairs))
+                            : dim3((unsigned)((N + kTensorCellsPerThread - 1) / kTensorCellsPerThread),
+                                   (unsigned)((pairs + kTensorPairsPerBlock - 1) / kTensorPairsPerBlock));
+    const unsigned step_threads = tau ? kTauTileThreads : kTensorPairsPerBlock;
     if (g_step.y > 65535) return fail(SCRNA_ENOTSUP, "too many genes for the tensor path");
     for (int64_t step = 1; step <= n_steps; ++step) {
         a.step = (int)step;
@@ -804,7 +830,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
                                             st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
                                             &gemm.algo, ctx->lt_workspace.p, ctx->lt_workspace.n, s);
         if (stt != CUBLAS_STATUS_SUCCESS) return lt_fail(stt, "cublasLtMatmul");
-        step_fn<<<g_step, kTensorPairsPerBlock, 0, s>>>(a);
+        step_fn<<<g_step, step_threads, 0, s>>>(a);
         CU(cudaGetLastError());
         ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
         if (pop) {
