@@ -324,6 +324,8 @@ static int measure(scrna_ctx* ctx, scrna_net* net, const FusedArgs& base, scrna_
     return err;
 }
 
+constexpr double kTuneMinUnits = 5e8;  // cell-gene-steps of a run worth measuring for (~2.5 ms)
+
 // The register-path kernel of a run: the static choice (choose_kernel), or with autotuning on
 // the cached or measured fastest variant for the network's shape.  A measurement runs on
 // `st`'s state buffers (state_alloc for N cells) with the kernel arguments `base` (NULL:
@@ -349,7 +351,10 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     }
     if (!c.found && !ctx->tune_path.empty())
         if (int r = lookup(ctx->tune_path, key, &c)) return r;
-    if (!c.found && ctx->tune_mode == 1 && may_measure) {
+    // A run shorter than kTuneMinUnits takes the static choice and leaves the cache alone: measuring
+    // the candidates (and loading their modules on first launch) would cost more than it can save.
+    const double run_units = (double)st->N * net->G * (double)n_steps_of(o);
+    if (!c.found && ctx->tune_mode == 1 && may_measure && run_units >= kTuneMinUnits) {
         NvtxRange nvtx_range_("scrna_autotune_measure");
         FusedArgs a{};
         if (base) a = *base;
