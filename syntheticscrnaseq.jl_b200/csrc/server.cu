@@ -2,7 +2,8 @@
 //
 // A worker thread owns the device side.  Submitted requests queue FIFO; at every chunk
 // boundary the worker admits queued requests while their device footprint fits the HBM
-// budget, then advances every running request by up to chunk_steps Euler steps with one
+// budget, then advances every running request by chunk_steps Euler steps (small requests by
+// a multiple of that, up to the largest request's work) with one
 // persistent work-queue launch per register-path kernel group (the same kernels as
 // scrna_cle_simulate).  State stays on the device between chunks, so a request's result
 // does not depend on what else runs beside it.  Finished requests keep their outputs on
@@ -83,6 +84,7 @@ struct scrna_server {
     DevBuf args_dev, items_dev, counters_dev;
     // the kernel groups of a chunk run side by side, one stream each, between two events
     static constexpr int kGroupStreams = 8;
+    static constexpr int64_t kMaxChunkMultiple = 16;
     cudaStream_t gstream[kGroupStreams] = {};
     cudaEvent_t ev_inputs = nullptr, ev_group[kGroupStreams] = {};
     int n_group_streams = kGroupStreams;  // SCRNA_SERVER_GROUP_STREAMS=1: the groups one after another
@@ -192,11 +194,19 @@ void scrna_server::run() {
         h_args.clear();
         std::map<std::tuple<int, int, int, int, int>, std::vector<TileWork>> groups;
         std::map<std::tuple<int, int, int, int, int>, std::pair<int, size_t>> shape;  // nw, smem
+        // Steps of each request in this chunk: chunk_steps, or up to kMaxChunkMultiple times that
+        // for a request whose work per step is that much smaller than the largest one's, so small
+        // requests finish in few chunks while the chunk's length stays set by the largest
+        // (results do not depend on the chunking).
+        double w_max = 0.0;
+        for (SrvRequest* r : run_set) w_max = std::max(w_max, (double)r->net->G * (double)r->N);
         for (size_t i = 0; i < run_set.size(); ++i) {
             SrvRequest* r = run_set[i];
             h_args.push_back(r->args);
+            const double ups = (double)r->net->G * (double)r->N;
+            const int64_t mult = std::min<int64_t>(kMaxChunkMultiple, std::max<int64_t>(1, (int64_t)(w_max / ups)));
             r->s0 = r->next;
-            r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps - 1);
+            r->s1 = r->n_steps == 0 ? 0 : std::min<int64_t>(r->n_steps, r->next + chunk_steps * mult - 1);
             const KernelChoice& kc = r->kc;
             // (warp kernel, genes per lane, in-edges, warps per block or block-kernel quads per thread, terms)
             auto key = std::make_tuple((int)kc.warp, kc.warp ? kc.gpl : 0, kc.warp ? kc.emax : 0,
@@ -214,6 +224,10 @@ void scrna_server::run() {
         h_items.clear();
         std::vector<size_t> offsets;
         for (auto& kv : groups) {
+            // longest step ranges first, so no long item starts at the end of the work queue
+            std::stable_sort(kv.second.begin(), kv.second.end(), [](const TileWork& x, const TileWork& y) {
+                return x.ctl.step_end - x.ctl.step_begin > y.ctl.step_end - y.ctl.step_begin;
+            });
             offsets.push_back(h_items.size());
             h_items.insert(h_items.end(), kv.second.begin(), kv.second.end());
         }
