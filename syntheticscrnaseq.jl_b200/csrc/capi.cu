@@ -265,27 +265,6 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     d.n_na = (int)n->na.size();
     d.n_na_src = (int)n->na_src.size();
     d.n_quads = (G + 3) / 4;
-    auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
-        cudaError_t e = b.ensure(bytes);
-        if (e != cudaSuccess) return e;
-        ctx->h2d_bytes += (int64_t)bytes;
-        if (bytes) return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
-        return cudaSuccess;
-    };
-    CU(up(n->b_in_edge, n->in_edge.data(), n->in_edge.size() * sizeof(float2)));
-    CU(up(n->b_na, n->na.data(), n->na.size() * sizeof(NonAdd)));
-    CU(up(n->b_na_src, n->na_src.data(), n->na_src.size() * sizeof(int32_t)));
-    CU(up(n->b_reg_gene, n->reg_gene.data(), n->reg_gene.size() * sizeof(int32_t)));
-    CU(up(n->b_in_w64, n->in_w64.data(), n->in_w64.size() * sizeof(double)));
-    CU(up(n->b_na_coef64, n->na_coef64.data(), n->na_coef64.size() * sizeof(double)));
-    CU(up(n->b_beta64, n->basals.data(), n->basals.size() * sizeof(double)));
-    d.in_edge = n->b_in_edge.as<float2>();
-    d.na = n->b_na.as<NonAdd>();
-    d.na_src = n->b_na_src.as<int32_t>();
-    d.reg_gene = n->b_reg_gene.as<int32_t>();
-    d.in_w64 = n->b_in_w64.as<double>();
-    d.na_coef64 = n->b_na_coef64.as<double>();
-    d.beta64 = n->b_beta64.as<double>();
     for (int g = 0; g < G; ++g) d.bursty = d.bursty || std::isfinite(n->k_on[g]);
     // tables of the warp-per-cell-group kernel (small networks): per gene its additive
     // edges then one edge per term targeting it (term j's value sits in slot n_reg+3+j)
@@ -304,9 +283,11 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
     if (terms_per_lane(gpl) > kLaneTerms && gpl == 4) gpl = 2;
     const int tmax = terms_per_lane(gpl);
     lane_ok = lane_ok && tmax <= kLaneTerms;
+    std::vector<int2> li;
+    std::vector<LaneTerm> lt;
     if (lane_ok) {
         const int zero_slot = d.n_reg, one_slot = d.n_reg + 1;  // constant slots of the kernel's rows
-        std::vector<int2> li((size_t)G * kLaneEdges, make_int2(zero_slot, 0));
+        li.assign((size_t)G * kLaneEdges, make_int2(zero_slot, 0));
         for (int g = 0; g < G; ++g) {
             int k = 0;
             for (int e = n->in_begin[g]; e < n->in_end[g]; ++e, ++k) {
@@ -321,7 +302,7 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
                 li[(size_t)g * kLaneEdges + k] = make_int2(d.n_reg + 3 + e, wbits);
             }
         }
-        std::vector<LaneTerm> lt(std::max<size_t>(n->na.size(), 1));
+        lt.assign(std::max<size_t>(n->na.size(), 1), LaneTerm{});
         for (size_t e = 0; e < n->na.size(); ++e) {
             const NonAdd& na = n->na[e];
             LaneTerm t{};
@@ -333,10 +314,43 @@ extern "C" int scrna_net_create(scrna_ctx* ctx, int32_t G, const double* basals,
             }
             lt[e] = t;
         }
-        CU(up(n->b_lane_in, li.data(), li.size() * sizeof(int2)));
-        CU(up(n->b_lane_term, lt.data(), lt.size() * sizeof(LaneTerm)));
-        d.lane_in = n->b_lane_in.as<int2>();
-        d.lane_term = n->b_lane_term.as<LaneTerm>();
+    }
+    // every table in one device allocation and one copy (parts 256-byte aligned)
+    struct Part { const void* src; size_t bytes; size_t off; };
+    std::vector<Part> parts;
+    size_t total = 0, payload = 0;
+    auto add = [&](const void* src, size_t bytes) {
+        parts.push_back(Part{src, bytes, total});
+        total += (bytes + 255) & ~(size_t)255;
+        payload += bytes;
+        return parts.size() - 1;
+    };
+    const size_t p_in = add(n->in_edge.data(), n->in_edge.size() * sizeof(float2));
+    const size_t p_na = add(n->na.data(), n->na.size() * sizeof(NonAdd));
+    const size_t p_na_src = add(n->na_src.data(), n->na_src.size() * sizeof(int32_t));
+    const size_t p_reg = add(n->reg_gene.data(), n->reg_gene.size() * sizeof(int32_t));
+    const size_t p_w64 = add(n->in_w64.data(), n->in_w64.size() * sizeof(double));
+    const size_t p_coef64 = add(n->na_coef64.data(), n->na_coef64.size() * sizeof(double));
+    const size_t p_beta64 = add(n->basals.data(), n->basals.size() * sizeof(double));
+    const size_t p_li = lane_ok ? add(li.data(), li.size() * sizeof(int2)) : 0;
+    const size_t p_lt = lane_ok ? add(lt.data(), lt.size() * sizeof(LaneTerm)) : 0;
+    std::vector<unsigned char> staging(std::max<size_t>(total, 16), 0);
+    for (const Part& pt : parts)
+        if (pt.bytes) std::memcpy(staging.data() + pt.off, pt.src, pt.bytes);
+    CU(n->b_tables.ensure(staging.size()));
+    CU(cudaMemcpy(n->b_tables.p, staging.data(), staging.size(), cudaMemcpyHostToDevice));
+    ctx->h2d_bytes += (int64_t)payload;
+    unsigned char* base = n->b_tables.as<unsigned char>();
+    d.in_edge = reinterpret_cast<float2*>(base + parts[p_in].off);
+    d.na = reinterpret_cast<NonAdd*>(base + parts[p_na].off);
+    d.na_src = reinterpret_cast<int32_t*>(base + parts[p_na_src].off);
+    d.reg_gene = reinterpret_cast<int32_t*>(base + parts[p_reg].off);
+    d.in_w64 = reinterpret_cast<double*>(base + parts[p_w64].off);
+    d.na_coef64 = reinterpret_cast<double*>(base + parts[p_coef64].off);
+    d.beta64 = reinterpret_cast<double*>(base + parts[p_beta64].off);
+    if (lane_ok) {
+        d.lane_in = reinterpret_cast<int2*>(base + parts[p_li].off);
+        d.lane_term = reinterpret_cast<LaneTerm*>(base + parts[p_lt].off);
         d.lane_gpl = gpl;
         d.lane_emax = emax;
         d.lane_tmax = tmax;

@@ -94,7 +94,7 @@ struct scrna_net {
     std::vector<double> na_coef64;
     std::vector<int32_t> na_src;
     NetDev dev;
-    DevBuf b_in_edge, b_na, b_na_src, b_reg_gene, b_in_w64, b_na_coef64, b_beta64, b_lane_in, b_lane_term;
+    DevBuf b_tables;  // the network's upload-time tables (NetDev's pointers) in one allocation
     // per-run tables cached for the last (kinetics, dt, population mode)
     DevBuf b_genes, b_ginit, b_quad_tel;
     // tensor-core path: W = A_eff as 16-bit [G][Kp] (K-major), nonadd sources compacted

@@ -150,10 +150,9 @@ void scrna_server::run() {
                     ++i;
                 }
             }
-            // FIFO admission by device footprint
+            // FIFO admission by device footprint (a cancelled request has left the queue already)
             while (!queue.empty()) {
                 SrvRequest* r = queue.front();
-                if (r->state == SCRNA_REQ_CANCELLED) { queue.pop_front(); continue; }
                 if (r->footprint > budget) {
                     r->state = SCRNA_REQ_FAILED;
                     r->error = "request does not fit the device memory budget";
@@ -165,6 +164,9 @@ void scrna_server::run() {
                 if (used + r->footprint > budget) break;
                 used += r->footprint;
                 r->admitted = true;
+                // RUNNING from here: a cancellation during the set-up below becomes a flag honoured at
+                // the next chunk boundary, so scrna_wait cannot free the request while it is set up
+                r->state = SCRNA_REQ_RUNNING;
                 queue.pop_front();
                 admitted.push_back(r);
             }
@@ -178,7 +180,6 @@ void scrna_server::run() {
                 stats.failed++;
                 cv_done.notify_all();
             } else {
-                r->state = SCRNA_REQ_RUNNING;
                 active.push_back(r);
             }
         }
@@ -452,8 +453,13 @@ extern "C" int scrna_cancel(scrna_server* s, uint64_t ticket) {
     auto it = s->reqs.find(ticket);
     if (it == s->reqs.end()) return fail(SCRNA_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
     SrvRequest* r = it->second;
-    if (r->state == SCRNA_REQ_QUEUED) r->state = SCRNA_REQ_CANCELLED;  // never on the device
-    else if (r->state == SCRNA_REQ_RUNNING) r->cancel = true;         // dropped at the next chunk boundary
+    if (r->state == SCRNA_REQ_QUEUED) {  // never on the device: out of the queue before scrna_wait frees it
+        s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), r), s->queue.end());
+        r->state = SCRNA_REQ_CANCELLED;
+        s->cv_done.notify_all();
+    } else if (r->state == SCRNA_REQ_RUNNING) {
+        r->cancel = true;  // dropped at the next chunk boundary (admitted requests are RUNNING)
+    }
     s->cv_done.notify_all();
     s->cv_work.notify_all();
     return SCRNA_OK;

@@ -110,3 +110,26 @@ def test_server_pool_spreads_requests_and_matches_simulate(pkg):
     pool.close()
     for c in ctxs:
         c.close()
+
+
+def test_cancel_queued_requests_then_keep_serving(pkg):
+    """Requests cancelled while still queued leave the queue at once, so waiting on them (which
+    frees them) cannot race the worker's admission; requests cancelled during admission are
+    dropped at the next chunk boundary.  Repeated, with new requests submitted in between,
+    every surviving request still completes with the result of a lone run."""
+    kin = pkg.WORKLOAD_KINETICS
+    net = pkg.sample_network(30, seed=5)
+    h = pkg.NetHandle(net)
+    want = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=150, T=0.3, readout="protein", seed=9)
+    srv = pkg.Server(chunk_steps=10)
+    for rep in range(6):
+        doomed = [srv.submit(h, pkg.CLE(0.01), kin, cell_num=5000, T=20.0, seed=rep * 10 + k) for k in range(4)]
+        keep = srv.submit(h, pkg.CLE(0.01), kin, cell_num=150, T=0.3, readout="protein", seed=9)
+        for t in doomed:
+            srv.cancel(t)
+            with pytest.raises(pkg.ScrnaError):
+                srv.wait(t, WAIT_MS)
+        assert np.array_equal(srv.wait(keep, WAIT_MS)[0], want)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["bytes_in_use"] == 0
+    srv.close()
