@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -594,6 +595,9 @@ int scrna::tau_lockstep_default() {
 }
 
 const float* scrna::switch_log2_table(scrna_ctx* ctx) {
+    // built once per context, under a lock: a server's worker shares its caller's context
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
     if (ctx->log2_tab_ready) return ctx->log2_tab.as<float>();
     const uint32_t n = 1u << 18;
     if (ctx->log2_tab.ensure((size_t)n * 4) != cudaSuccess) return nullptr;

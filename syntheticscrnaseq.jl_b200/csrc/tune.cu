@@ -324,6 +324,13 @@ static int measure(scrna_ctx* ctx, scrna_net* net, const FusedArgs& base, scrna_
     return err;
 }
 
+// The last choice of a context (reported by scrna_autotune_last_choice), written under the tuner's
+// lock: a server's worker and its caller may choose kernels on one context at once.
+static void set_last(scrna_ctx* ctx, const scrna_tune_choice& c) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx->tune_last = c;
+}
+
 constexpr double kTuneMinUnits = 5e8;  // cell-gene-steps of a run worth measuring for (~2.5 ms)
 
 // The register-path kernel of a run: the static choice (choose_kernel), or with autotuning on
@@ -335,7 +342,7 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
                         scrna_state* st, KernelChoice* out, const FusedArgs* base, cudaStream_t stream,
                         bool may_measure) {
     *out = choose_kernel(net, o->path);
-    ctx->tune_last = scrna_tune_choice{out->warp ? 1 : 0, out->warp ? out->gpl : 0, out->warp ? out->nw1 : 0, 0, 0.0};
+    set_last(ctx, scrna_tune_choice{out->warp ? 1 : 0, out->warp ? out->gpl : 0, out->warp ? out->nw1 : 0, 0, 0.0});
     const int path = o->path;
     if (ctx->tune_mode == 0 || (path != SCRNA_PATH_AUTO && path != SCRNA_PATH_REGISTER && path != SCRNA_PATH_WARP))
         return SCRNA_OK;
@@ -371,7 +378,7 @@ int choose_kernel_tuned(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* ki
     for (const auto& cand : candidates(net, path))
         if (cand.kernel == c.kernel && cand.genes_per_lane == c.genes_per_lane && cand.block_warps == c.block_warps) {
             *out = choice_from(net, c);
-            ctx->tune_last = c;
+            set_last(ctx, c);
             return SCRNA_OK;
         }
     return SCRNA_OK;
@@ -381,7 +388,7 @@ int tc_choose_slices(scrna_ctx* ctx, int G, int64_t N, bool bursty, int dtype, b
                      const std::function<int(int, double*)>& measure, int* S, bool* measured) {
     *S = 7;
     *measured = false;
-    ctx->tune_last = scrna_tune_choice{2, 224, 0, 0, 0.0};
+    set_last(ctx, scrna_tune_choice{2, 224, 0, 0, 0.0});
     if (ctx->tune_mode == 0) return SCRNA_OK;
     char buf[160];
     std::snprintf(buf, sizeof buf, "%s|tc|G%d|d%d|b%d|h%d|N%d", ctx->tune_arch, G, dtype, bursty ? 1 : 0,
@@ -412,7 +419,7 @@ int tc_choose_slices(scrna_ctx* ctx, int G, int64_t N, bool bursty, int dtype, b
         ctx->tune_mem[key] = c;
     }
     *S = c.genes_per_lane / 32;
-    ctx->tune_last = c;
+    set_last(ctx, c);
     return SCRNA_OK;
 }
 
@@ -432,7 +439,10 @@ extern "C" int scrna_ctx_set_autotune(scrna_ctx* ctx, int32_t mode, const char* 
 
 extern "C" int scrna_autotune_last_choice(const scrna_ctx* ctx, scrna_tune_choice* out) {
     if (!ctx || !out) return fail(SCRNA_EINVAL, "NULL argument");
-    *out = ctx->tune_last;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        *out = ctx->tune_last;
+    }
     return SCRNA_OK;
 }
 
