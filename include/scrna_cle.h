@@ -183,8 +183,11 @@ int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* 
  * in the CLE: cooperative / redundant edges and telegraph gating (tauleap_binomial.jl:84-137).
  * With a population: Hill of the concentration P / V, transcription x V, decay without
  * dilution, initial counts max(1, round(steady state x V)), and the readout is M / V, P / V
- * (capture counts are drawn from the molecule counts).  Register path (block tiles), G <= 512,
- * FP32 precision only. */
+ * (capture counts are drawn from the molecule counts).  Paths: the block-tile register kernel
+ * up to 512 genes; beyond that, or with opts->path TENSOR or TENSOR_LIBRARY, the tensor path's
+ * library-GEMM variant (populations included; without regulation its counts equal the register
+ * path's); SCRNA_PATH_WARP is rejected.  FP32 counts; SCRNA_PRECISION_FP32_F16 selects FP16
+ * instead of BF16 contraction inputs on the tensor path. */
 int scrna_tauleap_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                            const scrna_population* pop, const scrna_capture* cap,
                            const scrna_cle_opts* opts, double* out, int32_t* counts,
