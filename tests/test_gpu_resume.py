@@ -78,3 +78,19 @@ def test_checkpoint_restore_resume(pkg):
     other = pkg.DeviceRun(pkg.sample_network(11, seed=1), pkg.CLE(0.01), kin, T=0.5, cell_num=400)
     with pytest.raises(pkg.ScrnaError):
         other.restore(data)
+
+
+def test_tensor_path_state_is_not_resumable(pkg):
+    """A tensor-path run keeps no register-path state between calls: continuing it or taking a
+    checkpoint is refused with an error, and the run's own results stay readable."""
+    net = pkg.sample_network(30, seed=3, bursty=True)
+    run = pkg.DeviceRun(net, pkg.CLE(0.01), pkg.WORKLOAD_KINETICS, cell_num=64, T=0.0, n_steps=20,
+                        readout="both", path="tensor_library")
+    run.launch()
+    X = run.read()
+    with pytest.raises(pkg.ScrnaError):
+        run.resume(n_steps=40)
+    with pytest.raises(pkg.ScrnaError):
+        run.checkpoint()
+    assert np.array_equal(run.read(), X)
+    run.close()
