@@ -105,9 +105,7 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
         owned.emplace_back(st, scrna_state_destroy);
         x.st = st;
         const NetDev& d = x.net->dev;
-        const double density = (double)d.n_in / ((double)x.net->G * x.net->G);
-        // the tau-leap and populations leave the register path only for networks it cannot hold
-        x.tensor = d.n_quads > fused_max_quads() || (!tau && !x.pop && x.net->G >= 256 && density >= 0.05);
+        x.tensor = auto_tensor(x.net, tau, N);
         if (!x.tensor) {
             if (int r = state_alloc(st, x.pop != nullptr, false)) return r;
             const int G = x.net->G, nq = (G + 3) / 4;
@@ -136,7 +134,7 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
                 return r;
             }
             x.args.lane_nw1 = x.kc.nw1;
-            if (x.kc.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
+            if (x.kc.smem > kMaxDynamicSmem) return fail(SCRNA_ENOTSUP, "network %d needs too much shared memory", b);
             x.st->have_counts = cap != nullptr;
         }
     }

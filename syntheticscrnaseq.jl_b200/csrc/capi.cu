@@ -610,6 +610,29 @@ const float* scrna::switch_log2_table(scrna_ctx* ctx) {
     return ctx->log2_tab.as<float>();
 }
 
+// Whether the automatic path runs a network of N cells on the tensor path: always when the
+// register path cannot hold it; the tau-leap beyond 128 genes, where the register path's
+// threads hold pairs or quads of genes at its register limit and fit one block an SM, while
+// the tensor form keeps the state in HBM at full occupancy with the same counts (exact
+// regulation; ms a step, register / tensor: 200 sampled genes 0.145 / 0.086 at 20,000 cells,
+// 300 genes 0.055 / 0.018 at 1,000 and 0.280 / 0.124 at 20,000; 100 genes 0.041 / 0.050);
+// the CLE and its populations for regulation of at least 5 % density over 256 genes or
+// more, where the register path's in-edge loops cost more than the contraction.  The tensor
+// path's step has a floor of about 20 us (its launches) whatever N; the register path's
+// step at small N is one cell tile's latency, which for up to 64 gene quads (4 a thread) the
+// CLE keeps below that floor.  Measured on a B200 (ms a step, register / tensor, 256 genes
+// at 5 %): CLE 0.012 / 0.025 at 1,000 and 4,000 cells, 0.062 / 0.050 at 20,000, with a
+// population 0.020 / 0.027 at 4,000 and 0.102 / 0.050 at 20,000; 400 genes at 5 %: CLE
+// 0.047 / 0.026 at 1,000 cells, with a population 0.063 / 0.022.
+bool scrna::auto_tensor(const scrna_net* net, bool tau, int64_t N) {
+    const NetDev& d = net->dev;
+    if (!register_path_holds(d)) return true;
+    if (tau) return net->G > 128;
+    const double density = (double)d.n_in / ((double)net->G * net->G);
+    if (net->G < 256 || density < 0.05) return false;
+    return d.n_quads > 64 || N >= 8192;
+}
+
 // Register-path kernel of a network: warp-per-cell-group (genes per lane, in-edges and
 // terms per gene) or block tiles.
 scrna::KernelChoice scrna::choose_kernel(const scrna_net* net, int path) {
@@ -641,7 +664,7 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
     const int64_t n_steps = n_steps_of(o);
     if (n_steps >= (1ll << 31)) return fail(SCRNA_EINVAL, "too many steps");
     const FusedLaunch L = fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads);
-    if (L.smem > 227 * 1024) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
+    if (L.smem > kMaxDynamicSmem) return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", L.smem);
     cudaStream_t s = ctx->stream;
     // kernel choice: the lane kernel for small networks, block tiles otherwise (or as tuned)
     const bool warp_ok = d.lane_in != nullptr;
@@ -655,7 +678,7 @@ static int run_fused(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, 
         kc.block = tau_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src,
                             tau_genes_per_unit(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, st->N));
         kc.smem = kc.block.smem;
-        if (kc.block.smem > 227 * 1024)
+        if (kc.block.smem > kMaxDynamicSmem)
             return fail(SCRNA_ENOTSUP, "network tables need %zu bytes of shared memory", kc.block.smem);
     }
     else if (int r = choose_kernel_tuned(ctx, net, kin, o, st, &kc, nullptr, nullptr, start == 0)) return r;
@@ -735,7 +758,9 @@ int scrna::resume_register_run(scrna_ctx* ctx, scrna_net* net, const scrna_kinet
     if (cap && !st->capture) return fail(SCRNA_EINVAL, "state was created without capture buffers");
     if (o->readout != st->readout) return fail(SCRNA_EINVAL, "readout differs from the state's readout");
     if (o->precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "continuations run the FP32 register path");
-    if (o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK &&
+    // (a tau-leap run of the tensor path continues on the register path, with the same counts)
+    const bool tensor_tau = tau && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY);
+    if (!tensor_tau && o->path != SCRNA_PATH_AUTO && o->path != SCRNA_PATH_REGISTER && o->path != SCRNA_PATH_BLOCK &&
         o->path != SCRNA_PATH_WARP)
         return fail(SCRNA_ENOTSUP, "continuations run the register path");
     const int64_t total = n_steps_of(o);
@@ -746,6 +771,7 @@ int scrna::resume_register_run(scrna_ctx* ctx, scrna_net* net, const scrna_kinet
     if (int r = ensure_gene_tables(net, kin, o->dt, pop != nullptr)) return r;
     if (int r = state_alloc(st, pop != nullptr, false)) return r;
     st->have_counts = cap != nullptr;
+    st->last_tensor = false;  // (a tensor-form tau-leap run left its state in the register layout)
     return run_fused(ctx, net, kin, pop, cap, o, st, tau, st->steps_done, st->epoch);
 }
 
@@ -821,13 +847,8 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
     if (int r = set_device(ctx)) return r;
     if (int r = ensure_gene_tables(net, kin, o->dt, pop != nullptr)) return r;
     // kernel family: tensor cores for large dense networks (or when asked), else the register path
-    const NetDev& nd = net->dev;
-    const double density = (double)nd.n_in / ((double)net->G * net->G);
-    // (the tau-leap takes the tensor path only when asked or when the register path cannot hold it)
     const bool tensor = !plain && (o->path == SCRNA_PATH_TENSOR || o->path == SCRNA_PATH_TENSOR_LIBRARY ||
-                                   (o->path == SCRNA_PATH_AUTO &&
-                                    (nd.n_quads > fused_max_quads() ||
-                                     (!tau && !pop && net->G >= 256 && density >= 0.05))));
+                                   (o->path == SCRNA_PATH_AUTO && auto_tensor(net, tau, N)));
     if (tensor) {
         st->has_register_state = false;
         st->have_counts = cap != nullptr;
@@ -838,7 +859,15 @@ static int run_device(scrna_ctx* ctx, const scrna_net* cnet, const scrna_kinetic
         if (tau || pop || o->path == SCRNA_PATH_TENSOR_LIBRARY || net->G > 4096) {
             st->last_tensor = true;
             st->last_tau = tau;
-            return tensor_run(ctx, net, kin, cap, o, st, dtype, tau, pop);
+            if (int r = tensor_run(ctx, net, kin, cap, o, st, dtype, tau, pop)) return r;
+            // an exact tau-leap state is the register path's: where that path holds the
+            // network, the state continues and checkpoints as one of its runs
+            if (tau && tau_tensor_exact(net, dtype) && register_path_holds(net->dev)) {
+                if (int r = tensor_state_to_register(ctx, st)) return r;
+                st->steps_done = n_steps_of(o);
+                st->has_register_state = true;
+            }
+            return SCRNA_OK;
         }
         st->last_tensor = false;  // the fused kernel keeps the register path's gene-major state
         st->last_cell_major = false;

@@ -102,6 +102,7 @@ struct scrna_net {
     int32_t t_dtype = -1;              // 0 bf16, 1 fp16
     int32_t t_n_src = 0;               // distinct genes read by cooperative/redundant edges
     DevBuf t_w16, t_na, t_na_src, t_src_gene, t_src_of_gene;
+    DevBuf t_slot_of_gene;             // gene -> regulator slot or -1 (the tau-leap's exact regulation)
     bool cache_valid = false;
     double c_dt = 0, c_kin[6] = {0};
     bool c_pop = false;
@@ -170,6 +171,14 @@ int state_relayout(scrna_ctx* ctx, scrna_state* st, bool to_cell_major);
 int resume_register_run(scrna_ctx* ctx, scrna_net* net, const scrna_kinetics* kin, const scrna_population* pop,
                         const scrna_capture* cap, const scrna_cle_opts* o, scrna_state* st, bool tau);
 int fused_max_quads();
+// The register path takes the network (gene count and shared-memory tables).
+bool register_path_holds(const NetDev& d);
+// The automatic path's choice of the tensor path for a network of N cells.
+bool auto_tensor(const scrna_net* net, bool tau, int64_t N);
+// The tau-leap's tensor form with the register path's exact FP32 regulation (no GEMM).
+bool tau_tensor_exact(const scrna_net* n, int dtype);
+// Copies a tensor-form tau-leap state into the register path's gene-major buffers.
+int tensor_state_to_register(scrna_ctx* ctx, scrna_state* st);
 cudaError_t fused_queue_launch(const FusedArgs* args, const TileWork* items, int n_items, int* counter, int upt,
                                int nw, size_t smem, bool pop, int grid, TileCtl shared_ctl, int use_shared,
                                cudaStream_t st);

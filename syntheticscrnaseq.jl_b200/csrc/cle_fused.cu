@@ -35,6 +35,13 @@ FusedLaunch fused_plan(int G, int n_reg, int n_in, int n_na, int n_na_src, int n
 
 int fused_max_quads() { return 8 * 16; }
 
+// Whether the register path can run a network: at most 512 genes and its tables (in gene
+// quads, the smallest layout of every kernel of the path) within a block's shared memory.
+bool register_path_holds(const NetDev& d) {
+    return d.n_quads <= fused_max_quads() &&
+           fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads).smem <= kMaxDynamicSmem;
+}
+
 cudaError_t fused_launch(const FusedArgs& a, const FusedLaunch& L, bool pop, cudaStream_t st) {
     switch (L.upt * 2 + (pop ? 1 : 0)) {
         case 2: return fused_launch_t<1, false, false>(a, L.nw, L.smem, st);
@@ -168,6 +175,9 @@ int tau_genes_per_unit(int G, int n_reg, int n_in, int n_na, int n_na_src, int64
     }
     const FusedLaunch one = tau_plan(G, n_reg, n_in, n_na, n_na_src, 1);
     const FusedLaunch two = tau_plan(G, n_reg, n_in, n_na, n_na_src, 2);
+    // larger units where the tables, with one telegraph-flag byte per unit, outgrow shared memory
+    if (two.smem > kMaxDynamicSmem) return 4;
+    if (one.smem > kMaxDynamicSmem) return two.qg;
     if (one.qg != 1) return two.qg;  // too many genes for single-gene units
     if (one.nw > two.nw) return 1;
     int dev = 0, sms = 148;

@@ -1,6 +1,7 @@
 // Internal structures shared by the host side of the library (capi.cu) and the
 // kernels.  Not part of the public ABI.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 
 namespace scrna {
@@ -40,6 +41,7 @@ struct NonAdd {
 constexpr int kLaneEdges = 8;  // in-edges per gene (additive + terms)
 constexpr int kLaneTerms = 2;  // terms evaluated per lane
 constexpr int kLaneSrc = 3;    // sources per term
+constexpr size_t kMaxDynamicSmem = 227 * 1024;  // opt-in shared memory of one block (sm_100a)
 struct LaneTerm {
     float coef;
     int32_t kind;

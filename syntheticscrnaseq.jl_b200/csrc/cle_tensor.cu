@@ -58,6 +58,11 @@ struct TensorArgs {
     const float* act32_cur;  // [n_src][N]: source-major, 32 cells of a warp in one 128-byte row piece
     float* act32_next;
     float p_dec_m, p_dec_p;  // binomial tau-leap: decay probabilities 1 - exp(-mu dt)
+    // exact regulation (the tau-leap): reg holds the register path's FP32 regulation, cneg
+    // included, from the slot-major activations act32 [n_reg][N] (src_of_gene: the slots)
+    int32_t exact_reg;
+    const float2* in_edge;   // the register path's additive in-edges {w, slot bits}
+    const int32_t* na_slot;  // the register path's term sources (regulator slots)
     // population (cle.jl:143-284, ext:409-529, tau-leap ext:531-663); V == nullptr without one.
     // The daughter buffers are cell-major [N][ld] like the state.
     double* V;               // [N] volume at the start of the step
@@ -309,6 +314,60 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
     }
 }
 
+// Exact regulation of the tau-leap's cell-major form: reg[c][g] in FP32 with the register
+// path's operations in its order (the regulation of cle_fused.cuh: the repression constant,
+// the additive in-edges in table order, then the cooperative and redundant terms), from the
+// slot-major activations of the step's start, so the counts equal the register path's bit for
+// bit.  Block: 32 cells (the lanes) x 64 genes (8 warps, 8 genes each); the activations of a
+// lane's cell are one 128-byte row piece per slot, each edge a broadcast load.  The block's
+// results go through shared memory so the stores run along genes.
+constexpr int kExactCells = 32, kExactGenes = 64, kExactThreads = 256;
+
+__global__ void __launch_bounds__(kExactThreads) tensor_exact_reg_kernel(const TensorArgs a) {
+    __shared__ float s_out[kExactCells][kExactGenes + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t c0 = (int64_t)blockIdx.x * kExactCells;
+    const int g0 = blockIdx.y * kExactGenes;
+    const int64_t c = c0 + lane;
+    const bool live = c < a.N;
+    const float* act = a.act32_cur + (live ? c : 0);
+    const size_t N = (size_t)a.N;
+#pragma unroll 1
+    for (int j = 0; j < kExactGenes / 8; ++j) {
+        const int gi = warp + 8 * j;
+        const int g = g0 + gi;
+        float reg = 0.0f;
+        if (g < a.G && live) {
+            const GeneRec gr = a.genes[g];
+            reg = gr.cneg;
+            for (int e = gr.in_begin; e < gr.in_end; ++e) {
+                const float2 ed = __ldg(a.in_edge + e);
+                reg = fmaf(ed.x, act[(size_t)__float_as_int(ed.y) * N], reg);
+            }
+            const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
+            for (int e = nab; e < nab + nac; ++e) {
+                const NonAdd na = a.na[e];
+                float prod = 1.0f;
+                if (na.kind == 0) {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[(size_t)__ldg(a.na_slot + t) * N];
+                    reg = fmaf(na.coef, prod, reg);
+                } else {
+                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[(size_t)__ldg(a.na_slot + t) * N];
+                    reg = fmaf(na.coef, 1.0f - prod, reg);
+                }
+            }
+        }
+        s_out[lane][gi] = reg;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kExactCells * kExactGenes; i += kExactThreads) {
+        const int r = i / kExactGenes, gi = i - r * kExactGenes;
+        const int64_t cc = c0 + r;
+        const int g = g0 + gi;
+        if (cc < a.N && g < a.ld) a.reg[(size_t)cc * a.ld + g] = s_out[r][gi];
+    }
+}
+
 // One binomial tau-leap step after the GEMM (ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks
 // of any size), on tiles of 32 cells x 16 gene pairs.  The draws are bound by latency and warp
 // divergence, not by HBM: a warp's lanes are the 32 cells of one gene pair, whose Poisson means
@@ -374,8 +433,11 @@ __global__ void __launch_bounds__(kTauTileThreads) tensor_tau_step_kernel(const 
         w[0] = philox_rk(gcell, (uint32_t)s, (uint32_t)g0, c3, a.rk0, a.rk1);
         w[1] = has1 ? philox_rk(gcell, (uint32_t)s, (uint32_t)(g0 + 1), c3, a.rk0, a.rk1) : make_uint4(0u, 0u, 0u, 0u);
         const float2 rg = s_reg[r][q];
-        float tx0 = fmaxf(__fadd_rn(__fadd_rn(rg.x, r0.cneg), r0.beta), 0.0f);
-        float tx1 = fmaxf(__fadd_rn(__fadd_rn(rg.y, r1.cneg), r1.beta), 0.0f);
+        // the GEMM's sum takes the repression constant afterwards; the exact form holds it
+        const float reg0 = a.exact_reg ? rg.x : __fadd_rn(rg.x, r0.cneg);
+        const float reg1 = a.exact_reg ? rg.y : __fadd_rn(rg.y, r1.cneg);
+        float tx0 = fmaxf(__fadd_rn(reg0, r0.beta), 0.0f);
+        float tx1 = fmaxf(__fadd_rn(reg1, r1.beta), 0.0f);
         if (a.V) {
             tx0 = __fmul_rn(tx0, Vf);
             tx1 = __fmul_rn(tx1, Vf);
@@ -437,7 +499,7 @@ __global__ void __launch_bounds__(kTauTileThreads) tensor_tau_step_kernel(const 
         const size_t e = (size_t)cc * rs + k;
         reinterpret_cast<float2*>(a.M)[e] = s_m[rr][q];
         reinterpret_cast<float2*>(a.P)[e] = s_p[rr][q];
-        reinterpret_cast<T2*>(a.act16)[(size_t)cc * (a.Kp >> 1) + k] = s_act[rr][q];
+        if (!a.exact_reg) reinterpret_cast<T2*>(a.act16)[(size_t)cc * (a.Kp >> 1) + k] = s_act[rr][q];
         if (BURSTY && s_sw[rr][q]) {
             reinterpret_cast<uchar2*>(a.prom)[e] = s_on[rr][q];
             reinterpret_cast<int4*>(a.NS)[e] = s_ns[rr][q];
@@ -552,6 +614,56 @@ __global__ void tensor_replace_kernel(const TensorArgs a) {
     if (src_idx >= 0) a.act32_next[(size_t)src_idx * a.N + c] = act;
 }
 
+// The tau-leap's cell-major state [N][ld] into the register path's gene-major [G][N] (counts,
+// promoters, switching times), through shared-memory tiles of 32 cells x 32 genes so both
+// sides run along their rows.  With exact regulation both forms hold the same state bit for
+// bit, so a continuation or a checkpoint takes it as the register path's own.
+__global__ void tensor_to_gene_major_kernel(int G, int ld, int64_t N, const float* __restrict__ tM,
+                                            const float* __restrict__ tP, const uint8_t* __restrict__ tprom,
+                                            const int2* __restrict__ tNS, float* M, float* P, uint8_t* prom, int2* NS) {
+    __shared__ float sm[32][33], sp[32][33];
+    __shared__ int2 sns[32][33];
+    __shared__ uint8_t spr[32][33];
+    const int64_t c0 = (int64_t)blockIdx.x * 32;
+    const int g0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {  // row r: cell c0 + r, lanes along genes
+        const int64_t c = c0 + r;
+        const int g = g0 + tx;
+        if (c < N && g < G) {
+            const size_t e = (size_t)c * ld + g;
+            sm[r][tx] = tM[e];
+            sp[r][tx] = tP[e];
+            spr[r][tx] = tprom[e];
+            sns[r][tx] = tNS[e];
+        }
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // row r: gene g0 + r, lanes along cells
+        const int g = g0 + r;
+        const int64_t c = c0 + tx;
+        if (c < N && g < G) {
+            const size_t e = (size_t)g * N + c;
+            M[e] = sm[tx][r];
+            P[e] = sp[tx][r];
+            prom[e] = spr[tx][r];
+            NS[e] = sns[tx][r];
+        }
+    }
+}
+
+int tensor_state_to_register(scrna_ctx* ctx, scrna_state* st) {
+    if (int r = state_alloc(st, st->last_pop, false)) return r;
+    const dim3 grid((unsigned)((st->N + 31) / 32), (unsigned)((st->G + 31) / 32));
+    tensor_to_gene_major_kernel<<<grid, dim3(32, 8), 0, ctx->stream>>>(
+        st->G, st->t_ld, st->N, st->tM.as<float>(), st->tP.as<float>(), st->tprom.as<uint8_t>(), st->tNS.as<int2>(),
+        st->M.as<float>(), st->P.as<float>(), st->prom.as<uint8_t>(), st->NS.as<int2>());
+    CU(cudaGetLastError());
+    ctx->launches++;
+    st->last_cell_major = false;
+    return SCRNA_OK;
+}
+
 // Readout: cell-major FP32 state -> cells x G (x2) column-major Float64, through a
 // shared-memory tile so both the reads and the writes are coalesced.
 // With V (a tau-leap population) the readout is the concentrations M / V, P / V (ext:654-661).
@@ -649,6 +761,10 @@ int tensor_prepare_net(scrna_net* n, int dtype) {
     CU(n->t_src_of_gene.ensure((size_t)G * 4));
     CU(cudaMemcpy(n->t_src_of_gene.p, src_of_gene.data(), (size_t)G * 4, cudaMemcpyHostToDevice));
     n->ctx->h2d_bytes += (int64_t)(w.size() * 4 + na_src.size() * 4 + (size_t)G * 4);
+    std::vector<int32_t> slot_of_gene(n->reg_slot.begin(), n->reg_slot.end());
+    CU(n->t_slot_of_gene.ensure((size_t)G * 4));
+    CU(cudaMemcpy(n->t_slot_of_gene.p, slot_of_gene.data(), (size_t)G * 4, cudaMemcpyHostToDevice));
+    n->ctx->h2d_bytes += (int64_t)G * 4;
     n->t_kp = Kp;
     n->t_n_src = (int)src_gene.size();
     n->t_dtype = dtype;
@@ -706,10 +822,23 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
 
 int64_t run_steps(const scrna_cle_opts* o);
 
+// Whether the tau-leap's tensor form takes the exact FP32 regulation (the register path's
+// counts bit for bit) or the 16-bit GEMM: exact at FP32 precision (dtype 0), the FP16 GEMM
+// when FP16 inputs were asked for; SCRNA_TAU_TENSOR_EXACT=0 or 1 forces one.  On a B200 the
+// GEMM form is 1.3-1.5x faster on networks of >= 5 % density (ms a step at 20,000 cells, exact
+// / GEMM: 300 genes at 10 % 0.251 / 0.195, 500 genes at 10 % 0.551 / 0.370) and no faster
+// on sparse ones (300 sampled genes 0.124 / 0.155).
+bool tau_tensor_exact(const scrna_net* n, int dtype) {
+    (void)n;
+    if (const char* e = std::getenv("SCRNA_TAU_TENSOR_EXACT")) return std::atoi(e) != 0;
+    return dtype == 0;
+}
+
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
                const scrna_cle_opts* o, scrna_state* st, int dtype, bool tau, const scrna_population* pop) {
     if (int r = tensor_prepare_net(n, dtype)) return r;
-    const int G = n->G, Kp = n->t_kp, n_src = n->t_n_src, ld = tensor_ld(G);
+    const bool exact = tau && tau_tensor_exact(n, dtype);
+    const int G = n->G, Kp = n->t_kp, n_src = exact ? n->dev.n_reg : n->t_n_src, ld = tensor_ld(G);
     const int64_t N = st->N;
     const size_t gn = (size_t)G * N, ln = (size_t)ld * N;
     CU(st->tM.ensure(ln * 4));
@@ -750,7 +879,10 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.ginit = n->b_ginit.as<GeneInit>();
     a.na = n->dev.na;
     a.na_src = n->t_na_src.as<int32_t>();
-    a.src_of_gene = n->t_src_of_gene.as<int32_t>();
+    a.src_of_gene = exact ? n->t_slot_of_gene.as<int32_t>() : n->t_src_of_gene.as<int32_t>();
+    a.exact_reg = exact ? 1 : 0;
+    a.in_edge = n->dev.in_edge;
+    a.na_slot = n->dev.na_src;
     a.n_terms = (int)n->na.size();
     a.reg = st->treg.as<float>();
     a.M = st->tM.as<float>(); a.P = st->tP.as<float>();
@@ -791,7 +923,9 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     ctx->launches++;
 
     LtGemm gemm;
-    if (int r = lt_setup(ctx, gemm, dtype, G, ld, Kp, N)) return r;
+    if (!exact)
+        if (int r = lt_setup(ctx, gemm, dtype, G, ld, Kp, N)) return r;
+    const dim3 g_exact((unsigned)((N + kExactCells - 1) / kExactCells), (unsigned)((ld + kExactGenes - 1) / kExactGenes));
     const float alpha = 1.0f, beta = 0.0f;
     const int64_t n_steps = run_steps(o);
     const int pairs = ld / 2;
@@ -822,14 +956,20 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         a.step = (int)step;
         a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
         a.act32_next = st->tact32[step & 1].as<float>();
-        if (a.n_terms > 0) {  // term columns from the previous step's activations
-            CU(terms_launch(dtype, a, s));
+        if (exact) {  // the register path's FP32 regulation instead of the terms and the GEMM
+            tensor_exact_reg_kernel<<<g_exact, kExactThreads, 0, s>>>(a);
+            CU(cudaGetLastError());
             ctx->launches += 1;
+        } else {
+            if (a.n_terms > 0) {  // term columns from the previous step's activations
+                CU(terms_launch(dtype, a, s));
+                ctx->launches += 1;
+            }
+            cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,
+                                                st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
+                                                &gemm.algo, ctx->lt_workspace.p, ctx->lt_workspace.n, s);
+            if (stt != CUBLAS_STATUS_SUCCESS) return lt_fail(stt, "cublasLtMatmul");
         }
-        cublasStatus_t stt = cublasLtMatmul((cublasLtHandle_t)ctx->lt_handle, gemm.op, &alpha, n->t_w16.p, gemm.la,
-                                            st->tact16.p, gemm.lb, &beta, st->treg.p, gemm.lc, st->treg.p, gemm.lc,
-                                            &gemm.algo, ctx->lt_workspace.p, ctx->lt_workspace.n, s);
-        if (stt != CUBLAS_STATUS_SUCCESS) return lt_fail(stt, "cublasLtMatmul");
         step_fn<<<g_step, step_threads, 0, s>>>(a);
         CU(cudaGetLastError());
         ctx->launches += 1;  // the library GEMM is not counted as this library's kernel
@@ -848,6 +988,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
             }
         }
     }
+    st->epoch = pop ? a.epoch : 0;
     dim3 rgrid((unsigned)((N + 31) / 32), (unsigned)((G + 31) / 32));
     tensor_readout_kernel<<<rgrid, dim3(32, 8), 0, s>>>(G, ld, N, st->tM.as<float>(), st->tP.as<float>(), st->readout,
                                                         st->out.as<double>(), pop && tau ? a.V : nullptr);

@@ -377,7 +377,8 @@ extern "C" int scrna_submit(scrna_server* s, const scrna_request* q, uint64_t* t
     if (int r = validate_run(q->net, &q->kin, nullptr, cap, &q->opts)) return r;
     if (q->opts.precision != SCRNA_PRECISION_FP32) return fail(SCRNA_ENOTSUP, "the server runs the FP32 path");
     const scrna_net* n = q->net;
-    if (n->dev.n_quads > fused_max_quads()) return fail(SCRNA_ENOTSUP, "the server runs register-path networks (G <= 512)");
+    if (!register_path_holds(n->dev))
+        return fail(SCRNA_ENOTSUP, "the server runs register-path networks (G <= 512, tables within shared memory)");
     if (q->opts.cell_num <= 0) return fail(SCRNA_EINVAL, "cell_num must be positive");
     if (q->opts.cell_offset < 0 || q->opts.cell_offset + q->opts.cell_num > (1ll << 32)) return fail(SCRNA_EINVAL, "cell indices must fit 32 bits");
     auto* r = new SrvRequest();

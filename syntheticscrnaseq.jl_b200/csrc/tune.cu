@@ -248,8 +248,7 @@ KernelChoice choice_from(const scrna_net* net, const scrna_tune_choice& c) {
 static std::vector<scrna_tune_choice> candidates(const scrna_net* net, int path) {
     const NetDev& d = net->dev;
     std::vector<scrna_tune_choice> out;
-    const bool block_ok = path != SCRNA_PATH_WARP && d.n_quads <= fused_max_quads() &&
-                          fused_plan(d.G, d.n_reg, d.n_in, d.n_na, d.n_na_src, d.n_quads).smem <= 227 * 1024;
+    const bool block_ok = path != SCRNA_PATH_WARP && register_path_holds(d);
     if (block_ok) out.push_back(scrna_tune_choice{0, 0, 0, 0, 0.0});
     if (d.lane_in && path != SCRNA_PATH_BLOCK)
         for (int gpl : {2, 4}) {

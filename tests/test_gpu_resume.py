@@ -94,3 +94,28 @@ def test_tensor_path_state_is_not_resumable(pkg):
         run.checkpoint()
     assert np.array_equal(run.read(), X)
     run.close()
+
+
+@pytest.mark.parametrize("population", [False, True])
+def test_tauleap_tensor_form_resumes_and_checkpoints(pkg, population):
+    """A tau-leap run of 300 genes, which the automatic path runs on the tensor form, leaves
+    the register path's state: it continues there, directly and through a checkpoint, bit for
+    bit one run of the total length."""
+    net = pkg.sample_network(300, seed=7, bursty=True)
+    kin = pkg.WORKLOAD_KINETICS
+    pop = pkg.PopulationConfig(cell_num=300, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
+    kw = dict(cell_num=300, readout="both", seed=5, population=pop if population else None)
+    alg = pkg.BinomialTauLeap(0.01)
+    full, part = _pair(pkg, net, alg, kin, 0.55, 1.2, **kw)
+    _same(full, part, population)
+    first = pkg.DeviceRun(net, alg, kin, T=0.55, path="tensor", **kw)
+    first.launch()
+    data = first.checkpoint()
+    second = pkg.DeviceRun(net, alg, kin, T=0.55, **kw)
+    second.restore(data)
+    second.resume(T=1.2)
+    _same(full, second, population)
+    first.resume(T=1.2)  # asked of the tensor path: continues on the register path
+    _same(full, first, population)
+    for r in (full, part, first, second):
+        r.close()

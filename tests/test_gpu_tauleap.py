@@ -11,6 +11,8 @@ The kernel draws a thread unit's Poisson counts either in lock step or one after
 (SCRNA_TAU_LOCKSTEP=1 / 0 forces one; lock step by default), for units of gene pairs or
 quads or single genes (SCRNA_TAU_GENES_PER_THREAD=2 / 4 / 1; pairs by default): every combination gives the same
 bits, so the bit-exact cases run under several.
+Beyond 128 genes the automatic path runs the tau-leap's tensor form, whose FP32 regulation
+follows the register path's operations, so its counts are the register path's bit for bit.
 Statistical pins of the reference: test/test_analytical_moments.jl:85-96 (means within 3 %,
 variance and Fano within 15 % of the exact two-stage moments) and test/test_gpu_parity.jl:32-42.
 """
@@ -97,10 +99,36 @@ def test_schedules_equal_on_regulated_network(pkg, monkeypatch, G):
         monkeypatch.setenv("SCRNA_TAU_LOCKSTEP", mode)
         monkeypatch.setenv("SCRNA_TAU_GENES_PER_THREAD", unit)
         outs.append(_tau_run(pkg, net, kin, cell_num=700, T=0.0, n_steps=250, seed=3, readout="both", dt=0.01,
-                             population=pop).read_raw())
+                             population=pop, path="register").read_raw())
     for o in outs[1:]:
         for k in ("M", "P", "prom", "V"):
             assert np.array_equal(outs[0][k], o[k]), k
+
+
+@pytest.mark.parametrize("kind,G", [("sampled", 129), ("sampled", 300), ("dense", 300)])
+def test_tensor_form_equals_register_path(pkg, kind, G):
+    """The tau-leap's tensor form (regulation in FP32 with the register path's operations in
+    its order, state cell-major in HBM, gene pairs in lock step) against the register path on
+    regulated networks: counts, promoters and volumes bit for bit, with and without a
+    population.  The automatic path takes the tensor form beyond 128 genes, so its results
+    are the register path's as well."""
+    if kind == "sampled":
+        net = pkg.sample_network(G, seed=G, bursty=True)
+    else:
+        net = pkg.dense_network(G, seed=G, density=0.1, n_coop=4, n_redun=4)
+    kin = pkg.WORKLOAD_KINETICS
+    pop = pkg.PopulationConfig(cell_num=500, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
+    for population in (None, pop):
+        outs = [_tau_run(pkg, net, kin, cell_num=500, T=0.0, n_steps=120, seed=3, readout="both", dt=0.01,
+                         population=population, path=path) for path in ("register", "tensor", "auto")]
+        raws = [r.read_raw() for r in outs]
+        Xs = [r.read() for r in outs]
+        for r in outs:
+            r.close()
+        for k in ("M", "P", "prom") + (("V",) if population else ()):
+            assert np.array_equal(raws[0][k], raws[1][k]), (population is not None, k)
+            assert np.array_equal(raws[0][k], raws[2][k]), (population is not None, k)
+        assert np.array_equal(Xs[0], Xs[1]) and np.array_equal(Xs[0], Xs[2])
 
 
 def test_means_outside_the_quotient_range_bit_exact(pkg, orc, schedule):

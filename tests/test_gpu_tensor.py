@@ -83,6 +83,26 @@ def test_auto_picks_tensor_for_large_dense(pkg):
     assert np.array_equal(a, b)
 
 
+def test_auto_routing_of_dense_networks(pkg):
+    """The automatic path on networks of >= 256 genes at >= 5 % density (here 10 %): the
+    tau-leap and populations run on the tensor path (the library-GEMM variant, their tensor
+    form); the CLE of 256 genes (64 gene quads) stays on the register path below 8,192 cells
+    and moves to the tensor path from there on."""
+    kin = pkg.WORKLOAD_KINETICS
+    net = _dense(pkg, 400, seed=4, density=0.1)
+    pop = pkg.PopulationConfig(cell_num=300, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0), div_check_interval=10)
+    for alg, population in ((pkg.BinomialTauLeap(0.01), None), (pkg.BinomialTauLeap(0.01), pop), (pkg.CLE(0.01), pop)):
+        kw = dict(cell_num=300, T=0.2, readout="both", seed=3, population=population)
+        a = pkg.simulate(net, alg, kin, **kw)
+        b = pkg.simulate(net, alg, kin, path="tensor_library", **kw)
+        assert np.array_equal(a, b), (type(alg).__name__, population is not None)
+    net = _dense(pkg, 256, seed=5, density=0.1)
+    for N, path in ((1000, "register"), (8192, "tensor")):
+        a = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=0.05, readout="both", seed=1)
+        b = pkg.simulate(net, pkg.CLE(0.01), kin, cell_num=N, T=0.05, readout="both", seed=1, path=path)
+        assert np.array_equal(a, b), N
+
+
 @pytest.mark.parametrize("G,N,bursty", [(300, 333, False), (520, 700, True)])
 def test_fused_matches_library_gemm_path(pkg, G, N, bursty):
     """Ragged tiles (G not a multiple of 256, N not of 128): the fused tcgen05 kernel and the
