@@ -57,7 +57,9 @@ enum scrna_precision {
 
 /* Kernel family for the FP32 precision.  AUTO picks the register path for sparse
  * networks (the lane-per-gene-unit kernel when the network fits it, G <= 512, block tiles
- * otherwise) and the tensor-core path for large dense ones.  BLOCK and WARP force one
+ * otherwise) and the tensor-core path for dense ones (>= 5 % of the G x G edges over >= 256
+ * genes; at up to 256 genes from 8,192 cells) and for networks the register path cannot hold
+ * (more than 512 genes, or tables beyond shared memory).  BLOCK and WARP force one
  * register-path kernel (both give identical results).  TENSOR is the fused tcgen05
  * contraction + Euler step; TENSOR_LIBRARY the same step with the contraction done by a
  * library GEMM (cuBLASLt) and a separate update kernel, kept for comparison. */
@@ -184,10 +186,14 @@ int scrna_cle_simulate_batch(scrna_ctx* ctx, int32_t B, const scrna_net* const* 
  * With a population: Hill of the concentration P / V, transcription x V, decay without
  * dilution, initial counts max(1, round(steady state x V)), and the readout is M / V, P / V
  * (capture counts are drawn from the molecule counts).  Paths: the block-tile register kernel
- * up to 512 genes; beyond that, or with opts->path TENSOR or TENSOR_LIBRARY, the tensor path's
- * library-GEMM variant (populations included; without regulation its counts equal the register
- * path's); SCRNA_PATH_WARP is rejected.  FP32 counts; SCRNA_PRECISION_FP32_F16 selects FP16
- * instead of BF16 contraction inputs on the tensor path. */
+ * (REGISTER, BLOCK; up to 512 genes with its tables within shared memory) or the tensor form
+ * (TENSOR, TENSOR_LIBRARY; any G, populations included): the state cell-major in device memory
+ * and the draws over gene pairs; SCRNA_PATH_WARP is rejected.  At SCRNA_PRECISION_FP32 the
+ * tensor form's regulation is the register path's FP32 arithmetic for every network that path
+ * holds (and sparse ones beyond it), so both give the same counts bit for bit; AUTO takes the
+ * tensor form beyond 128 genes (where it is faster) or when the register path cannot hold the
+ * network.  Dense networks beyond the register path take the regulation from a BF16 GEMM, and
+ * SCRNA_PRECISION_FP32_F16 from an FP16 GEMM. */
 int scrna_tauleap_simulate(scrna_ctx* ctx, const scrna_net* net, const scrna_kinetics* kin,
                            const scrna_population* pop, const scrna_capture* cap,
                            const scrna_cle_opts* opts, double* out, int32_t* counts,
@@ -294,6 +300,9 @@ int scrna_state_write_mtx(scrna_ctx* ctx, scrna_state* st, const char* dir, cons
  * A run of the register path (CLE or tau-leap) is a pure function of its inputs and of
  * increments keyed by (seed, stream, cell, step, gene), and its state is exact between
  * launches, so a run continued from step T1 to T2 equals one run of T2 steps bit for bit.
+ * A tau-leap run of the tensor form at FP32 precision leaves the same state (for networks the
+ * register path holds), so it continues and checkpoints the same way; other tensor-path runs
+ * keep no state to continue.
  * The reference's nearest counterpart returns the final population state for inspection
  * (simulate_with_state, src/algorithms/tauleap_binomial.jl:270-324).
  * scrna_cle_resume / scrna_tauleap_resume: continue the run `st` holds (from a run on this

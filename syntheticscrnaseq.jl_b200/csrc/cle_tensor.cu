@@ -368,15 +368,16 @@ __global__ void __launch_bounds__(kExactThreads) tensor_exact_reg_kernel(const T
     }
 }
 
-// One binomial tau-leap step after the GEMM (ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks
-// of any size), on tiles of 32 cells x 16 gene pairs.  The draws are bound by latency and warp
+// One binomial tau-leap step after the regulation (the exact kernel above, or the GEMM with
+// FP16 inputs; ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks of any size), on tiles of
+// 32 cells x 16 gene pairs.  The draws are bound by latency and warp
 // divergence, not by HBM: a warp's lanes are the 32 cells of one gene pair, whose Poisson means
 // are alike (lanes over different genes would wait for the gene with the longest chains).  The
 // tile moves between the cell-major state and shared memory along gene pairs (coalesced), and
 // the compute reads it along cells.  Per (cell, gene): the tau-leap's Philox block (tag 9),
 // switching from its spare bits, and the pair's draws in lock step (tau_update_unit, the
-// register path's arithmetic); without regulation the GEMM gives exactly 0, so the counts equal
-// the register path's and the oracle's bit for bit.
+// register path's arithmetic); with the exact regulation the counts equal the register path's
+// bit for bit, and without regulation (the GEMM then gives exactly 0) the oracle's as well.
 constexpr int kTauTileCells = 32, kTauTilePairs = 16, kTauTileThreads = 256;
 
 template <class T, bool BURSTY, int HN>
@@ -823,15 +824,19 @@ static int lt_setup(scrna_ctx* ctx, LtGemm& g, int dtype, int G, int ld, int Kp,
 int64_t run_steps(const scrna_cle_opts* o);
 
 // Whether the tau-leap's tensor form takes the exact FP32 regulation (the register path's
-// counts bit for bit) or the 16-bit GEMM: exact at FP32 precision (dtype 0), the FP16 GEMM
-// when FP16 inputs were asked for; SCRNA_TAU_TENSOR_EXACT=0 or 1 forces one.  On a B200 the
-// GEMM form is 1.3-1.5x faster on networks of >= 5 % density (ms a step at 20,000 cells, exact
-// / GEMM: 300 genes at 10 % 0.251 / 0.195, 500 genes at 10 % 0.551 / 0.370) and no faster
-// on sparse ones (300 sampled genes 0.124 / 0.155).
+// counts bit for bit) or the 16-bit GEMM (SCRNA_TAU_TENSOR_EXACT=0 or 1 forces one).  At FP32
+// precision: exact for every network the register path holds, so the tau-leap's counts are the
+// same on either path, and beyond it for sparse networks (at most 8 edge reads a gene); the
+// BF16 GEMM for dense networks beyond it, as the CLE.  FP16 inputs: the FP16 GEMM.  Each edge
+// of the exact form is one load of a 32-cell activation row, which once a tile's rows outgrow
+// L1 come from L2.  ms a step on a B200, exact / GEMM: 300 sampled genes x 20,000 cells
+// 0.124 / 0.155; 300 genes at 10 % 0.251 / 0.195; 600 genes at 10 % 0.577 / 0.254; 2,000
+// genes at 2 % x 65,536 cells 6.96 / 2.52, at 10 % 23.8 / 3.63.
 bool tau_tensor_exact(const scrna_net* n, int dtype) {
-    (void)n;
     if (const char* e = std::getenv("SCRNA_TAU_TENSOR_EXACT")) return std::atoi(e) != 0;
-    return dtype == 0;
+    if (dtype != 0) return false;
+    if (register_path_holds(n->dev)) return true;
+    return (int64_t)n->dev.n_in + n->dev.n_na_src <= 8ll * n->G;
 }
 
 int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const scrna_capture* cap,
