@@ -314,63 +314,37 @@ __global__ void __launch_bounds__(kTensorPairsPerBlock) tensor_step_kernel(const
     }
 }
 
-// Exact regulation of the tau-leap's cell-major form: reg[c][g] in FP32 with the register
-// path's operations in its order (the regulation of cle_fused.cuh: the repression constant,
-// the additive in-edges in table order, then the cooperative and redundant terms), from the
-// slot-major activations of the step's start, so the counts equal the register path's bit for
-// bit.  Block: 32 cells (the lanes) x 64 genes (8 warps, 8 genes each); the activations of a
-// lane's cell are one 128-byte row piece per slot, each edge a broadcast load.  The block's
-// results go through shared memory so the stores run along genes.
-constexpr int kExactCells = 32, kExactGenes = 64, kExactThreads = 256;
-
-__global__ void __launch_bounds__(kExactThreads) tensor_exact_reg_kernel(const TensorArgs a) {
-    __shared__ float s_out[kExactCells][kExactGenes + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t c0 = (int64_t)blockIdx.x * kExactCells;
-    const int g0 = blockIdx.y * kExactGenes;
-    const int64_t c = c0 + lane;
-    const bool live = c < a.N;
-    const float* act = a.act32_cur + (live ? c : 0);
+// Exact regulation of the tau-leap's tensor form: the regulation of gene `gr` in one cell in
+// FP32 with the register path's operations in its order (the regulation of cle_fused.cuh: the
+// repression constant, the additive in-edges in table order, then the cooperative and
+// redundant terms), from the slot-major activations of the step's start (`act`: the cell's
+// element of slot 0; lanes over consecutive cells read one 128-byte row piece per slot, each
+// edge a broadcast load), so the counts equal the register path's bit for bit.
+__device__ __forceinline__ float exact_regulation(const TensorArgs& a, const GeneRec& gr, const float* act) {
     const size_t N = (size_t)a.N;
-#pragma unroll 1
-    for (int j = 0; j < kExactGenes / 8; ++j) {
-        const int gi = warp + 8 * j;
-        const int g = g0 + gi;
-        float reg = 0.0f;
-        if (g < a.G && live) {
-            const GeneRec gr = a.genes[g];
-            reg = gr.cneg;
-            for (int e = gr.in_begin; e < gr.in_end; ++e) {
-                const float2 ed = __ldg(a.in_edge + e);
-                reg = fmaf(ed.x, act[(size_t)__float_as_int(ed.y) * N], reg);
-            }
-            const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
-            for (int e = nab; e < nab + nac; ++e) {
-                const NonAdd na = a.na[e];
-                float prod = 1.0f;
-                if (na.kind == 0) {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[(size_t)__ldg(a.na_slot + t) * N];
-                    reg = fmaf(na.coef, prod, reg);
-                } else {
-                    for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[(size_t)__ldg(a.na_slot + t) * N];
-                    reg = fmaf(na.coef, 1.0f - prod, reg);
-                }
-            }
+    float reg = gr.cneg;
+    for (int e = gr.in_begin; e < gr.in_end; ++e) {
+        const float2 ed = __ldg(a.in_edge + e);
+        reg = fmaf(ed.x, act[(size_t)__float_as_int(ed.y) * N], reg);
+    }
+    const int nab = gr.na_range >> 16, nac = gr.na_range & 0xFFFF;
+    for (int e = nab; e < nab + nac; ++e) {
+        const NonAdd na = a.na[e];
+        float prod = 1.0f;
+        if (na.kind == 0) {
+            for (int t = na.src_begin; t < na.src_end; ++t) prod *= act[(size_t)__ldg(a.na_slot + t) * N];
+            reg = fmaf(na.coef, prod, reg);
+        } else {
+            for (int t = na.src_begin; t < na.src_end; ++t) prod *= 1.0f - act[(size_t)__ldg(a.na_slot + t) * N];
+            reg = fmaf(na.coef, 1.0f - prod, reg);
         }
-        s_out[lane][gi] = reg;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kExactCells * kExactGenes; i += kExactThreads) {
-        const int r = i / kExactGenes, gi = i - r * kExactGenes;
-        const int64_t cc = c0 + r;
-        const int g = g0 + gi;
-        if (cc < a.N && g < a.ld) a.reg[(size_t)cc * a.ld + g] = s_out[r][gi];
-    }
+    return reg;
 }
 
-// One binomial tau-leap step after the regulation (the exact kernel above, or the GEMM with
-// FP16 inputs; ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks of any size), on tiles of
-// 32 cells x 16 gene pairs.  The draws are bound by latency and warp
+// One binomial tau-leap step, with the regulation computed here (exact_regulation above) or
+// taken from the GEMM (ext/SyntheticscRNAseqCUDAExt.jl:215-399 for networks of any size), on
+// tiles of 32 cells x 16 gene pairs.  The draws are bound by latency and warp
 // divergence, not by HBM: a warp's lanes are the 32 cells of one gene pair, whose Poisson means
 // are alike (lanes over different genes would wait for the gene with the longest chains).  The
 // tile moves between the cell-major state and shared memory along gene pairs (coalesced), and
@@ -401,7 +375,7 @@ __global__ void __launch_bounds__(kTauTileThreads) tensor_tau_step_kernel(const 
         const int k = k0 + q;
         if (c >= a.N || k >= pairs) continue;
         const size_t e = (size_t)c * rs + k;
-        s_reg[r][q] = reinterpret_cast<const float2*>(a.reg)[e];
+        if (!a.exact_reg) s_reg[r][q] = reinterpret_cast<const float2*>(a.reg)[e];
         s_m[r][q] = reinterpret_cast<const float2*>(a.M)[e];
         s_p[r][q] = reinterpret_cast<const float2*>(a.P)[e];
         if (BURSTY) {
@@ -433,10 +407,16 @@ __global__ void __launch_bounds__(kTauTileThreads) tensor_tau_step_kernel(const 
         uint4 w[2];
         w[0] = philox_rk(gcell, (uint32_t)s, (uint32_t)g0, c3, a.rk0, a.rk1);
         w[1] = has1 ? philox_rk(gcell, (uint32_t)s, (uint32_t)(g0 + 1), c3, a.rk0, a.rk1) : make_uint4(0u, 0u, 0u, 0u);
-        const float2 rg = s_reg[r][q];
-        // the GEMM's sum takes the repression constant afterwards; the exact form holds it
-        const float reg0 = a.exact_reg ? rg.x : __fadd_rn(rg.x, r0.cneg);
-        const float reg1 = a.exact_reg ? rg.y : __fadd_rn(rg.y, r1.cneg);
+        float reg0, reg1;
+        if (a.exact_reg) {
+            const float* act = a.act32_cur + c;
+            reg0 = exact_regulation(a, r0, act);
+            reg1 = has1 ? exact_regulation(a, r1, act) : 0.0f;
+        } else {  // the GEMM's sum, which takes the repression constant afterwards
+            const float2 rg = s_reg[r][q];
+            reg0 = __fadd_rn(rg.x, r0.cneg);
+            reg1 = __fadd_rn(rg.y, r1.cneg);
+        }
         float tx0 = fmaxf(__fadd_rn(reg0, r0.beta), 0.0f);
         float tx1 = fmaxf(__fadd_rn(reg1, r1.beta), 0.0f);
         if (a.V) {
@@ -850,7 +830,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     CU(st->tP.ensure(ln * 4));
     CU(st->tprom.ensure(ln));
     CU(st->tNS.ensure(ln * sizeof(int2)));
-    CU(st->treg.ensure(ln * 4));
+    if (!exact) CU(st->treg.ensure(ln * 4));  // the GEMM's output (the exact form has none)
     st->t_ld = ld;
     CU(st->tact16.ensure((size_t)N * Kp * 2));
     for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
@@ -930,7 +910,6 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     LtGemm gemm;
     if (!exact)
         if (int r = lt_setup(ctx, gemm, dtype, G, ld, Kp, N)) return r;
-    const dim3 g_exact((unsigned)((N + kExactCells - 1) / kExactCells), (unsigned)((ld + kExactGenes - 1) / kExactGenes));
     const float alpha = 1.0f, beta = 0.0f;
     const int64_t n_steps = run_steps(o);
     const int pairs = ld / 2;
@@ -961,11 +940,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         a.step = (int)step;
         a.act32_cur = st->tact32[(step - 1) & 1].as<float>();
         a.act32_next = st->tact32[step & 1].as<float>();
-        if (exact) {  // the register path's FP32 regulation instead of the terms and the GEMM
-            tensor_exact_reg_kernel<<<g_exact, kExactThreads, 0, s>>>(a);
-            CU(cudaGetLastError());
-            ctx->launches += 1;
-        } else {
+        if (!exact) {  // (the exact form computes its regulation inside the step kernel)
             if (a.n_terms > 0) {  // term columns from the previous step's activations
                 CU(terms_launch(dtype, a, s));
                 ctx->launches += 1;
