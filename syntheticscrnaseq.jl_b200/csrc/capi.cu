@@ -614,8 +614,9 @@ const float* scrna::switch_log2_table(scrna_ctx* ctx) {
 // register path cannot hold it; the tau-leap beyond 128 genes, where the register path's
 // threads hold pairs or quads of genes at its register limit and fit one block an SM, while
 // the tensor form keeps the state in HBM at full occupancy with the same counts (exact
-// regulation; ms a step, register / tensor: 200 sampled genes 0.145 / 0.086 at 20,000 cells,
-// 300 genes 0.055 / 0.018 at 1,000 and 0.280 / 0.124 at 20,000; 100 genes 0.041 / 0.050);
+// regulation; ms a step, register / tensor: 129 sampled genes 0.027 / 0.009 at 1,000 cells
+// and 0.144 / 0.051 at 20,000, 300 genes 0.055 / 0.012 and 0.281 / 0.107; 128 genes 0.009 /
+// 0.008 and 0.040 / 0.047);
 // the CLE and its populations for regulation of at least 5 % density over 256 genes or
 // more, where the register path's in-edge loops cost more than the contraction.  The tensor
 // path's step has a floor of about 20 us (its launches) whatever N; the register path's

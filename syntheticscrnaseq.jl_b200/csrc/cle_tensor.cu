@@ -810,8 +810,8 @@ int64_t run_steps(const scrna_cle_opts* o);
 // BF16 GEMM for dense networks beyond it, as the CLE.  FP16 inputs: the FP16 GEMM.  Each edge
 // of the exact form is one load of a 32-cell activation row, which once a tile's rows outgrow
 // L1 come from L2.  ms a step on a B200, exact / GEMM: 300 sampled genes x 20,000 cells
-// 0.124 / 0.155; 300 genes at 10 % 0.251 / 0.195; 600 genes at 10 % 0.577 / 0.254; 2,000
-// genes at 2 % x 65,536 cells 6.96 / 2.52, at 10 % 23.8 / 3.63.
+// 0.106 / 0.153; 300 genes at 10 % 0.251 / 0.202; 600 genes at 10 % 0.634 / 0.263; 2,000
+// genes at 2 % x 65,536 cells 7.34 / 2.61, at 10 % 24.8 / 3.78.
 bool tau_tensor_exact(const scrna_net* n, int dtype) {
     if (const char* e = std::getenv("SCRNA_TAU_TENSOR_EXACT")) return std::atoi(e) != 0;
     if (dtype != 0) return false;
