@@ -147,20 +147,12 @@ int batch_simulate(scrna_ctx* ctx, int32_t B, const scrna_net* const* nets, cons
 }
 
 int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* cap) {
-    // dense networks: tensor-core path, one after another on the context stream
+    // tensor-path networks: their tables first (the first preparation of a network waits for
+    // the device), so that their runs below overlap the register-path groups
     for (BatchNet* x : all)
-        if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
+        if (x->tensor) {
             if (int r = ensure_gene_tables(x->net, x->kin, x->o.dt, x->pop != nullptr)) return r;
-            // the tau-leap and populations: library-GEMM variant only
-            const bool fused = !x->tau && !x->pop && x->net->G <= 4096;
-            x->st->last_tensor = !fused;
-            x->st->last_plain = false;
-            x->st->last_pop = x->pop != nullptr;
-            x->st->last_tau = x->tau;
-            x->st->have_counts = cap != nullptr;
-            if (int r = fused ? tc_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)
-                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0, x->tau, x->pop))
-                return r;
+            if (int r = tensor_prepare_net(x->net, 0)) return r;
         }
     // register-path networks: one persistent launch (or one captured chunk sequence) per group
     std::map<GroupKey, std::unique_ptr<Group>> groups;
@@ -288,8 +280,22 @@ int run_batch(scrna_ctx* ctx, std::vector<BatchNet*>& all, const scrna_capture* 
             ctx->launches += (int64_t)chunks.size();
         }
         CU(cudaEventRecord(g.done, g.stream));
-        CU(cudaStreamWaitEvent(ctx->stream, g.done, 0));
     }
+    // tensor-path networks, one after another on the context stream while the groups run
+    for (BatchNet* x : all)
+        if (x->tensor) {  // the fused tcgen05 kernel (gene-major state); beyond its gene limit the library GEMM
+            // the tau-leap and populations: library-GEMM variant only
+            const bool fused = !x->tau && !x->pop && x->net->G <= 4096;
+            x->st->last_tensor = !fused;
+            x->st->last_plain = false;
+            x->st->last_pop = x->pop != nullptr;
+            x->st->last_tau = x->tau;
+            x->st->have_counts = cap != nullptr;
+            if (int r = fused ? tc_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0)
+                              : tensor_run(ctx, x->net, x->kin, cap, &x->o, x->st, 0, x->tau, x->pop))
+                return r;
+        }
+    for (auto& kv : groups) CU(cudaStreamWaitEvent(ctx->stream, kv.second->done, 0));
     CU(cudaStreamSynchronize(ctx->stream));
     cudaEventDestroy(start);
     return SCRNA_OK;
