@@ -216,3 +216,24 @@ def test_tauleap_capture_and_validation(pkg, orc):
         Xt, ct, et = pkg.simulate(net, pkg.BinomialTauLeap(0.02), kin, cell_num=400, T=3.0, readout="protein",
                                   seed=12, capture=cap, path=path)
         assert np.array_equal(Xt, X) and np.array_equal(ct, counts) and np.array_equal(et, eff), path
+
+
+def test_regulated_batch_across_both_forms_bit_exact(pkg):
+    """A batch of regulated tau-leap networks on both sides of 128 genes (the register path's
+    grouped launch and the tensor form, running side by side): every network's readout and
+    capture equal its single run on the register path bit for bit, populations included."""
+    nets = [pkg.sample_network(40, seed=41, bursty=True), pkg.sample_network(200, seed=42, bursty=True),
+            pkg.sample_network(12, seed=43, bursty=True), pkg.sample_network(300, seed=44, bursty=True)]
+    kin = pkg.WORKLOAD_KINETICS
+    cells = [300, 250, 400, 200]
+    pops = [None, pkg.PopulationConfig(cell_num=250, growth_rate=0.7, V_div=2.0, V_init=(1.0, 2.0),
+                                       div_check_interval=10), None, None]
+    cap = pkg.CaptureModel(efficiency=0.3, efficiency_std=0.4, readout="protein")
+    alg = pkg.BinomialTauLeap(0.01)
+    outs, counts = pkg.simulate_gpu_batch(nets, alg, kin, cell_num=cells, T=0.8, readout="both", seed=9, stream=30,
+                                          populations=pops, capture=cap)
+    for b, net in enumerate(nets):
+        X, c, _ = pkg.simulate(net, alg, kin, population=pops[b], cell_num=cells[b], T=0.8, readout="both", seed=9,
+                               stream=30 + b, capture=cap, path="register")
+        assert np.array_equal(outs[b], X), b
+        assert np.array_equal(counts[b], c), b
