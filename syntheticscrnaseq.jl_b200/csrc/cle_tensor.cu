@@ -120,7 +120,7 @@ __global__ void tensor_init_kernel(const TensorArgs a) {
     }
     a.NS[sidx] = ns;
     const float act = hill_act(a.V && a.tau ? __fdiv_rn(p0, (float)V) : p0, a.Kn, a.hill_n, a.hill_int);
-    reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
+    if (!a.exact_reg) reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
     const int src = a.src_of_gene[g];
     if (src >= 0) a.act32_next[(size_t)src * a.N + c] = act;
 }
@@ -590,7 +590,7 @@ __global__ void tensor_replace_kernel(const TensorArgs a) {
         V = a.V[c];
     }
     const float act = tensor_hill<HN>(a.tau ? __fdiv_rn(p, (float)V) : p, a);
-    reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
+    if (!a.exact_reg) reinterpret_cast<T*>(a.act16)[c * a.Kp + g] = to16<T>(act);
     const int src_idx = a.src_of_gene[g];
     if (src_idx >= 0) a.act32_next[(size_t)src_idx * a.N + c] = act;
 }
@@ -832,7 +832,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     CU(st->tNS.ensure(ln * sizeof(int2)));
     if (!exact) CU(st->treg.ensure(ln * 4));  // the GEMM's output (the exact form has none)
     st->t_ld = ld;
-    CU(st->tact16.ensure((size_t)N * Kp * 2));
+    if (!exact) CU(st->tact16.ensure((size_t)N * Kp * 2));  // the GEMM's 16-bit activations
     for (int k = 0; k < 2; ++k) CU(st->tact32[k].ensure(std::max<size_t>((size_t)N * n_src, 1) * 4));
     CU(st->out.ensure(gn * (st->readout == SCRNA_READOUT_BOTH ? 2 : 1) * 8));
     if (cap) {
@@ -840,7 +840,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
         CU(st->eff.ensure((size_t)N * 8));
     }
     cudaStream_t s = ctx->stream;
-    CU(cudaMemsetAsync(st->tact16.p, 0, (size_t)N * Kp * 2, s));  // zero K padding
+    if (!exact) CU(cudaMemsetAsync(st->tact16.p, 0, (size_t)N * Kp * 2, s));  // zero K padding
     TensorArgs a{};
     a.G = G; a.ld = ld; a.Kp = Kp; a.n_src = n_src; a.N = N; a.cell_offset = o->cell_offset;
     a.k_t = (float)kin->k_t;
@@ -872,7 +872,7 @@ int tensor_run(scrna_ctx* ctx, scrna_net* n, const scrna_kinetics* kin, const sc
     a.reg = st->treg.as<float>();
     a.M = st->tM.as<float>(); a.P = st->tP.as<float>();
     a.prom = st->tprom.as<uint8_t>(); a.NS = st->tNS.as<int2>();
-    a.act16 = st->tact16.p;
+    a.act16 = exact ? nullptr : st->tact16.p;
     a.act32_cur = st->tact32[1].as<float>();
     a.act32_next = st->tact32[0].as<float>();
     if (pop) {  // population buffers (the register path's, as cell-major arrays)
